@@ -1,0 +1,408 @@
+#!/usr/bin/env python
+"""Benchmark: joint gravity + TMI forward + objective-gradient evaluations per
+second on the multi-unit contact model (4 lithology groups on a 24x24x12 grid
+of 100 m voxels, ~19k triangles, 64x64 stations 1 m above the flat top,
+control-point stride 4, z-free vertices).
+
+One step = one evaluation at one parameter vector: parameter scatter
+(control-point interpolation + shared-vertex averaging), gz and TMI at every
+station over every facet, joint misfit, and the misfit gradient with respect
+to every DOF (analytic vertex derivatives contracted with the weighted
+residuals; the Jacobian is never formed).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line on rank 0.  `value` is whole-job evaluations/s with the
+parameter vector resident in HBM; `e2e` is the same through the C ABI with
+host buffers (H2D of the parameters and D2H of objective + gradient inside
+the timed region).  Multi-GPU runs are independent replicas (weak scaling):
+the path needs no exchange on one model.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "fwd+grad evals/s (joint gz+TMI forward and objective gradient)"
+WORKLOAD = "multi-unit contact model: 4 groups, 24x24x12 voxels of 100 m, 64x64 stations at 1 m, CP stride 4"
+L2_FLUSH_BYTES = 256 << 20
+
+# Algorithmic work per station-facet pair (frozen; derived from the FP64
+# restatement in oracle/litho_oracle.c with per-facet constants hoisted):
+#   forward gz+TMI pair: 137 floating-point operations (add/sub/mul count 1,
+#   an FMA 2) plus 3 sqrt, 9 div, 3 log, 1 atan2;
+#   gradient pair (both data types): 331 operations plus 3 sqrt, 9 div,
+#   3 log, 1 atan2.
+FLOPS_FWD_PAIR = 137
+FLOPS_GRAD_PAIR = 331
+# FP64 CUDA-core peak of a B200 (nominal): 148 SMs x 64 FP64 FMA/clk x 2 x 1.965 GHz.
+FP64_PEAK_TFLOPS_NOMINAL = 148 * 64 * 2 * 1.965e9 / 1e12
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-stations", type=int, default=48)
+    return ap.parse_args()
+
+
+def make_problem():
+    import numpy as np
+
+    from lithoinv3d_b200 import synth
+
+    p = synth.voxel_contact_model()
+    model = p.build_model()
+    return p, model
+
+
+def synthetic_data(p, model):
+    """Observations of a seeded true model (x0 + N(0, 5 m)) plus 1% noise,
+    computed once by the GPU forward (setup only, untimed)."""
+    import numpy as np
+
+    x0 = model.assemble_parameters()
+    rng = np.random.default_rng(1234)
+    x_true = x0 + rng.normal(0.0, 5.0, len(x0))
+    ctx = p.make_context(model)
+    gz, tmi = ctx.forward(x_true)
+    ctx.close()
+    gstd = np.full(len(gz), 0.01 * np.std(gz))
+    mstd = np.full(len(tmi), 0.01 * np.std(tmi))
+    gobs = gz + gstd * rng.normal(size=len(gz))
+    mobs = tmi + mstd * rng.normal(size=len(tmi))
+    return x0, gobs, gstd, mobs, mstd
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.path = f"/tmp/litho_clocks_{os.getpid()}.csv"
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if self.proc is None or not self.path or not os.path.exists(self.path):
+            return None
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as fh:
+            for line in fh:
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    mx = float(f[2])
+                except ValueError:
+                    continue
+                for n, v in zip(names, f[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(p, x0, gobs, gstd, mobs, mstd, n_sta: int):
+    """The reference's own CPU path (oracle/_ref, single-threaded as the
+    reference is) timed on a bounded station sample of the same workload,
+    scaled to whole-workload evaluations/s.  Falls back to the C restatement
+    (kind "port") when the compiled reference is absent."""
+    import numpy as np
+
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_bindings as ob
+    from lithoinv3d_b200 import synth
+
+    S = len(p.grav_xyz)
+    idx = np.linspace(0, S - 1, n_sta).astype(int)
+    sub = synth.Problem(p.name, p.densities, p.susceptibilities, p.meshes, p.grav_xyz[idx], p.mag_xyz[idx],
+                        inducing=p.inducing, axis_scale=p.axis_scale, cp_stride=p.cp_stride)
+    if ob.ref_available():
+        rm = ob.RefModel(sub, gobs[idx], gstd[idx], mobs[idx], mstd[idx])
+        t0 = time.perf_counter()
+        rm.objective(x0)
+        rm.gradient(x0)
+        dt = time.perf_counter() - t0
+        kind = "reference"
+    else:
+        model = sub.build_model()
+        om = ob.OracleModel(model.tables(), sub.densities, sub.susceptibilities, sub.inducing)
+        t0 = time.perf_counter()
+        om.scatter(x0)
+        om.forward_gz(sub.grav_xyz)
+        om.forward_tmi(sub.mag_xyz)
+        om.jacobian(sub.grav_xyz, 0)
+        om.forward_gz(sub.grav_xyz)
+        om.jacobian(sub.mag_xyz, 1)
+        om.forward_tmi(sub.mag_xyz)
+        dt = time.perf_counter() - t0
+        kind = "port"
+    per_eval = dt * S / n_sta
+    return {"value": 1.0 / per_eval, "unit": "evals/s", "cores": 1, "kind": kind,
+            "sample": f"one objective+gradient evaluation on {n_sta} of {S} stations "
+                      f"({dt:.1f} s), scaled by station count"}
+
+
+def _ref_worker(args):
+    import numpy as np
+
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_bindings as ob
+    from lithoinv3d_b200 import synth
+
+    idx, seed_data = args
+    p, model = make_problem()
+    x0, gobs, gstd, mobs, mstd = seed_data
+    sub = synth.Problem(p.name, p.densities, p.susceptibilities, p.meshes, p.grav_xyz[idx], p.mag_xyz[idx],
+                        inducing=p.inducing, axis_scale=p.axis_scale, cp_stride=p.cp_stride)
+    rm = ob.RefModel(sub, gobs[idx], gstd[idx], mobs[idx], mstd[idx])
+    t0 = time.perf_counter()
+    rm.objective(x0)
+    rm.gradient(x0)
+    return time.perf_counter() - t0
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU implementation (oracle/_ref, or
+    the C restatement when the reference could not be compiled) on all host
+    cores, one single-threaded process per core over a station sample."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import multiprocessing as mp
+
+    import numpy as np
+
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_bindings as ob
+
+    p, model = make_problem()
+    ncore = os.cpu_count() or 1
+    per = 4
+    S = len(p.grav_xyz)
+    n_sample = min(S, per * ncore)
+    # observations from the C restatement (the GPU is not used on this arm)
+    om = ob.OracleModel(model.tables(), p.densities, p.susceptibilities, p.inducing)
+    x0 = model.assemble_parameters()
+    rng = np.random.default_rng(1234)
+    x_true = x0 + rng.normal(0.0, 5.0, len(x0))
+    om.scatter(x_true)
+    idx_all = np.linspace(0, S - 1, n_sample).astype(int)
+    gz = np.zeros(S)
+    tmi = np.zeros(S)
+    gz[idx_all] = om.forward_gz(p.grav_xyz[idx_all])
+    tmi[idx_all] = om.forward_tmi(p.mag_xyz[idx_all])
+    gstd = np.full(S, 0.01 * np.std(gz[idx_all]))
+    mstd = np.full(S, 0.01 * np.std(tmi[idx_all]))
+    data = (x0, gz + gstd * rng.normal(size=S), gstd, tmi + mstd * rng.normal(size=S), mstd)
+    chunks = [idx_all[i::ncore] for i in range(ncore)]
+    kind = "reference" if ob.ref_available() else "port"
+    ctx = mp.get_context("spawn")
+    times = []
+    with ctx.Pool(ncore) as pool:
+        for step in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            pool.map(_ref_worker, [(c, data) for c in chunks])
+            dt = time.perf_counter() - t0
+            if step >= args.warmup:
+                times.append(dt)
+    t_step = sum(times) / len(times)
+    value = (n_sample / S) / t_step
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3 * S / n_sample,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)", "config": {"workload": WORKLOAD, "stations_sampled": int(n_sample)},
+            "cpu_baseline": {"value": value, "unit": "evals/s", "cores": ncore, "kind": kind,
+                             "sample": f"{n_sample} of {S} stations per step split over {ncore} single-threaded "
+                                       f"processes (the reference has no threading); evals/s scaled by "
+                                       f"station count"},
+            "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import numpy as np
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from lithoinv3d_b200 import PREC_FP64, PREC_MIXED
+
+    p, model = make_problem()
+    x0, gobs, gstd, mobs, mstd = synthetic_data(p, model)
+    ctx = p.make_context(model, device=local, grav_obs=gobs, grav_std=gstd, mag_obs=mobs, mag_std=mstd)
+    ctx.set_precision(PREC_MIXED if args.precision == "mixed" else PREC_FP64)
+    np_ = model.n_dofs
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    xs = [torch.tensor(x0 + d, dtype=torch.float64, device=dev) for d in (0.0, 0.5)]
+    d_f = torch.zeros(1, dtype=torch.float64, device=dev)
+    d_g = torch.zeros(np_, dtype=torch.float64, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    torch.cuda.synchronize()
+
+    def step(i):
+        ctx.objective_grad_device(xs[i % 2].data_ptr(), d_f.data_ptr(), d_g.data_ptr())
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+
+    # ---- device-resident timing: per-step events on the library's stream ----
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    ctx.reset_counters()
+    ctx.set_profiling(True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        for i in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(float(i))  # evicts L2 between steps (outside the events)
+                evs[i][0].record(stream)
+            step(i)
+            with torch.cuda.stream(stream):
+                evs[i][1].record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    total_ms = sum(step_ms)
+    fwd_ms, fwd_n, grad_ms, grad_n = ctx.kernel_times()
+    ctx.set_profiling(False)
+    cnt = ctx.counters()
+    launches = int(cnt.launches)
+    pairs_fwd = int(cnt.forward_pairs)
+    pairs_grad = int(cnt.gradient_pairs)
+
+    # ---- end to end through the C ABI with pinned host buffers ----
+    hx = torch.from_numpy(x0.copy()).pin_memory()
+    hg = torch.zeros(np_, dtype=torch.float64).pin_memory()
+    hx_np, hg_np = hx.numpy(), hg.numpy()
+    import ctypes as C
+
+    lib = ctx.lib
+    fbuf = np.zeros(1)
+    e2e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for i in range(2):
+        lib.lf_objective_grad(ctx.h, hx_np.ctypes.data_as(C.POINTER(C.c_double)),
+                              fbuf.ctypes.data_as(C.POINTER(C.c_double)), hg_np.ctypes.data_as(C.POINTER(C.c_double)))
+    torch.cuda.synchronize()
+    for i in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(float(i))
+            e2e_ev[i][0].record(stream)
+        st = lib.lf_objective_grad(ctx.h, hx_np.ctypes.data_as(C.POINTER(C.c_double)),
+                                   fbuf.ctypes.data_as(C.POINTER(C.c_double)),
+                                   hg_np.ctypes.data_as(C.POINTER(C.c_double)))
+        assert st == 0, st
+        with torch.cuda.stream(stream):
+            e2e_ev[i][1].record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = sum(a.elapsed_time(b) for a, b in e2e_ev)
+
+    # max over ranks (replicas)
+    tot = torch.tensor([total_ms, e2e_ms], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(tot, op=dist.ReduceOp.MAX)
+    total_ms, e2e_ms = float(tot[0]), float(tot[1])
+    ms_per_step = total_ms / args.steps
+    value = world * args.steps / (total_ms / 1e3)
+    e2e_value = world * args.steps / (e2e_ms / 1e3)
+
+    # dominant kernel roofline (FP64 CUDA-core pipe)
+    grad_per_launch_ms = grad_ms / max(grad_n, 1)
+    fwd_per_launch_ms = fwd_ms / max(fwd_n, 1)
+    if grad_ms >= fwd_ms:
+        kname, kms, kflops = "k_gradient_fp64", grad_per_launch_ms, FLOPS_GRAD_PAIR * pairs_grad / max(grad_n, 1)
+    else:
+        kname, kms, kflops = "k_forward_fp64", fwd_per_launch_ms, FLOPS_FWD_PAIR * pairs_fwd / max(fwd_n, 1)
+    achieved = kflops / (kms / 1e3) / 1e12
+    roofline = {"bound": "fp64", "kernel": kname, "achieved": achieved, "peak": FP64_PEAK_TFLOPS_NOMINAL,
+                "unit": "TFLOP/s", "frac": achieved / FP64_PEAK_TFLOPS_NOMINAL, "traffic": None,
+                "peak_source": "nominal FP64 CUDA-core rate (148 SMs x 64 FMA/clk x 1.965 GHz); "
+                               "no measured FP64 peak in MEASURED_PEAKS.json",
+                "kernel_ms_per_launch": kms,
+                "pairs_per_s": {"forward": pairs_fwd / max(fwd_ms / 1e3, 1e-12),
+                                "gradient": pairs_grad / max(grad_ms / 1e3, 1e-12)}}
+
+    line = {"metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+            "data": "synthetic (seeded voxel model and observations)",
+            "config": {"workload": WORKLOAD, "triangles": p.n_triangles(), "stations": len(p.grav_xyz),
+                       "dofs": np_, "parallelism": f"replicas x{world}", "l2": "flushed between steps (256 MiB write)",
+                       "precision": args.precision},
+            "e2e": {"value": e2e_value, "unit": "evals/s", "h2d_bytes_per_step": 8 * np_,
+                    "d2h_bytes_per_step": 8 * (np_ + 1)},
+            "gpu_launches": launches, "roofline": roofline}
+    clk = clocks.summary()
+    line["clocks"] = clk
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline(p, x0, gobs, gstd, mobs, mstd, args.cpu_stations)
+        except Exception as e:  # the baseline is reported, never the target
+            line["cpu_baseline"] = {"value": None, "error": str(e)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,246 @@
+/*
+ * litho_gpu.h -- C ABI of the B200 LithoInv hot path.
+ *
+ * The library replaces the reference's forward-operator hot path:
+ *   - the polyhedron gz / TMI forward over every station x triangle pair
+ *     (GravityForward::compute, modules/litho-forward/src/forward/gravity_forward.cpp:105-118;
+ *      MagneticForward::compute, modules/litho-forward/src/forward/magnetic_forward.cpp:81-94),
+ *   - the vertex Jacobian (computeGravityAnalyticJacobian gravity_forward.cpp:184-292;
+ *      computeMagneticAnalyticJacobian magnetic_forward.cpp:196-306),
+ *   - its contraction into the objective gradient (ObjectiveFunction::dataMisfitGradient
+ *      modules/litho-inversion/src/inversion/objective.cpp:42-55; JointObjective::gradient
+ *      modules/litho-inversion/src/inversion/joint_objective.cpp:42-111),
+ *   - the parameter scatter (LithologyModel::applyParameterVector
+ *      modules/litho-model/src/litho/lithology_model.cpp:210-248) and DOF gather
+ *      (gravity_forward.cpp:269-289),
+ *   - the projected L-BFGS driver (LBFGSBOptimizer::minimize
+ *      modules/litho-inversion/src/inversion/lbfgsb_optimizer.cpp:162-263) on the host.
+ *
+ * Conventions: plain pointers and sizes; every call returns an lf_status.
+ * Host arrays are copied in; device buffers belong to the context.  One CUDA
+ * stream per context; a context must not be used by two threads at once
+ * (the reference operators are not re-entrant either).  No CPU fallback:
+ * without a usable CUDA device, lf_create returns LF_ECUDA.
+ */
+#ifndef LITHO_GPU_H
+#define LITHO_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    LF_OK = 0,
+    LF_EINVAL = 1,    /* bad argument (null pointer, size, index, NaN/Inf input) */
+    LF_ECUDA = 2,     /* CUDA runtime error or no device */
+    LF_ENOMEM = 3,    /* device allocation failed */
+    LF_ESTATE = 4,    /* call out of order (e.g. no model set) */
+    LF_ETIMEOUT = 5,  /* a bounded device wait expired */
+    LF_ENUMERIC = 6   /* non-finite result detected */
+} lf_status;
+
+/* VertexFreedom numbering of modules/litho-surface/include/litho_invert/surface/surface_mesh.h:9-19 */
+enum { LF_FIXED = 0, LF_Z_ONLY, LF_X_ONLY, LF_Y_ONLY, LF_ALONG_VECTOR, LF_XY_FREE, LF_XZ_FREE,
+       LF_YZ_FREE, LF_XYZ_FREE };
+
+/* RemanentMagnetizationMode, modules/litho-model/include/litho_invert/litho/litho_group.h:7-11 */
+enum { LF_REM_EFFECTIVE_SUSCEPTIBILITY = 0, LF_REM_FIXED_VECTOR = 1, LF_REM_VECTOR = 2 };
+
+/* Precision modes for lf_set_precision. */
+enum {
+    LF_PREC_FP64 = 0,   /* FP64 throughout, reference operation order (parity mode) */
+    LF_PREC_MIXED = 1   /* FP32 bulk, FP64 where the conditioning test asks for it */
+};
+
+/* Which data type a per-type call addresses. */
+enum { LF_GRAVITY = 0, LF_MAGNETIC = 1 };
+
+/* ------------------------------------------------------------------------ */
+/* Host model builder (setup time).                                         */
+/* Mirrors LithologyModel / SurfaceMesh setup semantics.                    */
+/* ------------------------------------------------------------------------ */
+typedef struct lf_model lf_model;
+
+lf_status lf_model_create(lf_model** out);
+void lf_model_destroy(lf_model* m);
+
+/* LithologyModel::addGroup (lithology_model.cpp:16-28) + LithoGroup fields
+ * (litho_group.h:13-34).  rem_vec may be NULL.  *out_index receives the group
+ * index; duplicate ids are rejected with LF_EINVAL. */
+lf_status lf_model_add_group(lf_model* m, int id, double density_gcc, double susceptibility_si,
+                             double rem_magnitude, double rem_inclination_deg,
+                             double rem_declination_deg, const double* rem_vec3, int* out_index);
+
+/* LithologyModel::setGroupMesh (lithology_model.cpp:58-66) of a closed mesh:
+ * nv vertices (xyz[3*nv], freedom[nv] in LF_* numbering), nt triangles
+ * (tri[3*nt], mesh-local, CCW seen from outside). */
+lf_status lf_model_set_group_mesh(lf_model* m, int group_index, int nv, const double* xyz,
+                                  const uint8_t* freedom, int nt, const int32_t* tri);
+
+/* SurfaceMesh::setAxisScale / setBounds (surface_mesh.cpp:178-181, 249-252)
+ * for one group's mesh, or every mesh when group_index < 0. */
+lf_status lf_model_set_axis_scale(lf_model* m, int group_index, int axis, double scale);
+lf_status lf_model_set_depth_bounds(lf_model* m, int group_index, double min_z, double max_z);
+/* SurfaceMesh::setInteriorGrid (surface_mesh.cpp:675-678) */
+lf_status lf_model_set_interior_grid(lf_model* m, int group_index, int interior_dim, int padding_rings);
+
+/* LithologyModel::setControlPointStride (lithology_model.cpp:864-1040). */
+lf_status lf_model_set_control_point_stride(lf_model* m, int stride, int* out_dof_count);
+/* SurfaceMesh::setControlPointStride, regular N x N grid path (surface_mesh.cpp:319-431). */
+lf_status lf_model_set_mesh_control_point_stride(lf_model* m, int group_index, int stride,
+                                                 int* out_cp_count);
+/* LithologyModel::buildSharedVertexSync (lithology_model.cpp:585-618). */
+lf_status lf_model_build_shared_vertex_sync(lf_model* m);
+/* LithologyModel::applyModelBounds (lithology_model.cpp:808-850). */
+lf_status lf_model_apply_model_bounds(lf_model* m, double margin_multiplier);
+
+/* Counts: groups, vertices, triangles, global DOFs (totalDofCount), refs,
+ * interpolation entries, shared-sync groups, shared-sync entries. */
+typedef struct {
+    int n_groups, n_vertices, n_triangles, n_dofs, n_refs, n_interp, n_sync, n_sync_entries;
+} lf_model_info;
+lf_status lf_model_get_info(lf_model* m, lf_model_info* info);
+
+/* LithologyModel::assembleParameterVector (lithology_model.cpp:194-208) and
+ * getBounds (:250-282); arrays of n_dofs. */
+lf_status lf_model_assemble_parameters(lf_model* m, double* params);
+lf_status lf_model_get_bounds(lf_model* m, double* lower, double* upper);
+/* Host copy of the scatter (applyParameterVector) and the current positions
+ * (all meshes, group order, xyz[3*n_vertices]). */
+lf_status lf_model_apply_parameters(lf_model* m, const double* params);
+lf_status lf_model_get_positions(lf_model* m, double* xyz);
+
+/* Flat tables (sizes from lf_model_get_info).  Any pointer may be NULL. */
+lf_status lf_model_export_tables(lf_model* m, double* pos, int32_t* tri, int32_t* grp_tri_off,
+                                 int32_t* dof_off, int32_t* ref_vertex, uint8_t* ref_axis,
+                                 double* ref_scale, int32_t* interp_off, int32_t* interp_src,
+                                 double* interp_w, int32_t* sync_off, int32_t* sync_vertex);
+
+/* ------------------------------------------------------------------------ */
+/* Device context.                                                          */
+/* ------------------------------------------------------------------------ */
+typedef struct lf_ctx lf_ctx;
+
+/* Creates a context on CUDA device `device` with its own stream. */
+lf_status lf_create(lf_ctx** out, int device);
+void lf_destroy(lf_ctx* ctx);
+/* Last error message of this context (static storage owned by ctx). */
+const char* lf_last_error(const lf_ctx* ctx);
+/* The cudaStream_t (as void*) every launch of this context goes to. */
+void* lf_stream(lf_ctx* ctx);
+
+/* Uploads geometry, group properties and DOF tables from a host model. */
+lf_status lf_set_model(lf_ctx* ctx, lf_model* m);
+
+/* Same, from raw tables (for integrators that build the tables from their
+ * own LithologyModel).  group arrays have n_groups entries; interp_* and
+ * sync_* may be NULL (no control points / no shared vertices). */
+lf_status lf_set_model_tables(lf_ctx* ctx, int n_groups, const double* density,
+                              const double* susceptibility, const double* rem_magnitude,
+                              const double* rem_inclination, const double* rem_declination,
+                              const double* rem_vec3, int nv, const double* xyz, int nt,
+                              const int32_t* tri, const int32_t* grp_tri_off, int n_dofs,
+                              const int32_t* dof_off, const int32_t* ref_vertex,
+                              const uint8_t* ref_axis, const double* ref_scale,
+                              const int32_t* interp_off, const int32_t* interp_src,
+                              const double* interp_w, int n_sync, const int32_t* sync_off,
+                              const int32_t* sync_vertex);
+
+/* MagneticForward ctor (magnetic_forward.cpp:57-67) + setRemanenceMode. */
+lf_status lf_set_field(lf_ctx* ctx, double inc_deg, double dec_deg, double field_nt,
+                       int remanence_mode);
+
+/* Station sets (GravityPoint / MagneticPoint, core/common.h:16-41): xyz[3n],
+ * observed data and standard deviations (std <= 0 means weight 1). obs/std
+ * may be NULL (zero data, unit weights).  n may be 0 (data type unused). */
+lf_status lf_set_gravity_data(lf_ctx* ctx, int n, const double* xyz, const double* obs,
+                              const double* std);
+lf_status lf_set_magnetic_data(lf_ctx* ctx, int n, const double* xyz, const double* obs,
+                               const double* std);
+
+/* JointObjective weights (joint_objective.h:31-49): alpha_mag; reference-model
+ * regularisation ReferenceModelRegularization (reference_model.cpp:16-25)
+ * with weight ref_weight around ref_params (NULL or ref_weight <= 0: off). */
+lf_status lf_set_objective(lf_ctx* ctx, double alpha_mag, double ref_weight,
+                           const double* ref_params);
+
+lf_status lf_set_precision(lf_ctx* ctx, int mode);
+
+/* Forward at params (host arrays): gz[n_grav] mGal, tmi[n_mag] nT; either
+ * output may be NULL. */
+lf_status lf_forward(lf_ctx* ctx, const double* params, double* gz, double* tmi);
+
+/* Objective components at params: out5 = {gravity misfit, magnetic misfit,
+ * regularisation, constraint penalty (0), total} (JointComponents,
+ * joint_objective.h:55-63). */
+lf_status lf_objective(lf_ctx* ctx, const double* params, double* out5);
+
+/* Objective and its gradient in one fused evaluation (the Jacobian is never
+ * formed): *f = total objective, grad[n_dofs]. */
+lf_status lf_objective_grad(lf_ctx* ctx, const double* params, double* f, double* grad);
+
+/* Dense Jacobian J[n_data x n_dofs] (row-major) of gravity (which = LF_GRAVITY)
+ * or TMI (LF_MAGNETIC) at params, with the reference's DOF gather semantics:
+ * each DOF collects its control-point vertices' own derivative times the axis
+ * scale.  Analytic derivative (the reference uses forward differences with
+ * h = 1e-4 m).  Intended for small problems and parity checks. */
+lf_status lf_jacobian(lf_ctx* ctx, const double* params, int which, double* J);
+
+/* Current device vertex positions after the last scatter, xyz[3*n_vertices]
+ * (the reference leaves the shared LithologyModel at the last parameters:
+ * gravity_forward.cpp:106). */
+lf_status lf_get_positions(lf_ctx* ctx, double* xyz);
+
+/* Device-resident variants: the same evaluations on device pointers (inputs
+ * already in HBM, results left in HBM, stream-ordered on lf_stream). */
+lf_status lf_forward_device(lf_ctx* ctx, const double* d_params, double* d_gz, double* d_tmi);
+lf_status lf_objective_grad_device(lf_ctx* ctx, const double* d_params, double* d_f,
+                                   double* d_grad);
+
+/* Projected L-BFGS ("L-BFGS-B") on the device objective; semantics of
+ * LBFGSBOptimizer (lbfgsb_optimizer.cpp:33-263, options lbfgsb_optimizer.h:13-57). */
+typedef struct {
+    int max_iterations;      /* default 500 (optimizer.h:36) */
+    double tolerance;        /* ftol, default 1e-6 (optimizer.h:35) */
+    int history_size;        /* default 10 */
+    double armijo_c1;        /* default 1e-4 */
+    int line_search_max_iter;/* default 50 */
+    int disable_line_search; /* default 0 */
+    double initial_gamma;    /* > 0: H0 = gamma*I for the first step (warm start); 0 = steepest descent */
+} lf_lbfgsb_options;
+typedef struct {
+    int iterations;
+    int converged;
+    int evaluations;         /* objective-only evaluations */
+    int gradients;           /* objective+gradient evaluations */
+    double final_value;
+    char message[96];
+} lf_lbfgsb_result;
+void lf_lbfgsb_default_options(lf_lbfgsb_options* opt);
+lf_status lf_lbfgsb_minimize(lf_ctx* ctx, const double* x0, const double* lower,
+                             const double* upper, const lf_lbfgsb_options* opt, double* x_out,
+                             lf_lbfgsb_result* result);
+
+/* Work counters: station-facet pairs evaluated by the forward and gradient
+ * kernels since the last reset, and kernel launches. */
+typedef struct {
+    uint64_t forward_pairs, gradient_pairs, launches;
+} lf_counters;
+lf_status lf_get_counters(lf_ctx* ctx, lf_counters* c);
+lf_status lf_reset_counters(lf_ctx* ctx);
+
+/* Kernel timing on the context's stream: when enabled, every launch of the
+ * forward pair kernel and of the gradient pair kernel is bracketed by CUDA
+ * events.  lf_get_kernel_times synchronises the stream and returns the summed
+ * durations (ms) and launch counts since profiling was (re)enabled. */
+lf_status lf_set_profiling(lf_ctx* ctx, int enabled);
+lf_status lf_get_kernel_times(lf_ctx* ctx, double* forward_ms, int* forward_launches,
+                              double* gradient_ms, int* gradient_launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LITHO_GPU_H */

@@ -1,0 +1,1020 @@
+// C ABI implementation: contexts, device buffers and the launch sequence of
+// one forward / objective / objective+gradient evaluation.
+#include "../../include/litho_gpu.h"
+#include "kernels_fp64.cuh"
+#include "lbfgsb.hpp"
+#include "model_builder.hpp"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+using namespace litho_b200;
+
+struct lf_model {
+    LithologyModelHost host;
+};
+
+namespace {
+
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    cudaError_t reserve(size_t count) {
+        if (count <= n && p) return cudaSuccess;
+        release();
+        if (count == 0) return cudaSuccess;
+        cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+        if (e != cudaSuccess) { p = nullptr; return e; }
+        n = count;
+        return cudaSuccess;
+    }
+};
+
+struct GroupProps {
+    double density, chi, remMag, remInc, remDec, remVec[3];
+};
+
+struct StationSet {
+    int n = 0;
+    std::vector<double> xyz, obs, w;
+    DevBuf<double> d_xyz, d_obs, d_w, d_pred, d_coef;
+};
+
+constexpr double kGSI = 6.67430e-11, kDensityScale = 1000.0, kMs2ToMgal = 1e5;
+
+}  // namespace
+
+struct lf_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    int precision = LF_PREC_FP64;
+
+    // model
+    bool hasModel = false;
+    int G = 0, V = 0, T = 0, np = 0;
+    std::vector<GroupProps> groups;
+    std::vector<int32_t> grpTriOff;
+    double inc = 90.0, dec = 0.0, fieldNT = 50000.0;
+    int remMode = 0;
+    d3 fdir{0, 0, -1};
+    std::vector<GroupConst> gconst;
+
+    DevBuf<double> d_pos, d_fc, d_gc, d_params, d_grad, d_vgrad, d_out5, d_f, d_refp;
+    DevBuf<int32_t> d_tri, d_dofOff, d_refVertex, d_interpOff, d_interpSrc, d_interpRows, d_syncOff,
+        d_syncVertex, d_vfOff, d_vf, d_gradVerts, d_chunkBegin, d_chunkEnd, d_chunkGroup;
+    DevBuf<uint8_t> d_refAxis, d_faceNeeds;
+    DevBuf<double> d_refScale, d_interpW;
+    DevBuf<int16_t> d_faceGroup;
+    DevBuf<GroupConst> d_groups;
+    int nInterpRows = 0, nSync = 0, nGradVerts = 0;
+
+    // forward chunking
+    std::vector<int32_t> chunkBegin, chunkEnd, chunkGroup;
+    int chunkCapacityS = 0;
+
+    // data
+    StationSet grav, mag;
+    bool sameStations = false;
+    double alphaMag = 1.0, refWeight = 0.0;
+    bool hasRef = false;
+
+    // workspaces
+    DevBuf<double> d_partG, d_partM, d_partGrad, d_blockG, d_blockM, d_ones, d_jac;
+
+    lf_counters counters{0, 0, 0};
+
+    // optional per-kernel timing (events on `stream`)
+    bool profiling = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> evFwd, evGrad;
+    size_t nFwd = 0, nGrad = 0;
+};
+
+static void clear_events(std::vector<std::pair<cudaEvent_t, cudaEvent_t>>& v) {
+    for (auto& e : v) {
+        cudaEventDestroy(e.first);
+        cudaEventDestroy(e.second);
+    }
+    v.clear();
+}
+
+// Records a begin event for a profiled launch; returns the slot or -1.
+static int prof_begin(lf_ctx* c, std::vector<std::pair<cudaEvent_t, cudaEvent_t>>& v, size_t& n) {
+    if (!c->profiling) return -1;
+    if (n == v.size()) {
+        cudaEvent_t a, b;
+        if (cudaEventCreate(&a) != cudaSuccess) return -1;
+        if (cudaEventCreate(&b) != cudaSuccess) { cudaEventDestroy(a); return -1; }
+        v.push_back({a, b});
+    }
+    cudaEventRecord(v[n].first, c->stream);
+    return static_cast<int>(n++);
+}
+static void prof_end(lf_ctx* c, std::vector<std::pair<cudaEvent_t, cudaEvent_t>>& v, int slot) {
+    if (slot >= 0) cudaEventRecord(v[slot].second, c->stream);
+}
+
+#define LF_TRY_CUDA(ctx, expr)                                                           \
+    do {                                                                                 \
+        cudaError_t e__ = (expr);                                                        \
+        if (e__ != cudaSuccess) {                                                        \
+            (ctx)->err = std::string(#expr) + ": " + cudaGetErrorString(e__);            \
+            return e__ == cudaErrorMemoryAllocation ? LF_ENOMEM : LF_ECUDA;              \
+        }                                                                                \
+    } while (0)
+
+#define LF_CHECK_LAUNCH(ctx) LF_TRY_CUDA(ctx, cudaGetLastError())
+
+static lf_status fail(lf_ctx* ctx, lf_status st, const std::string& msg) {
+    if (ctx) ctx->err = msg;
+    return st;
+}
+
+static bool finite_all(const double* p, size_t n) {
+    for (size_t i = 0; i < n; ++i)
+        if (!std::isfinite(p[i])) return false;
+    return true;
+}
+
+template <typename T>
+static cudaError_t upload(DevBuf<T>& b, const T* h, size_t n, cudaStream_t s) {
+    cudaError_t e = b.reserve(n);
+    if (e != cudaSuccess || n == 0) return e;
+    return cudaMemcpyAsync(b.p, h, n * sizeof(T), cudaMemcpyHostToDevice, s);
+}
+
+static inline int cdiv(long long a, long long b) { return static_cast<int>((a + b - 1) / b); }
+
+// ------------------------------------------------------------------ model --
+extern "C" lf_status lf_model_create(lf_model** out) {
+    if (!out) return LF_EINVAL;
+    *out = new (std::nothrow) lf_model();
+    return *out ? LF_OK : LF_ENOMEM;
+}
+extern "C" void lf_model_destroy(lf_model* m) { delete m; }
+
+extern "C" lf_status lf_model_add_group(lf_model* m, int id, double density, double chi, double remMag,
+                                        double remInc, double remDec, const double* remVec, int* outIndex) {
+    if (!m || !std::isfinite(density) || !std::isfinite(chi)) return LF_EINVAL;
+    Group g;
+    g.id = id;
+    g.density = density;
+    g.susceptibility = chi;
+    g.remMagnitude = remMag;
+    g.remInclination = remInc;
+    g.remDeclination = remDec;
+    if (remVec) g.remVector = {remVec[0], remVec[1], remVec[2]};
+    int idx = m->host.addGroup(g);
+    if (outIndex) *outIndex = idx;
+    return idx < 0 ? LF_EINVAL : LF_OK;
+}
+
+extern "C" lf_status lf_model_set_group_mesh(lf_model* m, int gi, int nv, const double* xyz, const uint8_t* freedom,
+                                             int nt, const int32_t* tri) {
+    if (!m || gi < 0 || gi >= m->host.groupCount() || nv < 0 || nt < 0) return LF_EINVAL;
+    if ((nv && (!xyz || !freedom)) || (nt && !tri)) return LF_EINVAL;
+    if (!finite_all(xyz, static_cast<size_t>(nv) * 3)) return LF_EINVAL;
+    Mesh mesh;
+    mesh.pos.resize(nv);
+    mesh.freedom.assign(freedom, freedom + nv);
+    for (int v = 0; v < nv; ++v) {
+        mesh.pos[v] = {xyz[3 * v], xyz[3 * v + 1], xyz[3 * v + 2]};
+        if (freedom[v] > XYZ_FREE) return LF_EINVAL;
+    }
+    mesh.tri.resize(static_cast<size_t>(nt) * 3);
+    for (int k = 0; k < 3 * nt; ++k) {
+        if (tri[k] < 0 || tri[k] >= nv) return LF_EINVAL;
+        mesh.tri[k] = static_cast<uint32_t>(tri[k]);
+    }
+    return m->host.setGroupMesh(gi, std::move(mesh)) == 0 ? LF_OK : LF_EINVAL;
+}
+
+template <typename Fn>
+static lf_status for_meshes(lf_model* m, int gi, Fn fn) {
+    if (!m) return LF_EINVAL;
+    if (gi >= 0) {
+        Mesh* mesh = m->host.mesh(gi);
+        if (!mesh) return LF_EINVAL;
+        fn(*mesh);
+    } else {
+        for (int g = 0; g < m->host.meshCount(); ++g)
+            if (Mesh* mesh = m->host.mesh(g)) fn(*mesh);
+    }
+    m->host.markDirty();
+    return LF_OK;
+}
+
+extern "C" lf_status lf_model_set_axis_scale(lf_model* m, int gi, int axis, double scale) {
+    if (axis < 0 || axis > 2 || !(scale != 0.0) || !std::isfinite(scale)) return LF_EINVAL;
+    return for_meshes(m, gi, [&](Mesh& me) { me.axisScale[axis] = scale; });
+}
+extern "C" lf_status lf_model_set_depth_bounds(lf_model* m, int gi, double minZ, double maxZ) {
+    return for_meshes(m, gi, [&](Mesh& me) { me.minDepth = minZ; me.maxDepth = maxZ; });
+}
+extern "C" lf_status lf_model_set_interior_grid(lf_model* m, int gi, int dim, int rings) {
+    if (dim < 0 || rings < 0) return LF_EINVAL;
+    return for_meshes(m, gi, [&](Mesh& me) {
+        me.interiorGridDim = dim;
+        me.paddingRings = rings;
+        me.rebuildDofMappings();
+    });
+}
+extern "C" lf_status lf_model_set_control_point_stride(lf_model* m, int stride, int* outDofs) {
+    if (!m) return LF_EINVAL;
+    uint32_t n = m->host.setControlPointStride(stride);
+    if (outDofs) *outDofs = static_cast<int>(n);
+    return LF_OK;
+}
+extern "C" lf_status lf_model_set_mesh_control_point_stride(lf_model* m, int gi, int stride, int* outCp) {
+    if (!m || gi < 0) return LF_EINVAL;
+    Mesh* mesh = m->host.mesh(gi);
+    if (!mesh) return LF_EINVAL;
+    uint32_t n = mesh->setControlPointStrideGrid(stride);
+    mesh->rebuildDofMappings();
+    m->host.markDirty();
+    if (outCp) *outCp = static_cast<int>(n);
+    return LF_OK;
+}
+extern "C" lf_status lf_model_build_shared_vertex_sync(lf_model* m) {
+    if (!m) return LF_EINVAL;
+    m->host.buildSharedVertexSync();
+    return LF_OK;
+}
+extern "C" lf_status lf_model_apply_model_bounds(lf_model* m, double margin) {
+    if (!m) return LF_EINVAL;
+    m->host.applyModelBounds(margin);
+    return LF_OK;
+}
+extern "C" lf_status lf_model_get_info(lf_model* m, lf_model_info* info) {
+    if (!m || !info) return LF_EINVAL;
+    ModelTables t = m->host.tables();
+    info->n_groups = t.nGroups;
+    info->n_vertices = t.nVertices;
+    info->n_triangles = t.nTriangles;
+    info->n_dofs = t.nDofs;
+    info->n_refs = static_cast<int>(t.refVertex.size());
+    info->n_interp = static_cast<int>(t.interpSrc.size());
+    info->n_sync = static_cast<int>(t.syncOff.size()) - 1;
+    info->n_sync_entries = static_cast<int>(t.syncVertex.size());
+    return LF_OK;
+}
+extern "C" lf_status lf_model_assemble_parameters(lf_model* m, double* params) {
+    if (!m || !params) return LF_EINVAL;
+    auto p = m->host.assembleParameterVector();
+    std::copy(p.begin(), p.end(), params);
+    return LF_OK;
+}
+extern "C" lf_status lf_model_get_bounds(lf_model* m, double* lo, double* hi) {
+    if (!m || !lo || !hi) return LF_EINVAL;
+    std::vector<double> l, h;
+    m->host.getBounds(l, h);
+    std::copy(l.begin(), l.end(), lo);
+    std::copy(h.begin(), h.end(), hi);
+    return LF_OK;
+}
+extern "C" lf_status lf_model_apply_parameters(lf_model* m, const double* params) {
+    if (!m || !params) return LF_EINVAL;
+    uint32_t n = m->host.totalDofCount();
+    if (!finite_all(params, n)) return LF_EINVAL;
+    m->host.applyParameterVector(std::vector<double>(params, params + n));
+    return LF_OK;
+}
+extern "C" lf_status lf_model_get_positions(lf_model* m, double* xyz) {
+    if (!m || !xyz) return LF_EINVAL;
+    ModelTables t = m->host.tables();
+    std::copy(t.pos.begin(), t.pos.end(), xyz);
+    return LF_OK;
+}
+extern "C" lf_status lf_model_export_tables(lf_model* m, double* pos, int32_t* tri, int32_t* grpTriOff, int32_t* dofOff,
+                                            int32_t* refVertex, uint8_t* refAxis, double* refScale, int32_t* interpOff,
+                                            int32_t* interpSrc, double* interpW, int32_t* syncOff, int32_t* syncVertex) {
+    if (!m) return LF_EINVAL;
+    ModelTables t = m->host.tables();
+    auto cp = [](auto* dst, const auto& v) {
+        if (dst) std::copy(v.begin(), v.end(), dst);
+    };
+    cp(pos, t.pos); cp(tri, t.tri); cp(grpTriOff, t.grpTriOff); cp(dofOff, t.dofOff);
+    cp(refVertex, t.refVertex); cp(refAxis, t.refAxis); cp(refScale, t.refScale);
+    cp(interpOff, t.interpOff); cp(interpSrc, t.interpSrc); cp(interpW, t.interpW);
+    cp(syncOff, t.syncOff); cp(syncVertex, t.syncVertex);
+    return LF_OK;
+}
+
+// ---------------------------------------------------------------- context --
+extern "C" lf_status lf_create(lf_ctx** out, int device) {
+    if (!out) return LF_EINVAL;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) {
+        cudaGetLastError();
+        return LF_ECUDA;
+    }
+    if (device < 0 || device >= n) return LF_EINVAL;
+    lf_ctx* c = new (std::nothrow) lf_ctx();
+    if (!c) return LF_ENOMEM;
+    c->device = device;
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return LF_ECUDA;
+    }
+    *out = c;
+    return LF_OK;
+}
+
+extern "C" void lf_destroy(lf_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    clear_events(c->evFwd);
+    clear_events(c->evGrad);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+extern "C" const char* lf_last_error(const lf_ctx* c) { return c ? c->err.c_str() : "null context"; }
+extern "C" void* lf_stream(lf_ctx* c) { return c ? static_cast<void*>(c->stream) : nullptr; }
+
+// Group magnetisation (MagneticForward ctor magnetic_forward.cpp:57-67 and
+// buildGroupMagnetization :100-134) and gravity scales (gravity_forward.cpp:176, :230).
+static void compute_group_consts(lf_ctx* c) {
+    double I = c->inc * kPi / 180.0, D = c->dec * kPi / 180.0;
+    double cI = std::cos(I);
+    c->fdir = {cI * std::cos(D), cI * std::sin(D), -std::sin(I)};
+    c->gconst.resize(c->G);
+    for (int g = 0; g < c->G; ++g) {
+        const GroupProps& p = c->groups[g];
+        GroupConst& k = c->gconst[g];
+        k.gscale_fwd = kGSI * p.density * kDensityScale * kMs2ToMgal;
+        k.gscale_jac = (kGSI * kDensityScale * kMs2ToMgal) * p.density;
+        double induced = p.chi * c->fieldNT / 100.0;
+        double M[3] = {induced * c->fdir.x, induced * c->fdir.y, induced * c->fdir.z};
+        if (c->remMode == LF_REM_FIXED_VECTOR) {
+            double Ir = p.remInc * kPi / 180.0, Dr = p.remDec * kPi / 180.0, cr = std::cos(Ir);
+            double R[3] = {cr * std::cos(Dr), cr * std::sin(Dr), -std::sin(Ir)};
+            for (int i = 0; i < 3; ++i) M[i] += p.remMag * R[i];
+        } else if (c->remMode == LF_REM_VECTOR) {
+            for (int i = 0; i < 3; ++i) M[i] += p.remVec[i];
+        }
+        double amp = std::sqrt(M[0] * M[0] + M[1] * M[1] + M[2] * M[2]);
+        if (amp < kEps) {
+            k.mdir[0] = c->fdir.x; k.mdir[1] = c->fdir.y; k.mdir[2] = c->fdir.z;
+        } else {
+            for (int i = 0; i < 3; ++i) k.mdir[i] = M[i] / amp;
+        }
+        k.mscale = amp * 100.0 / (4.0 * kPi);
+        k.mag_active = amp < kEps ? 0 : 1;
+    }
+}
+
+static lf_status upload_groups(lf_ctx* c) {
+    compute_group_consts(c);
+    LF_TRY_CUDA(c, upload(c->d_groups, c->gconst.data(), c->gconst.size(), c->stream));
+    return LF_OK;
+}
+
+extern "C" lf_status lf_set_model_tables(lf_ctx* c, int G, const double* density, const double* chi,
+                                         const double* remMag, const double* remInc, const double* remDec,
+                                         const double* remVec, int nv, const double* xyz, int nt, const int32_t* tri,
+                                         const int32_t* grpTriOff, int np, const int32_t* dofOff,
+                                         const int32_t* refVertex, const uint8_t* refAxis, const double* refScale,
+                                         const int32_t* interpOff, const int32_t* interpSrc, const double* interpW,
+                                         int nSync, const int32_t* syncOff, const int32_t* syncVertex) {
+    if (!c) return LF_EINVAL;
+    if (G <= 0 || G > 32000 || nv <= 0 || nt <= 0 || np < 0 || !density || !xyz || !tri || !grpTriOff ||
+        (np > 0 && (!dofOff || !refVertex || !refAxis || !refScale)))
+        return fail(c, LF_EINVAL, "lf_set_model_tables: bad sizes or null arrays");
+    if (!finite_all(xyz, (size_t)nv * 3)) return fail(c, LF_EINVAL, "non-finite vertex position");
+    if (grpTriOff[0] != 0 || grpTriOff[G] != nt) return fail(c, LF_EINVAL, "grp_tri_off must span [0, nt]");
+    for (int g = 0; g < G; ++g)
+        if (grpTriOff[g + 1] < grpTriOff[g]) return fail(c, LF_EINVAL, "grp_tri_off not monotone");
+    for (int k = 0; k < 3 * nt; ++k)
+        if (tri[k] < 0 || tri[k] >= nv) return fail(c, LF_EINVAL, "triangle index out of range");
+    int nref = np > 0 ? dofOff[np] : 0;
+    if (np > 0 && dofOff[0] != 0) return fail(c, LF_EINVAL, "dof_off[0] must be 0");
+    for (int d = 0; d < np; ++d)
+        if (dofOff[d + 1] < dofOff[d]) return fail(c, LF_EINVAL, "dof_off not monotone");
+    for (int r = 0; r < nref; ++r)
+        if (refVertex[r] < 0 || refVertex[r] >= nv || refAxis[r] > 2 || !std::isfinite(refScale[r]))
+            return fail(c, LF_EINVAL, "bad DOF ref");
+    int nInterp = interpOff ? interpOff[nv] : 0;
+    if (interpOff) {
+        if (interpOff[0] != 0 || !interpSrc || !interpW) return fail(c, LF_EINVAL, "bad interpolation table");
+        for (int v = 0; v < nv; ++v)
+            if (interpOff[v + 1] < interpOff[v]) return fail(c, LF_EINVAL, "interp_off not monotone");
+        for (int k = 0; k < nInterp; ++k)
+            if (interpSrc[k] < 0 || interpSrc[k] >= nv || interpOff[interpSrc[k] + 1] != interpOff[interpSrc[k]])
+                return fail(c, LF_EINVAL, "interpolation source must be a control point");
+    }
+    if (nSync > 0) {
+        if (!syncOff || !syncVertex || syncOff[0] != 0) return fail(c, LF_EINVAL, "bad shared-vertex table");
+        for (int s = 0; s < nSync; ++s)
+            if (syncOff[s + 1] < syncOff[s]) return fail(c, LF_EINVAL, "sync_off not monotone");
+        for (int k = 0; k < syncOff[nSync]; ++k)
+            if (syncVertex[k] < 0 || syncVertex[k] >= nv) return fail(c, LF_EINVAL, "sync vertex out of range");
+    }
+    cudaSetDevice(c->device);
+    c->G = G; c->V = nv; c->T = nt; c->np = np;
+    c->groups.resize(G);
+    for (int g = 0; g < G; ++g) {
+        GroupProps& p = c->groups[g];
+        p.density = density[g];
+        p.chi = chi ? chi[g] : 0.0;
+        p.remMag = remMag ? remMag[g] : 0.0;
+        p.remInc = remInc ? remInc[g] : 0.0;
+        p.remDec = remDec ? remDec[g] : 0.0;
+        for (int i = 0; i < 3; ++i) p.remVec[i] = remVec ? remVec[3 * g + i] : 0.0;
+    }
+    c->grpTriOff.assign(grpTriOff, grpTriOff + G + 1);
+    lf_status st = upload_groups(c);
+    if (st != LF_OK) return st;
+
+    // geometry + tables
+    LF_TRY_CUDA(c, upload(c->d_pos, xyz, (size_t)nv * 3, c->stream));
+    LF_TRY_CUDA(c, upload(c->d_tri, tri, (size_t)nt * 3, c->stream));
+    std::vector<int16_t> faceGroup(nt);
+    for (int g = 0; g < G; ++g)
+        for (int f = grpTriOff[g]; f < grpTriOff[g + 1]; ++f) faceGroup[f] = static_cast<int16_t>(g);
+    LF_TRY_CUDA(c, upload(c->d_faceGroup, faceGroup.data(), faceGroup.size(), c->stream));
+    std::vector<int32_t> dofOffV(np + 1, 0);
+    if (np > 0) dofOffV.assign(dofOff, dofOff + np + 1);
+    LF_TRY_CUDA(c, upload(c->d_dofOff, dofOffV.data(), dofOffV.size(), c->stream));
+    LF_TRY_CUDA(c, upload(c->d_refVertex, refVertex, (size_t)nref, c->stream));
+    LF_TRY_CUDA(c, upload(c->d_refAxis, refAxis, (size_t)nref, c->stream));
+    LF_TRY_CUDA(c, upload(c->d_refScale, refScale, (size_t)nref, c->stream));
+    std::vector<int32_t> rows;
+    if (interpOff) {
+        for (int v = 0; v < nv; ++v)
+            if (interpOff[v + 1] > interpOff[v]) rows.push_back(v);
+        LF_TRY_CUDA(c, upload(c->d_interpOff, interpOff, (size_t)nv + 1, c->stream));
+        LF_TRY_CUDA(c, upload(c->d_interpSrc, interpSrc, (size_t)nInterp, c->stream));
+        LF_TRY_CUDA(c, upload(c->d_interpW, interpW, (size_t)nInterp, c->stream));
+    }
+    c->nInterpRows = static_cast<int>(rows.size());
+    LF_TRY_CUDA(c, upload(c->d_interpRows, rows.data(), rows.size(), c->stream));
+    c->nSync = nSync > 0 ? nSync : 0;
+    if (c->nSync) {
+        LF_TRY_CUDA(c, upload(c->d_syncOff, syncOff, (size_t)nSync + 1, c->stream));
+        LF_TRY_CUDA(c, upload(c->d_syncVertex, syncVertex, (size_t)syncOff[nSync], c->stream));
+    }
+    // vertex -> (facet, corner) incidence, DOF vertices, facets needing gradients
+    std::vector<int32_t> vfOff(nv + 1, 0), vf(3 * (size_t)nt);
+    for (int k = 0; k < 3 * nt; ++k) vfOff[tri[k] + 1]++;
+    for (int v = 0; v < nv; ++v) vfOff[v + 1] += vfOff[v];
+    {
+        std::vector<int32_t> fill(vfOff.begin(), vfOff.end() - 1);
+        for (int k = 0; k < 3 * nt; ++k) vf[fill[tri[k]]++] = k;  // k = facet*3 + corner
+    }
+    LF_TRY_CUDA(c, upload(c->d_vfOff, vfOff.data(), vfOff.size(), c->stream));
+    LF_TRY_CUDA(c, upload(c->d_vf, vf.data(), vf.size(), c->stream));
+    std::vector<uint8_t> vneed(nv, 0), fneed(nt, 0);
+    for (int r = 0; r < nref; ++r) vneed[refVertex[r]] = 1;
+    std::vector<int32_t> gverts;
+    for (int v = 0; v < nv; ++v)
+        if (vneed[v]) gverts.push_back(v);
+    for (int f = 0; f < nt; ++f)
+        fneed[f] = vneed[tri[3 * f]] | vneed[tri[3 * f + 1]] | vneed[tri[3 * f + 2]];
+    c->nGradVerts = static_cast<int>(gverts.size());
+    LF_TRY_CUDA(c, upload(c->d_gradVerts, gverts.data(), gverts.size(), c->stream));
+    LF_TRY_CUDA(c, upload(c->d_faceNeeds, fneed.data(), fneed.size(), c->stream));
+    LF_TRY_CUDA(c, c->d_fc.reserve((size_t)NFC * nt));
+    LF_TRY_CUDA(c, c->d_gc.reserve((size_t)NGC * nt));
+    LF_TRY_CUDA(c, c->d_params.reserve(std::max(np, 1)));
+    LF_TRY_CUDA(c, c->d_grad.reserve(std::max(np, 1)));
+    LF_TRY_CUDA(c, c->d_vgrad.reserve((size_t)nv * 3));
+    LF_TRY_CUDA(c, cudaMemsetAsync(c->d_vgrad.p, 0, (size_t)nv * 3 * sizeof(double), c->stream));
+    LF_TRY_CUDA(c, c->d_out5.reserve(5));
+    LF_TRY_CUDA(c, c->d_f.reserve(1));
+    c->chunkCapacityS = 0;
+    c->hasRef = false;
+    c->hasModel = true;
+    LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
+    return LF_OK;
+}
+
+extern "C" lf_status lf_set_model(lf_ctx* c, lf_model* m) {
+    if (!c || !m) return LF_EINVAL;
+    ModelTables t = m->host.tables();
+    int G = t.nGroups;
+    std::vector<double> rho(G), chi(G), rm(G), ri(G), rd(G), rv(3 * G);
+    for (int g = 0; g < G; ++g) {
+        const Group& gr = m->host.group(g);
+        rho[g] = gr.density; chi[g] = gr.susceptibility; rm[g] = gr.remMagnitude;
+        ri[g] = gr.remInclination; rd[g] = gr.remDeclination;
+        rv[3 * g] = gr.remVector.x; rv[3 * g + 1] = gr.remVector.y; rv[3 * g + 2] = gr.remVector.z;
+    }
+    int nSync = static_cast<int>(t.syncOff.size()) - 1;
+    return lf_set_model_tables(c, G, rho.data(), chi.data(), rm.data(), ri.data(), rd.data(), rv.data(), t.nVertices,
+                               t.pos.data(), t.nTriangles, t.tri.data(), t.grpTriOff.data(), t.nDofs,
+                               t.dofOff.data(), t.refVertex.data(), t.refAxis.data(), t.refScale.data(),
+                               t.interpOff.data(), t.interpSrc.data(), t.interpW.data(), nSync,
+                               t.syncOff.data(), t.syncVertex.data());
+}
+
+extern "C" lf_status lf_set_field(lf_ctx* c, double inc, double dec, double field, int remMode) {
+    if (!c || !std::isfinite(inc) || !std::isfinite(dec) || !std::isfinite(field) || remMode < 0 || remMode > 2)
+        return LF_EINVAL;
+    c->inc = inc; c->dec = dec; c->fieldNT = field; c->remMode = remMode;
+    if (c->hasModel) return upload_groups(c);
+    return LF_OK;
+}
+
+static lf_status set_stations(lf_ctx* c, StationSet& s, int n, const double* xyz, const double* obs, const double* sd) {
+    if (!c || n < 0 || (n > 0 && !xyz)) return LF_EINVAL;
+    if (!finite_all(xyz, (size_t)n * 3)) return fail(c, LF_EINVAL, "non-finite station position");
+    if (obs && !finite_all(obs, n)) return fail(c, LF_EINVAL, "non-finite observation");
+    cudaSetDevice(c->device);
+    s.n = n;
+    s.xyz.assign(xyz, xyz + 3 * (size_t)n);
+    s.obs.assign(n, 0.0);
+    s.w.assign(n, 1.0);
+    for (int i = 0; i < n; ++i) {
+        if (obs) s.obs[i] = obs[i];
+        if (sd && sd[i] > 0) s.w[i] = 1.0 / sd[i];  // objective.cpp:26
+    }
+    LF_TRY_CUDA(c, upload(s.d_xyz, s.xyz.data(), s.xyz.size(), c->stream));
+    LF_TRY_CUDA(c, upload(s.d_obs, s.obs.data(), s.obs.size(), c->stream));
+    LF_TRY_CUDA(c, upload(s.d_w, s.w.data(), s.w.size(), c->stream));
+    LF_TRY_CUDA(c, s.d_pred.reserve(std::max(n, 1)));
+    LF_TRY_CUDA(c, s.d_coef.reserve(std::max(n, 1)));
+    c->sameStations = c->grav.n > 0 && c->grav.n == c->mag.n && c->grav.xyz == c->mag.xyz;
+    c->chunkCapacityS = 0;
+    LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
+    return LF_OK;
+}
+
+extern "C" lf_status lf_set_gravity_data(lf_ctx* c, int n, const double* xyz, const double* obs, const double* sd) {
+    return c ? set_stations(c, c->grav, n, xyz, obs, sd) : LF_EINVAL;
+}
+extern "C" lf_status lf_set_magnetic_data(lf_ctx* c, int n, const double* xyz, const double* obs, const double* sd) {
+    return c ? set_stations(c, c->mag, n, xyz, obs, sd) : LF_EINVAL;
+}
+
+extern "C" lf_status lf_set_objective(lf_ctx* c, double alpha, double refWeight, const double* refParams) {
+    if (!c || !std::isfinite(alpha) || !std::isfinite(refWeight)) return LF_EINVAL;
+    if (!c->hasModel) return fail(c, LF_ESTATE, "lf_set_objective before lf_set_model");
+    c->alphaMag = alpha;
+    c->refWeight = refWeight;
+    c->hasRef = refParams && refWeight > 0.0;
+    if (c->hasRef) {
+        if (!finite_all(refParams, c->np)) return fail(c, LF_EINVAL, "non-finite reference parameters");
+        LF_TRY_CUDA(c, upload(c->d_refp, refParams, (size_t)c->np, c->stream));
+        LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
+    }
+    return LF_OK;
+}
+
+extern "C" lf_status lf_set_precision(lf_ctx* c, int mode) {
+    if (!c || (mode != LF_PREC_FP64 && mode != LF_PREC_MIXED)) return LF_EINVAL;
+    c->precision = mode;
+    return LF_OK;
+}
+
+// --------------------------------------------------------------- internals --
+static constexpr int kFwdThreads = 128;
+static constexpr int kFwdFacetTile = 32;
+static constexpr int kGradThreads = 128;
+static constexpr int kGradStationTile = 64;
+static constexpr int kTargetBlocks = 148 * 4;
+
+// Facet chunks for the forward: contiguous ranges inside one group, sized so
+// that station tiles x chunks fill the GPU.
+static void plan_chunks(lf_ctx* c, int S) {
+    if (c->chunkCapacityS == S && !c->chunkBegin.empty()) return;
+    int sBlocks = std::max(1, cdiv(S, kFwdThreads));
+    int want = std::max(1, cdiv(kTargetBlocks, sBlocks));
+    int chunkSize = std::max(64, cdiv(c->T, want));
+    c->chunkBegin.clear(); c->chunkEnd.clear(); c->chunkGroup.clear();
+    for (int g = 0; g < c->G; ++g)
+        for (int f = c->grpTriOff[g]; f < c->grpTriOff[g + 1]; f += chunkSize) {
+            c->chunkBegin.push_back(f);
+            c->chunkEnd.push_back(std::min(f + chunkSize, c->grpTriOff[g + 1]));
+            c->chunkGroup.push_back(g);
+        }
+    c->chunkCapacityS = S;
+}
+
+static lf_status upload_chunks(lf_ctx* c) {
+    LF_TRY_CUDA(c, upload(c->d_chunkBegin, c->chunkBegin.data(), c->chunkBegin.size(), c->stream));
+    LF_TRY_CUDA(c, upload(c->d_chunkEnd, c->chunkEnd.data(), c->chunkEnd.size(), c->stream));
+    LF_TRY_CUDA(c, upload(c->d_chunkGroup, c->chunkGroup.data(), c->chunkGroup.size(), c->stream));
+    return LF_OK;
+}
+
+static lf_status scatter(lf_ctx* c, const double* d_params) {
+    if (c->np > 0) {
+        k_scatter_dofs<<<cdiv(c->np, 256), 256, 0, c->stream>>>(c->np, d_params, c->d_dofOff.p, c->d_refVertex.p,
+                                                                  c->d_refAxis.p, c->d_refScale.p, c->d_pos.p);
+        c->counters.launches++;
+    }
+    if (c->nInterpRows > 0) {
+        k_interpolate<<<cdiv(c->nInterpRows, 256), 256, 0, c->stream>>>(c->nInterpRows, c->d_interpRows.p,
+                                                                         c->d_interpOff.p, c->d_interpSrc.p,
+                                                                         c->d_interpW.p, c->d_pos.p);
+        c->counters.launches++;
+    }
+    if (c->nSync > 0) {
+        k_sync_shared<<<cdiv(c->nSync, 256), 256, 0, c->stream>>>(c->nSync, c->d_syncOff.p, c->d_syncVertex.p,
+                                                                   c->d_pos.p);
+        c->counters.launches++;
+    }
+    LF_CHECK_LAUNCH(c);
+    return LF_OK;
+}
+
+template <bool GZ, bool TMI>
+static lf_status forward_set(lf_ctx* c, const StationSet& s, double* d_gz, double* d_tmi) {
+    int S = s.n;
+    if (S == 0) return LF_OK;
+    plan_chunks(c, S);
+    lf_status st = upload_chunks(c);
+    if (st != LF_OK) return st;
+    int nch = static_cast<int>(c->chunkBegin.size());
+    if (GZ) LF_TRY_CUDA(c, c->d_partG.reserve((size_t)nch * S));
+    if (TMI) LF_TRY_CUDA(c, c->d_partM.reserve((size_t)nch * S));
+    dim3 grid(cdiv(S, kFwdThreads), nch);
+    int slot = prof_begin(c, c->evFwd, c->nFwd);
+    k_forward_fp64<GZ, TMI, kFwdFacetTile><<<grid, kFwdThreads, 0, c->stream>>>(
+        S, s.d_xyz.p, c->T, c->d_fc.p, c->d_chunkBegin.p, c->d_chunkEnd.p, GZ ? c->d_partG.p : nullptr,
+        TMI ? c->d_partM.p : nullptr);
+    prof_end(c, c->evFwd, slot);
+    k_forward_reduce<<<cdiv(S, 256), 256, 0, c->stream>>>(S, nch, c->d_chunkGroup.p, c->d_groups.p,
+                                                          GZ ? c->d_partG.p : nullptr, TMI ? c->d_partM.p : nullptr,
+                                                          GZ ? d_gz : nullptr, TMI ? d_tmi : nullptr);
+    c->counters.launches += 2;
+    c->counters.forward_pairs += (uint64_t)S * (uint64_t)c->T * ((GZ && TMI) ? 2 : 1);
+    LF_CHECK_LAUNCH(c);
+    return LF_OK;
+}
+
+// Positions must be current.  Writes grav.d_pred / mag.d_pred.
+static lf_status forward_all(lf_ctx* c) {
+    k_face_prep_fwd<<<cdiv(c->T, 128), 128, 0, c->stream>>>(c->T, c->d_tri.p, c->d_pos.p, c->d_faceGroup.p,
+                                                            c->d_groups.p, c->fdir, c->d_fc.p);
+    c->counters.launches++;
+    LF_CHECK_LAUNCH(c);
+    if (c->sameStations) return forward_set<true, true>(c, c->grav, c->grav.d_pred.p, c->mag.d_pred.p);
+    lf_status st = forward_set<true, false>(c, c->grav, c->grav.d_pred.p, nullptr);
+    if (st != LF_OK) return st;
+    return forward_set<false, true>(c, c->mag, nullptr, c->mag.d_pred.p);
+}
+
+static lf_status residuals(lf_ctx* c, bool wantCoef) {
+    int nbg = cdiv(std::max(c->grav.n, 1), 256), nbm = cdiv(std::max(c->mag.n, 1), 256);
+    LF_TRY_CUDA(c, c->d_blockG.reserve(nbg));
+    LF_TRY_CUDA(c, c->d_blockM.reserve(nbm));
+    if (c->grav.n > 0)
+        k_residual<<<nbg, 256, 0, c->stream>>>(c->grav.n, c->grav.d_pred.p, c->grav.d_obs.p, c->grav.d_w.p, 1.0,
+                                               wantCoef ? c->grav.d_coef.p : nullptr, c->d_blockG.p);
+    else
+        LF_TRY_CUDA(c, cudaMemsetAsync(c->d_blockG.p, 0, sizeof(double) * nbg, c->stream));
+    bool magOn = c->mag.n > 0 && c->alphaMag > 0.0;  // joint_objective.cpp:48, :123
+    if (magOn)
+        k_residual<<<nbm, 256, 0, c->stream>>>(c->mag.n, c->mag.d_pred.p, c->mag.d_obs.p, c->mag.d_w.p, c->alphaMag,
+                                               wantCoef ? c->mag.d_coef.p : nullptr, c->d_blockM.p);
+    else
+        LF_TRY_CUDA(c, cudaMemsetAsync(c->d_blockM.p, 0, sizeof(double) * nbm, c->stream));
+    c->counters.launches += 2;
+    LF_CHECK_LAUNCH(c);
+    return LF_OK;
+}
+
+static lf_status objective_final(lf_ctx* c, const double* d_params, double* d_f) {
+    int nbg = cdiv(std::max(c->grav.n, 1), 256), nbm = cdiv(std::max(c->mag.n, 1), 256);
+    k_objective_final<<<1, 256, 0, c->stream>>>(nbg, c->d_blockG.p, nbm, c->d_blockM.p, c->alphaMag, c->np, d_params,
+                                                c->hasRef ? c->d_refp.p : nullptr, c->refWeight, c->d_out5.p, d_f);
+    c->counters.launches++;
+    LF_CHECK_LAUNCH(c);
+    return LF_OK;
+}
+
+// Gradient kernels over one station set with the given adjoints; writes
+// chunks [chunk0, chunk0 + nchunks) of d_partGrad.
+static lf_status gradient_set(lf_ctx* c, const StationSet& s, const double* gcoef, const double* mcoef,
+                              int stationsPerChunk, int chunk0, int nchunks) {
+    if (s.n == 0 || nchunks == 0) return LF_OK;
+    dim3 grid(cdiv(c->T, kGradThreads), nchunks);
+    int slot = prof_begin(c, c->evGrad, c->nGrad);
+    k_gradient_fp64<kGradStationTile><<<grid, kGradThreads, 0, c->stream>>>(
+        c->T, c->d_gc.p, s.n, s.d_xyz.p, gcoef, mcoef, stationsPerChunk, c->d_faceGroup.p, c->d_groups.p, c->fdir,
+        c->d_partGrad.p + (size_t)chunk0 * 9 * c->T);
+    prof_end(c, c->evGrad, slot);
+    c->counters.launches++;
+    c->counters.gradient_pairs += (uint64_t)s.n * (uint64_t)c->T;
+    LF_CHECK_LAUNCH(c);
+    return LF_OK;
+}
+
+static int grad_chunks_for(lf_ctx* c, int S) {
+    int fBlocks = std::max(1, cdiv(c->T, kGradThreads));
+    int want = std::max(1, cdiv(kTargetBlocks, fBlocks));
+    return std::max(1, std::min(want, cdiv(S, 16)));
+}
+
+static lf_status gradient_all(lf_ctx* c, const double* d_params, double* d_grad) {
+    bool gOn = c->grav.n > 0, mOn = c->mag.n > 0 && c->alphaMag > 0.0;
+    k_face_prep_grad<<<cdiv(c->T, 128), 128, 0, c->stream>>>(c->T, c->d_tri.p, c->d_pos.p, c->d_faceGroup.p,
+                                                             c->d_groups.p, c->d_faceNeeds.p, 1, 1, c->fdir,
+                                                             c->d_gc.p);
+    c->counters.launches++;
+    LF_CHECK_LAUNCH(c);
+    int chunksG = 0, chunksM = 0, spcG = 1, spcM = 1;
+    if (c->sameStations && gOn) {
+        chunksG = grad_chunks_for(c, c->grav.n);
+        spcG = cdiv(c->grav.n, chunksG);
+        chunksG = cdiv(c->grav.n, spcG);
+    } else {
+        if (gOn) { chunksG = grad_chunks_for(c, c->grav.n); spcG = cdiv(c->grav.n, chunksG); chunksG = cdiv(c->grav.n, spcG); }
+        if (mOn) { chunksM = grad_chunks_for(c, c->mag.n); spcM = cdiv(c->mag.n, chunksM); chunksM = cdiv(c->mag.n, spcM); }
+    }
+    int total = chunksG + chunksM;
+    if (total == 0) {
+        LF_TRY_CUDA(c, cudaMemsetAsync(c->d_vgrad.p, 0, sizeof(double) * 3 * c->V, c->stream));
+    } else {
+        LF_TRY_CUDA(c, c->d_partGrad.reserve((size_t)total * 9 * c->T));
+        lf_status st;
+        if (c->sameStations && gOn) {
+            st = gradient_set(c, c->grav, c->grav.d_coef.p, mOn ? c->mag.d_coef.p : nullptr, spcG, 0, chunksG);
+        } else {
+            st = gradient_set(c, c->grav, c->grav.d_coef.p, nullptr, spcG, 0, chunksG);
+            if (st == LF_OK) st = gradient_set(c, c->mag, nullptr, c->mag.d_coef.p, spcM, chunksG, chunksM);
+        }
+        if (st != LF_OK) return st;
+        if (c->nGradVerts > 0) {
+            k_vertex_reduce<<<cdiv(c->nGradVerts, 128), 128, 0, c->stream>>>(c->nGradVerts, c->d_gradVerts.p,
+                                                                              c->d_vfOff.p, c->d_vf.p, c->T, total,
+                                                                              c->d_partGrad.p, c->d_vgrad.p);
+            c->counters.launches++;
+        }
+    }
+    if (c->np > 0) {
+        k_dof_gather<<<cdiv(c->np, 256), 256, 0, c->stream>>>(c->np, c->d_dofOff.p, c->d_refVertex.p, c->d_refAxis.p,
+                                                              c->d_refScale.p, c->d_vgrad.p, d_params,
+                                                              c->hasRef ? c->d_refp.p : nullptr, c->refWeight, d_grad);
+        c->counters.launches++;
+    }
+    LF_CHECK_LAUNCH(c);
+    return LF_OK;
+}
+
+static lf_status check_ready(lf_ctx* c) {
+    if (!c) return LF_EINVAL;
+    if (!c->hasModel) return fail(c, LF_ESTATE, "no model set");
+    if (c->grav.n == 0 && c->mag.n == 0) return fail(c, LF_ESTATE, "no station data set");
+    cudaSetDevice(c->device);
+    return LF_OK;
+}
+
+static lf_status params_to_device(lf_ctx* c, const double* params) {
+    if (c->np > 0 && !params) return fail(c, LF_EINVAL, "null params");
+    if (!finite_all(params, c->np)) return fail(c, LF_EINVAL, "non-finite parameter");
+    if (c->np > 0)
+        LF_TRY_CUDA(c, cudaMemcpyAsync(c->d_params.p, params, sizeof(double) * c->np, cudaMemcpyHostToDevice, c->stream));
+    return LF_OK;
+}
+
+#define LF_RET_IF(x)                      \
+    do {                                  \
+        lf_status s__ = (x);              \
+        if (s__ != LF_OK) return s__;     \
+    } while (0)
+
+// ------------------------------------------------------------ public API --
+extern "C" lf_status lf_forward_device(lf_ctx* c, const double* d_params, double* d_gz, double* d_tmi) {
+    LF_RET_IF(check_ready(c));
+    LF_RET_IF(scatter(c, d_params));
+    LF_RET_IF(forward_all(c));
+    if (d_gz && c->grav.n)
+        LF_TRY_CUDA(c, cudaMemcpyAsync(d_gz, c->grav.d_pred.p, sizeof(double) * c->grav.n, cudaMemcpyDeviceToDevice, c->stream));
+    if (d_tmi && c->mag.n)
+        LF_TRY_CUDA(c, cudaMemcpyAsync(d_tmi, c->mag.d_pred.p, sizeof(double) * c->mag.n, cudaMemcpyDeviceToDevice, c->stream));
+    return LF_OK;
+}
+
+extern "C" lf_status lf_forward(lf_ctx* c, const double* params, double* gz, double* tmi) {
+    LF_RET_IF(check_ready(c));
+    LF_RET_IF(params_to_device(c, params));
+    LF_RET_IF(scatter(c, c->d_params.p));
+    LF_RET_IF(forward_all(c));
+    if (gz && c->grav.n)
+        LF_TRY_CUDA(c, cudaMemcpyAsync(gz, c->grav.d_pred.p, sizeof(double) * c->grav.n, cudaMemcpyDeviceToHost, c->stream));
+    if (tmi && c->mag.n)
+        LF_TRY_CUDA(c, cudaMemcpyAsync(tmi, c->mag.d_pred.p, sizeof(double) * c->mag.n, cudaMemcpyDeviceToHost, c->stream));
+    LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
+    return LF_OK;
+}
+
+static lf_status objective_device(lf_ctx* c, const double* d_params) {
+    LF_RET_IF(scatter(c, d_params));
+    LF_RET_IF(forward_all(c));
+    LF_RET_IF(residuals(c, false));
+    return objective_final(c, d_params, c->d_f.p);
+}
+
+extern "C" lf_status lf_objective(lf_ctx* c, const double* params, double* out5) {
+    LF_RET_IF(check_ready(c));
+    if (!out5) return LF_EINVAL;
+    LF_RET_IF(params_to_device(c, params));
+    LF_RET_IF(objective_device(c, c->d_params.p));
+    LF_TRY_CUDA(c, cudaMemcpyAsync(out5, c->d_out5.p, sizeof(double) * 5, cudaMemcpyDeviceToHost, c->stream));
+    LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (!std::isfinite(out5[4])) return fail(c, LF_ENUMERIC, "non-finite objective");
+    return LF_OK;
+}
+
+extern "C" lf_status lf_objective_grad_device(lf_ctx* c, const double* d_params, double* d_f, double* d_grad) {
+    LF_RET_IF(check_ready(c));
+    LF_RET_IF(scatter(c, d_params));
+    LF_RET_IF(forward_all(c));
+    LF_RET_IF(residuals(c, true));
+    LF_RET_IF(objective_final(c, d_params, d_f ? d_f : c->d_f.p));
+    return gradient_all(c, d_params, d_grad ? d_grad : c->d_grad.p);
+}
+
+extern "C" lf_status lf_objective_grad(lf_ctx* c, const double* params, double* f, double* grad) {
+    LF_RET_IF(check_ready(c));
+    LF_RET_IF(params_to_device(c, params));
+    LF_RET_IF(lf_objective_grad_device(c, c->d_params.p, c->d_f.p, c->d_grad.p));
+    if (f) LF_TRY_CUDA(c, cudaMemcpyAsync(f, c->d_f.p, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (grad && c->np)
+        LF_TRY_CUDA(c, cudaMemcpyAsync(grad, c->d_grad.p, sizeof(double) * c->np, cudaMemcpyDeviceToHost, c->stream));
+    LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (f && !std::isfinite(*f)) return fail(c, LF_ENUMERIC, "non-finite objective");
+    return LF_OK;
+}
+
+extern "C" lf_status lf_jacobian(lf_ctx* c, const double* params, int which, double* J) {
+    LF_RET_IF(check_ready(c));
+    if (!J || (which != LF_GRAVITY && which != LF_MAGNETIC)) return LF_EINVAL;
+    StationSet& s = which == LF_GRAVITY ? c->grav : c->mag;
+    if (s.n == 0) return fail(c, LF_ESTATE, "no stations of the requested type");
+    LF_RET_IF(params_to_device(c, params));
+    LF_RET_IF(scatter(c, c->d_params.p));
+    k_face_prep_grad<<<cdiv(c->T, 128), 128, 0, c->stream>>>(c->T, c->d_tri.p, c->d_pos.p, c->d_faceGroup.p,
+                                                             c->d_groups.p, c->d_faceNeeds.p, which == LF_GRAVITY,
+                                                             which == LF_MAGNETIC, c->fdir, c->d_gc.p);
+    LF_CHECK_LAUNCH(c);
+    std::vector<double> ones(s.n, 1.0);
+    LF_TRY_CUDA(c, upload(c->d_ones, ones.data(), ones.size(), c->stream));
+    int np = std::max(c->np, 1);
+    // stations per batch so that the partial buffer stays below ~256 MB
+    size_t per = (size_t)9 * c->T * sizeof(double);
+    int batch = static_cast<int>(std::max<size_t>(1, std::min<size_t>((size_t)s.n, ((size_t)256 << 20) / per)));
+    LF_TRY_CUDA(c, c->d_partGrad.reserve((size_t)batch * 9 * c->T));
+    LF_TRY_CUDA(c, c->d_jac.reserve((size_t)batch * np));
+    for (int s0 = 0; s0 < s.n; s0 += batch) {
+        int nb = std::min(batch, s.n - s0);
+        dim3 grid(cdiv(c->T, kGradThreads), nb);
+        const double* g1 = which == LF_GRAVITY ? c->d_ones.p : nullptr;
+        const double* m1 = which == LF_MAGNETIC ? c->d_ones.p : nullptr;
+        k_gradient_fp64<kGradStationTile><<<grid, kGradThreads, 0, c->stream>>>(
+            c->T, c->d_gc.p, nb, s.d_xyz.p + 3 * (size_t)s0, g1, m1, 1, c->d_faceGroup.p, c->d_groups.p, c->fdir,
+            c->d_partGrad.p);
+        if (c->np > 0) {
+            dim3 g2(cdiv(c->np, 128), nb);
+            k_jacobian_gather<<<g2, 128, 0, c->stream>>>(nb, c->np, c->d_dofOff.p, c->d_refVertex.p, c->d_refAxis.p,
+                                                         c->d_refScale.p, c->d_vfOff.p, c->d_vf.p, c->T,
+                                                         c->d_partGrad.p, c->d_jac.p, c->np);
+            LF_TRY_CUDA(c, cudaMemcpyAsync(J + (size_t)s0 * c->np, c->d_jac.p, sizeof(double) * (size_t)nb * c->np,
+                                           cudaMemcpyDeviceToHost, c->stream));
+        }
+        LF_CHECK_LAUNCH(c);
+    }
+    LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
+    return LF_OK;
+}
+
+extern "C" lf_status lf_get_positions(lf_ctx* c, double* xyz) {
+    if (!c || !xyz) return LF_EINVAL;
+    if (!c->hasModel) return fail(c, LF_ESTATE, "no model set");
+    cudaSetDevice(c->device);
+    LF_TRY_CUDA(c, cudaMemcpyAsync(xyz, c->d_pos.p, sizeof(double) * 3 * c->V, cudaMemcpyDeviceToHost, c->stream));
+    LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
+    return LF_OK;
+}
+
+extern "C" void lf_lbfgsb_default_options(lf_lbfgsb_options* o) {
+    if (!o) return;
+    o->max_iterations = 500;
+    o->tolerance = 1e-6;
+    o->history_size = 10;
+    o->armijo_c1 = 1e-4;
+    o->line_search_max_iter = 50;
+    o->disable_line_search = 0;
+    o->initial_gamma = 0.0;
+}
+
+extern "C" lf_status lf_lbfgsb_minimize(lf_ctx* c, const double* x0, const double* lo, const double* hi,
+                                        const lf_lbfgsb_options* opt, double* xOut, lf_lbfgsb_result* res) {
+    LF_RET_IF(check_ready(c));
+    if (!x0 || !lo || !hi || !xOut) return LF_EINVAL;
+    lf_lbfgsb_options o;
+    lf_lbfgsb_default_options(&o);
+    if (opt) o = *opt;
+    LbfgsbOptions lo2;
+    lo2.maxIterations = o.max_iterations;
+    lo2.tolerance = o.tolerance;
+    lo2.historySize = std::max(1, o.history_size);
+    lo2.armijoC1 = o.armijo_c1;
+    lo2.lineSearchMaxIter = o.line_search_max_iter;
+    lo2.disableLineSearch = o.disable_line_search != 0;
+    lo2.initialGamma = o.initial_gamma;
+    int n = c->np;
+    lf_status status = LF_OK;
+    int nEval = 0, nGrad = 0;
+    // Objective values of the last gradient evaluation are reused when the
+    // optimizer asks for f at the same point (results are deterministic).
+    std::vector<double> lastX;
+    double lastF = 0.0;
+    Objective f = [&](const std::vector<double>& x) -> double {
+        if (status != LF_OK) return std::numeric_limits<double>::quiet_NaN();
+        if (x == lastX) return lastF;
+        double out5[5];
+        status = lf_objective(c, x.data(), out5);
+        ++nEval;
+        return out5[4];
+    };
+    Gradient g = [&](const std::vector<double>& x) -> std::vector<double> {
+        std::vector<double> gr(n, 0.0);
+        if (status != LF_OK) return gr;
+        double fv = 0.0;
+        status = lf_objective_grad(c, x.data(), &fv, gr.data());
+        ++nGrad;
+        lastX = x;
+        lastF = fv;
+        return gr;
+    };
+    LbfgsbOptimizer optz(lo2);
+    LbfgsbResult r = optz.minimize(f, g, std::vector<double>(x0, x0 + n), std::vector<double>(lo, lo + n),
+                                   std::vector<double>(hi, hi + n));
+    if (status != LF_OK) return status;
+    std::copy(r.params.begin(), r.params.end(), xOut);
+    if (res) {
+        res->iterations = r.iterations;
+        res->converged = r.converged ? 1 : 0;
+        res->evaluations = nEval;
+        res->gradients = nGrad;
+        res->final_value = r.finalValue;
+        std::snprintf(res->message, sizeof(res->message), "%s", r.message.c_str());
+    }
+    return LF_OK;
+}
+
+extern "C" lf_status lf_get_counters(lf_ctx* c, lf_counters* out) {
+    if (!c || !out) return LF_EINVAL;
+    *out = c->counters;
+    return LF_OK;
+}
+extern "C" lf_status lf_set_profiling(lf_ctx* c, int enabled) {
+    if (!c) return LF_EINVAL;
+    cudaSetDevice(c->device);
+    LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->profiling = enabled != 0;
+    c->nFwd = c->nGrad = 0;
+    return LF_OK;
+}
+
+extern "C" lf_status lf_get_kernel_times(lf_ctx* c, double* fwdMs, int* fwdN, double* gradMs, int* gradN) {
+    if (!c) return LF_EINVAL;
+    cudaSetDevice(c->device);
+    LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
+    auto sum = [&](std::vector<std::pair<cudaEvent_t, cudaEvent_t>>& v, size_t n, double* out) -> lf_status {
+        double t = 0.0;
+        for (size_t i = 0; i < n; ++i) {
+            float ms = 0.f;
+            LF_TRY_CUDA(c, cudaEventElapsedTime(&ms, v[i].first, v[i].second));
+            t += ms;
+        }
+        if (out) *out = t;
+        return LF_OK;
+    };
+    lf_status st = sum(c->evFwd, c->nFwd, fwdMs);
+    if (st != LF_OK) return st;
+    st = sum(c->evGrad, c->nGrad, gradMs);
+    if (st != LF_OK) return st;
+    if (fwdN) *fwdN = static_cast<int>(c->nFwd);
+    if (gradN) *gradN = static_cast<int>(c->nGrad);
+    return LF_OK;
+}
+
+extern "C" lf_status lf_reset_counters(lf_ctx* c) {
+    if (!c) return LF_EINVAL;
+    c->counters = {0, 0, 0};
+    return LF_OK;
+}

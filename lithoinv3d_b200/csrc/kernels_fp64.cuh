@@ -1,0 +1,625 @@
+// FP64 device kernels of the LithoInv hot path (sm_100a).
+//
+// Forward (station-per-thread, facets staged in shared memory): the per-pair
+// arithmetic follows faceNagyContribution / magneticFacet / solidAngle /
+// lineIntegralTerm of the reference in the same operation order
+// (modules/litho-forward/src/forward/gravity_forward.cpp:13-42,
+//  modules/litho-forward/src/forward/magnetic_forward.cpp:312-347,
+//  modules/litho-core/src/core/geometry.cpp:10-52); the station-independent
+// facet quantities (unit normal, edge vectors, lengths, in-plane edge normals,
+// magnetic direction products) are computed once per facet by face_prep_fwd.
+//
+// Gradient (facet-per-thread, stations staged in shared memory): the
+// derivative of every facet term with respect to its three vertices, in
+// closed form, contracted with the per-station weighted residual in the same
+// pass so the Jacobian is never stored.  Derivation (per facet, local frame
+// with origin at vertex a, x along a->b, z along the unit normal):
+//   d Lambda_e / d p2 = ( e_hat - q W ) / d2,   d Lambda_e / d p1 = (-e_hat - q W) / d1,
+//   d Omega / d p1 += (e_hat x r1) W / d1,      d Omega / d p2 += (e_hat x r1) W / d2,
+// with r1 = p1 - o, q = r1 - (r1.e_hat) e_hat, W = L / (d1 d2 + r1.r2); the
+// station-independent factors (n_z, n_hat, in-plane edge normals, magnetic
+// direction products) are differentiated once per facet from accumulated
+// station sums.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace litho_b200 {
+
+constexpr double kEps = 1e-15;
+constexpr double kPi = 3.14159265358979323846;
+
+// ---------------------------------------------------------------- layouts --
+// Forward facet constants, SoA [NFC][T].
+enum FwdConst {
+    FC_AX = 0, FC_AY, FC_AZ, FC_BX, FC_BY, FC_BZ, FC_CX, FC_CY, FC_CZ,
+    FC_NX, FC_NY, FC_NZ,
+    FC_E0X, FC_E0Y, FC_E0Z, FC_E1X, FC_E1Y, FC_E1Z, FC_E2X, FC_E2Y, FC_E2Z,
+    FC_L0, FC_L1, FC_L2,
+    FC_P0X, FC_P0Y, FC_P0Z, FC_P1X, FC_P1Y, FC_P1Z, FC_P2X, FC_P2Y, FC_P2Z,
+    FC_MF, FC_MT0, FC_MT1, FC_MT2,
+    FC_VALID,
+    NFC
+};
+
+// Gradient facet constants (local frame), SoA [NGC][T].
+enum GradConst {
+    GC_AX = 0, GC_AY, GC_AZ,           // origin (vertex a)
+    GC_XX, GC_XY, GC_XZ,               // local x axis (global components)
+    GC_YX, GC_YY, GC_YZ,               // local y axis
+    GC_ZX, GC_ZY, GC_ZZ,               // local z axis = unit normal
+    GC_L0, GC_CX, GC_CY,               // b = (L0, 0, 0), c = (CX, CY, 0)
+    GC_E1X, GC_E1Y, GC_L1,             // edge b->c direction and length
+    GC_E2X, GC_E2Y, GC_L2,             // edge c->a direction and length
+    GC_GS,                             // gz scale of the facet's group (0: no gravity)
+    GC_MS,                             // TMI scale of the facet's group (0: skipped)
+    GC_MF, GC_MT0, GC_MT1, GC_MT2,     // magnetic direction products
+    GC_FLAGS,                          // bit0 valid facet, bit1 needs gradient
+    NGC
+};
+
+struct GroupConst {
+    double gscale_fwd;  // G * rho * 1e3 * 1e5 (forward association)
+    double gscale_jac;  // (G * 1e3 * 1e5) * rho (Jacobian association)
+    double mscale;      // magnetization amplitude * 100 / (4 pi)
+    double mdir[3];
+    int mag_active;     // amplitude >= 1e-15 (the Jacobian skips weaker groups)
+};
+
+// ------------------------------------------------------------- utilities --
+struct d3 { double x, y, z; };
+__device__ __forceinline__ d3 mk3(double x, double y, double z) { return {x, y, z}; }
+__device__ __forceinline__ d3 operator-(d3 a, d3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ d3 operator+(d3 a, d3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ d3 operator*(d3 a, double s) { return {a.x * s, a.y * s, a.z * s}; }
+__device__ __forceinline__ double dot3(d3 a, d3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ d3 cross3(d3 a, d3 b) {
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ double norm3(d3 a) { return sqrt(dot3(a, a)); }
+
+// lineIntegralTerm branch semantics (geometry.cpp:39-51) given s1, s2, d1, d2.
+__device__ __forceinline__ double lambda_from(double s1, double s2, double d1, double d2, bool* live) {
+    double num = s2 + d2, den = s1 + d1;
+    *live = false;
+    if (fabs(den) < kEps) return 0.0;  // covers the "both ~0" branch too
+    if (num <= 0.0 || den <= 0.0) return 0.0;
+    *live = true;
+    return log(num / den);
+}
+
+// ------------------------------------------------------------- scatter ----
+// LithologyModel::applyParameterVector (lithology_model.cpp:210-248) step 1:
+// every global DOF writes the (vertex, axis) slots it controls.
+__global__ void k_scatter_dofs(int np, const double* __restrict__ params, const int32_t* __restrict__ dof_off,
+                               const int32_t* __restrict__ ref_vertex, const uint8_t* __restrict__ ref_axis,
+                               const double* __restrict__ ref_scale, double* __restrict__ pos) {
+    int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= np) return;
+    double val = params[d];
+    for (int r = dof_off[d]; r < dof_off[d + 1]; ++r)
+        pos[3 * ref_vertex[r] + ref_axis[r]] = __dmul_rn(val, ref_scale[r]);
+}
+
+// Step 2: interpolateFromControlPoints (surface_mesh.cpp:610-623); rows only
+// read control-point vertices, which are never rows themselves.
+__global__ void k_interpolate(int nrows, const int32_t* __restrict__ rows, const int32_t* __restrict__ interp_off,
+                              const int32_t* __restrict__ interp_src, const double* __restrict__ interp_w,
+                              double* __restrict__ pos) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nrows) return;
+    int v = rows[i];
+    double px = 0.0, py = 0.0, pz = 0.0;
+    for (int k = interp_off[v]; k < interp_off[v + 1]; ++k) {
+        const double* q = pos + 3 * interp_src[k];
+        double w = interp_w[k];
+        px = __dadd_rn(px, __dmul_rn(q[0], w));
+        py = __dadd_rn(py, __dmul_rn(q[1], w));
+        pz = __dadd_rn(pz, __dmul_rn(q[2], w));
+    }
+    pos[3 * v] = px;
+    pos[3 * v + 1] = py;
+    pos[3 * v + 2] = pz;
+}
+
+// Step 3: shared-vertex averaging groups (lithology_model.cpp:235-247).
+__global__ void k_sync_shared(int ns, const int32_t* __restrict__ sync_off, const int32_t* __restrict__ sync_vertex,
+                              double* __restrict__ pos) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= ns) return;
+    int b = sync_off[s], e = sync_off[s + 1];
+    if (e - b < 2) return;
+    double ax = 0.0, ay = 0.0, az = 0.0;
+    for (int k = b; k < e; ++k) {
+        const double* q = pos + 3 * sync_vertex[k];
+        ax = __dadd_rn(ax, q[0]);
+        ay = __dadd_rn(ay, q[1]);
+        az = __dadd_rn(az, q[2]);
+    }
+    double n = static_cast<double>(e - b);
+    ax = __ddiv_rn(ax, n); ay = __ddiv_rn(ay, n); az = __ddiv_rn(az, n);
+    for (int k = b; k < e; ++k) {
+        double* q = pos + 3 * sync_vertex[k];
+        q[0] = ax; q[1] = ay; q[2] = az;
+    }
+}
+
+// ------------------------------------------------------- facet constants --
+__global__ void k_face_prep_fwd(int T, const int32_t* __restrict__ tri, const double* __restrict__ pos,
+                                const int16_t* __restrict__ face_group, const GroupConst* __restrict__ groups,
+                                d3 fdir, double* __restrict__ fc) {
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= T) return;
+    const double* pa = pos + 3 * tri[3 * f];
+    const double* pb = pos + 3 * tri[3 * f + 1];
+    const double* pc = pos + 3 * tri[3 * f + 2];
+    d3 v[3] = {mk3(pa[0], pa[1], pa[2]), mk3(pb[0], pb[1], pb[2]), mk3(pc[0], pc[1], pc[2])};
+    d3 n = cross3(v[1] - v[0], v[2] - v[0]);
+    double area2 = norm3(n);
+    bool valid = !(area2 < kEps);
+    d3 un = valid ? mk3(n.x / area2, n.y / area2, n.z / area2) : mk3(0, 0, 0);
+    const GroupConst& g = groups[face_group[f]];
+    d3 m = mk3(g.mdir[0], g.mdir[1], g.mdir[2]);
+    double out[NFC];
+    out[FC_AX] = v[0].x; out[FC_AY] = v[0].y; out[FC_AZ] = v[0].z;
+    out[FC_BX] = v[1].x; out[FC_BY] = v[1].y; out[FC_BZ] = v[1].z;
+    out[FC_CX] = v[2].x; out[FC_CY] = v[2].y; out[FC_CZ] = v[2].z;
+    out[FC_NX] = un.x; out[FC_NY] = un.y; out[FC_NZ] = un.z;
+    out[FC_MF] = dot3(m, un) * dot3(fdir, un);
+    for (int i = 0; i < 3; ++i) {
+        d3 e = v[(i + 1) % 3] - v[i];
+        double L = norm3(e);
+        d3 eh = (L < kEps) ? mk3(0, 0, 0) : mk3(e.x / L, e.y / L, e.z / L);
+        d3 perp = cross3(un, eh);
+        out[FC_E0X + 3 * i] = e.x; out[FC_E0Y + 3 * i] = e.y; out[FC_E0Z + 3 * i] = e.z;
+        out[FC_L0 + i] = L;
+        out[FC_P0X + 3 * i] = perp.x; out[FC_P0Y + 3 * i] = perp.y; out[FC_P0Z + 3 * i] = perp.z;
+        out[FC_MT0 + i] = dot3(m, perp) * dot3(fdir, perp);
+    }
+    out[FC_VALID] = valid ? 1.0 : 0.0;
+    for (int k = 0; k < NFC; ++k) fc[(size_t)k * T + f] = out[k];
+}
+
+__global__ void k_face_prep_grad(int T, const int32_t* __restrict__ tri, const double* __restrict__ pos,
+                                 const int16_t* __restrict__ face_group, const GroupConst* __restrict__ groups,
+                                 const uint8_t* __restrict__ face_needs, int want_grav, int want_mag, d3 fdir,
+                                 double* __restrict__ gc) {
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= T) return;
+    const double* pa = pos + 3 * tri[3 * f];
+    const double* pb = pos + 3 * tri[3 * f + 1];
+    const double* pc = pos + 3 * tri[3 * f + 2];
+    d3 a = mk3(pa[0], pa[1], pa[2]), b = mk3(pb[0], pb[1], pb[2]), c = mk3(pc[0], pc[1], pc[2]);
+    d3 n = cross3(b - a, c - a);
+    double area2 = norm3(n);
+    double L0 = norm3(b - a), L1 = norm3(c - b), L2 = norm3(a - c);
+    bool valid = !(area2 < kEps) && !(L0 < kEps) && !(L1 < kEps) && !(L2 < kEps);
+    double out[NGC];
+    for (int k = 0; k < NGC; ++k) out[k] = 0.0;
+    if (valid) {
+        d3 zh = n * (1.0 / area2);
+        d3 xh = (b - a) * (1.0 / L0);
+        d3 yh = cross3(zh, xh);
+        d3 ca = c - a;
+        double cx = dot3(ca, xh), cy = dot3(ca, yh);
+        const GroupConst& g = groups[face_group[f]];
+        d3 m = mk3(g.mdir[0], g.mdir[1], g.mdir[2]);
+        out[GC_AX] = a.x; out[GC_AY] = a.y; out[GC_AZ] = a.z;
+        out[GC_XX] = xh.x; out[GC_XY] = xh.y; out[GC_XZ] = xh.z;
+        out[GC_YX] = yh.x; out[GC_YY] = yh.y; out[GC_YZ] = yh.z;
+        out[GC_ZX] = zh.x; out[GC_ZY] = zh.y; out[GC_ZZ] = zh.z;
+        out[GC_L0] = L0; out[GC_CX] = cx; out[GC_CY] = cy;
+        out[GC_E1X] = (cx - L0) / L1; out[GC_E1Y] = cy / L1; out[GC_L1] = L1;
+        out[GC_E2X] = -cx / L2; out[GC_E2Y] = -cy / L2; out[GC_L2] = L2;
+        out[GC_GS] = want_grav ? g.gscale_jac : 0.0;
+        out[GC_MS] = (want_mag && g.mag_active) ? -g.mscale : 0.0;
+        // magnetic direction products in the local frame
+        d3 ml = mk3(dot3(m, xh), dot3(m, yh), dot3(m, zh));
+        d3 fl = mk3(dot3(fdir, xh), dot3(fdir, yh), dot3(fdir, zh));
+        out[GC_MF] = ml.z * fl.z;
+        double ex[3] = {1.0, out[GC_E1X], out[GC_E2X]}, ey[3] = {0.0, out[GC_E1Y], out[GC_E2Y]};
+        for (int i = 0; i < 3; ++i) {
+            // in-plane edge normal perp = z x e = (-ey, ex, 0)
+            double mp = -ml.x * ey[i] + ml.y * ex[i], fp = -fl.x * ey[i] + fl.y * ex[i];
+            out[GC_MT0 + i] = mp * fp;
+        }
+        out[GC_FLAGS] = 1.0 + (face_needs[f] ? 2.0 : 0.0);
+    }
+    for (int k = 0; k < NGC; ++k) gc[(size_t)k * T + f] = out[k];
+}
+
+// ------------------------------------------------------------- forward ----
+// One pair (station o, facet in shared memory slot j) in the reference's
+// operation order.  Adds the gz facet factor to *gz and the TMI facet factor
+// to *tmi.
+template <bool GZ, bool TMI>
+__device__ __forceinline__ void pair_forward_fp64(const double* __restrict__ s, int j, int stride, d3 o,
+                                                  double* gz, double* tmi) {
+#define F(k) s[(k) * stride + j]
+    if (F(FC_VALID) == 0.0) return;
+    d3 ra = mk3(F(FC_AX) - o.x, F(FC_AY) - o.y, F(FC_AZ) - o.z);
+    d3 rb = mk3(F(FC_BX) - o.x, F(FC_BY) - o.y, F(FC_BZ) - o.z);
+    d3 rc = mk3(F(FC_CX) - o.x, F(FC_CY) - o.y, F(FC_CZ) - o.z);
+    double la = norm3(ra), lb = norm3(rb), lc = norm3(rc);
+    double omega = 0.0;
+    if (!(la < kEps || lb < kEps || lc < kEps)) {
+        double num = dot3(ra, cross3(rb, rc));
+        double den = la * lb * lc + dot3(ra, rb) * lc + dot3(ra, rc) * lb + dot3(rb, rc) * la;
+        omega = 2.0 * atan2(num, den);
+    }
+    d3 un = mk3(F(FC_NX), F(FC_NY), F(FC_NZ));
+    double h = dot3(ra, un);
+    d3 r[3] = {ra, rb, rc};
+    double l[3] = {la, lb, lc};
+    double dsum = 0.0, tsum = 0.0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        double L = F(FC_L0 + i);
+        if (L < kEps) continue;
+        d3 e = mk3(F(FC_E0X + 3 * i), F(FC_E0Y + 3 * i), F(FC_E0Z + 3 * i));
+        d3 r1 = r[i], r2 = r[(i + 1) % 3];
+        double s1 = dot3(r1, e) / L, s2 = dot3(r2, e) / L;
+        bool live;
+        double lam = lambda_from(s1, s2, l[i], l[(i + 1) % 3], &live);
+        if (GZ) {
+            d3 p = mk3(F(FC_P0X + 3 * i), F(FC_P0Y + 3 * i), F(FC_P0Z + 3 * i));
+            double dperp = -dot3(r1, p);
+            dsum += dperp * lam;
+        }
+        if (TMI) tsum += F(FC_MT0 + i) * lam;
+    }
+    if (GZ) *gz += un.z * (dsum - h * omega);
+    if (TMI) *tmi += F(FC_MF) * omega + tsum;
+#undef F
+}
+
+// Grid: x = station tiles of blockDim.x, y = facet chunks (each inside one
+// group).  Writes the chunk's unscaled facet sums per station.
+template <bool GZ, bool TMI, int FT>
+__global__ void __launch_bounds__(128) k_forward_fp64(int S, const double* __restrict__ sta, int T,
+                                                      const double* __restrict__ fc, const int32_t* __restrict__ chunk_begin,
+                                                      const int32_t* __restrict__ chunk_end, double* __restrict__ part_gz,
+                                                      double* __restrict__ part_tmi) {
+    __shared__ double sm[NFC * FT];
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    int chunk = blockIdx.y;
+    int fb = chunk_begin[chunk], fe = chunk_end[chunk];
+    d3 o = mk3(0, 0, 0);
+    if (s < S) o = mk3(sta[3 * s], sta[3 * s + 1], sta[3 * s + 2]);
+    double gz = 0.0, tmi = 0.0;
+    for (int f0 = fb; f0 < fe; f0 += FT) {
+        int nf = min(FT, fe - f0);
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < NFC * FT; idx += blockDim.x) {
+            int k = idx / FT, j = idx % FT;
+            sm[idx] = (j < nf) ? fc[(size_t)k * T + f0 + j] : 0.0;
+        }
+        __syncthreads();
+        if (s < S)
+            for (int j = 0; j < nf; ++j) pair_forward_fp64<GZ, TMI>(sm, j, FT, o, &gz, &tmi);
+    }
+    if (s < S) {
+        if (GZ) part_gz[(size_t)chunk * S + s] = gz;
+        if (TMI) part_tmi[(size_t)chunk * S + s] = tmi;
+    }
+}
+
+// Sums chunk partials group by group and applies the group scales:
+// gz = sum_g (sum_f face) * G*rho*1e3*1e5 (gravityClosedMesh :162-178),
+// tmi = sum_g -(amp*100/(4 pi)) * sum_f facet (magneticClosedMeshVector :367-386).
+__global__ void k_forward_reduce(int S, int nchunks, const int32_t* __restrict__ chunk_group,
+                                 const GroupConst* __restrict__ groups, const double* __restrict__ part_gz,
+                                 const double* __restrict__ part_tmi, double* __restrict__ gz, double* __restrict__ tmi) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= S) return;
+    double accg = 0.0, acct = 0.0;
+    int c = 0;
+    while (c < nchunks) {
+        int g = chunk_group[c];
+        double tg = 0.0, tt = 0.0;
+        for (; c < nchunks && chunk_group[c] == g; ++c) {
+            if (part_gz) tg += part_gz[(size_t)c * S + s];
+            if (part_tmi) tt += part_tmi[(size_t)c * S + s];
+        }
+        accg += tg * groups[g].gscale_fwd;
+        acct += -groups[g].mscale * tt;
+    }
+    if (gz) gz[s] = accg;
+    if (tmi) tmi[s] = acct;
+}
+
+// ----------------------------------------------------------- residuals ----
+// ObjectiveFunction misfit (objective.cpp:22-31, 83-105): w = 1/std or 1;
+// adjoint c = -alpha * w^2 * (obs - pred); per-block partial misfit sums.
+__global__ void k_residual(int S, const double* __restrict__ pred, const double* __restrict__ obs,
+                           const double* __restrict__ w, double alpha, double* __restrict__ coef,
+                           double* __restrict__ block_misfit) {
+    __shared__ double red[256];
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    double mis = 0.0;
+    if (s < S) {
+        double ws = w[s];
+        double r = obs[s] - pred[s];
+        double res = ws * r;
+        mis = 0.5 * res * res;
+        if (coef) coef[s] = -alpha * (ws * ws * r);
+    }
+    red[threadIdx.x] = mis;
+    __syncthreads();
+    for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+        if (threadIdx.x < k) red[threadIdx.x] += red[threadIdx.x + k];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) block_misfit[blockIdx.x] = red[0];
+}
+
+// ------------------------------------------------------------ gradient ----
+struct StationTile {
+    // per station: x, y, z, gravity adjoint, magnetic adjoint
+    double v[5];
+};
+
+// Per-facet accumulators over stations (local frame).
+struct GradAcc {
+    d3 va, vb, vc;      // vertex-direct terms
+    double alam[3];     // sum Gs * Lambda_i       (d_perp direct on p1)
+    double aom;         // sum Gs * Omega          (h direct on a)
+    double ai;          // sum G0 * I              (n_z factor)
+    d3 bh;              // sum Gs * Omega * r_a    (h through n_hat)
+    d3 bl[3];           // sum Gs * Lambda_i * r1  (d_perp through perp_i)
+    double amf;         // sum Ts * Omega          (MF)
+    double amt[3];      // sum Ts * Lambda_i       (MT_i)
+};
+
+__device__ __forceinline__ void edge_terms(d3 r1, d3 r2, double d1, double d2, double ex, double ey, double L,
+                                           double inv1, double inv2, double kom, double Gs, double Ts, double mt,
+                                           double dperp, double lam, bool live, d3* g1, d3* g2) {
+    // kappa_i = Gs * d_perp + Ts * MT_i
+    double kl = live ? (Gs * dperp + Ts * mt) : 0.0;
+    double dw = d1 * d2 + dot3(r1, r2);
+    double W = dw > 1e-300 ? L / dw : 0.0;
+    double s1 = r1.x * ex + r1.y * ey;
+    d3 q = mk3(r1.x - s1 * ex, r1.y - s1 * ey, r1.z);
+    d3 Z = mk3(ey * r1.z, -ex * r1.z, ex * r1.y - ey * r1.x);  // e_hat x r1, e_hat = (ex, ey, 0)
+    d3 P = mk3(W * (kom * Z.x - kl * q.x), W * (kom * Z.y - kl * q.y), W * (kom * Z.z - kl * q.z));
+    *g1 = *g1 + mk3((P.x - kl * ex) * inv1, (P.y - kl * ey) * inv1, P.z * inv1);
+    *g2 = *g2 + mk3((P.x + kl * ex) * inv2, (P.y + kl * ey) * inv2, P.z * inv2);
+}
+
+// Grid: x = facet tiles of blockDim.x, y = station chunks.  part layout:
+// [chunk][9][T] (vertex a xyz, b xyz, c xyz; global frame).
+template <int ST>
+__global__ void __launch_bounds__(128) k_gradient_fp64(int T, const double* __restrict__ gc, int S,
+                                                       const double* __restrict__ sta, const double* __restrict__ gcoef,
+                                                       const double* __restrict__ mcoef, int stations_per_chunk,
+                                                       const int16_t* __restrict__ face_group,
+                                                       const GroupConst* __restrict__ groups, d3 fdir,
+                                                       double* __restrict__ part) {
+    __shared__ double st[5 * ST];
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    int chunk = blockIdx.y;
+    int sb = chunk * stations_per_chunk, se = min(S, sb + stations_per_chunk);
+    bool active = false;
+    double C[NGC];
+    if (f < T) {
+#pragma unroll
+        for (int k = 0; k < NGC; ++k) C[k] = gc[(size_t)k * T + f];
+        int flags = static_cast<int>(C[GC_FLAGS]);
+        active = (flags & 1) && (flags & 2) && (C[GC_GS] != 0.0 || C[GC_MS] != 0.0);
+    }
+    GradAcc A;
+    A.va = A.vb = A.vc = mk3(0, 0, 0);
+    A.bh = mk3(0, 0, 0);
+    for (int i = 0; i < 3; ++i) { A.alam[i] = 0; A.bl[i] = mk3(0, 0, 0); A.amt[i] = 0; }
+    A.aom = A.ai = A.amf = 0.0;
+    double nz = 0, gsn = 0, ms = 0;
+    if (active) { nz = C[GC_ZZ]; gsn = C[GC_GS]; ms = C[GC_MS]; }
+    const double L0 = active ? C[GC_L0] : 0, cx = active ? C[GC_CX] : 0, cy = active ? C[GC_CY] : 0;
+    const double area2 = L0 * cy;
+    for (int s0 = sb; s0 < se; s0 += ST) {
+        int ns = min(ST, se - s0);
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < ns; idx += blockDim.x) {
+            int sIdx = s0 + idx;
+            st[5 * idx + 0] = sta[3 * sIdx];
+            st[5 * idx + 1] = sta[3 * sIdx + 1];
+            st[5 * idx + 2] = sta[3 * sIdx + 2];
+            st[5 * idx + 3] = gcoef ? gcoef[sIdx] : 0.0;
+            st[5 * idx + 4] = mcoef ? mcoef[sIdx] : 0.0;
+        }
+        __syncthreads();
+        if (!active) continue;
+        for (int j = 0; j < ns; ++j) {
+            double G0 = st[5 * j + 3] * gsn;   // gravity adjoint x group scale
+            double Gs = G0 * nz;               // ... x n_z
+            double Ts = st[5 * j + 4] * ms;    // magnetic adjoint x group TMI scale
+            if (Gs == 0.0 && Ts == 0.0 && G0 == 0.0) continue;
+            d3 dd = mk3(st[5 * j] - C[GC_AX], st[5 * j + 1] - C[GC_AY], st[5 * j + 2] - C[GC_AZ]);
+            double x = dd.x * C[GC_XX] + dd.y * C[GC_XY] + dd.z * C[GC_XZ];
+            double y = dd.x * C[GC_YX] + dd.y * C[GC_YY] + dd.z * C[GC_YZ];
+            double z = dd.x * C[GC_ZX] + dd.y * C[GC_ZY] + dd.z * C[GC_ZZ];
+            d3 ra = mk3(-x, -y, -z), rb = mk3(L0 - x, -y, -z), rc = mk3(cx - x, cy - y, -z);
+            double z2 = z * z;
+            double la = sqrt(x * x + y * y + z2), lb = sqrt(rb.x * rb.x + y * y + z2),
+                   lc = sqrt(rc.x * rc.x + rc.y * rc.y + z2);
+            if (la < kEps || lb < kEps || lc < kEps) continue;  // station on a vertex: not differentiable
+            double h = -z;
+            double Nn = h * area2;
+            double Dd = la * lb * lc + dot3(ra, rb) * lc + dot3(ra, rc) * lb + dot3(rb, rc) * la;
+            double om = 2.0 * atan2(Nn, Dd);
+            double ia = 1.0 / la, ib = 1.0 / lb, ic = 1.0 / lc;
+            // edges: 0 a->b (e=(1,0)), 1 b->c, 2 c->a
+            double e1x = C[GC_E1X], e1y = C[GC_E1Y], e2x = C[GC_E2X], e2y = C[GC_E2Y];
+            bool lv0, lv1, lv2;
+            double lam0 = lambda_from(-x, L0 - x, la, lb, &lv0);
+            double s11 = rb.x * e1x + rb.y * e1y, s12 = rc.x * e1x + rc.y * e1y;
+            double lam1 = lambda_from(s11, s12, lb, lc, &lv1);
+            double s21 = rc.x * e2x + rc.y * e2y, s22 = ra.x * e2x + ra.y * e2y;
+            double lam2 = lambda_from(s21, s22, lc, la, &lv2);
+            // d_perp_i = -r1 . perp_i, perp_i = (-ey, ex, 0)
+            double dp0 = y;                         // -(r_a.y * 1)
+            double dp1 = rb.x * e1y - rb.y * e1x;
+            double dp2 = rc.x * e2y - rc.y * e2x;
+            double I = dp0 * lam0 + dp1 * lam1 + dp2 * lam2 - h * om;
+            double kom = -Gs * h + Ts * C[GC_MF];
+            edge_terms(ra, rb, la, lb, 1.0, 0.0, L0, ia, ib, kom, Gs, Ts, C[GC_MT0], dp0, lam0, lv0, &A.va, &A.vb);
+            edge_terms(rb, rc, lb, lc, e1x, e1y, C[GC_L1], ib, ic, kom, Gs, Ts, C[GC_MT1], dp1, lam1, lv1, &A.vb, &A.vc);
+            edge_terms(rc, ra, lc, la, e2x, e2y, C[GC_L2], ic, ia, kom, Gs, Ts, C[GC_MT2], dp2, lam2, lv2, &A.vc, &A.va);
+            A.alam[0] += Gs * lam0; A.alam[1] += Gs * lam1; A.alam[2] += Gs * lam2;
+            A.aom += Gs * om;
+            A.ai += G0 * I;
+            A.bh = A.bh + ra * (Gs * om);
+            A.bl[0] = A.bl[0] + ra * (Gs * lam0);
+            A.bl[1] = A.bl[1] + rb * (Gs * lam1);
+            A.bl[2] = A.bl[2] + rc * (Gs * lam2);
+            A.amf += Ts * om;
+            A.amt[0] += Ts * lam0; A.amt[1] += Ts * lam1; A.amt[2] += Ts * lam2;
+        }
+    }
+    if (f >= T) return;
+    double outv[9];
+    if (!active) {
+        for (int k = 0; k < 9; ++k) outv[k] = 0.0;
+    } else {
+        // ---- per-facet finalisation in the local frame ----
+        d3 xh = mk3(C[GC_XX], C[GC_XY], C[GC_XZ]), yh = mk3(C[GC_YX], C[GC_YY], C[GC_YZ]),
+           zh = mk3(C[GC_ZX], C[GC_ZY], C[GC_ZZ]);
+        const GroupConst& g = groups[face_group[f]];
+        d3 mg = mk3(g.mdir[0], g.mdir[1], g.mdir[2]);
+        d3 ml = mk3(dot3(mg, xh), dot3(mg, yh), dot3(mg, zh));
+        d3 fl = mk3(dot3(fdir, xh), dot3(fdir, yh), dot3(fdir, zh));
+        d3 nh = mk3(0, 0, 1);
+        d3 eh[3] = {mk3(1, 0, 0), mk3(C[GC_E1X], C[GC_E1Y], 0), mk3(C[GC_E2X], C[GC_E2Y], 0)};
+        double Ls[3] = {L0, C[GC_L1], C[GC_L2]};
+        d3 vbar[3] = {A.va, A.vb, A.vc};
+        // n_hat adjoint
+        d3 nbar = A.bh * -1.0;
+        {
+            double mn = ml.z, fn = fl.z;
+            nbar = nbar + (ml * fn + fl * mn) * A.amf;
+            // n_z = n_hat . e_z(global); e_z in local coordinates
+            nbar = nbar + mk3(xh.z, yh.z, zh.z) * A.ai;
+        }
+        // vertex-direct: h on a, d_perp on p1
+        vbar[0] = vbar[0] + nh * (-A.aom);
+        for (int i = 0; i < 3; ++i) {
+            d3 perp = cross3(nh, eh[i]);
+            vbar[i] = vbar[i] + perp * (-A.alam[i]);
+            double mp = dot3(ml, perp), fp = dot3(fl, perp);
+            d3 pbar = A.bl[i] * -1.0 + (ml * fp + fl * mp) * A.amt[i];
+            // perp = n x e: n_bar += e x pbar, e_bar = pbar x n
+            nbar = nbar + cross3(eh[i], pbar);
+            d3 ebar = cross3(pbar, nh);
+            double pe = dot3(ebar, eh[i]);
+            d3 eraw = (ebar - eh[i] * pe) * (1.0 / Ls[i]);
+            vbar[(i + 1) % 3] = vbar[(i + 1) % 3] + eraw;
+            vbar[i] = vbar[i] - eraw;
+        }
+        // n_hat = n / |n|, n = (b-a) x (c-a)
+        double pn = dot3(nbar, nh);
+        d3 nraw = (nbar - nh * pn) * (1.0 / area2);
+        d3 u = mk3(L0, 0, 0), w = mk3(cx, cy, 0);
+        d3 ubar = cross3(w, nraw), wbar = cross3(nraw, u);
+        vbar[1] = vbar[1] + ubar;
+        vbar[2] = vbar[2] + wbar;
+        vbar[0] = vbar[0] - ubar - wbar;
+        for (int v = 0; v < 3; ++v) {
+            d3 gv = xh * vbar[v].x + yh * vbar[v].y + zh * vbar[v].z;
+            outv[3 * v] = gv.x; outv[3 * v + 1] = gv.y; outv[3 * v + 2] = gv.z;
+        }
+    }
+    for (int k = 0; k < 9; ++k) part[((size_t)chunk * 9 + k) * T + f] = outv[k];
+}
+
+// Sums facet partials into vertex gradients (deterministic order: chunks,
+// then the vertex's incident (facet, corner) list), for the vertices listed.
+__global__ void k_vertex_reduce(int nverts, const int32_t* __restrict__ verts, const int32_t* __restrict__ vf_off,
+                                const int32_t* __restrict__ vf, int T, int nchunks, const double* __restrict__ part,
+                                double* __restrict__ vgrad) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nverts) return;
+    int v = verts[i];
+    double gx = 0, gy = 0, gz = 0;
+    for (int c = 0; c < nchunks; ++c)
+        for (int k = vf_off[v]; k < vf_off[v + 1]; ++k) {
+            int f = vf[k] / 3, corner = vf[k] % 3;
+            const double* p = part + ((size_t)c * 9 + 3 * corner) * T + f;
+            gx += p[0];
+            gy += p[(size_t)T];
+            gz += p[(size_t)2 * T];
+        }
+    vgrad[3 * v] = gx;
+    vgrad[3 * v + 1] = gy;
+    vgrad[3 * v + 2] = gz;
+}
+
+// grad[d] = sum_refs vgrad[vertex][axis] * axis scale + reference-model term
+// (gather of gravity_forward.cpp:269-289 contracted; reference_model.cpp:22-25).
+__global__ void k_dof_gather(int np, const int32_t* __restrict__ dof_off, const int32_t* __restrict__ ref_vertex,
+                             const uint8_t* __restrict__ ref_axis, const double* __restrict__ ref_scale,
+                             const double* __restrict__ vgrad, const double* __restrict__ params,
+                             const double* __restrict__ ref_params, double ref_weight, double* __restrict__ grad) {
+    int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= np) return;
+    double acc = 0.0;
+    for (int r = dof_off[d]; r < dof_off[d + 1]; ++r) acc += vgrad[3 * ref_vertex[r] + ref_axis[r]] * ref_scale[r];
+    if (ref_params) acc += ref_weight * (params[d] - ref_params[d]);
+    grad[d] = acc;
+}
+
+// Dense Jacobian rows from per-station facet partials (one chunk per
+// station): J[s][d] = sum_refs (sum_{(f,c) of v} part) * scale, with the
+// reference's |vertex gradient| < 1e-30 skip.
+__global__ void k_jacobian_gather(int nst, int np, const int32_t* __restrict__ dof_off,
+                                  const int32_t* __restrict__ ref_vertex, const uint8_t* __restrict__ ref_axis,
+                                  const double* __restrict__ ref_scale, const int32_t* __restrict__ vf_off,
+                                  const int32_t* __restrict__ vf, int T, const double* __restrict__ part,
+                                  double* __restrict__ J, int ld) {
+    int d = blockIdx.x * blockDim.x + threadIdx.x;
+    int s = blockIdx.y;
+    if (d >= np || s >= nst) return;
+    double acc = 0.0;
+    for (int r = dof_off[d]; r < dof_off[d + 1]; ++r) {
+        int v = ref_vertex[r], ax = ref_axis[r];
+        double pg = 0.0;
+        for (int k = vf_off[v]; k < vf_off[v + 1]; ++k) {
+            int f = vf[k] / 3, corner = vf[k] % 3;
+            pg += part[((size_t)s * 9 + 3 * corner + ax) * T + f];
+        }
+        if (fabs(pg) < 1e-30) continue;
+        acc += pg * ref_scale[r];
+    }
+    J[(size_t)s * ld + d] = acc;
+}
+
+// Final deterministic reduction of block partials and objective assembly:
+// out = {grav misfit, mag misfit, reg, 0, total}.
+__global__ void k_objective_final(int nbg, const double* __restrict__ bg, int nbm, const double* __restrict__ bm,
+                                  double alpha, int np, const double* __restrict__ params,
+                                  const double* __restrict__ ref_params, double ref_weight, double* __restrict__ out5,
+                                  double* __restrict__ f_out) {
+    __shared__ double red[256];
+    double reg = 0.0;
+    if (ref_params)
+        for (int d = threadIdx.x; d < np; d += blockDim.x) {
+            double dd = params[d] - ref_params[d];
+            reg += dd * dd;
+        }
+    red[threadIdx.x] = reg;
+    __syncthreads();
+    for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+        if (threadIdx.x < k) red[threadIdx.x] += red[threadIdx.x + k];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        double g = 0.0, m = 0.0;
+        for (int i = 0; i < nbg; ++i) g += bg[i];
+        for (int i = 0; i < nbm; ++i) m += bm[i];
+        double r = ref_params ? 0.5 * ref_weight * red[0] : 0.0;
+        double total = g + alpha * m + r;
+        out5[0] = g; out5[1] = m; out5[2] = r; out5[3] = 0.0; out5[4] = total;
+        if (f_out) *f_out = total;
+    }
+}
+
+}  // namespace litho_b200

@@ -1,0 +1,446 @@
+/*
+ * litho_oracle.c -- TEST INFRASTRUCTURE ONLY.
+ *
+ * A plain-C, single-threaded FP64 restatement of LithoInv's forward /
+ * Jacobian / parameter-scatter path.  It is the checker that the CUDA
+ * implementation is compared against; nothing in the product library links,
+ * loads or calls it.  Only tests/, __graft_entry__.smoke() and bench.py's
+ * cpu_baseline leg may use it.
+ *
+ * Parity of this restatement is pinned against the reference's own C++
+ * sources compiled unmodified (oracle/Makefile -> oracle/_ref/) by
+ * tests/test_oracle_pin.py, and against the committed golden vectors in
+ * tests/golden/.
+ *
+ * Every function cites the reference function it restates (paths are
+ * relative to the reference project root).  The arithmetic is written in the
+ * same operation order as the reference so that, compiled without FMA
+ * contraction, results agree with the reference to the last bit or close.
+ *
+ * Data layout shared by every model-level function (row-major, int32 indices):
+ *   pos[V*3]            vertex positions (metres), one slot per (mesh, vertex)
+ *   tri[T*3]            triangles as global vertex indices, grouped by lithology
+ *   grp_tri_off[G+1]    triangles of group g are tri[grp_tri_off[g] .. grp_tri_off[g+1])
+ *   sta[S*3]            observation stations
+ *   dof_off[np+1]       global DOF d owns refs dof_off[d] .. dof_off[d+1]
+ *   ref_vertex/axis/scale  per ref: global vertex, axis (0,1,2), axis scale
+ *   interp_off[V+1], interp_src, interp_w   control-point interpolation rows
+ *   sync_off[ns+1], sync_vertex             shared-vertex averaging groups
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define LO_EPS 1e-15
+#define LO_PI 3.14159265358979323846
+
+/* gravity_forward.h:37-41 */
+#define LO_G_SI 6.67430e-11
+#define LO_DENSITY_SCALE 1000.0
+#define LO_M_S2_TO_MGAL 1e5
+
+typedef struct { double x, y, z; } v3;
+
+static inline v3 mk(const double *p) { v3 r = {p[0], p[1], p[2]}; return r; }
+static inline v3 sub(v3 a, v3 b) { v3 r = {a.x - b.x, a.y - b.y, a.z - b.z}; return r; }
+static inline v3 add(v3 a, v3 b) { v3 r = {a.x + b.x, a.y + b.y, a.z + b.z}; return r; }
+static inline v3 scl(v3 a, double s) { v3 r = {a.x * s, a.y * s, a.z * s}; return r; }
+static inline v3 dvs(v3 a, double s) { v3 r = {a.x / s, a.y / s, a.z / s}; return r; }
+static inline double dot(v3 a, v3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline v3 cross(v3 a, v3 b) {
+    v3 r = {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+    return r;
+}
+static inline double norm(v3 a) { return sqrt(dot(a, a)); }
+static inline double comp(v3 a, int k) { return k == 0 ? a.x : (k == 1 ? a.y : a.z); }
+static inline void setc(v3 *a, int k, double v) {
+    if (k == 0) a->x = v; else if (k == 1) a->y = v; else a->z = v;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Geometry primitives: modules/litho-core/src/core/geometry.cpp            */
+/* ------------------------------------------------------------------------ */
+
+/* solidAngle, geometry.cpp:10-30 (van Oosterom & Strackee). */
+static double solid_angle(v3 a, v3 b, v3 c, v3 o) {
+    v3 ra = sub(a, o), rb = sub(b, o), rc = sub(c, o);
+    double la = norm(ra), lb = norm(rb), lc = norm(rc);
+    if (la < LO_EPS || lb < LO_EPS || lc < LO_EPS) return 0.0;
+    /* tripleProduct(a,b,c) = a.dot(b.cross(c)), core/geometry.h:7-9 */
+    double num = dot(ra, cross(rb, rc));
+    double den = la * lb * lc + dot(ra, rb) * lc + dot(ra, rc) * lb + dot(rb, rc) * la;
+    return 2.0 * atan2(num, den);
+}
+
+/* lineIntegralTerm, geometry.cpp:32-52. */
+static double line_integral_term(v3 a, v3 b, v3 o) {
+    v3 ra = sub(a, o), rb = sub(b, o), e = sub(b, a);
+    double L = norm(e);
+    if (L < LO_EPS) return 0.0;
+    double s1 = dot(ra, e) / L;
+    double s2 = dot(rb, e) / L;
+    double d1 = norm(ra), d2 = norm(rb);
+    double num = s2 + d2, den = s1 + d1;
+    if (fabs(den) < LO_EPS && fabs(num) < LO_EPS) return 0.0;
+    if (fabs(den) < LO_EPS) return 0.0;
+    if (num <= 0.0 || den <= 0.0) return 0.0;
+    return log(num / den);
+}
+
+/* faceNagyContribution, modules/litho-forward/src/forward/gravity_forward.cpp:13-42.
+ * Returns n_z * (sum_i d_perp_i * Lambda_i - h * Omega). */
+static double face_nagy(v3 obs, v3 a, v3 b, v3 c) {
+    v3 n = cross(sub(b, a), sub(c, a));
+    double area_x2 = norm(n);
+    if (area_x2 < LO_EPS) return 0.0;
+    v3 un = dvs(n, area_x2);
+    double nz = un.z;
+    double omega = solid_angle(a, b, c, obs);
+    double h = dot(sub(a, obs), un);
+    double d_sum = 0.0;
+    v3 vs[3] = {a, b, c};
+    for (int i = 0; i < 3; ++i) {
+        v3 p1 = vs[i], p2 = vs[(i + 1) % 3];
+        v3 e = sub(p2, p1);
+        double L = norm(e);
+        if (L < LO_EPS) continue;
+        v3 eh = dvs(e, L);
+        v3 perp = cross(un, eh);
+        double dperp = dot(sub(obs, p1), perp);
+        double lam = line_integral_term(p1, p2, obs);
+        d_sum += dperp * lam;
+    }
+    return nz * (d_sum - h * omega);
+}
+
+/* MagneticForward::magneticFacet, modules/litho-forward/src/forward/magnetic_forward.cpp:312-347. */
+static double magnetic_facet(v3 obs, v3 a, v3 b, v3 c, v3 mdir, v3 fdir) {
+    v3 n = cross(sub(b, a), sub(c, a));
+    double area_x2 = norm(n);
+    if (area_x2 < LO_EPS) return 0.0;
+    v3 nh = dvs(n, area_x2);
+    double omega = solid_angle(a, b, c, obs);
+    double mn = dot(mdir, nh), fn = dot(fdir, nh);
+    double contribution = mn * fn * omega;
+    v3 vs[3] = {a, b, c};
+    for (int i = 0; i < 3; ++i) {
+        v3 p1 = vs[i], p2 = vs[(i + 1) % 3];
+        v3 e = sub(p2, p1);
+        double L = norm(e);
+        if (L < LO_EPS) continue;
+        v3 eh = dvs(e, L);
+        v3 t = cross(nh, eh);
+        double mt = dot(mdir, t), ft = dot(fdir, t);
+        double lam = line_integral_term(p1, p2, obs);
+        contribution += mt * ft * lam;
+    }
+    return contribution;
+}
+
+/* Face evaluation selector used by the per-face finite-difference gradient. */
+typedef struct { int kind; v3 mdir, fdir; } facefn;
+
+static double face_eval(const facefn *f, v3 obs, v3 a, v3 b, v3 c) {
+    return f->kind == 0 ? face_nagy(obs, a, b, c) : magnetic_facet(obs, a, b, c, f->mdir, f->fdir);
+}
+
+/* faceNagyWithGradient, gravity_forward.cpp:48-85, and
+ * magneticFacetWithGradient, magnetic_forward.cpp:14-50: value plus forward
+ * differences with h = 1e-4 m on each of the 9 vertex coordinates. */
+static void face_with_fd_gradient(const facefn *f, v3 obs, v3 a, v3 b, v3 c,
+                                  double *value, v3 *ga, v3 *gb, v3 *gc) {
+    const double h = 1e-4;
+    double v = face_eval(f, obs, a, b, c);
+    *value = v;
+    for (int k = 0; k < 3; ++k) {
+        v3 p = a; setc(&p, k, comp(a, k) + h);
+        setc(ga, k, (face_eval(f, obs, p, b, c) - v) / h);
+    }
+    for (int k = 0; k < 3; ++k) {
+        v3 p = b; setc(&p, k, comp(b, k) + h);
+        setc(gb, k, (face_eval(f, obs, a, p, c) - v) / h);
+    }
+    for (int k = 0; k < 3; ++k) {
+        v3 p = c; setc(&p, k, comp(c, k) + h);
+        setc(gc, k, (face_eval(f, obs, a, b, p) - v) / h);
+    }
+}
+
+/* Central-difference derivative of one face term with one Richardson step
+ * (error O(h^4)).  NOT part of the reference: this is the "true derivative"
+ * the analytic device gradient is checked against. */
+static double face_central(const facefn *f, v3 obs, v3 a, v3 b, v3 c, int which, int k, double h) {
+    v3 vp[3] = {a, b, c}, vm[3] = {a, b, c};
+    setc(&vp[which], k, comp(vp[which], k) + h);
+    setc(&vm[which], k, comp(vm[which], k) - h);
+    double fp = face_eval(f, obs, vp[0], vp[1], vp[2]);
+    double fm = face_eval(f, obs, vm[0], vm[1], vm[2]);
+    return (fp - fm) / (2.0 * h);
+}
+
+static void face_true_gradient(const facefn *f, v3 obs, v3 a, v3 b, v3 c, double h,
+                               v3 *ga, v3 *gb, v3 *gc) {
+    v3 *out[3] = {ga, gb, gc};
+    for (int w = 0; w < 3; ++w)
+        for (int k = 0; k < 3; ++k) {
+            double d1 = face_central(f, obs, a, b, c, w, k, h);
+            double d2 = face_central(f, obs, a, b, c, w, k, 0.5 * h);
+            setc(out[w], k, (4.0 * d2 - d1) / 3.0);
+        }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Exported primitives (for pinning and golden vectors)                     */
+/* ------------------------------------------------------------------------ */
+
+double lo_solid_angle(const double *a, const double *b, const double *c, const double *o) {
+    return solid_angle(mk(a), mk(b), mk(c), mk(o));
+}
+double lo_line_integral_term(const double *a, const double *b, const double *o) {
+    return line_integral_term(mk(a), mk(b), mk(o));
+}
+double lo_face_nagy(const double *o, const double *a, const double *b, const double *c) {
+    return face_nagy(mk(o), mk(a), mk(b), mk(c));
+}
+double lo_magnetic_facet(const double *o, const double *a, const double *b, const double *c,
+                         const double *mdir, const double *fdir) {
+    return magnetic_facet(mk(o), mk(a), mk(b), mk(c), mk(mdir), mk(fdir));
+}
+/* grad9 = (ga, gb, gc) as 9 doubles; kind 0 = gravity face, 1 = magnetic facet */
+double lo_face_fd_gradient(int kind, const double *o, const double *a, const double *b,
+                           const double *c, const double *mdir, const double *fdir, double *grad9) {
+    facefn f; f.kind = kind;
+    if (kind) { f.mdir = mk(mdir); f.fdir = mk(fdir); }
+    double v; v3 ga, gb, gc;
+    face_with_fd_gradient(&f, mk(o), mk(a), mk(b), mk(c), &v, &ga, &gb, &gc);
+    double g[9] = {ga.x, ga.y, ga.z, gb.x, gb.y, gb.z, gc.x, gc.y, gc.z};
+    memcpy(grad9, g, sizeof g);
+    return v;
+}
+void lo_face_true_gradient(int kind, const double *o, const double *a, const double *b,
+                           const double *c, const double *mdir, const double *fdir, double h,
+                           double *grad9) {
+    facefn f; f.kind = kind;
+    if (kind) { f.mdir = mk(mdir); f.fdir = mk(fdir); }
+    v3 ga, gb, gc;
+    face_true_gradient(&f, mk(o), mk(a), mk(b), mk(c), h, &ga, &gb, &gc);
+    double g[9] = {ga.x, ga.y, ga.z, gb.x, gb.y, gb.z, gc.x, gc.y, gc.z};
+    memcpy(grad9, g, sizeof g);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Magnetization: MagneticForward ctor magnetic_forward.cpp:57-67 and       */
+/* buildGroupMagnetization :100-134                                          */
+/* ------------------------------------------------------------------------ */
+
+/* Field unit vector (cosI cosD, cosI sinD, -sinI). */
+void lo_field_unit_vector(double inc_deg, double dec_deg, double *out3) {
+    double I = inc_deg * LO_PI / 180.0, D = dec_deg * LO_PI / 180.0;
+    double cI = cos(I);
+    out3[0] = cI * cos(D);
+    out3[1] = cI * sin(D);
+    out3[2] = -sin(I);
+}
+
+/* mode 0 = EffectiveSusceptibility, 1 = FixedVectorPerGroup, 2 = VectorPerGroup. */
+void lo_group_magnetization(double susceptibility, double field_nT, const double *fdir, int mode,
+                            double rem_mag, double rem_inc, double rem_dec, const double *rem_vec,
+                            double *amp, double *dir3) {
+    v3 F = mk(fdir);
+    double induced = susceptibility * field_nT / 100.0;
+    v3 M = scl(F, induced);
+    if (mode == 1) {
+        double I = rem_inc * LO_PI / 180.0, D = rem_dec * LO_PI / 180.0;
+        double cI = cos(I);
+        v3 R = {cI * cos(D), cI * sin(D), -sin(I)};
+        M = add(M, scl(R, rem_mag));
+    } else if (mode == 2) {
+        M = add(M, mk(rem_vec));
+    }
+    double a = norm(M);
+    *amp = a;
+    v3 d = (a < LO_EPS) ? F : dvs(M, a);
+    dir3[0] = d.x; dir3[1] = d.y; dir3[2] = d.z;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Parameter scatter: LithologyModel::applyParameterVector                 */
+/* modules/litho-model/src/litho/lithology_model.cpp:210-248, with          */
+/* SurfaceMesh::interpolateFromControlPoints surface_mesh.cpp:610-623.      */
+/* ------------------------------------------------------------------------ */
+void lo_scatter(int np, const double *params, const int32_t *dof_off, const int32_t *ref_vertex,
+                const uint8_t *ref_axis, const double *ref_scale, int V, const int32_t *interp_off,
+                const int32_t *interp_src, const double *interp_w, int ns, const int32_t *sync_off,
+                const int32_t *sync_vertex, double *pos) {
+    /* 1. each global DOF writes every (mesh, local DOF) it controls */
+    for (int d = 0; d < np; ++d) {
+        double val = params[d];
+        for (int r = dof_off[d]; r < dof_off[d + 1]; ++r)
+            pos[3 * ref_vertex[r] + ref_axis[r]] = val * ref_scale[r];
+    }
+    /* 2. non-control-point vertices of CP meshes = sum w * CP position.
+     * Rows only read control-point vertices, which are never rows. */
+    if (interp_off) {
+        for (int v = 0; v < V; ++v) {
+            int b = interp_off[v], e = interp_off[v + 1];
+            if (b == e) continue;
+            v3 p = {0.0, 0.0, 0.0};
+            for (int k = b; k < e; ++k) p = add(p, scl(mk(pos + 3 * interp_src[k]), interp_w[k]));
+            pos[3 * v] = p.x; pos[3 * v + 1] = p.y; pos[3 * v + 2] = p.z;
+        }
+    }
+    /* 3. shared-vertex averaging groups (lithology_model.cpp:235-247) */
+    for (int s = 0; s < ns; ++s) {
+        int b = sync_off[s], e = sync_off[s + 1];
+        if (e - b < 2) continue;
+        v3 avg = {0.0, 0.0, 0.0};
+        for (int k = b; k < e; ++k) avg = add(avg, mk(pos + 3 * sync_vertex[k]));
+        avg = dvs(avg, (double)(e - b));
+        for (int k = b; k < e; ++k) {
+            pos[3 * sync_vertex[k]] = avg.x;
+            pos[3 * sync_vertex[k] + 1] = avg.y;
+            pos[3 * sync_vertex[k] + 2] = avg.z;
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Forward: GravityForward::compute gravity_forward.cpp:105-118 ->          */
+/* computeUnitGravity :124-130 -> gravityClosedMesh :162-178.                */
+/* ------------------------------------------------------------------------ */
+void lo_forward_gz(int S, const double *sta, int G, const int32_t *grp_tri_off,
+                   const int32_t *tri, const double *pos, const double *rho, double *gz) {
+    for (int s = 0; s < S; ++s) {
+        v3 o = mk(sta + 3 * s);
+        double acc = 0.0;
+        for (int g = 0; g < G; ++g) {
+            if (grp_tri_off[g + 1] == grp_tri_off[g]) continue;
+            double total = 0.0;
+            for (int t = grp_tri_off[g]; t < grp_tri_off[g + 1]; ++t)
+                total += face_nagy(o, mk(pos + 3 * tri[3 * t]), mk(pos + 3 * tri[3 * t + 1]),
+                                   mk(pos + 3 * tri[3 * t + 2]));
+            double scale = LO_G_SI * rho[g] * LO_DENSITY_SCALE * LO_M_S2_TO_MGAL;
+            acc += total * scale;
+        }
+        gz[s] = acc;
+    }
+}
+
+/* MagneticForward::compute magnetic_forward.cpp:81-94 -> computeUnitMagnetic
+ * :136-146 -> magneticClosedMeshVector :367-386. */
+void lo_forward_tmi(int S, const double *sta, int G, const int32_t *grp_tri_off,
+                    const int32_t *tri, const double *pos, const double *mag_amp,
+                    const double *mag_dir, const double *fdir, double *tmi) {
+    v3 F = mk(fdir);
+    for (int s = 0; s < S; ++s) {
+        v3 o = mk(sta + 3 * s);
+        double acc = 0.0;
+        for (int g = 0; g < G; ++g) {
+            if (grp_tri_off[g + 1] == grp_tri_off[g]) continue;
+            v3 m = mk(mag_dir + 3 * g);
+            double gf = 0.0;
+            for (int t = grp_tri_off[g]; t < grp_tri_off[g + 1]; ++t)
+                gf += magnetic_facet(o, mk(pos + 3 * tri[3 * t]), mk(pos + 3 * tri[3 * t + 1]),
+                                     mk(pos + 3 * tri[3 * t + 2]), m, F);
+            double scale = mag_amp[g] * 100.0 / (4.0 * LO_PI);
+            acc += -scale * gf;
+        }
+        tmi[s] = acc;
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Dense Jacobian with the reference's semantics:                           */
+/* computeGravityAnalyticJacobian gravity_forward.cpp:184-292 and           */
+/* computeMagneticAnalyticJacobian magnetic_forward.cpp:196-306.            */
+/*  - per (station, face): forward-FD gradient, h = 1e-4 (kind < 2) or the  */
+/*    Richardson central "true" derivative (kind >= 2, test truth only);    */
+/*  - vertex gradients accumulated per mesh with faceScale;                 */
+/*  - gather: J(i, dof) += vg[vertex][axis] * axisScale for each ref,       */
+/*    skipping |vg| < 1e-30 (reference semantics, kind < 2 only).           */
+/* J is row-major S x np.  `kind`: 0 gravity-FD, 1 magnetic-FD,             */
+/* 2 gravity-true, 3 magnetic-true.                                          */
+/* ------------------------------------------------------------------------ */
+void lo_jacobian(int kind, int S, const double *sta, int G, const int32_t *grp_tri_off,
+                 const int32_t *tri, int V, const double *pos, const double *rho,
+                 const double *mag_amp, const double *mag_dir, const double *fdir, int np,
+                 const int32_t *dof_off, const int32_t *ref_vertex, const uint8_t *ref_axis,
+                 const double *ref_scale, double true_h, double *J) {
+    int mag = kind & 1, truth = kind >= 2;
+    double *vg = (double *)calloc((size_t)V * 3, sizeof(double));
+    const double gscale = LO_G_SI * LO_DENSITY_SCALE * LO_M_S2_TO_MGAL;
+    const double kInv4Pi = 1.0 / (4.0 * LO_PI);
+    facefn f; f.kind = mag;
+    if (mag) f.fdir = mk(fdir);
+    for (int s = 0; s < S; ++s) {
+        v3 o = mk(sta + 3 * s);
+        memset(vg, 0, sizeof(double) * (size_t)V * 3);
+        for (int g = 0; g < G; ++g) {
+            if (grp_tri_off[g + 1] == grp_tri_off[g]) continue;
+            double faceScale;
+            if (mag) {
+                if (mag_amp[g] < LO_EPS) continue;
+                faceScale = -mag_amp[g] * 100.0 * kInv4Pi;
+                f.mdir = mk(mag_dir + 3 * g);
+            } else {
+                faceScale = gscale * rho[g];
+            }
+            for (int t = grp_tri_off[g]; t < grp_tri_off[g + 1]; ++t) {
+                int ia = tri[3 * t], ib = tri[3 * t + 1], ic = tri[3 * t + 2];
+                v3 ga, gb, gc; double val;
+                if (truth)
+                    face_true_gradient(&f, o, mk(pos + 3 * ia), mk(pos + 3 * ib), mk(pos + 3 * ic),
+                                       true_h, &ga, &gb, &gc);
+                else
+                    face_with_fd_gradient(&f, o, mk(pos + 3 * ia), mk(pos + 3 * ib),
+                                          mk(pos + 3 * ic), &val, &ga, &gb, &gc);
+                int ids[3] = {ia, ib, ic};
+                v3 gs[3] = {ga, gb, gc};
+                for (int w = 0; w < 3; ++w) {
+                    v3 c = scl(gs[w], faceScale);
+                    vg[3 * ids[w]] += c.x;
+                    vg[3 * ids[w] + 1] += c.y;
+                    vg[3 * ids[w] + 2] += c.z;
+                }
+            }
+        }
+        double *row = J + (size_t)s * np;
+        for (int d = 0; d < np; ++d) {
+            double acc = 0.0;
+            for (int r = dof_off[d]; r < dof_off[d + 1]; ++r) {
+                double pg = vg[3 * ref_vertex[r] + ref_axis[r]];
+                if (!truth && fabs(pg) < 1e-30) continue;
+                acc += pg * ref_scale[r];
+            }
+            row[d] = acc;
+        }
+    }
+    free(vg);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Objective: ObjectiveFunction modules/litho-inversion/src/inversion/      */
+/* objective.cpp:22-55; w = 1/std if std > 0 else 1.                         */
+/* ------------------------------------------------------------------------ */
+double lo_misfit(int S, const double *pred, const double *obs, const double *std) {
+    double m = 0.0;
+    for (int i = 0; i < S; ++i) {
+        double w = (std[i] > 0) ? (1.0 / std[i]) : 1.0;
+        double res = w * (obs[i] - pred[i]);
+        m += 0.5 * res * res;
+    }
+    return m;
+}
+
+/* dataMisfitGradient objective.cpp:42-55: -J^T (w^2 r); alpha scales the
+ * result as JointObjective::gradient does for magnetics (joint_objective.cpp:46-58). */
+void lo_misfit_gradient(int S, int np, const double *J, const double *pred, const double *obs,
+                        const double *std, double alpha, double *grad_accum) {
+    for (int i = 0; i < S; ++i) {
+        double w = (std[i] > 0) ? (1.0 / std[i]) : 1.0;
+        double wr = w * w * (obs[i] - pred[i]);
+        const double *row = J + (size_t)i * np;
+        for (int d = 0; d < np; ++d) grad_accum[d] += -alpha * row[d] * wr;
+    }
+}

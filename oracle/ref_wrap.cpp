@@ -1,0 +1,300 @@
+// ref_wrap.cpp -- TEST INFRASTRUCTURE ONLY.
+//
+// A thin extern "C" harness around the reference's own, unmodified C++
+// classes (LithologyModel, SurfaceMesh, GravityForward, MagneticForward,
+// ObjectiveFunction, JointObjective, ReferenceModelRegularization,
+// LBFGSBOptimizer).  oracle/Makefile compiles it together with the
+// reference's sources into oracle/_ref/libref_litho.so.  It is used to pin
+// the C restatement (oracle/litho_oracle.c) and the product's DOF builder,
+// and, as `kind: "reference"`, as the timed CPU baseline.  Nothing in the
+// product library links or loads it.
+#include <litho_invert/forward/gravity_forward.h>
+#include <litho_invert/forward/magnetic_forward.h>
+#include <litho_invert/inversion/joint_objective.h>
+#include <litho_invert/inversion/lbfgsb_optimizer.h>
+#include <litho_invert/inversion/objective.h>
+#include <litho_invert/litho/lithology_model.h>
+#include <litho_invert/regularization/reference_model.h>
+#include <litho_invert/regularization/smoothness.h>
+
+#include <array>
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+using namespace litho_invert;
+
+namespace {
+struct RefCtx {
+    std::shared_ptr<LithologyModel> model = std::make_shared<LithologyModel>();
+    GravityData grav;
+    MagneticData mag;
+    double inc = 90.0, dec = 0.0, field = 50000.0;
+    int remMode = 0;
+    std::shared_ptr<GravityForward> gf;
+    std::shared_ptr<MagneticForward> mf;
+    std::shared_ptr<ObjectiveFunction> gobj;
+    std::shared_ptr<JointObjective> jobj;
+    std::shared_ptr<ReferenceModelRegularization> refReg;
+    double alphaMag = 1.0;
+    double refWeight = 0.0;
+    VectorXd refParams;
+    bool built = false;
+
+    void build() {
+        gf = std::make_shared<GravityForward>(model, grav);
+        mf = std::make_shared<MagneticForward>(model, mag, inc, dec, field);
+        mf->setRemanenceMode(static_cast<RemanentMagnetizationMode>(remMode));
+        gobj = std::make_shared<ObjectiveFunction>(gf, grav);
+        if (refWeight > 0.0 && refParams.size() > 0) {
+            refReg = std::make_shared<ReferenceModelRegularization>(model);
+            refReg->setWeight(refWeight);
+            refReg->captureReference(refParams);
+            gobj->addRegularization(refReg);
+        }
+        jobj = std::make_shared<JointObjective>(gobj, mag.empty() ? nullptr : mf, mag, alphaMag);
+        built = true;
+    }
+    void ensure() { if (!built) build(); }
+};
+VectorXd toVec(int n, const double* p) {
+    VectorXd v(n);
+    for (int i = 0; i < n; ++i) v[i] = p[i];
+    return v;
+}
+void fromVec(const VectorXd& v, double* p) {
+    for (Eigen::Index i = 0; i < v.size(); ++i) p[i] = v[i];
+}
+void fromMat(const MatrixXd& J, double* p) {  // row-major out
+    for (Eigen::Index i = 0; i < J.rows(); ++i)
+        for (Eigen::Index j = 0; j < J.cols(); ++j) p[i * J.cols() + j] = J(i, j);
+}
+}  // namespace
+
+extern "C" {
+
+void* ref_new() { return new RefCtx(); }
+void ref_free(void* h) { delete static_cast<RefCtx*>(h); }
+
+// Adds a group (LithoGroup, litho_group.h:13-34).  LithoGroup::isValid rejects
+// density <= 0, so the density is written after addGroup, as a caller must.
+int ref_add_group(void* h, int id, double density, double susceptibility, double rem_mag,
+                  double rem_inc, double rem_dec, const double* rem_vec) {
+    auto* c = static_cast<RefCtx*>(h);
+    LithoGroup g(id, "group" + std::to_string(id), 1.0, susceptibility);
+    g.remanence_magnitude = rem_mag;
+    g.remanence_inclination = rem_inc;
+    g.remanence_declination = rem_dec;
+    if (rem_vec) g.magnetization = Vector3d(rem_vec[0], rem_vec[1], rem_vec[2]);
+    int idx = c->model->addGroup(g);
+    if (idx >= 0) c->model->group(idx).density = density;
+    c->built = false;
+    return idx;
+}
+
+// freedom[v] uses the VertexFreedom numbering (surface_mesh.h:9-19).
+int ref_set_mesh(void* h, int group, int nv, const double* xyz, const uint8_t* freedom, int nt,
+                 const int32_t* tri, const double* axis_scale3, double min_z, double max_z) {
+    auto* c = static_cast<RefCtx*>(h);
+    auto mesh = std::make_shared<SurfaceMesh>();
+    for (int v = 0; v < nv; ++v)
+        mesh->addVertex(Vector3d(xyz[3 * v], xyz[3 * v + 1], xyz[3 * v + 2]),
+                        static_cast<VertexFreedom>(freedom[v]));
+    for (int t = 0; t < nt; ++t) mesh->addTriangle(tri[3 * t], tri[3 * t + 1], tri[3 * t + 2]);
+    for (int a = 0; a < 3; ++a) mesh->setAxisScale(a, axis_scale3[a]);
+    mesh->setBounds(min_z, max_z);
+    c->model->setGroupMesh(group, mesh);
+    c->built = false;
+    return 0;
+}
+
+int ref_set_control_point_stride(void* h, int stride) {
+    auto* c = static_cast<RefCtx*>(h);
+    return static_cast<int>(c->model->setControlPointStride(stride));
+}
+void ref_build_shared_sync(void* h) { static_cast<RefCtx*>(h)->model->buildSharedVertexSync(); }
+void ref_apply_model_bounds(void* h, double margin) {
+    static_cast<RefCtx*>(h)->model->applyModelBounds(margin);
+}
+
+int ref_dof_count(void* h) { return static_cast<int>(static_cast<RefCtx*>(h)->model->totalDofCount()); }
+
+int ref_vertex_count(void* h) {
+    auto* c = static_cast<RefCtx*>(h);
+    int n = 0;
+    for (int m = 0; m < c->model->groupMeshCount(); ++m)
+        if (c->model->groupMesh(m)) n += static_cast<int>(c->model->groupMesh(m)->vertexCount());
+    return n;
+}
+
+// Global DOF tables: for each global DOF, its (global vertex, axis, axis
+// scale) refs in (mesh, local DOF) order.  Returns the number of refs.
+int ref_dof_tables(void* h, int32_t* dof_off, int32_t* ref_vertex, uint8_t* ref_axis,
+                   double* ref_scale) {
+    auto* c = static_cast<RefCtx*>(h);
+    auto& M = *c->model;
+    int np = static_cast<int>(M.totalDofCount());
+    std::vector<std::vector<std::array<double, 3>>> refs(np);
+    int vbase = 0;
+    for (int m = 0; m < M.groupMeshCount(); ++m) {
+        const SurfaceMesh* mesh = M.groupMesh(m);
+        if (!mesh) continue;
+        const auto& maps = mesh->dofMappings();
+        for (int l = 0; l < static_cast<int>(maps.size()); ++l) {
+            int g = M.globalDofIndex(m, l);
+            if (g < 0) continue;
+            refs[g].push_back({double(vbase + maps[l].vertexIndex), double(maps[l].axis),
+                               mesh->axisScale(maps[l].axis)});
+        }
+        vbase += static_cast<int>(mesh->vertexCount());
+    }
+    int k = 0;
+    dof_off[0] = 0;
+    for (int g = 0; g < np; ++g) {
+        for (auto& r : refs[g]) {
+            ref_vertex[k] = static_cast<int32_t>(r[0]);
+            ref_axis[k] = static_cast<uint8_t>(r[1]);
+            ref_scale[k] = r[2];
+            ++k;
+        }
+        dof_off[g + 1] = k;
+    }
+    return k;
+}
+
+void ref_is_control_point(void* h, uint8_t* out) {
+    auto* c = static_cast<RefCtx*>(h);
+    int k = 0;
+    for (int m = 0; m < c->model->groupMeshCount(); ++m) {
+        const SurfaceMesh* mesh = c->model->groupMesh(m);
+        if (!mesh) continue;
+        for (uint32_t v = 0; v < mesh->vertexCount(); ++v) out[k++] = mesh->isControlPoint(v) ? 1 : 0;
+    }
+}
+
+void ref_assemble(void* h, double* params) { fromVec(static_cast<RefCtx*>(h)->model->assembleParameterVector(), params); }
+
+void ref_bounds(void* h, double* lo, double* hi) {
+    VectorXd l, u;
+    static_cast<RefCtx*>(h)->model->getBounds(l, u);
+    fromVec(l, lo);
+    fromVec(u, hi);
+}
+
+void ref_apply(void* h, const double* params) {
+    auto* c = static_cast<RefCtx*>(h);
+    c->model->applyParameterVector(toVec(static_cast<int>(c->model->totalDofCount()), params));
+}
+
+void ref_positions(void* h, double* out) {
+    auto* c = static_cast<RefCtx*>(h);
+    int k = 0;
+    for (int m = 0; m < c->model->groupMeshCount(); ++m) {
+        const SurfaceMesh* mesh = c->model->groupMesh(m);
+        if (!mesh) continue;
+        for (uint32_t v = 0; v < mesh->vertexCount(); ++v) {
+            const auto& p = mesh->vertex(v).position;
+            out[k++] = p.x(); out[k++] = p.y(); out[k++] = p.z();
+        }
+    }
+}
+
+void ref_set_gravity(void* h, int n, const double* xyz, const double* obs, const double* std) {
+    auto* c = static_cast<RefCtx*>(h);
+    c->grav.clear();
+    for (int i = 0; i < n; ++i)
+        c->grav.emplace_back(Vector3d(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]), obs ? obs[i] : 0.0,
+                             std ? std[i] : 0.0);
+    c->built = false;
+}
+
+void ref_set_magnetic(void* h, int n, const double* xyz, const double* obs, const double* std,
+                      double inc, double dec, double field, int rem_mode) {
+    auto* c = static_cast<RefCtx*>(h);
+    c->mag.clear();
+    for (int i = 0; i < n; ++i)
+        c->mag.emplace_back(Vector3d(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]), obs ? obs[i] : 0.0,
+                            std ? std[i] : 0.0);
+    c->inc = inc; c->dec = dec; c->field = field; c->remMode = rem_mode;
+    c->built = false;
+}
+
+void ref_set_objective(void* h, double alpha_mag, double ref_weight, const double* ref_params) {
+    auto* c = static_cast<RefCtx*>(h);
+    c->alphaMag = alpha_mag;
+    c->refWeight = ref_weight;
+    if (ref_params) c->refParams = toVec(static_cast<int>(c->model->totalDofCount()), ref_params);
+    c->built = false;
+}
+
+void ref_group_magnetization(void* h, int g, double* amp, double* dir3) {
+    auto* c = static_cast<RefCtx*>(h);
+    c->ensure();
+    Vector3d d;
+    c->mf->buildGroupMagnetization(g, *amp, d);
+    dir3[0] = d.x(); dir3[1] = d.y(); dir3[2] = d.z();
+}
+
+void ref_forward_gz(void* h, const double* params, double* out) {
+    auto* c = static_cast<RefCtx*>(h);
+    c->ensure();
+    fromVec(c->gf->compute(toVec(static_cast<int>(c->gf->parameterCount()), params)), out);
+}
+
+void ref_forward_tmi(void* h, const double* params, double* out) {
+    auto* c = static_cast<RefCtx*>(h);
+    c->ensure();
+    fromVec(c->mf->compute(toVec(static_cast<int>(c->mf->parameterCount()), params)), out);
+}
+
+void ref_jacobian_gz(void* h, const double* params, double* J) {
+    auto* c = static_cast<RefCtx*>(h);
+    c->ensure();
+    fromMat(c->gf->computeJacobian(toVec(static_cast<int>(c->gf->parameterCount()), params)), J);
+}
+
+void ref_jacobian_tmi(void* h, const double* params, double* J) {
+    auto* c = static_cast<RefCtx*>(h);
+    c->ensure();
+    fromMat(c->mf->computeJacobian(toVec(static_cast<int>(c->mf->parameterCount()), params)), J);
+}
+
+// JointObjective::evaluateComponents (joint_objective.cpp:113-173):
+// out5 = {gravityMisfit, magneticMisfit, regularization, constraint, total}.
+void ref_objective(void* h, const double* params, double* out5) {
+    auto* c = static_cast<RefCtx*>(h);
+    c->ensure();
+    auto r = c->jobj->evaluateComponents(toVec(static_cast<int>(c->jobj->parameterCount()), params));
+    out5[0] = r.gravityMisfit; out5[1] = r.magneticMisfit; out5[2] = r.regularization;
+    out5[3] = r.constraintPenalty; out5[4] = r.total;
+}
+
+// JointObjective::gradient (joint_objective.cpp:42-111).
+void ref_gradient(void* h, const double* params, double* grad) {
+    auto* c = static_cast<RefCtx*>(h);
+    c->ensure();
+    fromVec(c->jobj->gradient(toVec(static_cast<int>(c->jobj->parameterCount()), params)), grad);
+}
+
+// LBFGSBOptimizer::minimize (lbfgsb_optimizer.cpp:162-263) on the joint
+// objective, with the reference's defaults unless overridden.
+int ref_lbfgsb(void* h, const double* x0, const double* lo, const double* hi, int max_iter,
+               double ftol, int history, double* x_out, double* f_out) {
+    auto* c = static_cast<RefCtx*>(h);
+    c->ensure();
+    int np = static_cast<int>(c->jobj->parameterCount());
+    LBFGSBOptimizer opt;
+    opt.setMaxIterations(max_iter);
+    opt.setTolerance(ftol);
+    opt.setHistorySize(history);
+    auto f = [c](const VectorXd& x) { return c->jobj->evaluate(x); };
+    auto g = [c](const VectorXd& x) { return c->jobj->gradient(x); };
+    auto res = opt.minimize(f, g, toVec(np, x0), toVec(np, lo), toVec(np, hi));
+    fromVec(res.params, x_out);
+    *f_out = res.finalValue;
+    return res.iterations;
+}
+
+}  // extern "C"
