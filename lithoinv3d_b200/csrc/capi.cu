@@ -415,7 +415,8 @@ extern "C" lf_status lf_set_model_tables(lf_ctx* c, int G, const double* density
             return fail(c, LF_EINVAL, "bad DOF ref");
     int nInterp = interpOff ? interpOff[nv] : 0;
     if (interpOff) {
-        if (interpOff[0] != 0 || !interpSrc || !interpW) return fail(c, LF_EINVAL, "bad interpolation table");
+        if (interpOff[0] != 0 || (nInterp > 0 && (!interpSrc || !interpW)))
+            return fail(c, LF_EINVAL, "bad interpolation table");
         for (int v = 0; v < nv; ++v)
             if (interpOff[v + 1] < interpOff[v]) return fail(c, LF_EINVAL, "interp_off not monotone");
         for (int k = 0; k < nInterp; ++k)
@@ -423,7 +424,8 @@ extern "C" lf_status lf_set_model_tables(lf_ctx* c, int G, const double* density
                 return fail(c, LF_EINVAL, "interpolation source must be a control point");
     }
     if (nSync > 0) {
-        if (!syncOff || !syncVertex || syncOff[0] != 0) return fail(c, LF_EINVAL, "bad shared-vertex table");
+        if (!syncOff || syncOff[0] != 0 || (syncOff[nSync] > 0 && !syncVertex))
+            return fail(c, LF_EINVAL, "bad shared-vertex table");
         for (int s = 0; s < nSync; ++s)
             if (syncOff[s + 1] < syncOff[s]) return fail(c, LF_EINVAL, "sync_off not monotone");
         for (int k = 0; k < syncOff[nSync]; ++k)
@@ -875,7 +877,7 @@ extern "C" lf_status lf_jacobian(lf_ctx* c, const double* params, int which, dou
     int np = std::max(c->np, 1);
     // stations per batch so that the partial buffer stays below ~256 MB
     size_t per = (size_t)9 * c->T * sizeof(double);
-    int batch = static_cast<int>(std::max<size_t>(1, std::min<size_t>((size_t)s.n, ((size_t)256 << 20) / per)));
+    int batch = static_cast<int>(std::max<size_t>(1, std::min<size_t>({(size_t)s.n, ((size_t)256 << 20) / per, (size_t)65535})));
     LF_TRY_CUDA(c, c->d_partGrad.reserve((size_t)batch * 9 * c->T));
     LF_TRY_CUDA(c, c->d_jac.reserve((size_t)batch * np));
     for (int s0 = 0; s0 < s.n; s0 += batch) {

@@ -16,6 +16,7 @@
 #include <litho_invert/litho/lithology_model.h>
 #include <litho_invert/regularization/reference_model.h>
 #include <litho_invert/regularization/smoothness.h>
+#include <litho_invert/core/geometry.h>
 
 #include <array>
 #include <cstdint>
@@ -297,4 +298,27 @@ int ref_lbfgsb(void* h, const double* x0, const double* lo, const double* hi, in
     return res.iterations;
 }
 
+}  // extern "C"
+
+// Geometry primitives and static facet functions of the reference
+// (core/geometry.cpp:10-52, GravityForward::gravityFacet gravity_forward.cpp:153-158,
+// MagneticForward::magneticFacet magnetic_forward.cpp:312-347) for golden vectors.
+extern "C" {
+double ref_solid_angle(const double* a, const double* b, const double* c, const double* o) {
+    return solidAngle(Vector3d(a[0], a[1], a[2]), Vector3d(b[0], b[1], b[2]), Vector3d(c[0], c[1], c[2]),
+                      Vector3d(o[0], o[1], o[2]));
+}
+double ref_line_integral_term(const double* a, const double* b, const double* o) {
+    return lineIntegralTerm(Vector3d(a[0], a[1], a[2]), Vector3d(b[0], b[1], b[2]), Vector3d(o[0], o[1], o[2]));
+}
+double ref_gravity_facet(const double* o, const double* a, const double* b, const double* c) {
+    return GravityForward::gravityFacet(Vector3d(o[0], o[1], o[2]), Vector3d(a[0], a[1], a[2]),
+                                        Vector3d(b[0], b[1], b[2]), Vector3d(c[0], c[1], c[2]));
+}
+double ref_magnetic_facet(const double* o, const double* a, const double* b, const double* c, const double* m,
+                          const double* f) {
+    return MagneticForward::magneticFacet(Vector3d(o[0], o[1], o[2]), Vector3d(a[0], a[1], a[2]),
+                                          Vector3d(b[0], b[1], b[2]), Vector3d(c[0], c[1], c[2]),
+                                          Vector3d(m[0], m[1], m[2]), Vector3d(f[0], f[1], f[2]));
+}
 }  // extern "C"
