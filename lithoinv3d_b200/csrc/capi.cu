@@ -660,7 +660,7 @@ static lf_status forward_set(lf_ctx* c, const StationSet& s, double* d_gz, doubl
                                                           GZ ? c->d_partG.p : nullptr, TMI ? c->d_partM.p : nullptr,
                                                           GZ ? d_gz : nullptr, TMI ? d_tmi : nullptr);
     c->counters.launches += 2;
-    c->counters.forward_pairs += (uint64_t)S * (uint64_t)c->T * ((GZ && TMI) ? 2 : 1);
+    c->counters.forward_pairs += (uint64_t)S * (uint64_t)c->T;
     LF_CHECK_LAUNCH(c);
     return LF_OK;
 }

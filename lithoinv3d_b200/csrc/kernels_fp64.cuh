@@ -145,6 +145,22 @@ __global__ void k_sync_shared(int ns, const int32_t* __restrict__ sync_off, cons
 }
 
 // ------------------------------------------------------- facet constants --
+// Exact-order helpers: no FMA contraction, the reference's left-to-right
+// evaluation.  Facets collapsed by the control-point interpolation have a
+// twice-area of ~1e-12 (above the reference's 1e-15 cutoff), so their unit
+// normal is pure rounding; the TMI facet term does not vanish with the area,
+// so it is reproduced only when the normal is rounded exactly as on the CPU.
+__device__ __forceinline__ d3 sub_rn(d3 a, d3 b) { return {__dsub_rn(a.x, b.x), __dsub_rn(a.y, b.y), __dsub_rn(a.z, b.z)}; }
+__device__ __forceinline__ double dot_rn(d3 a, d3 b) {
+    return __dadd_rn(__dadd_rn(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y)), __dmul_rn(a.z, b.z));
+}
+__device__ __forceinline__ d3 cross_rn(d3 a, d3 b) {
+    return {__dsub_rn(__dmul_rn(a.y, b.z), __dmul_rn(a.z, b.y)), __dsub_rn(__dmul_rn(a.z, b.x), __dmul_rn(a.x, b.z)),
+            __dsub_rn(__dmul_rn(a.x, b.y), __dmul_rn(a.y, b.x))};
+}
+__device__ __forceinline__ double norm_rn(d3 a) { return __dsqrt_rn(dot_rn(a, a)); }
+__device__ __forceinline__ d3 div_rn(d3 a, double s) { return {__ddiv_rn(a.x, s), __ddiv_rn(a.y, s), __ddiv_rn(a.z, s)}; }
+
 __global__ void k_face_prep_fwd(int T, const int32_t* __restrict__ tri, const double* __restrict__ pos,
                                 const int16_t* __restrict__ face_group, const GroupConst* __restrict__ groups,
                                 d3 fdir, double* __restrict__ fc) {
@@ -154,10 +170,11 @@ __global__ void k_face_prep_fwd(int T, const int32_t* __restrict__ tri, const do
     const double* pb = pos + 3 * tri[3 * f + 1];
     const double* pc = pos + 3 * tri[3 * f + 2];
     d3 v[3] = {mk3(pa[0], pa[1], pa[2]), mk3(pb[0], pb[1], pb[2]), mk3(pc[0], pc[1], pc[2])};
-    d3 n = cross3(v[1] - v[0], v[2] - v[0]);
-    double area2 = norm3(n);
+    // faceNagyContribution / magneticFacet: n = (b-a) x (c-a), unit_n = n / |n|
+    d3 n = cross_rn(sub_rn(v[1], v[0]), sub_rn(v[2], v[0]));
+    double area2 = norm_rn(n);
     bool valid = !(area2 < kEps);
-    d3 un = valid ? mk3(n.x / area2, n.y / area2, n.z / area2) : mk3(0, 0, 0);
+    d3 un = valid ? div_rn(n, area2) : mk3(0, 0, 0);
     const GroupConst& g = groups[face_group[f]];
     d3 m = mk3(g.mdir[0], g.mdir[1], g.mdir[2]);
     double out[NFC];
@@ -165,16 +182,16 @@ __global__ void k_face_prep_fwd(int T, const int32_t* __restrict__ tri, const do
     out[FC_BX] = v[1].x; out[FC_BY] = v[1].y; out[FC_BZ] = v[1].z;
     out[FC_CX] = v[2].x; out[FC_CY] = v[2].y; out[FC_CZ] = v[2].z;
     out[FC_NX] = un.x; out[FC_NY] = un.y; out[FC_NZ] = un.z;
-    out[FC_MF] = dot3(m, un) * dot3(fdir, un);
+    out[FC_MF] = __dmul_rn(dot_rn(m, un), dot_rn(fdir, un));  // mn * fn
     for (int i = 0; i < 3; ++i) {
-        d3 e = v[(i + 1) % 3] - v[i];
-        double L = norm3(e);
-        d3 eh = (L < kEps) ? mk3(0, 0, 0) : mk3(e.x / L, e.y / L, e.z / L);
-        d3 perp = cross3(un, eh);
+        d3 e = sub_rn(v[(i + 1) % 3], v[i]);
+        double L = norm_rn(e);
+        d3 eh = (L < kEps) ? mk3(0, 0, 0) : div_rn(e, L);
+        d3 perp = cross_rn(un, eh);
         out[FC_E0X + 3 * i] = e.x; out[FC_E0Y + 3 * i] = e.y; out[FC_E0Z + 3 * i] = e.z;
         out[FC_L0 + i] = L;
         out[FC_P0X + 3 * i] = perp.x; out[FC_P0Y + 3 * i] = perp.y; out[FC_P0Z + 3 * i] = perp.z;
-        out[FC_MT0 + i] = dot3(m, perp) * dot3(fdir, perp);
+        out[FC_MT0 + i] = __dmul_rn(dot_rn(m, perp), dot_rn(fdir, perp));  // mt * ft
     }
     out[FC_VALID] = valid ? 1.0 : 0.0;
     for (int k = 0; k < NFC; ++k) fc[(size_t)k * T + f] = out[k];
@@ -193,7 +210,12 @@ __global__ void k_face_prep_grad(int T, const int32_t* __restrict__ tri, const d
     d3 n = cross3(b - a, c - a);
     double area2 = norm3(n);
     double L0 = norm3(b - a), L1 = norm3(c - b), L2 = norm3(a - c);
-    bool valid = !(area2 < kEps) && !(L0 < kEps) && !(L1 < kEps) && !(L2 < kEps);
+    // Facets collapsed onto a line (twice-area below 1e-10 of the longest edge
+    // squared, e.g. by control-point interpolation) carry a kink in their
+    // facet term: its central difference is zero and so is their derivative
+    // contribution here.
+    double Lmax = fmax(L0, fmax(L1, L2));
+    bool valid = !(area2 < kEps) && !(L0 < kEps) && !(L1 < kEps) && !(L2 < kEps) && !(area2 < 1e-10 * Lmax * Lmax);
     double out[NGC];
     for (int k = 0; k < NGC; ++k) out[k] = 0.0;
     if (valid) {
