@@ -26,7 +26,7 @@ struct PosKey {
 };
 }  // namespace
 
-// SurfaceMesh::isPaddingVertex, surface_mesh.cpp:680-689.
+// SurfaceMesh::isPaddingVertex, surface_mesh.cpp:676-685.
 bool Mesh::isPadding(uint32_t v) const {
     if (paddingRings <= 0) return false;
     int full = interiorGridDim + 2 * paddingRings;
@@ -168,7 +168,7 @@ uint32_t Mesh::setControlPointStrideGrid(int stride) {
     return static_cast<uint32_t>(cpIndices.size());
 }
 
-// LithologyModel::addGroup, lithology_model.cpp:16-28 (the reference also
+// LithologyModel::addGroup, lithology_model.cpp:17-28 (the reference also
 // rejects density <= 0 through LithoGroup::isValid; this host model accepts
 // any density contrast, which callers of the reference set after adding).
 int LithologyModelHost::addGroup(const Group& g) {
