@@ -67,24 +67,24 @@ typedef struct lf_model lf_model;
 lf_status lf_model_create(lf_model** out);
 void lf_model_destroy(lf_model* m);
 
-/* LithologyModel::addGroup (lithology_model.cpp:16-28) + LithoGroup fields
+/* LithologyModel::addGroup (lithology_model.cpp:17-28) + LithoGroup fields
  * (litho_group.h:13-34).  rem_vec may be NULL.  *out_index receives the group
  * index; duplicate ids are rejected with LF_EINVAL. */
 lf_status lf_model_add_group(lf_model* m, int id, double density_gcc, double susceptibility_si,
                              double rem_magnitude, double rem_inclination_deg,
                              double rem_declination_deg, const double* rem_vec3, int* out_index);
 
-/* LithologyModel::setGroupMesh (lithology_model.cpp:58-66) of a closed mesh:
+/* LithologyModel::setGroupMesh (lithology_model.cpp:62-69) of a closed mesh:
  * nv vertices (xyz[3*nv], freedom[nv] in LF_* numbering), nt triangles
  * (tri[3*nt], mesh-local, CCW seen from outside). */
 lf_status lf_model_set_group_mesh(lf_model* m, int group_index, int nv, const double* xyz,
                                   const uint8_t* freedom, int nt, const int32_t* tri);
 
-/* SurfaceMesh::setAxisScale / setBounds (surface_mesh.cpp:178-181, 249-252)
+/* SurfaceMesh::setAxisScale / setBounds (surface_mesh.cpp:180-182, 250-253)
  * for one group's mesh, or every mesh when group_index < 0. */
 lf_status lf_model_set_axis_scale(lf_model* m, int group_index, int axis, double scale);
 lf_status lf_model_set_depth_bounds(lf_model* m, int group_index, double min_z, double max_z);
-/* SurfaceMesh::setInteriorGrid (surface_mesh.cpp:675-678) */
+/* SurfaceMesh::setInteriorGrid (surface_mesh.cpp:671-674) */
 lf_status lf_model_set_interior_grid(lf_model* m, int group_index, int interior_dim, int padding_rings);
 
 /* LithologyModel::setControlPointStride (lithology_model.cpp:864-1040). */
