@@ -240,6 +240,30 @@ lf_status lf_set_profiling(lf_ctx* ctx, int enabled);
 lf_status lf_get_kernel_times(lf_ctx* ctx, double* forward_ms, int* forward_launches,
                               double* gradient_ms, int* gradient_launches);
 
+/* ------------------------------------------------------------------------ */
+/* Allocation-free forward.  No counterpart in the reference: for callers    */
+/* that cannot call cudaMalloc (a host framework owning all device memory   */
+/* through its own pool, a fixed memory budget, a real-time loop that must  */
+/* not allocate).                                                            */
+/* ------------------------------------------------------------------------ */
+/* gz (mGal) and TMI (nT) of one closed triangulated body (induced
+ * magnetisation, density contrast density_gcc, susceptibility_si, inducing
+ * field inc/dec/field_nt) at ns stations -- the single-group case of
+ * lf_forward.  Every array is caller-owned DEVICE memory: d_xyz[3*nv],
+ * d_tri[3*nt], d_sta[3*ns], d_gz[ns], d_tmi[ns] (either output may be NULL).
+ * Allocates nothing: its scratch is one 8 MiB __device__ array inside the
+ * library, so 38*nt + 2*ns must not exceed 1,048,544 (e.g. nt <= 16384 facets
+ * with ns <= 212,000 stations); larger sizes return LF_EINVAL.  The first
+ * call on a device looks the scratch address up (cudaGetSymbolAddress): make
+ * it before any stream capture.  Calls share the scratch, so calls that
+ * overlap on the GPU race: serialise them.  Triangle indices outside [0, nv)
+ * return LF_EINVAL.  Runs on `stream` (a cudaStream_t, NULL = default stream)
+ * and returns after the stream has finished the call. */
+lf_status lf_forward_noalloc(int nv, const double* d_xyz, int nt, const int32_t* d_tri, int ns,
+                             const double* d_sta, double density_gcc, double susceptibility_si,
+                             double inc_deg, double dec_deg, double field_nt, double* d_gz,
+                             double* d_tmi, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

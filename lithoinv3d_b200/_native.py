@@ -76,6 +76,8 @@ SIGNATURES = {
     "lf_get_counters": (C.c_int, [_vp, C.POINTER(Counters)]),
     "lf_reset_counters": (C.c_int, [_vp]),
     "lf_set_profiling": (C.c_int, [_vp, C.c_int]),
+    "lf_forward_noalloc": (C.c_int, [C.c_int, _vp, C.c_int, _vp, C.c_int, _vp, C.c_double, C.c_double, C.c_double,
+                                     C.c_double, C.c_double, _vp, _vp, _vp]),
     "lf_get_kernel_times": (C.c_int, [_vp, _dp, C.POINTER(C.c_int), _dp, C.POINTER(C.c_int)]),
 }
 
