@@ -325,6 +325,7 @@ def main():
     fwd_ms, fwd_n, grad_ms, grad_n = ctx.kernel_times()
     ctx.set_profiling(False)
     cnt = ctx.counters()
+    near_frac = ctx.near_pairs() / max(cnt.forward_pairs, 1) if args.precision == "mixed" else 1.0
     launches = int(cnt.launches)
     pairs_fwd = int(cnt.forward_pairs)
     pairs_grad = int(cnt.gradient_pairs)
@@ -386,7 +387,7 @@ def main():
             "data": "synthetic (seeded voxel model and observations)",
             "config": {"workload": WORKLOAD, "triangles": p.n_triangles(), "stations": len(p.grav_xyz),
                        "dofs": np_, "parallelism": f"replicas x{world}", "l2": "flushed between steps (256 MiB write)",
-                       "precision": args.precision},
+                       "precision": args.precision, "fp64_near_pair_fraction": round(near_frac, 4)},
             "e2e": {"value": e2e_value, "unit": "evals/s", "h2d_bytes_per_step": 8 * np_,
                     "d2h_bytes_per_step": 8 * (np_ + 1)},
             "gpu_launches": launches, "roofline": roofline}

@@ -169,6 +169,14 @@ lf_status lf_set_objective(lf_ctx* ctx, double alpha_mag, double ref_weight,
 
 lf_status lf_set_precision(lf_ctx* ctx, int mode);
 
+/* Mixed path: a facet whose centroid lies at least tau x its longest edge
+ * from a station tile's bounding box is evaluated in FP32 (quadrature for gz,
+ * analytic TMI); nearer facets in FP64.  Default 3.  tau <= 0: every facet in
+ * FP64 (local frame). */
+lf_status lf_set_far_field_ratio(lf_ctx* ctx, double tau);
+/* Station-facet pairs the mixed forward evaluated in FP64 since lf_set_model. */
+lf_status lf_get_near_pairs(lf_ctx* ctx, unsigned long long* n);
+
 /* Forward at params (host arrays): gz[n_grav] mGal, tmi[n_mag] nT; either
  * output may be NULL. */
 lf_status lf_forward(lf_ctx* ctx, const double* params, double* gz, double* tmi);

@@ -64,6 +64,8 @@ SIGNATURES = {
     "lf_set_magnetic_data": (C.c_int, [_vp, C.c_int, _dp, _dp, _dp]),
     "lf_set_objective": (C.c_int, [_vp, C.c_double, C.c_double, _dp]),
     "lf_set_precision": (C.c_int, [_vp, C.c_int]),
+    "lf_set_far_field_ratio": (C.c_int, [_vp, C.c_double]),
+    "lf_get_near_pairs": (C.c_int, [_vp, C.POINTER(C.c_ulonglong)]),
     "lf_forward": (C.c_int, [_vp, _dp, _dp, _dp]),
     "lf_objective": (C.c_int, [_vp, _dp, _dp]),
     "lf_objective_grad": (C.c_int, [_vp, _dp, _dp, _dp]),

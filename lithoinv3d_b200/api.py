@@ -223,6 +223,14 @@ class Context:
     def set_precision(self, mode: int):
         self._check(self.lib.lf_set_precision(self.h, mode), "set_precision")
 
+    def set_far_field_ratio(self, tau: float):
+        self._check(self.lib.lf_set_far_field_ratio(self.h, tau), "set_far_field_ratio")
+
+    def near_pairs(self) -> int:
+        n = C.c_ulonglong(0)
+        self._check(self.lib.lf_get_near_pairs(self.h, C.byref(n)), "near_pairs")
+        return n.value
+
     def forward(self, params):
         p = f64(params)
         gz = np.zeros(self.n_grav)

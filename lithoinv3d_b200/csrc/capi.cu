@@ -1,7 +1,7 @@
 // C ABI implementation: contexts, device buffers and the launch sequence of
 // one forward / objective / objective+gradient evaluation.
 #include "../../include/litho_gpu.h"
-#include "kernels_fp64.cuh"
+#include "kernels_mixed.cuh"
 #include "lbfgsb.hpp"
 #include "model_builder.hpp"
 
@@ -51,10 +51,15 @@ struct GroupProps {
     double density, chi, remMag, remInc, remDec, remVec[3];
 };
 
+// A station set lives on the device in Morton order of (x, y), so that a
+// tile of consecutive stations is spatially compact (the mixed-precision
+// near/far test is per tile).  perm[i] = caller index of device slot i.
 struct StationSet {
     int n = 0;
-    std::vector<double> xyz, obs, w;
-    DevBuf<double> d_xyz, d_obs, d_w, d_pred, d_coef;
+    std::vector<double> xyz, obs, w;  // caller order
+    std::vector<int32_t> perm;
+    DevBuf<double> d_xyz, d_obs, d_w, d_pred, d_coef, d_out;
+    DevBuf<int32_t> d_perm;
 };
 
 constexpr double kGSI = 6.67430e-11, kDensityScale = 1000.0, kMs2ToMgal = 1e5;
@@ -77,7 +82,9 @@ struct lf_ctx {
     d3 fdir{0, 0, -1};
     std::vector<GroupConst> gconst;
 
-    DevBuf<double> d_pos, d_fc, d_gc, d_params, d_grad, d_vgrad, d_out5, d_f, d_refp;
+    DevBuf<double> d_pos, d_fc, d_gc, d_mc, d_params, d_grad, d_vgrad, d_out5, d_f, d_refp;
+    DevBuf<unsigned long long> d_nearPairs;
+    float tau = 3.0f;  // far-field ratio of the mixed path
     DevBuf<int32_t> d_tri, d_dofOff, d_refVertex, d_interpOff, d_interpSrc, d_interpRows, d_syncOff,
         d_syncVertex, d_vfOff, d_vf, d_gradVerts, d_chunkBegin, d_chunkEnd, d_chunkGroup;
     DevBuf<uint8_t> d_refAxis, d_faceNeeds;
@@ -141,6 +148,12 @@ static void prof_end(lf_ctx* c, std::vector<std::pair<cudaEvent_t, cudaEvent_t>>
     } while (0)
 
 #define LF_CHECK_LAUNCH(ctx) LF_TRY_CUDA(ctx, cudaGetLastError())
+
+#define LF_RET_IF(x)                      \
+    do {                                  \
+        lf_status s__ = (x);              \
+        if (s__ != LF_OK) return s__;     \
+    } while (0)
 
 static lf_status fail(lf_ctx* ctx, lf_status st, const std::string& msg) {
     if (ctx) ctx->err = msg;
@@ -496,6 +509,9 @@ extern "C" lf_status lf_set_model_tables(lf_ctx* c, int G, const double* density
     LF_TRY_CUDA(c, upload(c->d_gradVerts, gverts.data(), gverts.size(), c->stream));
     LF_TRY_CUDA(c, upload(c->d_faceNeeds, fneed.data(), fneed.size(), c->stream));
     LF_TRY_CUDA(c, c->d_fc.reserve((size_t)NFC * nt));
+    LF_TRY_CUDA(c, c->d_mc.reserve((size_t)NMC * nt));
+    LF_TRY_CUDA(c, c->d_nearPairs.reserve(1));
+    LF_TRY_CUDA(c, cudaMemsetAsync(c->d_nearPairs.p, 0, sizeof(unsigned long long), c->stream));
     LF_TRY_CUDA(c, c->d_gc.reserve((size_t)NGC * nt));
     LF_TRY_CUDA(c, c->d_params.reserve(std::max(np, 1)));
     LF_TRY_CUDA(c, c->d_grad.reserve(std::max(np, 1)));
@@ -550,12 +566,45 @@ static lf_status set_stations(lf_ctx* c, StationSet& s, int n, const double* xyz
         if (obs) s.obs[i] = obs[i];
         if (sd && sd[i] > 0) s.w[i] = 1.0 / sd[i];  // objective.cpp:26
     }
-    LF_TRY_CUDA(c, upload(s.d_xyz, s.xyz.data(), s.xyz.size(), c->stream));
-    LF_TRY_CUDA(c, upload(s.d_obs, s.obs.data(), s.obs.size(), c->stream));
-    LF_TRY_CUDA(c, upload(s.d_w, s.w.data(), s.w.size(), c->stream));
+    // Morton order of (x, y) quantised to 16 bits over the set's extent
+    s.perm.resize(n);
+    {
+        double lo[2] = {1e300, 1e300}, hi[2] = {-1e300, -1e300};
+        for (int i = 0; i < n; ++i)
+            for (int k = 0; k < 2; ++k) {
+                lo[k] = std::min(lo[k], s.xyz[3 * i + k]);
+                hi[k] = std::max(hi[k], s.xyz[3 * i + k]);
+            }
+        std::vector<std::pair<uint32_t, int32_t>> key(n);
+        for (int i = 0; i < n; ++i) {
+            uint32_t q[2];
+            for (int k = 0; k < 2; ++k) {
+                double span = hi[k] - lo[k];
+                q[k] = span > 0 ? static_cast<uint32_t>((s.xyz[3 * i + k] - lo[k]) / span * 65535.0) : 0u;
+            }
+            uint32_t m = 0;
+            for (int b = 0; b < 16; ++b) m |= ((q[0] >> b) & 1u) << (2 * b) | ((q[1] >> b) & 1u) << (2 * b + 1);
+            key[i] = {m, i};
+        }
+        std::stable_sort(key.begin(), key.end());
+        for (int i = 0; i < n; ++i) s.perm[i] = key[i].second;
+    }
+    std::vector<double> px(3 * (size_t)n), po(n), pw(n);
+    for (int i = 0; i < n; ++i) {
+        int j = s.perm[i];
+        px[3 * i] = s.xyz[3 * j]; px[3 * i + 1] = s.xyz[3 * j + 1]; px[3 * i + 2] = s.xyz[3 * j + 2];
+        po[i] = s.obs[j];
+        pw[i] = s.w[j];
+    }
+    LF_TRY_CUDA(c, upload(s.d_xyz, px.data(), px.size(), c->stream));
+    LF_TRY_CUDA(c, upload(s.d_obs, po.data(), po.size(), c->stream));
+    LF_TRY_CUDA(c, upload(s.d_w, pw.data(), pw.size(), c->stream));
+    LF_TRY_CUDA(c, upload(s.d_perm, s.perm.data(), s.perm.size(), c->stream));
     LF_TRY_CUDA(c, s.d_pred.reserve(std::max(n, 1)));
     LF_TRY_CUDA(c, s.d_coef.reserve(std::max(n, 1)));
-    c->sameStations = c->grav.n > 0 && c->grav.n == c->mag.n && c->grav.xyz == c->mag.xyz;
+    LF_TRY_CUDA(c, s.d_out.reserve(std::max(n, 1)));
+    c->sameStations = c->grav.n > 0 && c->grav.n == c->mag.n && c->grav.xyz == c->mag.xyz &&
+                      c->grav.perm == c->mag.perm;
     c->chunkCapacityS = 0;
     LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
     return LF_OK;
@@ -579,6 +628,21 @@ extern "C" lf_status lf_set_objective(lf_ctx* c, double alpha, double refWeight,
         LF_TRY_CUDA(c, upload(c->d_refp, refParams, (size_t)c->np, c->stream));
         LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
     }
+    return LF_OK;
+}
+
+extern "C" lf_status lf_set_far_field_ratio(lf_ctx* c, double tau) {
+    if (!c || !std::isfinite(tau)) return LF_EINVAL;
+    c->tau = tau <= 0.0 ? 3.0e38f : static_cast<float>(tau);
+    return LF_OK;
+}
+
+extern "C" lf_status lf_get_near_pairs(lf_ctx* c, unsigned long long* n) {
+    if (!c || !n) return LF_EINVAL;
+    if (!c->hasModel) return fail(c, LF_ESTATE, "no model set");
+    cudaSetDevice(c->device);
+    LF_TRY_CUDA(c, cudaMemcpyAsync(n, c->d_nearPairs.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+    LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
     return LF_OK;
 }
 
@@ -665,8 +729,43 @@ static lf_status forward_set(lf_ctx* c, const StationSet& s, double* d_gz, doubl
     return LF_OK;
 }
 
+template <bool GZ, bool TMI>
+static lf_status forward_set_mixed(lf_ctx* c, const StationSet& s, double* d_gz, double* d_tmi) {
+    int S = s.n;
+    if (S == 0) return LF_OK;
+    plan_chunks(c, S);
+    lf_status st = upload_chunks(c);
+    if (st != LF_OK) return st;
+    int nch = static_cast<int>(c->chunkBegin.size());
+    if (GZ) LF_TRY_CUDA(c, c->d_partG.reserve((size_t)nch * S));
+    if (TMI) LF_TRY_CUDA(c, c->d_partM.reserve((size_t)nch * S));
+    dim3 grid(cdiv(S, kFwdThreads), nch);
+    int slot = prof_begin(c, c->evFwd, c->nFwd);
+    k_forward_mixed<GZ, TMI, kFwdFacetTile><<<grid, kFwdThreads, 0, c->stream>>>(
+        S, s.d_xyz.p, c->T, c->d_mc.p, c->d_chunkBegin.p, c->d_chunkEnd.p, c->tau, GZ ? c->d_partG.p : nullptr,
+        TMI ? c->d_partM.p : nullptr, c->d_nearPairs.p);
+    prof_end(c, c->evFwd, slot);
+    k_forward_reduce_mixed<<<cdiv(S, 256), 256, 0, c->stream>>>(S, nch, GZ ? c->d_partG.p : nullptr,
+                                                                TMI ? c->d_partM.p : nullptr, GZ ? d_gz : nullptr,
+                                                                TMI ? d_tmi : nullptr);
+    c->counters.launches += 2;
+    c->counters.forward_pairs += (uint64_t)S * (uint64_t)c->T;
+    LF_CHECK_LAUNCH(c);
+    return LF_OK;
+}
+
 // Positions must be current.  Writes grav.d_pred / mag.d_pred.
 static lf_status forward_all(lf_ctx* c) {
+    if (c->precision == LF_PREC_MIXED) {
+        k_face_prep_mixed<<<cdiv(c->T, 128), 128, 0, c->stream>>>(c->T, c->d_tri.p, c->d_pos.p, c->d_faceGroup.p,
+                                                                  c->d_groups.p, c->fdir, c->d_mc.p);
+        c->counters.launches++;
+        LF_CHECK_LAUNCH(c);
+        if (c->sameStations) return forward_set_mixed<true, true>(c, c->grav, c->grav.d_pred.p, c->mag.d_pred.p);
+        lf_status st = forward_set_mixed<true, false>(c, c->grav, c->grav.d_pred.p, nullptr);
+        if (st != LF_OK) return st;
+        return forward_set_mixed<false, true>(c, c->mag, nullptr, c->mag.d_pred.p);
+    }
     k_face_prep_fwd<<<cdiv(c->T, 128), 128, 0, c->stream>>>(c->T, c->d_tri.p, c->d_pos.p, c->d_faceGroup.p,
                                                             c->d_groups.p, c->fdir, c->d_fc.p);
     c->counters.launches++;
@@ -775,6 +874,21 @@ static lf_status gradient_all(lf_ctx* c, const double* d_params, double* d_grad)
     return LF_OK;
 }
 
+__global__ void k_unpermute(int n, const int32_t* __restrict__ perm, const double* __restrict__ src,
+                            double* __restrict__ dst) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[perm[i]] = src[i];
+}
+
+// Device predictions (Morton slot order) -> caller order.
+static lf_status unpermute_device(lf_ctx* c, const StationSet& s, const double* src, double* dst) {
+    if (s.n == 0) return LF_OK;
+    k_unpermute<<<cdiv(s.n, 256), 256, 0, c->stream>>>(s.n, s.d_perm.p, src, dst);
+    c->counters.launches++;
+    LF_CHECK_LAUNCH(c);
+    return LF_OK;
+}
+
 static lf_status check_ready(lf_ctx* c) {
     if (!c) return LF_EINVAL;
     if (!c->hasModel) return fail(c, LF_ESTATE, "no model set");
@@ -791,21 +905,14 @@ static lf_status params_to_device(lf_ctx* c, const double* params) {
     return LF_OK;
 }
 
-#define LF_RET_IF(x)                      \
-    do {                                  \
-        lf_status s__ = (x);              \
-        if (s__ != LF_OK) return s__;     \
-    } while (0)
 
 // ------------------------------------------------------------ public API --
 extern "C" lf_status lf_forward_device(lf_ctx* c, const double* d_params, double* d_gz, double* d_tmi) {
     LF_RET_IF(check_ready(c));
     LF_RET_IF(scatter(c, d_params));
     LF_RET_IF(forward_all(c));
-    if (d_gz && c->grav.n)
-        LF_TRY_CUDA(c, cudaMemcpyAsync(d_gz, c->grav.d_pred.p, sizeof(double) * c->grav.n, cudaMemcpyDeviceToDevice, c->stream));
-    if (d_tmi && c->mag.n)
-        LF_TRY_CUDA(c, cudaMemcpyAsync(d_tmi, c->mag.d_pred.p, sizeof(double) * c->mag.n, cudaMemcpyDeviceToDevice, c->stream));
+    if (d_gz && c->grav.n) LF_RET_IF(unpermute_device(c, c->grav, c->grav.d_pred.p, d_gz));
+    if (d_tmi && c->mag.n) LF_RET_IF(unpermute_device(c, c->mag, c->mag.d_pred.p, d_tmi));
     return LF_OK;
 }
 
@@ -814,10 +921,14 @@ extern "C" lf_status lf_forward(lf_ctx* c, const double* params, double* gz, dou
     LF_RET_IF(params_to_device(c, params));
     LF_RET_IF(scatter(c, c->d_params.p));
     LF_RET_IF(forward_all(c));
-    if (gz && c->grav.n)
-        LF_TRY_CUDA(c, cudaMemcpyAsync(gz, c->grav.d_pred.p, sizeof(double) * c->grav.n, cudaMemcpyDeviceToHost, c->stream));
-    if (tmi && c->mag.n)
-        LF_TRY_CUDA(c, cudaMemcpyAsync(tmi, c->mag.d_pred.p, sizeof(double) * c->mag.n, cudaMemcpyDeviceToHost, c->stream));
+    if (gz && c->grav.n) {
+        LF_RET_IF(unpermute_device(c, c->grav, c->grav.d_pred.p, c->grav.d_out.p));
+        LF_TRY_CUDA(c, cudaMemcpyAsync(gz, c->grav.d_out.p, sizeof(double) * c->grav.n, cudaMemcpyDeviceToHost, c->stream));
+    }
+    if (tmi && c->mag.n) {
+        LF_RET_IF(unpermute_device(c, c->mag, c->mag.d_pred.p, c->mag.d_out.p));
+        LF_TRY_CUDA(c, cudaMemcpyAsync(tmi, c->mag.d_out.p, sizeof(double) * c->mag.n, cudaMemcpyDeviceToHost, c->stream));
+    }
     LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
     return LF_OK;
 }
@@ -880,6 +991,7 @@ extern "C" lf_status lf_jacobian(lf_ctx* c, const double* params, int which, dou
     int batch = static_cast<int>(std::max<size_t>(1, std::min<size_t>({(size_t)s.n, ((size_t)256 << 20) / per, (size_t)65535})));
     LF_TRY_CUDA(c, c->d_partGrad.reserve((size_t)batch * 9 * c->T));
     LF_TRY_CUDA(c, c->d_jac.reserve((size_t)batch * np));
+    std::vector<double> rows;
     for (int s0 = 0; s0 < s.n; s0 += batch) {
         int nb = std::min(batch, s.n - s0);
         dim3 grid(cdiv(c->T, kGradThreads), nb);
@@ -893,8 +1005,13 @@ extern "C" lf_status lf_jacobian(lf_ctx* c, const double* params, int which, dou
             k_jacobian_gather<<<g2, 128, 0, c->stream>>>(nb, c->np, c->d_dofOff.p, c->d_refVertex.p, c->d_refAxis.p,
                                                          c->d_refScale.p, c->d_vfOff.p, c->d_vf.p, c->T,
                                                          c->d_partGrad.p, c->d_jac.p, c->np);
-            LF_TRY_CUDA(c, cudaMemcpyAsync(J + (size_t)s0 * c->np, c->d_jac.p, sizeof(double) * (size_t)nb * c->np,
+            rows.resize((size_t)nb * c->np);
+            LF_TRY_CUDA(c, cudaMemcpyAsync(rows.data(), c->d_jac.p, sizeof(double) * (size_t)nb * c->np,
                                            cudaMemcpyDeviceToHost, c->stream));
+            LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
+            for (int r = 0; r < nb; ++r)
+                std::copy(rows.begin() + (size_t)r * c->np, rows.begin() + (size_t)(r + 1) * c->np,
+                          J + (size_t)s.perm[s0 + r] * c->np);
         }
         LF_CHECK_LAUNCH(c);
     }
