@@ -807,16 +807,30 @@ static lf_status objective_final(lf_ctx* c, const double* d_params, double* d_f)
 
 // Gradient kernels over one station set with the given adjoints; writes
 // chunks [chunk0, chunk0 + nchunks) of d_partGrad.
+// FP64 mode: one FP64 kernel over every (facet, station) pair.  Mixed mode:
+// the FP64 kernel takes the near tiles and writes chunks [chunk0, +nchunks);
+// the FP32 far-field kernel takes the rest and writes chunks shifted by
+// farOffset.
 static lf_status gradient_set(lf_ctx* c, const StationSet& s, const double* gcoef, const double* mcoef,
-                              int stationsPerChunk, int chunk0, int nchunks) {
+                              int stationsPerChunk, int chunk0, int nchunks, int farOffset) {
     if (s.n == 0 || nchunks == 0) return LF_OK;
     dim3 grid(cdiv(c->T, kGradThreads), nchunks);
+    bool mixed = c->precision == LF_PREC_MIXED;
+    double tau = mixed ? static_cast<double>(c->tau) : 3.0e38;
     int slot = prof_begin(c, c->evGrad, c->nGrad);
     k_gradient_fp64<kGradStationTile><<<grid, kGradThreads, 0, c->stream>>>(
         c->T, c->d_gc.p, s.n, s.d_xyz.p, gcoef, mcoef, stationsPerChunk, c->d_faceGroup.p, c->d_groups.p, c->fdir,
-        c->d_partGrad.p + (size_t)chunk0 * 9 * c->T);
+        tau, c->d_partGrad.p + (size_t)chunk0 * 9 * c->T);
     prof_end(c, c->evGrad, slot);
     c->counters.launches++;
+    if (mixed) {
+        int slot2 = prof_begin(c, c->evGrad, c->nGrad);
+        k_gradient_far32<kGradStationTile><<<grid, kGradThreads, 0, c->stream>>>(
+            c->T, c->d_gc.p, s.n, s.d_xyz.p, gcoef, mcoef, stationsPerChunk, c->d_faceGroup.p, c->d_groups.p,
+            c->fdir, tau, c->d_partGrad.p + (size_t)(chunk0 + farOffset) * 9 * c->T);
+        prof_end(c, c->evGrad, slot2);
+        c->counters.launches++;
+    }
     c->counters.gradient_pairs += (uint64_t)s.n * (uint64_t)c->T;
     LF_CHECK_LAUNCH(c);
     return LF_OK;
@@ -845,22 +859,24 @@ static lf_status gradient_all(lf_ctx* c, const double* d_params, double* d_grad)
         if (mOn) { chunksM = grad_chunks_for(c, c->mag.n); spcM = cdiv(c->mag.n, chunksM); chunksM = cdiv(c->mag.n, spcM); }
     }
     int total = chunksG + chunksM;
+    int mult = c->precision == LF_PREC_MIXED ? 2 : 1;
     if (total == 0) {
         LF_TRY_CUDA(c, cudaMemsetAsync(c->d_vgrad.p, 0, sizeof(double) * 3 * c->V, c->stream));
     } else {
-        LF_TRY_CUDA(c, c->d_partGrad.reserve((size_t)total * 9 * c->T));
+        LF_TRY_CUDA(c, c->d_partGrad.reserve((size_t)total * mult * 9 * c->T));
         lf_status st;
         if (c->sameStations && gOn) {
-            st = gradient_set(c, c->grav, c->grav.d_coef.p, mOn ? c->mag.d_coef.p : nullptr, spcG, 0, chunksG);
+            st = gradient_set(c, c->grav, c->grav.d_coef.p, mOn ? c->mag.d_coef.p : nullptr, spcG, 0, chunksG, total);
         } else {
-            st = gradient_set(c, c->grav, c->grav.d_coef.p, nullptr, spcG, 0, chunksG);
-            if (st == LF_OK) st = gradient_set(c, c->mag, nullptr, c->mag.d_coef.p, spcM, chunksG, chunksM);
+            st = gradient_set(c, c->grav, c->grav.d_coef.p, nullptr, spcG, 0, chunksG, total);
+            if (st == LF_OK) st = gradient_set(c, c->mag, nullptr, c->mag.d_coef.p, spcM, chunksG, chunksM, total);
         }
         if (st != LF_OK) return st;
         if (c->nGradVerts > 0) {
             k_vertex_reduce<<<cdiv(c->nGradVerts, 128), 128, 0, c->stream>>>(c->nGradVerts, c->d_gradVerts.p,
-                                                                              c->d_vfOff.p, c->d_vf.p, c->T, total,
-                                                                              c->d_partGrad.p, c->d_vgrad.p);
+                                                                              c->d_vfOff.p, c->d_vf.p, c->T,
+                                                                              total * mult, c->d_partGrad.p,
+                                                                              c->d_vgrad.p);
             c->counters.launches++;
         }
     }
@@ -999,7 +1015,7 @@ extern "C" lf_status lf_jacobian(lf_ctx* c, const double* params, int which, dou
         const double* m1 = which == LF_MAGNETIC ? c->d_ones.p : nullptr;
         k_gradient_fp64<kGradStationTile><<<grid, kGradThreads, 0, c->stream>>>(
             c->T, c->d_gc.p, nb, s.d_xyz.p + 3 * (size_t)s0, g1, m1, 1, c->d_faceGroup.p, c->d_groups.p, c->fdir,
-            c->d_partGrad.p);
+            3.0e38, c->d_partGrad.p);
         if (c->np > 0) {
             dim3 g2(cdiv(c->np, 128), nb);
             k_jacobian_gather<<<g2, 128, 0, c->stream>>>(nb, c->np, c->d_dofOff.p, c->d_refVertex.p, c->d_refAxis.p,

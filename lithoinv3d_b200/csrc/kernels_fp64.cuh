@@ -408,16 +408,128 @@ __device__ __forceinline__ void edge_terms(d3 r1, d3 r2, double d1, double d2, d
     *g2 = *g2 + mk3((P.x + kl * ex) * inv2, (P.y + kl * ey) * inv2, P.z * inv2);
 }
 
+// Per-facet finalisation in the local frame: differentiates the facet
+// constants (n_z, the unit normal, the in-plane edge normals, the magnetic
+// direction products, the edge directions) once, from the station sums, and
+// returns d(contracted facet terms)/d(a, b, c) in the global frame.
+__device__ inline void grad_finalize(const double* C, const GradAcc& A, const GroupConst& g, d3 fdir, double outv[9]) {
+    const double L0 = C[GC_L0], cx = C[GC_CX], cy = C[GC_CY];
+    const double area2 = L0 * cy;
+    d3 xh = mk3(C[GC_XX], C[GC_XY], C[GC_XZ]), yh = mk3(C[GC_YX], C[GC_YY], C[GC_YZ]),
+       zh = mk3(C[GC_ZX], C[GC_ZY], C[GC_ZZ]);
+    d3 mg = mk3(g.mdir[0], g.mdir[1], g.mdir[2]);
+    d3 ml = mk3(dot3(mg, xh), dot3(mg, yh), dot3(mg, zh));
+    d3 fl = mk3(dot3(fdir, xh), dot3(fdir, yh), dot3(fdir, zh));
+    d3 nh = mk3(0, 0, 1);
+    d3 eh[3] = {mk3(1, 0, 0), mk3(C[GC_E1X], C[GC_E1Y], 0), mk3(C[GC_E2X], C[GC_E2Y], 0)};
+    double Ls[3] = {L0, C[GC_L1], C[GC_L2]};
+    d3 vbar[3] = {A.va, A.vb, A.vc};
+    // n_hat adjoint
+    d3 nbar = A.bh * -1.0;
+    {
+        double mn = ml.z, fn = fl.z;
+        nbar = nbar + (ml * fn + fl * mn) * A.amf;
+        // n_z = n_hat . e_z(global); e_z in local coordinates
+        nbar = nbar + mk3(xh.z, yh.z, zh.z) * A.ai;
+    }
+    // vertex-direct: h on a, d_perp on p1
+    vbar[0] = vbar[0] + nh * (-A.aom);
+    for (int i = 0; i < 3; ++i) {
+        d3 perp = cross3(nh, eh[i]);
+        vbar[i] = vbar[i] + perp * (-A.alam[i]);
+        double mp = dot3(ml, perp), fp = dot3(fl, perp);
+        d3 pbar = A.bl[i] * -1.0 + (ml * fp + fl * mp) * A.amt[i];
+        // perp = n x e: n_bar += e x pbar, e_bar = pbar x n
+        nbar = nbar + cross3(eh[i], pbar);
+        d3 ebar = cross3(pbar, nh);
+        double pe = dot3(ebar, eh[i]);
+        d3 eraw = (ebar - eh[i] * pe) * (1.0 / Ls[i]);
+        vbar[(i + 1) % 3] = vbar[(i + 1) % 3] + eraw;
+        vbar[i] = vbar[i] - eraw;
+    }
+    // n_hat = n / |n|, n = (b-a) x (c-a)
+    double pn = dot3(nbar, nh);
+    d3 nraw = (nbar - nh * pn) * (1.0 / area2);
+    d3 u = mk3(L0, 0, 0), w = mk3(cx, cy, 0);
+    d3 ubar = cross3(w, nraw), wbar = cross3(nraw, u);
+    vbar[1] = vbar[1] + ubar;
+    vbar[2] = vbar[2] + wbar;
+    vbar[0] = vbar[0] - ubar - wbar;
+    for (int v = 0; v < 3; ++v) {
+        d3 gv = xh * vbar[v].x + yh * vbar[v].y + zh * vbar[v].z;
+        outv[3 * v] = gv.x; outv[3 * v + 1] = gv.y; outv[3 * v + 2] = gv.z;
+    }
+}
+
+__device__ __forceinline__ void grad_acc_zero(GradAcc& A) {
+    A.va = A.vb = A.vc = mk3(0, 0, 0);
+    A.bh = mk3(0, 0, 0);
+    for (int i = 0; i < 3; ++i) { A.alam[i] = 0; A.bl[i] = mk3(0, 0, 0); A.amt[i] = 0; }
+    A.aom = A.ai = A.amf = 0.0;
+}
+
+// Warp-uniform far test of a facet against a station tile's bounding box
+// (centroid at least tau x longest edge away).  Facets that take no part
+// count as far, so a warp of inactive facets never blocks the decision.
+__device__ __forceinline__ bool facet_far(const double* C, bool active, const double* bbox, double tau) {
+    if (!active) return true;
+    if (tau >= 1e30) return false;
+    double L0 = C[GC_L0], cx = C[GC_CX], cy = C[GC_CY];
+    double px = (L0 + cx) / 3.0, py = cy / 3.0;
+    double c[3] = {C[GC_AX] + px * C[GC_XX] + py * C[GC_YX], C[GC_AY] + px * C[GC_XY] + py * C[GC_YY],
+                   C[GC_AZ] + px * C[GC_XZ] + py * C[GC_YZ]};
+    double size = fmax(L0, fmax(C[GC_L1], C[GC_L2]));
+    double d2 = 0.0;
+    for (int k = 0; k < 3; ++k) {
+        double dk = fmax(0.0, fmax(bbox[k] - c[k], c[k] - bbox[3 + k]));
+        d2 += dk * dk;
+    }
+    return d2 >= (tau * size) * (tau * size);
+}
+
+// Stages a tile of stations (x, y, z, gravity adjoint, magnetic adjoint)
+// and its bounding box (computed by warp 0).
+__device__ __forceinline__ void stage_stations(double* st, double* bbox, int s0, int ns, const double* __restrict__ sta,
+                                               const double* __restrict__ gcoef, const double* __restrict__ mcoef) {
+    for (int idx = threadIdx.x; idx < ns; idx += blockDim.x) {
+        int sIdx = s0 + idx;
+        st[5 * idx + 0] = sta[3 * sIdx];
+        st[5 * idx + 1] = sta[3 * sIdx + 1];
+        st[5 * idx + 2] = sta[3 * sIdx + 2];
+        st[5 * idx + 3] = gcoef ? gcoef[sIdx] : 0.0;
+        st[5 * idx + 4] = mcoef ? mcoef[sIdx] : 0.0;
+    }
+    if (threadIdx.x < 32) {
+        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+        for (int idx = threadIdx.x; idx < ns; idx += 32)
+            for (int k = 0; k < 3; ++k) {
+                double v = sta[3 * (s0 + idx) + k];
+                lo[k] = fmin(lo[k], v);
+                hi[k] = fmax(hi[k], v);
+            }
+        for (int k = 0; k < 3; ++k)
+            for (int off = 16; off > 0; off >>= 1) {
+                lo[k] = fmin(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], off));
+                hi[k] = fmax(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], off));
+            }
+        if (threadIdx.x == 0)
+            for (int k = 0; k < 3; ++k) { bbox[k] = lo[k]; bbox[3 + k] = hi[k]; }
+    }
+}
+
 // Grid: x = facet tiles of blockDim.x, y = station chunks.  part layout:
-// [chunk][9][T] (vertex a xyz, b xyz, c xyz; global frame).
+// [chunk][9][T] (vertex a xyz, b xyz, c xyz; global frame).  With tau
+// finite (mixed precision) a station tile whose bounding box is far from
+// every facet of the warp is skipped here; the FP32 far-field kernel takes it.
 template <int ST>
 __global__ void __launch_bounds__(128) k_gradient_fp64(int T, const double* __restrict__ gc, int S,
                                                        const double* __restrict__ sta, const double* __restrict__ gcoef,
                                                        const double* __restrict__ mcoef, int stations_per_chunk,
                                                        const int16_t* __restrict__ face_group,
-                                                       const GroupConst* __restrict__ groups, d3 fdir,
+                                                       const GroupConst* __restrict__ groups, d3 fdir, double tau,
                                                        double* __restrict__ part) {
     __shared__ double st[5 * ST];
+    __shared__ double bbox[6];
     int f = blockIdx.x * blockDim.x + threadIdx.x;
     int chunk = blockIdx.y;
     int sb = chunk * stations_per_chunk, se = min(S, sb + stations_per_chunk);
@@ -430,10 +542,7 @@ __global__ void __launch_bounds__(128) k_gradient_fp64(int T, const double* __re
         active = (flags & 1) && (flags & 2) && (C[GC_GS] != 0.0 || C[GC_MS] != 0.0);
     }
     GradAcc A;
-    A.va = A.vb = A.vc = mk3(0, 0, 0);
-    A.bh = mk3(0, 0, 0);
-    for (int i = 0; i < 3; ++i) { A.alam[i] = 0; A.bl[i] = mk3(0, 0, 0); A.amt[i] = 0; }
-    A.aom = A.ai = A.amf = 0.0;
+    grad_acc_zero(A);
     double nz = 0, gsn = 0, ms = 0;
     if (active) { nz = C[GC_ZZ]; gsn = C[GC_GS]; ms = C[GC_MS]; }
     const double L0 = active ? C[GC_L0] : 0, cx = active ? C[GC_CX] : 0, cy = active ? C[GC_CY] : 0;
@@ -441,16 +550,10 @@ __global__ void __launch_bounds__(128) k_gradient_fp64(int T, const double* __re
     for (int s0 = sb; s0 < se; s0 += ST) {
         int ns = min(ST, se - s0);
         __syncthreads();
-        for (int idx = threadIdx.x; idx < ns; idx += blockDim.x) {
-            int sIdx = s0 + idx;
-            st[5 * idx + 0] = sta[3 * sIdx];
-            st[5 * idx + 1] = sta[3 * sIdx + 1];
-            st[5 * idx + 2] = sta[3 * sIdx + 2];
-            st[5 * idx + 3] = gcoef ? gcoef[sIdx] : 0.0;
-            st[5 * idx + 4] = mcoef ? mcoef[sIdx] : 0.0;
-        }
+        stage_stations(st, bbox, s0, ns, sta, gcoef, mcoef);
         __syncthreads();
-        if (!active) continue;
+        bool allFar = __all_sync(0xffffffffu, facet_far(C, active, bbox, tau));
+        if (!active || allFar) continue;
         for (int j = 0; j < ns; ++j) {
             double G0 = st[5 * j + 3] * gsn;   // gravity adjoint x group scale
             double Gs = G0 * nz;               // ... x n_z
@@ -503,52 +606,7 @@ __global__ void __launch_bounds__(128) k_gradient_fp64(int T, const double* __re
     if (!active) {
         for (int k = 0; k < 9; ++k) outv[k] = 0.0;
     } else {
-        // ---- per-facet finalisation in the local frame ----
-        d3 xh = mk3(C[GC_XX], C[GC_XY], C[GC_XZ]), yh = mk3(C[GC_YX], C[GC_YY], C[GC_YZ]),
-           zh = mk3(C[GC_ZX], C[GC_ZY], C[GC_ZZ]);
-        const GroupConst& g = groups[face_group[f]];
-        d3 mg = mk3(g.mdir[0], g.mdir[1], g.mdir[2]);
-        d3 ml = mk3(dot3(mg, xh), dot3(mg, yh), dot3(mg, zh));
-        d3 fl = mk3(dot3(fdir, xh), dot3(fdir, yh), dot3(fdir, zh));
-        d3 nh = mk3(0, 0, 1);
-        d3 eh[3] = {mk3(1, 0, 0), mk3(C[GC_E1X], C[GC_E1Y], 0), mk3(C[GC_E2X], C[GC_E2Y], 0)};
-        double Ls[3] = {L0, C[GC_L1], C[GC_L2]};
-        d3 vbar[3] = {A.va, A.vb, A.vc};
-        // n_hat adjoint
-        d3 nbar = A.bh * -1.0;
-        {
-            double mn = ml.z, fn = fl.z;
-            nbar = nbar + (ml * fn + fl * mn) * A.amf;
-            // n_z = n_hat . e_z(global); e_z in local coordinates
-            nbar = nbar + mk3(xh.z, yh.z, zh.z) * A.ai;
-        }
-        // vertex-direct: h on a, d_perp on p1
-        vbar[0] = vbar[0] + nh * (-A.aom);
-        for (int i = 0; i < 3; ++i) {
-            d3 perp = cross3(nh, eh[i]);
-            vbar[i] = vbar[i] + perp * (-A.alam[i]);
-            double mp = dot3(ml, perp), fp = dot3(fl, perp);
-            d3 pbar = A.bl[i] * -1.0 + (ml * fp + fl * mp) * A.amt[i];
-            // perp = n x e: n_bar += e x pbar, e_bar = pbar x n
-            nbar = nbar + cross3(eh[i], pbar);
-            d3 ebar = cross3(pbar, nh);
-            double pe = dot3(ebar, eh[i]);
-            d3 eraw = (ebar - eh[i] * pe) * (1.0 / Ls[i]);
-            vbar[(i + 1) % 3] = vbar[(i + 1) % 3] + eraw;
-            vbar[i] = vbar[i] - eraw;
-        }
-        // n_hat = n / |n|, n = (b-a) x (c-a)
-        double pn = dot3(nbar, nh);
-        d3 nraw = (nbar - nh * pn) * (1.0 / area2);
-        d3 u = mk3(L0, 0, 0), w = mk3(cx, cy, 0);
-        d3 ubar = cross3(w, nraw), wbar = cross3(nraw, u);
-        vbar[1] = vbar[1] + ubar;
-        vbar[2] = vbar[2] + wbar;
-        vbar[0] = vbar[0] - ubar - wbar;
-        for (int v = 0; v < 3; ++v) {
-            d3 gv = xh * vbar[v].x + yh * vbar[v].y + zh * vbar[v].z;
-            outv[3 * v] = gv.x; outv[3 * v + 1] = gv.y; outv[3 * v + 2] = gv.z;
-        }
+        grad_finalize(C, A, groups[face_group[f]], fdir, outv);
     }
     for (int k = 0; k < 9; ++k) part[((size_t)chunk * 9 + k) * T + f] = outv[k];
 }
