@@ -58,7 +58,7 @@ struct StationSet {
     int n = 0;
     std::vector<double> xyz, obs, w;  // caller order
     std::vector<int32_t> perm;
-    DevBuf<double> d_xyz, d_obs, d_w, d_pred, d_coef, d_out;
+    DevBuf<double> d_xyz, d_obs, d_w, d_pred, d_coef, d_out, d_tileBox;
     DevBuf<int32_t> d_perm;
 };
 
@@ -600,6 +600,21 @@ static lf_status set_stations(lf_ctx* c, StationSet& s, int n, const double* xyz
     LF_TRY_CUDA(c, upload(s.d_obs, po.data(), po.size(), c->stream));
     LF_TRY_CUDA(c, upload(s.d_w, pw.data(), pw.size(), c->stream));
     LF_TRY_CUDA(c, upload(s.d_perm, s.perm.data(), s.perm.size(), c->stream));
+    // bounding box of every tile of kStationTile consecutive (Morton-ordered) stations
+    {
+        int nt = cdiv(std::max(n, 1), kStationTile);
+        std::vector<double> box(6 * (size_t)nt);
+        for (int t = 0; t < nt; ++t) {
+            double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+            for (int i = t * kStationTile; i < std::min(n, (t + 1) * kStationTile); ++i)
+                for (int k = 0; k < 3; ++k) {
+                    lo[k] = std::min(lo[k], px[3 * i + k]);
+                    hi[k] = std::max(hi[k], px[3 * i + k]);
+                }
+            for (int k = 0; k < 3; ++k) { box[6 * t + k] = lo[k]; box[6 * t + 3 + k] = hi[k]; }
+        }
+        LF_TRY_CUDA(c, upload(s.d_tileBox, box.data(), box.size(), c->stream));
+    }
     LF_TRY_CUDA(c, s.d_pred.reserve(std::max(n, 1)));
     LF_TRY_CUDA(c, s.d_coef.reserve(std::max(n, 1)));
     LF_TRY_CUDA(c, s.d_out.reserve(std::max(n, 1)));
@@ -655,8 +670,8 @@ extern "C" lf_status lf_set_precision(lf_ctx* c, int mode) {
 // --------------------------------------------------------------- internals --
 static constexpr int kFwdThreads = 128;
 static constexpr int kFwdFacetTile = 32;
-static constexpr int kGradThreads = 128;
-static constexpr int kGradStationTile = 64;
+static constexpr int kGradThreads = 32;             // one warp per CTA
+static constexpr int kTargetGradCTAs = 148 * 16;
 static constexpr int kTargetBlocks = 148 * 4;
 
 // Facet chunks for the forward: contiguous ranges inside one group, sized so
@@ -818,16 +833,16 @@ static lf_status gradient_set(lf_ctx* c, const StationSet& s, const double* gcoe
     bool mixed = c->precision == LF_PREC_MIXED;
     double tau = mixed ? static_cast<double>(c->tau) : 3.0e38;
     int slot = prof_begin(c, c->evGrad, c->nGrad);
-    k_gradient_fp64<kGradStationTile><<<grid, kGradThreads, 0, c->stream>>>(
-        c->T, c->d_gc.p, s.n, s.d_xyz.p, gcoef, mcoef, stationsPerChunk, c->d_faceGroup.p, c->d_groups.p, c->fdir,
-        tau, c->d_partGrad.p + (size_t)chunk0 * 9 * c->T);
+    k_gradient_fp64<<<grid, kGradThreads, 0, c->stream>>>(
+        c->T, c->d_gc.p, s.n, s.d_xyz.p, gcoef, mcoef, stationsPerChunk, s.d_tileBox.p, c->d_faceGroup.p,
+        c->d_groups.p, c->fdir, tau, c->d_partGrad.p + (size_t)chunk0 * 9 * c->T);
     prof_end(c, c->evGrad, slot);
     c->counters.launches++;
     if (mixed) {
         int slot2 = prof_begin(c, c->evGrad, c->nGrad);
-        k_gradient_far32<kGradStationTile><<<grid, kGradThreads, 0, c->stream>>>(
-            c->T, c->d_gc.p, s.n, s.d_xyz.p, gcoef, mcoef, stationsPerChunk, c->d_faceGroup.p, c->d_groups.p,
-            c->fdir, tau, c->d_partGrad.p + (size_t)(chunk0 + farOffset) * 9 * c->T);
+        k_gradient_far32<<<grid, kGradThreads, 0, c->stream>>>(
+            c->T, c->d_gc.p, s.n, s.d_xyz.p, gcoef, mcoef, stationsPerChunk, s.d_tileBox.p, c->d_faceGroup.p,
+            c->d_groups.p, c->fdir, tau, c->d_partGrad.p + (size_t)(chunk0 + farOffset) * 9 * c->T);
         prof_end(c, c->evGrad, slot2);
         c->counters.launches++;
     }
@@ -838,8 +853,18 @@ static lf_status gradient_set(lf_ctx* c, const StationSet& s, const double* gcoe
 
 static int grad_chunks_for(lf_ctx* c, int S) {
     int fBlocks = std::max(1, cdiv(c->T, kGradThreads));
-    int want = std::max(1, cdiv(kTargetBlocks, fBlocks));
-    return std::max(1, std::min(want, cdiv(S, 16)));
+    int want = std::max(1, cdiv(kTargetGradCTAs, fBlocks));
+    return std::max(1, std::min(want, cdiv(S, kStationTile)));
+}
+
+// Stations per gradient chunk: whole station tiles, so a chunk's tiles are
+// the precomputed ones.
+static void grad_split(lf_ctx* c, int S, int* chunks, int* spc) {
+    int n = grad_chunks_for(c, S);
+    int per = cdiv(S, n);
+    per = cdiv(per, kStationTile) * kStationTile;
+    *spc = per;
+    *chunks = cdiv(S, per);
 }
 
 static lf_status gradient_all(lf_ctx* c, const double* d_params, double* d_grad) {
@@ -851,12 +876,10 @@ static lf_status gradient_all(lf_ctx* c, const double* d_params, double* d_grad)
     LF_CHECK_LAUNCH(c);
     int chunksG = 0, chunksM = 0, spcG = 1, spcM = 1;
     if (c->sameStations && gOn) {
-        chunksG = grad_chunks_for(c, c->grav.n);
-        spcG = cdiv(c->grav.n, chunksG);
-        chunksG = cdiv(c->grav.n, spcG);
+        grad_split(c, c->grav.n, &chunksG, &spcG);
     } else {
-        if (gOn) { chunksG = grad_chunks_for(c, c->grav.n); spcG = cdiv(c->grav.n, chunksG); chunksG = cdiv(c->grav.n, spcG); }
-        if (mOn) { chunksM = grad_chunks_for(c, c->mag.n); spcM = cdiv(c->mag.n, chunksM); chunksM = cdiv(c->mag.n, spcM); }
+        if (gOn) grad_split(c, c->grav.n, &chunksG, &spcG);
+        if (mOn) grad_split(c, c->mag.n, &chunksM, &spcM);
     }
     int total = chunksG + chunksM;
     int mult = c->precision == LF_PREC_MIXED ? 2 : 1;
@@ -1013,9 +1036,9 @@ extern "C" lf_status lf_jacobian(lf_ctx* c, const double* params, int which, dou
         dim3 grid(cdiv(c->T, kGradThreads), nb);
         const double* g1 = which == LF_GRAVITY ? c->d_ones.p : nullptr;
         const double* m1 = which == LF_MAGNETIC ? c->d_ones.p : nullptr;
-        k_gradient_fp64<kGradStationTile><<<grid, kGradThreads, 0, c->stream>>>(
-            c->T, c->d_gc.p, nb, s.d_xyz.p + 3 * (size_t)s0, g1, m1, 1, c->d_faceGroup.p, c->d_groups.p, c->fdir,
-            3.0e38, c->d_partGrad.p);
+        k_gradient_fp64<<<grid, kGradThreads, 0, c->stream>>>(
+            c->T, c->d_gc.p, nb, s.d_xyz.p + 3 * (size_t)s0, g1, m1, 1, s.d_tileBox.p, c->d_faceGroup.p,
+            c->d_groups.p, c->fdir, 3.0e38, c->d_partGrad.p);
         if (c->np > 0) {
             dim3 g2(cdiv(c->np, 128), nb);
             k_jacobian_gather<<<g2, 128, 0, c->stream>>>(nb, c->np, c->d_dofOff.p, c->d_refVertex.p, c->d_refAxis.p,

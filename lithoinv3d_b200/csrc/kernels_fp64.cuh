@@ -487,49 +487,24 @@ __device__ __forceinline__ bool facet_far(const double* C, bool active, const do
     return d2 >= (tau * size) * (tau * size);
 }
 
-// Stages a tile of stations (x, y, z, gravity adjoint, magnetic adjoint)
-// and its bounding box (computed by warp 0).
-__device__ __forceinline__ void stage_stations(double* st, double* bbox, int s0, int ns, const double* __restrict__ sta,
-                                               const double* __restrict__ gcoef, const double* __restrict__ mcoef) {
-    for (int idx = threadIdx.x; idx < ns; idx += blockDim.x) {
-        int sIdx = s0 + idx;
-        st[5 * idx + 0] = sta[3 * sIdx];
-        st[5 * idx + 1] = sta[3 * sIdx + 1];
-        st[5 * idx + 2] = sta[3 * sIdx + 2];
-        st[5 * idx + 3] = gcoef ? gcoef[sIdx] : 0.0;
-        st[5 * idx + 4] = mcoef ? mcoef[sIdx] : 0.0;
-    }
-    if (threadIdx.x < 32) {
-        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-        for (int idx = threadIdx.x; idx < ns; idx += 32)
-            for (int k = 0; k < 3; ++k) {
-                double v = sta[3 * (s0 + idx) + k];
-                lo[k] = fmin(lo[k], v);
-                hi[k] = fmax(hi[k], v);
-            }
-        for (int k = 0; k < 3; ++k)
-            for (int off = 16; off > 0; off >>= 1) {
-                lo[k] = fmin(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], off));
-                hi[k] = fmax(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], off));
-            }
-        if (threadIdx.x == 0)
-            for (int k = 0; k < 3; ++k) { bbox[k] = lo[k]; bbox[3 + k] = hi[k]; }
-    }
-}
+// Station tiles: kStationTile consecutive stations (Morton order on the
+// device), bounding boxes precomputed per station set (tile_box[t][6]).
+constexpr int kStationTile = 64;
 
 // Grid: x = facet tiles of blockDim.x, y = station chunks.  part layout:
 // [chunk][9][T] (vertex a xyz, b xyz, c xyz; global frame).  With tau
 // finite (mixed precision) a station tile whose bounding box is far from
 // every facet of the warp is skipped here; the FP32 far-field kernel takes it.
-template <int ST>
-__global__ void __launch_bounds__(128) k_gradient_fp64(int T, const double* __restrict__ gc, int S,
-                                                       const double* __restrict__ sta, const double* __restrict__ gcoef,
-                                                       const double* __restrict__ mcoef, int stations_per_chunk,
-                                                       const int16_t* __restrict__ face_group,
-                                                       const GroupConst* __restrict__ groups, d3 fdir, double tau,
-                                                       double* __restrict__ part) {
-    __shared__ double st[5 * ST];
-    __shared__ double bbox[6];
+// One warp per CTA (32 facets); a warp walks its station chunk tile by
+// tile with warp-uniform loads and no block barriers, so warps that skip a
+// tile never wait for warps that work on it.
+__global__ void __launch_bounds__(32) k_gradient_fp64(int T, const double* __restrict__ gc, int S,
+                                                      const double* __restrict__ sta, const double* __restrict__ gcoef,
+                                                      const double* __restrict__ mcoef, int stations_per_chunk,
+                                                      const double* __restrict__ tile_box,
+                                                      const int16_t* __restrict__ face_group,
+                                                      const GroupConst* __restrict__ groups, d3 fdir, double tau,
+                                                      double* __restrict__ part) {
     int f = blockIdx.x * blockDim.x + threadIdx.x;
     int chunk = blockIdx.y;
     int sb = chunk * stations_per_chunk, se = min(S, sb + stations_per_chunk);
@@ -547,19 +522,16 @@ __global__ void __launch_bounds__(128) k_gradient_fp64(int T, const double* __re
     if (active) { nz = C[GC_ZZ]; gsn = C[GC_GS]; ms = C[GC_MS]; }
     const double L0 = active ? C[GC_L0] : 0, cx = active ? C[GC_CX] : 0, cy = active ? C[GC_CY] : 0;
     const double area2 = L0 * cy;
-    for (int s0 = sb; s0 < se; s0 += ST) {
-        int ns = min(ST, se - s0);
-        __syncthreads();
-        stage_stations(st, bbox, s0, ns, sta, gcoef, mcoef);
-        __syncthreads();
-        bool allFar = __all_sync(0xffffffffu, facet_far(C, active, bbox, tau));
+    for (int s0 = sb; s0 < se; s0 += kStationTile) {
+        int ns = min(kStationTile, se - s0);
+        bool allFar = __all_sync(0xffffffffu, facet_far(C, active, tile_box + 6 * (s0 / kStationTile), tau));
         if (!active || allFar) continue;
-        for (int j = 0; j < ns; ++j) {
-            double G0 = st[5 * j + 3] * gsn;   // gravity adjoint x group scale
-            double Gs = G0 * nz;               // ... x n_z
-            double Ts = st[5 * j + 4] * ms;    // magnetic adjoint x group TMI scale
+        for (int j = s0; j < s0 + ns; ++j) {
+            double G0 = (gcoef ? gcoef[j] : 0.0) * gsn;  // gravity adjoint x group scale
+            double Gs = G0 * nz;                          // ... x n_z
+            double Ts = (mcoef ? mcoef[j] : 0.0) * ms;    // magnetic adjoint x group TMI scale
             if (Gs == 0.0 && Ts == 0.0 && G0 == 0.0) continue;
-            d3 dd = mk3(st[5 * j] - C[GC_AX], st[5 * j + 1] - C[GC_AY], st[5 * j + 2] - C[GC_AZ]);
+            d3 dd = mk3(sta[3 * j] - C[GC_AX], sta[3 * j + 1] - C[GC_AY], sta[3 * j + 2] - C[GC_AZ]);
             double x = dd.x * C[GC_XX] + dd.y * C[GC_XY] + dd.z * C[GC_XZ];
             double y = dd.x * C[GC_YX] + dd.y * C[GC_YY] + dd.z * C[GC_YZ];
             double z = dd.x * C[GC_ZX] + dd.y * C[GC_ZY] + dd.z * C[GC_ZZ];

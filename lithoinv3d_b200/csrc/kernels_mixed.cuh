@@ -324,15 +324,13 @@ __global__ void __launch_bounds__(128) k_forward_mixed(int S, const double* __re
 // FP32 sums run over one station tile (<= 64 stations) and are flushed into
 // the FP64 accumulators, then the FP64 finalisation differentiates the facet
 // constants once.
-template <int ST>
-__global__ void __launch_bounds__(128) k_gradient_far32(int T, const double* __restrict__ gc, int S,
-                                                        const double* __restrict__ sta, const double* __restrict__ gcoef,
-                                                        const double* __restrict__ mcoef, int stations_per_chunk,
-                                                        const int16_t* __restrict__ face_group,
-                                                        const GroupConst* __restrict__ groups, d3 fdir, double tau,
-                                                        double* __restrict__ part) {
-    __shared__ double st[5 * ST];
-    __shared__ double bbox[6];
+__global__ void __launch_bounds__(32) k_gradient_far32(int T, const double* __restrict__ gc, int S,
+                                                       const double* __restrict__ sta, const double* __restrict__ gcoef,
+                                                       const double* __restrict__ mcoef, int stations_per_chunk,
+                                                       const double* __restrict__ tile_box,
+                                                       const int16_t* __restrict__ face_group,
+                                                       const GroupConst* __restrict__ groups, d3 fdir, double tau,
+                                                       double* __restrict__ part) {
     int f = blockIdx.x * blockDim.x + threadIdx.x;
     int chunk = blockIdx.y;
     int sb = chunk * stations_per_chunk, se = min(S, sb + stations_per_chunk);
@@ -363,12 +361,9 @@ __global__ void __launch_bounds__(128) k_gradient_far32(int T, const double* __r
         qx[q] = kRadonBb[q] * L0 + kRadonBc[q] * cx;
         qy[q] = kRadonBc[q] * cy;
     }
-    for (int s0 = sb; s0 < se; s0 += ST) {
-        int ns = min(ST, se - s0);
-        __syncthreads();
-        stage_stations(st, bbox, s0, ns, sta, gcoef, mcoef);
-        __syncthreads();
-        bool allFar = __all_sync(0xffffffffu, facet_far(C, active, bbox, tau));
+    for (int s0 = sb; s0 < se; s0 += kStationTile) {
+        int ns = min(kStationTile, se - s0);
+        bool allFar = __all_sync(0xffffffffu, facet_far(C, active, tile_box + 6 * (s0 / kStationTile), tau));
         if (!active || !allFar) continue;
         float q0 = 0.f;
         float dqx[7], dqy[7], dqz[7];
@@ -376,11 +371,11 @@ __global__ void __launch_bounds__(128) k_gradient_far32(int T, const double* __r
         for (int q = 0; q < 7; ++q) dqx[q] = dqy[q] = dqz[q] = 0.f;
         float vax = 0.f, vay = 0.f, vaz = 0.f, vbx = 0.f, vby = 0.f, vbz = 0.f, vcx = 0.f, vcy = 0.f, vcz = 0.f;
         float amf = 0.f, amt0 = 0.f, amt1 = 0.f, amt2 = 0.f;
-        for (int j = 0; j < ns; ++j) {
-            float G0 = (float)(st[5 * j + 3] * gsn);
-            float Ts = (float)(st[5 * j + 4] * ms);
+        for (int j = s0; j < s0 + ns; ++j) {
+            float G0 = (float)((gcoef ? gcoef[j] : 0.0) * gsn);
+            float Ts = (float)((mcoef ? mcoef[j] : 0.0) * ms);
             if (G0 == 0.f && Ts == 0.f) continue;
-            double ddx = st[5 * j] - C[GC_AX], ddy = st[5 * j + 1] - C[GC_AY], ddz = st[5 * j + 2] - C[GC_AZ];
+            double ddx = sta[3 * j] - C[GC_AX], ddy = sta[3 * j + 1] - C[GC_AY], ddz = sta[3 * j + 2] - C[GC_AZ];
             float dx = (float)ddx, dy = (float)ddy, dz = (float)ddz;
             float x = fmaf(dx, rx0, fmaf(dy, rx1, dz * rx2));
             float y = fmaf(dx, ry0, fmaf(dy, ry1, dz * ry2));
