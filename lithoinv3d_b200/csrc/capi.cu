@@ -670,8 +670,8 @@ extern "C" lf_status lf_set_precision(lf_ctx* c, int mode) {
 // --------------------------------------------------------------- internals --
 static constexpr int kFwdThreads = 128;
 static constexpr int kFwdFacetTile = 32;
-static constexpr int kGradThreads = 32;             // one warp per CTA
-static constexpr int kTargetGradCTAs = 148 * 16;
+static constexpr int kGradThreads = 32;             // Jacobian rows: one warp of facets per CTA
+static constexpr int kGradWarpsPerBlock = 4;        // objective gradient: one warp per facet
 static constexpr int kTargetBlocks = 148 * 4;
 
 // Facet chunks for the forward: contiguous ranges inside one group, sized so
@@ -821,50 +821,31 @@ static lf_status objective_final(lf_ctx* c, const double* d_params, double* d_f)
 }
 
 // Gradient kernels over one station set with the given adjoints; writes
-// chunks [chunk0, chunk0 + nchunks) of d_partGrad.
-// FP64 mode: one FP64 kernel over every (facet, station) pair.  Mixed mode:
-// the FP64 kernel takes the near tiles and writes chunks [chunk0, +nchunks);
-// the FP32 far-field kernel takes the rest and writes chunks shifted by
-// farOffset.
-static lf_status gradient_set(lf_ctx* c, const StationSet& s, const double* gcoef, const double* mcoef,
-                              int stationsPerChunk, int chunk0, int nchunks, int farOffset) {
-    if (s.n == 0 || nchunks == 0) return LF_OK;
-    dim3 grid(cdiv(c->T, kGradThreads), nchunks);
-    bool mixed = c->precision == LF_PREC_MIXED;
-    double tau = mixed ? static_cast<double>(c->tau) : 3.0e38;
-    int slot = prof_begin(c, c->evGrad, c->nGrad);
-    k_gradient_fp64<<<grid, kGradThreads, 0, c->stream>>>(
-        c->T, c->d_gc.p, s.n, s.d_xyz.p, gcoef, mcoef, stationsPerChunk, s.d_tileBox.p, c->d_faceGroup.p,
-        c->d_groups.p, c->fdir, tau, c->d_partGrad.p + (size_t)chunk0 * 9 * c->T);
-    prof_end(c, c->evGrad, slot);
+// facet partial slot `slot` of d_partGrad ([slot][9][T]).  FP64 mode: one
+// FP64 kernel over every (facet, station) pair.  Mixed mode: the FP64 kernel
+// takes each facet's near station tiles and the FP32 far-field kernel the
+// rest, writing slot + 1.  Returns the number of slots written.
+static int gradient_set(lf_ctx* c, const StationSet& s, const double* gcoef, const double* mcoef, int slot) {
+    if (s.n == 0) return 0;
+    const bool mixed = c->precision == LF_PREC_MIXED;
+    const double tau = mixed ? static_cast<double>(c->tau) : 3.0e38;
+    const int blocks = cdiv(c->T, kGradWarpsPerBlock);
+    int ev = prof_begin(c, c->evGrad, c->nGrad);
+    k_gradient_warp_fp64<<<blocks, 32 * kGradWarpsPerBlock, 0, c->stream>>>(
+        c->T, c->d_gc.p, s.n, s.d_xyz.p, gcoef, mcoef, s.d_tileBox.p, c->d_faceGroup.p, c->d_groups.p, c->fdir, tau,
+        c->d_partGrad.p + (size_t)slot * 9 * c->T);
+    prof_end(c, c->evGrad, ev);
     c->counters.launches++;
     if (mixed) {
-        int slot2 = prof_begin(c, c->evGrad, c->nGrad);
-        k_gradient_far32<<<grid, kGradThreads, 0, c->stream>>>(
-            c->T, c->d_gc.p, s.n, s.d_xyz.p, gcoef, mcoef, stationsPerChunk, s.d_tileBox.p, c->d_faceGroup.p,
-            c->d_groups.p, c->fdir, tau, c->d_partGrad.p + (size_t)(chunk0 + farOffset) * 9 * c->T);
-        prof_end(c, c->evGrad, slot2);
+        int ev2 = prof_begin(c, c->evGrad, c->nGrad);
+        k_gradient_warp_far32<<<blocks, 32 * kGradWarpsPerBlock, 0, c->stream>>>(
+            c->T, c->d_gc.p, s.n, s.d_xyz.p, gcoef, mcoef, s.d_tileBox.p, c->d_faceGroup.p, c->d_groups.p, c->fdir,
+            tau, c->d_partGrad.p + (size_t)(slot + 1) * 9 * c->T);
+        prof_end(c, c->evGrad, ev2);
         c->counters.launches++;
     }
     c->counters.gradient_pairs += (uint64_t)s.n * (uint64_t)c->T;
-    LF_CHECK_LAUNCH(c);
-    return LF_OK;
-}
-
-static int grad_chunks_for(lf_ctx* c, int S) {
-    int fBlocks = std::max(1, cdiv(c->T, kGradThreads));
-    int want = std::max(1, cdiv(kTargetGradCTAs, fBlocks));
-    return std::max(1, std::min(want, cdiv(S, kStationTile)));
-}
-
-// Stations per gradient chunk: whole station tiles, so a chunk's tiles are
-// the precomputed ones.
-static void grad_split(lf_ctx* c, int S, int* chunks, int* spc) {
-    int n = grad_chunks_for(c, S);
-    int per = cdiv(S, n);
-    per = cdiv(per, kStationTile) * kStationTile;
-    *spc = per;
-    *chunks = cdiv(S, per);
+    return mixed ? 2 : 1;
 }
 
 static lf_status gradient_all(lf_ctx* c, const double* d_params, double* d_grad) {
@@ -874,32 +855,25 @@ static lf_status gradient_all(lf_ctx* c, const double* d_params, double* d_grad)
                                                              c->d_gc.p);
     c->counters.launches++;
     LF_CHECK_LAUNCH(c);
-    int chunksG = 0, chunksM = 0, spcG = 1, spcM = 1;
-    if (c->sameStations && gOn) {
-        grad_split(c, c->grav.n, &chunksG, &spcG);
-    } else {
-        if (gOn) grad_split(c, c->grav.n, &chunksG, &spcG);
-        if (mOn) grad_split(c, c->mag.n, &chunksM, &spcM);
-    }
-    int total = chunksG + chunksM;
-    int mult = c->precision == LF_PREC_MIXED ? 2 : 1;
-    if (total == 0) {
+    const int perSet = c->precision == LF_PREC_MIXED ? 2 : 1;
+    const int sets = (c->sameStations && gOn) ? 1 : (int)gOn + (int)mOn;
+    const int slots = sets * perSet;
+    if (slots == 0) {
         LF_TRY_CUDA(c, cudaMemsetAsync(c->d_vgrad.p, 0, sizeof(double) * 3 * c->V, c->stream));
     } else {
-        LF_TRY_CUDA(c, c->d_partGrad.reserve((size_t)total * mult * 9 * c->T));
-        lf_status st;
+        LF_TRY_CUDA(c, c->d_partGrad.reserve((size_t)slots * 9 * c->T));
+        int used = 0;
         if (c->sameStations && gOn) {
-            st = gradient_set(c, c->grav, c->grav.d_coef.p, mOn ? c->mag.d_coef.p : nullptr, spcG, 0, chunksG, total);
+            used += gradient_set(c, c->grav, c->grav.d_coef.p, mOn ? c->mag.d_coef.p : nullptr, used);
         } else {
-            st = gradient_set(c, c->grav, c->grav.d_coef.p, nullptr, spcG, 0, chunksG, total);
-            if (st == LF_OK) st = gradient_set(c, c->mag, nullptr, c->mag.d_coef.p, spcM, chunksG, chunksM, total);
+            if (gOn) used += gradient_set(c, c->grav, c->grav.d_coef.p, nullptr, used);
+            if (mOn) used += gradient_set(c, c->mag, nullptr, c->mag.d_coef.p, used);
         }
-        if (st != LF_OK) return st;
+        LF_CHECK_LAUNCH(c);
         if (c->nGradVerts > 0) {
             k_vertex_reduce<<<cdiv(c->nGradVerts, 128), 128, 0, c->stream>>>(c->nGradVerts, c->d_gradVerts.p,
-                                                                              c->d_vfOff.p, c->d_vf.p, c->T,
-                                                                              total * mult, c->d_partGrad.p,
-                                                                              c->d_vgrad.p);
+                                                                              c->d_vfOff.p, c->d_vf.p, c->T, used,
+                                                                              c->d_partGrad.p, c->d_vgrad.p);
             c->counters.launches++;
         }
     }
@@ -1037,8 +1011,8 @@ extern "C" lf_status lf_jacobian(lf_ctx* c, const double* params, int which, dou
         const double* g1 = which == LF_GRAVITY ? c->d_ones.p : nullptr;
         const double* m1 = which == LF_MAGNETIC ? c->d_ones.p : nullptr;
         k_gradient_fp64<<<grid, kGradThreads, 0, c->stream>>>(
-            c->T, c->d_gc.p, nb, s.d_xyz.p + 3 * (size_t)s0, g1, m1, 1, s.d_tileBox.p, c->d_faceGroup.p,
-            c->d_groups.p, c->fdir, 3.0e38, c->d_partGrad.p);
+            c->T, c->d_gc.p, nb, s.d_xyz.p + 3 * (size_t)s0, g1, m1, 1, c->d_faceGroup.p, c->d_groups.p, c->fdir,
+            c->d_partGrad.p);
         if (c->np > 0) {
             dim3 g2(cdiv(c->np, 128), nb);
             k_jacobian_gather<<<g2, 128, 0, c->stream>>>(nb, c->np, c->d_dofOff.p, c->d_refVertex.p, c->d_refAxis.p,

@@ -468,119 +468,208 @@ __device__ __forceinline__ void grad_acc_zero(GradAcc& A) {
     A.aom = A.ai = A.amf = 0.0;
 }
 
-// Warp-uniform far test of a facet against a station tile's bounding box
-// (centroid at least tau x longest edge away).  Facets that take no part
-// count as far, so a warp of inactive facets never blocks the decision.
-__device__ __forceinline__ bool facet_far(const double* C, bool active, const double* bbox, double tau) {
-    if (!active) return true;
-    if (tau >= 1e30) return false;
-    double L0 = C[GC_L0], cx = C[GC_CX], cy = C[GC_CY];
-    double px = (L0 + cx) / 3.0, py = cy / 3.0;
-    double c[3] = {C[GC_AX] + px * C[GC_XX] + py * C[GC_YX], C[GC_AY] + px * C[GC_XY] + py * C[GC_YY],
-                   C[GC_AZ] + px * C[GC_XZ] + py * C[GC_YZ]};
-    double size = fmax(L0, fmax(C[GC_L1], C[GC_L2]));
-    double d2 = 0.0;
-    for (int k = 0; k < 3; ++k) {
-        double dk = fmax(0.0, fmax(bbox[k] - c[k], c[k] - bbox[3 + k]));
-        d2 += dk * dk;
-    }
-    return d2 >= (tau * size) * (tau * size);
-}
-
 // Station tiles: kStationTile consecutive stations (Morton order on the
-// device), bounding boxes precomputed per station set (tile_box[t][6]).
+// device), bounding boxes precomputed per station set (tile_box[t][6]:
+// min xyz, max xyz).
 constexpr int kStationTile = 64;
 
-// Grid: x = facet tiles of blockDim.x, y = station chunks.  part layout:
-// [chunk][9][T] (vertex a xyz, b xyz, c xyz; global frame).  With tau
-// finite (mixed precision) a station tile whose bounding box is far from
-// every facet of the warp is skipped here; the FP32 far-field kernel takes it.
-// One warp per CTA (32 facets); a warp walks its station chunk tile by
-// tile with warp-uniform loads and no block barriers, so warps that skip a
-// tile never wait for warps that work on it.
+// Near/far split of the mixed-precision gradient: a facet is far from a
+// station tile when its centroid lies at least tau x its longest edge from
+// the tile's bounding box.  Every operation is rounded explicitly, so the
+// near-field and far-field kernels, compiled separately, classify every
+// (facet, tile) identically and each pair is counted exactly once.
+// FarKey: the facet's centroid and squared threshold; th2 < 0 means
+// "everything near" (tau >= 1e30, the FP64 mode).
+struct FarKey {
+    double c0, c1, c2, th2;
+};
+
+__device__ __forceinline__ FarKey facet_far_key(const double* C, double tau) {
+    FarKey k;
+    const double L0 = C[GC_L0], cx = C[GC_CX], cy = C[GC_CY];
+    const double px = __ddiv_rn(__dadd_rn(L0, cx), 3.0), py = __ddiv_rn(cy, 3.0);
+    k.c0 = __dadd_rn(C[GC_AX], __dadd_rn(__dmul_rn(px, C[GC_XX]), __dmul_rn(py, C[GC_YX])));
+    k.c1 = __dadd_rn(C[GC_AY], __dadd_rn(__dmul_rn(px, C[GC_XY]), __dmul_rn(py, C[GC_YY])));
+    k.c2 = __dadd_rn(C[GC_AZ], __dadd_rn(__dmul_rn(px, C[GC_XZ]), __dmul_rn(py, C[GC_YZ])));
+    const double th = __dmul_rn(tau, fmax(L0, fmax(C[GC_L1], C[GC_L2])));
+    k.th2 = tau >= 1e30 ? -1.0 : __dmul_rn(th, th);
+    return k;
+}
+
+__device__ __forceinline__ bool tile_far(const FarKey& k, const double* __restrict__ bbox) {
+    if (k.th2 < 0.0) return false;
+    const double d0 = fmax(0.0, fmax(__dadd_rn(bbox[0], -k.c0), __dadd_rn(k.c0, -bbox[3])));
+    const double d1 = fmax(0.0, fmax(__dadd_rn(bbox[1], -k.c1), __dadd_rn(k.c1, -bbox[4])));
+    const double d2 = fmax(0.0, fmax(__dadd_rn(bbox[2], -k.c2), __dadd_rn(k.c2, -bbox[5])));
+    const double dd = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2));
+    return dd >= k.th2;
+}
+
+// One (facet, station) pair of the FP64 gradient: adds the station's terms,
+// weighted by its adjoints (gco gravity, mco magnetic), to the facet's
+// local-frame accumulators.  gsn / ms: the facet group's gz / TMI scales.
+__device__ __forceinline__ void pair_gradient_fp64(const double* C, double gsn, double ms, double ox, double oy,
+                                                   double oz, double gco, double mco, GradAcc& A) {
+    const double nz = C[GC_ZZ];
+    const double L0 = C[GC_L0], cx = C[GC_CX], cy = C[GC_CY];
+    const double area2 = L0 * cy;
+    double G0 = gco * gsn;  // gravity adjoint x group scale
+    double Gs = G0 * nz;    // ... x n_z
+    double Ts = mco * ms;   // magnetic adjoint x group TMI scale
+    if (Gs == 0.0 && Ts == 0.0 && G0 == 0.0) return;
+    d3 dd = mk3(ox - C[GC_AX], oy - C[GC_AY], oz - C[GC_AZ]);
+    double x = dd.x * C[GC_XX] + dd.y * C[GC_XY] + dd.z * C[GC_XZ];
+    double y = dd.x * C[GC_YX] + dd.y * C[GC_YY] + dd.z * C[GC_YZ];
+    double z = dd.x * C[GC_ZX] + dd.y * C[GC_ZY] + dd.z * C[GC_ZZ];
+    d3 ra = mk3(-x, -y, -z), rb = mk3(L0 - x, -y, -z), rc = mk3(cx - x, cy - y, -z);
+    double z2 = z * z;
+    double la = sqrt(x * x + y * y + z2), lb = sqrt(rb.x * rb.x + y * y + z2),
+           lc = sqrt(rc.x * rc.x + rc.y * rc.y + z2);
+    if (la < kEps || lb < kEps || lc < kEps) return;  // station on a vertex: not differentiable
+    double h = -z;
+    double Nn = h * area2;
+    double Dd = la * lb * lc + dot3(ra, rb) * lc + dot3(ra, rc) * lb + dot3(rb, rc) * la;
+    double om = 2.0 * atan2(Nn, Dd);
+    double ia = 1.0 / la, ib = 1.0 / lb, ic = 1.0 / lc;
+    // edges: 0 a->b (e=(1,0)), 1 b->c, 2 c->a
+    double e1x = C[GC_E1X], e1y = C[GC_E1Y], e2x = C[GC_E2X], e2y = C[GC_E2Y];
+    bool lv0, lv1, lv2;
+    double lam0 = lambda_from(-x, L0 - x, la, lb, &lv0);
+    double s11 = rb.x * e1x + rb.y * e1y, s12 = rc.x * e1x + rc.y * e1y;
+    double lam1 = lambda_from(s11, s12, lb, lc, &lv1);
+    double s21 = rc.x * e2x + rc.y * e2y, s22 = ra.x * e2x + ra.y * e2y;
+    double lam2 = lambda_from(s21, s22, lc, la, &lv2);
+    // d_perp_i = -r1 . perp_i, perp_i = (-ey, ex, 0)
+    double dp0 = y;  // -(r_a.y * 1)
+    double dp1 = rb.x * e1y - rb.y * e1x;
+    double dp2 = rc.x * e2y - rc.y * e2x;
+    double I = dp0 * lam0 + dp1 * lam1 + dp2 * lam2 - h * om;
+    double kom = -Gs * h + Ts * C[GC_MF];
+    edge_terms(ra, rb, la, lb, 1.0, 0.0, L0, ia, ib, kom, Gs, Ts, C[GC_MT0], dp0, lam0, lv0, &A.va, &A.vb);
+    edge_terms(rb, rc, lb, lc, e1x, e1y, C[GC_L1], ib, ic, kom, Gs, Ts, C[GC_MT1], dp1, lam1, lv1, &A.vb, &A.vc);
+    edge_terms(rc, ra, lc, la, e2x, e2y, C[GC_L2], ic, ia, kom, Gs, Ts, C[GC_MT2], dp2, lam2, lv2, &A.vc, &A.va);
+    A.alam[0] += Gs * lam0; A.alam[1] += Gs * lam1; A.alam[2] += Gs * lam2;
+    A.aom += Gs * om;
+    A.ai += G0 * I;
+    A.bh = A.bh + ra * (Gs * om);
+    A.bl[0] = A.bl[0] + ra * (Gs * lam0);
+    A.bl[1] = A.bl[1] + rb * (Gs * lam1);
+    A.bl[2] = A.bl[2] + rc * (Gs * lam2);
+    A.amf += Ts * om;
+    A.amt[0] += Ts * lam0; A.amt[1] += Ts * lam1; A.amt[2] += Ts * lam2;
+}
+
+__device__ __forceinline__ bool facet_grad_active(const double* C) {
+    int flags = static_cast<int>(C[GC_FLAGS]);
+    return (flags & 1) && (flags & 2) && (C[GC_GS] != 0.0 || C[GC_MS] != 0.0);
+}
+
+// Per-station facet gradients for dense Jacobian rows.  Grid: x = facet
+// warps (one facet per thread), y = station chunks of stations_per_chunk
+// consecutive stations; part layout [chunk][9][T] (vertex a xyz, b xyz,
+// c xyz; global frame).  Stations are warp-uniform loads.
 __global__ void __launch_bounds__(32) k_gradient_fp64(int T, const double* __restrict__ gc, int S,
                                                       const double* __restrict__ sta, const double* __restrict__ gcoef,
                                                       const double* __restrict__ mcoef, int stations_per_chunk,
-                                                      const double* __restrict__ tile_box,
                                                       const int16_t* __restrict__ face_group,
-                                                      const GroupConst* __restrict__ groups, d3 fdir, double tau,
+                                                      const GroupConst* __restrict__ groups, d3 fdir,
                                                       double* __restrict__ part) {
     int f = blockIdx.x * blockDim.x + threadIdx.x;
     int chunk = blockIdx.y;
     int sb = chunk * stations_per_chunk, se = min(S, sb + stations_per_chunk);
-    bool active = false;
-    double C[NGC];
-    if (f < T) {
-#pragma unroll
-        for (int k = 0; k < NGC; ++k) C[k] = gc[(size_t)k * T + f];
-        int flags = static_cast<int>(C[GC_FLAGS]);
-        active = (flags & 1) && (flags & 2) && (C[GC_GS] != 0.0 || C[GC_MS] != 0.0);
-    }
-    GradAcc A;
-    grad_acc_zero(A);
-    double nz = 0, gsn = 0, ms = 0;
-    if (active) { nz = C[GC_ZZ]; gsn = C[GC_GS]; ms = C[GC_MS]; }
-    const double L0 = active ? C[GC_L0] : 0, cx = active ? C[GC_CX] : 0, cy = active ? C[GC_CY] : 0;
-    const double area2 = L0 * cy;
-    for (int s0 = sb; s0 < se; s0 += kStationTile) {
-        int ns = min(kStationTile, se - s0);
-        bool allFar = __all_sync(0xffffffffu, facet_far(C, active, tile_box + 6 * (s0 / kStationTile), tau));
-        if (!active || allFar) continue;
-        for (int j = s0; j < s0 + ns; ++j) {
-            double G0 = (gcoef ? gcoef[j] : 0.0) * gsn;  // gravity adjoint x group scale
-            double Gs = G0 * nz;                          // ... x n_z
-            double Ts = (mcoef ? mcoef[j] : 0.0) * ms;    // magnetic adjoint x group TMI scale
-            if (Gs == 0.0 && Ts == 0.0 && G0 == 0.0) continue;
-            d3 dd = mk3(sta[3 * j] - C[GC_AX], sta[3 * j + 1] - C[GC_AY], sta[3 * j + 2] - C[GC_AZ]);
-            double x = dd.x * C[GC_XX] + dd.y * C[GC_XY] + dd.z * C[GC_XZ];
-            double y = dd.x * C[GC_YX] + dd.y * C[GC_YY] + dd.z * C[GC_YZ];
-            double z = dd.x * C[GC_ZX] + dd.y * C[GC_ZY] + dd.z * C[GC_ZZ];
-            d3 ra = mk3(-x, -y, -z), rb = mk3(L0 - x, -y, -z), rc = mk3(cx - x, cy - y, -z);
-            double z2 = z * z;
-            double la = sqrt(x * x + y * y + z2), lb = sqrt(rb.x * rb.x + y * y + z2),
-                   lc = sqrt(rc.x * rc.x + rc.y * rc.y + z2);
-            if (la < kEps || lb < kEps || lc < kEps) continue;  // station on a vertex: not differentiable
-            double h = -z;
-            double Nn = h * area2;
-            double Dd = la * lb * lc + dot3(ra, rb) * lc + dot3(ra, rc) * lb + dot3(rb, rc) * la;
-            double om = 2.0 * atan2(Nn, Dd);
-            double ia = 1.0 / la, ib = 1.0 / lb, ic = 1.0 / lc;
-            // edges: 0 a->b (e=(1,0)), 1 b->c, 2 c->a
-            double e1x = C[GC_E1X], e1y = C[GC_E1Y], e2x = C[GC_E2X], e2y = C[GC_E2Y];
-            bool lv0, lv1, lv2;
-            double lam0 = lambda_from(-x, L0 - x, la, lb, &lv0);
-            double s11 = rb.x * e1x + rb.y * e1y, s12 = rc.x * e1x + rc.y * e1y;
-            double lam1 = lambda_from(s11, s12, lb, lc, &lv1);
-            double s21 = rc.x * e2x + rc.y * e2y, s22 = ra.x * e2x + ra.y * e2y;
-            double lam2 = lambda_from(s21, s22, lc, la, &lv2);
-            // d_perp_i = -r1 . perp_i, perp_i = (-ey, ex, 0)
-            double dp0 = y;                         // -(r_a.y * 1)
-            double dp1 = rb.x * e1y - rb.y * e1x;
-            double dp2 = rc.x * e2y - rc.y * e2x;
-            double I = dp0 * lam0 + dp1 * lam1 + dp2 * lam2 - h * om;
-            double kom = -Gs * h + Ts * C[GC_MF];
-            edge_terms(ra, rb, la, lb, 1.0, 0.0, L0, ia, ib, kom, Gs, Ts, C[GC_MT0], dp0, lam0, lv0, &A.va, &A.vb);
-            edge_terms(rb, rc, lb, lc, e1x, e1y, C[GC_L1], ib, ic, kom, Gs, Ts, C[GC_MT1], dp1, lam1, lv1, &A.vb, &A.vc);
-            edge_terms(rc, ra, lc, la, e2x, e2y, C[GC_L2], ic, ia, kom, Gs, Ts, C[GC_MT2], dp2, lam2, lv2, &A.vc, &A.va);
-            A.alam[0] += Gs * lam0; A.alam[1] += Gs * lam1; A.alam[2] += Gs * lam2;
-            A.aom += Gs * om;
-            A.ai += G0 * I;
-            A.bh = A.bh + ra * (Gs * om);
-            A.bl[0] = A.bl[0] + ra * (Gs * lam0);
-            A.bl[1] = A.bl[1] + rb * (Gs * lam1);
-            A.bl[2] = A.bl[2] + rc * (Gs * lam2);
-            A.amf += Ts * om;
-            A.amt[0] += Ts * lam0; A.amt[1] += Ts * lam1; A.amt[2] += Ts * lam2;
-        }
-    }
     if (f >= T) return;
-    double outv[9];
-    if (!active) {
-        for (int k = 0; k < 9; ++k) outv[k] = 0.0;
-    } else {
+    double C[NGC];
+#pragma unroll
+    for (int k = 0; k < NGC; ++k) C[k] = gc[(size_t)k * T + f];
+    const bool active = facet_grad_active(C);
+    double outv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (active) {
+        GradAcc A;
+        grad_acc_zero(A);
+        const double gsn = C[GC_GS], ms = C[GC_MS];
+        for (int j = sb; j < se; ++j)
+            pair_gradient_fp64(C, gsn, ms, sta[3 * j], sta[3 * j + 1], sta[3 * j + 2], gcoef ? gcoef[j] : 0.0,
+                               mcoef ? mcoef[j] : 0.0, A);
         grad_finalize(C, A, groups[face_group[f]], fdir, outv);
     }
     for (int k = 0; k < 9; ++k) part[((size_t)chunk * 9 + k) * T + f] = outv[k];
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    return v;
+}
+
+__device__ __forceinline__ void grad_acc_warp_sum(GradAcc& A) {
+    A.va = mk3(warp_sum(A.va.x), warp_sum(A.va.y), warp_sum(A.va.z));
+    A.vb = mk3(warp_sum(A.vb.x), warp_sum(A.vb.y), warp_sum(A.vb.z));
+    A.vc = mk3(warp_sum(A.vc.x), warp_sum(A.vc.y), warp_sum(A.vc.z));
+    A.bh = mk3(warp_sum(A.bh.x), warp_sum(A.bh.y), warp_sum(A.bh.z));
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        A.alam[i] = warp_sum(A.alam[i]);
+        A.amt[i] = warp_sum(A.amt[i]);
+        A.bl[i] = mk3(warp_sum(A.bl[i].x), warp_sum(A.bl[i].y), warp_sum(A.bl[i].z));
+    }
+    A.aom = warp_sum(A.aom);
+    A.ai = warp_sum(A.ai);
+    A.amf = warp_sum(A.amf);
+}
+
+// Objective gradient, FP64: one warp per facet.  The warp visits the
+// facet's near station tiles (every tile when tau >= 1e30), lanes taking
+// the tile's stations in turn; per-lane sums are reduced across the warp
+// once per facet and lane 0 finalises.  The work of a facet is spread over
+// 32 lanes, so facets with many near tiles leave no long tail behind.
+// part layout [9][T].
+__global__ void __launch_bounds__(128) k_gradient_warp_fp64(int T, const double* __restrict__ gc, int S,
+                                                            const double* __restrict__ sta,
+                                                            const double* __restrict__ gcoef,
+                                                            const double* __restrict__ mcoef,
+                                                            const double* __restrict__ tile_box,
+                                                            const int16_t* __restrict__ face_group,
+                                                            const GroupConst* __restrict__ groups, d3 fdir, double tau,
+                                                            double* __restrict__ part) {
+    const int lane = threadIdx.x & 31;
+    const int f = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+    if (f >= T) return;  // warp-uniform
+    double C[NGC];
+#pragma unroll
+    for (int k = 0; k < NGC; ++k) C[k] = gc[(size_t)k * T + f];
+    double outv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (facet_grad_active(C)) {
+        GradAcc A;
+        grad_acc_zero(A);
+        const double gsn = C[GC_GS], ms = C[GC_MS];
+        const int ntiles = (S + kStationTile - 1) / kStationTile;
+        const FarKey key = facet_far_key(C, tau);
+        bool any = false;
+        for (int t0 = 0; t0 < ntiles; t0 += 32) {
+            const int t = t0 + lane;
+            const bool nearT = t < ntiles && !tile_far(key, tile_box + 6 * (size_t)t);
+            unsigned m = __ballot_sync(0xffffffffu, nearT);
+            any |= m != 0;
+            while (m) {
+                const int b = __ffs(m) - 1;
+                m &= m - 1;
+                const int s0 = (t0 + b) * kStationTile;
+#pragma unroll
+                for (int k = 0; k < kStationTile; k += 32) {
+                    const int j = s0 + k + lane;
+                    if (j < S)
+                        pair_gradient_fp64(C, gsn, ms, sta[3 * j], sta[3 * j + 1], sta[3 * j + 2],
+                                           gcoef ? gcoef[j] : 0.0, mcoef ? mcoef[j] : 0.0, A);
+                }
+            }
+        }
+        if (any) {
+            grad_acc_warp_sum(A);
+            if (lane == 0) grad_finalize(C, A, groups[face_group[f]], fdir, outv);
+        }
+    }
+    if (lane == 0)
+        for (int k = 0; k < 9; ++k) part[(size_t)k * T + f] = outv[k];
 }
 
 // Sums facet partials into vertex gradients (deterministic order: chunks,

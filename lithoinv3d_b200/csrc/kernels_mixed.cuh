@@ -313,156 +313,235 @@ __global__ void __launch_bounds__(128) k_forward_mixed(int S, const double* __re
 }
 
 // ---------------------------------------------------- far-field gradient --
-// Facet-per-thread twin of k_gradient_fp64 for the station tiles it skips
-// (every facet of the warp far from the tile).  In FP32:
+// Sums v[0..31] over the warp, transposed: on return lane L holds the warp
+// total of v[L] in v[0] (31 shuffles for 32 sums instead of 32 x 5).
+__device__ __forceinline__ float warp_transpose_sum32(float (&v)[32]) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int step = 16; step >= 1; step >>= 1) {
+        const bool upper = (lane & step) != 0;
+#pragma unroll
+        for (int i = 0; i < step; ++i) {
+            const float send = upper ? v[i] : v[i + step];
+            const float keep = upper ? v[i + step] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, step);
+        }
+    }
+    return v[0];
+}
+
+constexpr int kFarTerms = 23;      // far-field station sums per facet (listed below)
+constexpr int kFarFlushTiles = 4;  // far tiles summed per lane in FP32 between warp reductions
+
+// Far-field objective gradient in FP32: one warp per facet, lanes over the
+// stations of the facet's far tiles (exactly the tiles k_gradient_warp_fp64
+// leaves out: both classify with facet_far_key / tile_far).
 //  * gz: I = A sum_q w_q / r_q, so
 //      sum_s G0 dI/dv = (dA/dv) Q0 - A sum_q beta_qv D_q,
 //    Q0 = sum_s G0 sum_q w_q / r_q, D_q = sum_s G0 w_q (p_q - o) / r_q^3
-//    (G0 = gravity adjoint x group scale; n_z enters at the flush and, for
-//    its own derivative, through the shared finalisation);
+//    (G0 = gravity adjoint x group scale, beta_qv = barycentric weight of
+//    point q on vertex v; n_z enters at the end, its own derivative through
+//    the shared finalisation);
 //  * TMI: the closed-form d Omega / dv and d Lambda / dv of the FP64 kernel.
-// FP32 sums run over one station tile (<= 64 stations) and are flushed into
-// the FP64 accumulators, then the FP64 finalisation differentiates the facet
-// constants once.
-__global__ void __launch_bounds__(32) k_gradient_far32(int T, const double* __restrict__ gc, int S,
-                                                       const double* __restrict__ sta, const double* __restrict__ gcoef,
-                                                       const double* __restrict__ mcoef, int stations_per_chunk,
-                                                       const double* __restrict__ tile_box,
-                                                       const int16_t* __restrict__ face_group,
-                                                       const GroupConst* __restrict__ groups, d3 fdir, double tau,
-                                                       double* __restrict__ part) {
-    int f = blockIdx.x * blockDim.x + threadIdx.x;
-    int chunk = blockIdx.y;
-    int sb = chunk * stations_per_chunk, se = min(S, sb + stations_per_chunk);
-    bool active = false;
-    double C[NGC];
-    if (f < T) {
+// Each lane sums up to kFarFlushTiles tiles (8 stations) in FP32; the 23
+// sums are then reduced across the warp in one transposed pass and lane k
+// adds sum k to its FP64 total.  Lane 0 gathers the totals, forms the facet
+// accumulators in FP64 and finalises.  part layout [9][T].
+// Sums: 0 Q0; 1-3, 4-6, 7-9 sum_q beta_q{a,b,c} D_q; 10-12, 13-15, 16-18 TMI
+// vertex terms of a, b, c; 19 sum Ts Omega; 20-22 sum Ts Lambda_i.
+__global__ void __launch_bounds__(128) k_gradient_warp_far32(int T, const double* __restrict__ gc, int S,
+                                                             const double* __restrict__ sta,
+                                                             const double* __restrict__ gcoef,
+                                                             const double* __restrict__ mcoef,
+                                                             const double* __restrict__ tile_box,
+                                                             const int16_t* __restrict__ face_group,
+                                                             const GroupConst* __restrict__ groups, d3 fdir,
+                                                             double tau, double* __restrict__ part) {
+    const int lane = threadIdx.x & 31;
+    const int f = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+    if (f >= T) return;  // warp-uniform
+    bool active, any = false;
+    double tot = 0.0;
+    {
+        double C[NGC];
 #pragma unroll
-        for (int k = 0; k < NGC; ++k) C[k] = gc[(size_t)k * T + f];
-        int flags = static_cast<int>(C[GC_FLAGS]);
-        active = (flags & 1) && (flags & 2) && (C[GC_GS] != 0.0 || C[GC_MS] != 0.0);
-    } else {
-        for (int k = 0; k < NGC; ++k) C[k] = 0.0;
-    }
-    GradAcc A;
-    grad_acc_zero(A);
-    // FP32 facet constants
-    const float L0 = (float)C[GC_L0], cx = (float)C[GC_CX], cy = (float)C[GC_CY];
-    const float e1x = (float)C[GC_E1X], e1y = (float)C[GC_E1Y], L1 = (float)C[GC_L1];
-    const float e2x = (float)C[GC_E2X], e2y = (float)C[GC_E2Y], L2 = (float)C[GC_L2];
-    const float rx0 = (float)C[GC_XX], rx1 = (float)C[GC_XY], rx2 = (float)C[GC_XZ];
-    const float ry0 = (float)C[GC_YX], ry1 = (float)C[GC_YY], ry2 = (float)C[GC_YZ];
-    const float mf = (float)C[GC_MF], mt0 = (float)C[GC_MT0], mt1 = (float)C[GC_MT1], mt2 = (float)C[GC_MT2];
-    const float A2 = L0 * cy;
-    const double gsn = C[GC_GS], ms = C[GC_MS];
-    float qx[7], qy[7];
+        for (int k = 0; k < NGC; ++k) C[k] = __ldg(&gc[(size_t)k * T + f]);
+        active = facet_grad_active(C);
+        if (active) {
+            const float L0 = (float)C[GC_L0], cx = (float)C[GC_CX], cy = (float)C[GC_CY];
+            const float e1x = (float)C[GC_E1X], e1y = (float)C[GC_E1Y], L1 = (float)C[GC_L1];
+            const float e2x = (float)C[GC_E2X], e2y = (float)C[GC_E2Y], L2 = (float)C[GC_L2];
+            const float rx0 = (float)C[GC_XX], rx1 = (float)C[GC_XY], rx2 = (float)C[GC_XZ];
+            const float ry0 = (float)C[GC_YX], ry1 = (float)C[GC_YY], ry2 = (float)C[GC_YZ];
+            const float mf = (float)C[GC_MF], mt0 = (float)C[GC_MT0], mt1 = (float)C[GC_MT1],
+                        mt2 = (float)C[GC_MT2];
+            const float A2 = L0 * cy;
+            const double ax = C[GC_AX], ay = C[GC_AY], az = C[GC_AZ];
+            const double zx = C[GC_ZX], zy = C[GC_ZY], zz = C[GC_ZZ];
+            const double gsn = C[GC_GS], ms = C[GC_MS];
+            float qx[7], qy[7];
 #pragma unroll
-    for (int q = 0; q < 7; ++q) {
-        qx[q] = kRadonBb[q] * L0 + kRadonBc[q] * cx;
-        qy[q] = kRadonBc[q] * cy;
-    }
-    for (int s0 = sb; s0 < se; s0 += kStationTile) {
-        int ns = min(kStationTile, se - s0);
-        bool allFar = __all_sync(0xffffffffu, facet_far(C, active, tile_box + 6 * (s0 / kStationTile), tau));
-        if (!active || !allFar) continue;
-        float q0 = 0.f;
-        float dqx[7], dqy[7], dqz[7];
+            for (int q = 0; q < 7; ++q) {
+                qx[q] = kRadonBb[q] * L0 + kRadonBc[q] * cx;
+                qy[q] = kRadonBc[q] * cy;
+            }
+            float q0 = 0.f, dqx[7], dqy[7], dqz[7];
+            float vax = 0.f, vay = 0.f, vaz = 0.f, vbx = 0.f, vby = 0.f, vbz = 0.f, vcx = 0.f, vcy = 0.f, vcz = 0.f;
+            float amf = 0.f, amt0 = 0.f, amt1 = 0.f, amt2 = 0.f;
 #pragma unroll
-        for (int q = 0; q < 7; ++q) dqx[q] = dqy[q] = dqz[q] = 0.f;
-        float vax = 0.f, vay = 0.f, vaz = 0.f, vbx = 0.f, vby = 0.f, vbz = 0.f, vcx = 0.f, vcy = 0.f, vcz = 0.f;
-        float amf = 0.f, amt0 = 0.f, amt1 = 0.f, amt2 = 0.f;
-        for (int j = s0; j < s0 + ns; ++j) {
-            float G0 = (float)((gcoef ? gcoef[j] : 0.0) * gsn);
-            float Ts = (float)((mcoef ? mcoef[j] : 0.0) * ms);
-            if (G0 == 0.f && Ts == 0.f) continue;
-            double ddx = sta[3 * j] - C[GC_AX], ddy = sta[3 * j + 1] - C[GC_AY], ddz = sta[3 * j + 2] - C[GC_AZ];
-            float dx = (float)ddx, dy = (float)ddy, dz = (float)ddz;
-            float x = fmaf(dx, rx0, fmaf(dy, rx1, dz * rx2));
-            float y = fmaf(dx, ry0, fmaf(dy, ry1, dz * ry2));
-            float z = (float)(ddx * C[GC_ZX] + ddy * C[GC_ZY] + ddz * C[GC_ZZ]);
-            float z2 = z * z;
-            if (G0 != 0.f) {
-                float sw = 0.f;
+            for (int q = 0; q < 7; ++q) dqx[q] = dqy[q] = dqz[q] = 0.f;
+            int pending = 0;
+            auto flush = [&]() {
+                float v[32];
+                float sa0 = 0.f, sa1 = 0.f, sa2 = 0.f, sb0 = 0.f, sb1 = 0.f, sb2 = 0.f, sc0 = 0.f, sc1 = 0.f, sc2 = 0.f;
 #pragma unroll
                 for (int q = 0; q < 7; ++q) {
-                    float px = qx[q] - x, py = qy[q] - y;
-                    float rs = rsqrtf(fmaf(px, px, fmaf(py, py, z2)));
-                    float w = kRadonW[q] * rs;
-                    sw += w;
-                    float g3 = G0 * w * rs * rs;
-                    dqx[q] = fmaf(g3, px, dqx[q]);
-                    dqy[q] = fmaf(g3, py, dqy[q]);
-                    dqz[q] = fmaf(g3, -z, dqz[q]);
+                    const float bb = kRadonBb[q], bc = kRadonBc[q], ba = 1.f - bb - bc;
+                    sa0 = fmaf(ba, dqx[q], sa0); sa1 = fmaf(ba, dqy[q], sa1); sa2 = fmaf(ba, dqz[q], sa2);
+                    sb0 = fmaf(bb, dqx[q], sb0); sb1 = fmaf(bb, dqy[q], sb1); sb2 = fmaf(bb, dqz[q], sb2);
+                    sc0 = fmaf(bc, dqx[q], sc0); sc1 = fmaf(bc, dqy[q], sc1); sc2 = fmaf(bc, dqz[q], sc2);
+                    dqx[q] = dqy[q] = dqz[q] = 0.f;
                 }
-                q0 = fmaf(G0, sw, q0);
-            }
-            if (Ts != 0.f) {
-                float rbx = L0 - x, rcx = cx - x, rcy = cy - y;
-                float la = sqrtf(fmaf(x, x, fmaf(y, y, z2)));
-                float lb = sqrtf(fmaf(rbx, rbx, fmaf(y, y, z2)));
-                float lc = sqrtf(fmaf(rcx, rcx, fmaf(rcy, rcy, z2)));
-                float dab = fmaf(-x, rbx, fmaf(y, y, z2));
-                float dac = fmaf(-x, rcx, fmaf(-y, rcy, z2));
-                float dbc = fmaf(rbx, rcx, fmaf(-y, rcy, z2));
-                float den = la * lb * lc + dab * lc + dac * lb + dbc * la;
-                float om = 2.f * atan2f(-z * A2, den);
-                float s11 = fmaf(rbx, e1x, -y * e1y), s12 = fmaf(rcx, e1x, rcy * e1y);
-                float s21 = fmaf(rcx, e2x, rcy * e2y), s22 = fmaf(-x, e2x, -y * e2y);
-                float l0 = lam_f32(-x, rbx, la, lb, L0);
-                float l1 = lam_f32(s11, s12, lb, lc, L1);
-                float l2 = lam_f32(s21, s22, lc, la, L2);
-                float ia = 1.f / la, ib = 1.f / lb, ic = 1.f / lc;
-                float kom = Ts * mf;
-                // edge (p1 -> p2): W = L / (d1 d2 + r1.r2), q = r1 - s1 e, Z = e x r1,
-                // P = W (kom Z - kl q); p1 += (P - kl e)/d1, p2 += (P + kl e)/d2
-                auto edge = [&](float r1x, float r1y, float r2x, float r2y, float d1, float d2, float ex, float ey,
-                                float L, float s1, float kl, float i1, float i2, float& g1x, float& g1y, float& g1z,
-                                float& g2x, float& g2y, float& g2z) {
-                    float W = L / fmaf(d1, d2, fmaf(r1x, r2x, fmaf(r1y, r2y, z2)));
-                    float qxv = fmaf(-s1, ex, r1x), qyv = fmaf(-s1, ey, r1y), qzv = -z;
-                    float Zx = -ey * z, Zy = ex * z, Zz = fmaf(ex, r1y, -ey * r1x);  // e x r1, r1.z = -z
-                    float Px = W * fmaf(kom, Zx, -kl * qxv), Py = W * fmaf(kom, Zy, -kl * qyv),
-                          Pz = W * fmaf(kom, Zz, -kl * qzv);
-                    g1x = fmaf(fmaf(-kl, ex, Px), i1, g1x); g1y = fmaf(fmaf(-kl, ey, Py), i1, g1y); g1z = fmaf(Pz, i1, g1z);
-                    g2x = fmaf(fmaf(kl, ex, Px), i2, g2x); g2y = fmaf(fmaf(kl, ey, Py), i2, g2y); g2z = fmaf(Pz, i2, g2z);
-                };
-                edge(-x, -y, rbx, -y, la, lb, 1.f, 0.f, L0, -x, Ts * mt0, ia, ib, vax, vay, vaz, vbx, vby, vbz);
-                edge(rbx, -y, rcx, rcy, lb, lc, e1x, e1y, L1, s11, Ts * mt1, ib, ic, vbx, vby, vbz, vcx, vcy, vcz);
-                edge(rcx, rcy, -x, -y, lc, la, e2x, e2y, L2, s21, Ts * mt2, ic, ia, vcx, vcy, vcz, vax, vay, vaz);
-                amf = fmaf(Ts, om, amf);
-                amt0 = fmaf(Ts, l0, amt0); amt1 = fmaf(Ts, l1, amt1); amt2 = fmaf(Ts, l2, amt2);
-            }
-        }
-        // flush the tile into the FP64 accumulators (local frame)
-        const double nz = C[GC_ZZ];
-        const double Ar = 0.5 * C[GC_L0] * C[GC_CY];
-        double sa[3] = {0, 0, 0}, sbv[3] = {0, 0, 0}, sc[3] = {0, 0, 0};
+                v[0] = q0;
+                v[1] = sa0; v[2] = sa1; v[3] = sa2;
+                v[4] = sb0; v[5] = sb1; v[6] = sb2;
+                v[7] = sc0; v[8] = sc1; v[9] = sc2;
+                v[10] = vax; v[11] = vay; v[12] = vaz;
+                v[13] = vbx; v[14] = vby; v[15] = vbz;
+                v[16] = vcx; v[17] = vcy; v[18] = vcz;
+                v[19] = amf; v[20] = amt0; v[21] = amt1; v[22] = amt2;
 #pragma unroll
-        for (int q = 0; q < 7; ++q) {
-            double bb = kRadonBb[q], bc = kRadonBc[q], ba = 1.0 - bb - bc;
-            sa[0] += ba * dqx[q]; sa[1] += ba * dqy[q]; sa[2] += ba * dqz[q];
-            sbv[0] += bb * dqx[q]; sbv[1] += bb * dqy[q]; sbv[2] += bb * dqz[q];
-            sc[0] += bc * dqx[q]; sc[1] += bc * dqy[q]; sc[2] += bc * dqz[q];
+                for (int k = kFarTerms; k < 32; ++k) v[k] = 0.f;
+                tot += (double)warp_transpose_sum32(v);
+                q0 = 0.f;
+                vax = vay = vaz = vbx = vby = vbz = vcx = vcy = vcz = 0.f;
+                amf = amt0 = amt1 = amt2 = 0.f;
+            };
+            const int ntiles = (S + kStationTile - 1) / kStationTile;
+            const FarKey key = facet_far_key(C, tau);
+            for (int t0 = 0; t0 < ntiles; t0 += 32) {
+                const int t = t0 + lane;
+                const bool farT = t < ntiles && tile_far(key, tile_box + 6 * (size_t)t);
+                unsigned m = __ballot_sync(0xffffffffu, farT);
+                any |= m != 0;
+                while (m) {
+                    const int b = __ffs(m) - 1;
+                    m &= m - 1;
+                    const int s0 = (t0 + b) * kStationTile;
+#pragma unroll
+                    for (int k = 0; k < kStationTile; k += 32) {
+                        const int j = s0 + k + lane;
+                        float G0 = 0.f, Ts = 0.f;
+                        double ox = 0.0, oy = 0.0, oz = 0.0;
+                        if (j < S) {
+                            G0 = (float)((gcoef ? gcoef[j] : 0.0) * gsn);
+                            Ts = (float)((mcoef ? mcoef[j] : 0.0) * ms);
+                            ox = sta[3 * j]; oy = sta[3 * j + 1]; oz = sta[3 * j + 2];
+                        }
+                        if (G0 == 0.f && Ts == 0.f) continue;
+                        const double ddx = ox - ax, ddy = oy - ay, ddz = oz - az;
+                        const float dx = (float)ddx, dy = (float)ddy, dzf = (float)ddz;
+                        const float x = fmaf(dx, rx0, fmaf(dy, rx1, dzf * rx2));
+                        const float y = fmaf(dx, ry0, fmaf(dy, ry1, dzf * ry2));
+                        const float z = (float)(ddx * zx + ddy * zy + ddz * zz);
+                        const float z2 = z * z;
+                        if (G0 != 0.f) {
+                            float sw = 0.f;
+#pragma unroll
+                            for (int q = 0; q < 7; ++q) {
+                                const float px = qx[q] - x, py = qy[q] - y;
+                                const float rs = rsqrtf(fmaf(px, px, fmaf(py, py, z2)));
+                                const float w = kRadonW[q] * rs;
+                                sw += w;
+                                const float g3 = G0 * w * rs * rs;
+                                dqx[q] = fmaf(g3, px, dqx[q]);
+                                dqy[q] = fmaf(g3, py, dqy[q]);
+                                dqz[q] = fmaf(g3, -z, dqz[q]);
+                            }
+                            q0 = fmaf(G0, sw, q0);
+                        }
+                        if (Ts != 0.f) {
+                            const float rbx = L0 - x, rcx = cx - x, rcy = cy - y;
+                            const float la = sqrtf(fmaf(x, x, fmaf(y, y, z2)));
+                            const float lb = sqrtf(fmaf(rbx, rbx, fmaf(y, y, z2)));
+                            const float lc = sqrtf(fmaf(rcx, rcx, fmaf(rcy, rcy, z2)));
+                            const float dab = fmaf(-x, rbx, fmaf(y, y, z2));
+                            const float dac = fmaf(-x, rcx, fmaf(-y, rcy, z2));
+                            const float dbc = fmaf(rbx, rcx, fmaf(-y, rcy, z2));
+                            const float den = la * lb * lc + dab * lc + dac * lb + dbc * la;
+                            const float om = 2.f * atan2f(-z * A2, den);
+                            const float s11 = fmaf(rbx, e1x, -y * e1y), s12 = fmaf(rcx, e1x, rcy * e1y);
+                            const float s21 = fmaf(rcx, e2x, rcy * e2y), s22 = fmaf(-x, e2x, -y * e2y);
+                            const float l0 = lam_f32(-x, rbx, la, lb, L0);
+                            const float l1 = lam_f32(s11, s12, lb, lc, L1);
+                            const float l2 = lam_f32(s21, s22, lc, la, L2);
+                            const float ia = 1.f / la, ib = 1.f / lb, ic = 1.f / lc;
+                            const float kom = Ts * mf;
+                            // edge (p1 -> p2): W = L / (d1 d2 + r1.r2), q = r1 - s1 e, Z = e x r1,
+                            // P = W (kom Z - kl q); p1 += (P - kl e)/d1, p2 += (P + kl e)/d2
+                            auto edge = [&](float r1x, float r1y, float r2x, float r2y, float d1, float d2, float ex,
+                                            float ey, float L, float s1, float kl, float i1, float i2, float& g1x,
+                                            float& g1y, float& g1z, float& g2x, float& g2y, float& g2z) {
+                                const float W = L / fmaf(d1, d2, fmaf(r1x, r2x, fmaf(r1y, r2y, z2)));
+                                const float qxv = fmaf(-s1, ex, r1x), qyv = fmaf(-s1, ey, r1y), qzv = -z;
+                                const float Zx = -ey * z, Zy = ex * z, Zz = fmaf(ex, r1y, -ey * r1x);  // e x r1
+                                const float Px = W * fmaf(kom, Zx, -kl * qxv), Py = W * fmaf(kom, Zy, -kl * qyv),
+                                            Pz = W * fmaf(kom, Zz, -kl * qzv);
+                                g1x = fmaf(fmaf(-kl, ex, Px), i1, g1x);
+                                g1y = fmaf(fmaf(-kl, ey, Py), i1, g1y);
+                                g1z = fmaf(Pz, i1, g1z);
+                                g2x = fmaf(fmaf(kl, ex, Px), i2, g2x);
+                                g2y = fmaf(fmaf(kl, ey, Py), i2, g2y);
+                                g2z = fmaf(Pz, i2, g2z);
+                            };
+                            edge(-x, -y, rbx, -y, la, lb, 1.f, 0.f, L0, -x, Ts * mt0, ia, ib, vax, vay, vaz, vbx, vby,
+                                 vbz);
+                            edge(rbx, -y, rcx, rcy, lb, lc, e1x, e1y, L1, s11, Ts * mt1, ib, ic, vbx, vby, vbz, vcx,
+                                 vcy, vcz);
+                            edge(rcx, rcy, -x, -y, lc, la, e2x, e2y, L2, s21, Ts * mt2, ic, ia, vcx, vcy, vcz, vax,
+                                 vay, vaz);
+                            amf = fmaf(Ts, om, amf);
+                            amt0 = fmaf(Ts, l0, amt0);
+                            amt1 = fmaf(Ts, l1, amt1);
+                            amt2 = fmaf(Ts, l2, amt2);
+                        }
+                    }
+                    if (++pending == kFarFlushTiles) {
+                        flush();
+                        pending = 0;
+                    }
+                }
+            }
+            if (pending) flush();
         }
-        const double cxd = C[GC_CX], cyd = C[GC_CY], L0d = C[GC_L0];
-        // dA/da = (-cy, cx - L0, 0)/2, dA/db = (cy, -cx, 0)/2, dA/dc = (0, L0, 0)/2
-        A.va = A.va + mk3(nz * (-0.5 * cyd * q0 - Ar * sa[0]) + vax, nz * (0.5 * (cxd - L0d) * q0 - Ar * sa[1]) + vay,
-                          nz * (-Ar * sa[2]) + vaz);
-        A.vb = A.vb + mk3(nz * (0.5 * cyd * q0 - Ar * sbv[0]) + vbx, nz * (-0.5 * cxd * q0 - Ar * sbv[1]) + vby,
-                          nz * (-Ar * sbv[2]) + vbz);
-        A.vc = A.vc + mk3(nz * (-Ar * sc[0]) + vcx, nz * (0.5 * L0d * q0 - Ar * sc[1]) + vcy, nz * (-Ar * sc[2]) + vcz);
-        A.ai += Ar * q0;
-        A.amf += amf;
-        A.amt[0] += amt0; A.amt[1] += amt1; A.amt[2] += amt2;
     }
-    if (f >= T) return;
-    double outv[9];
-    if (!active) {
-        for (int k = 0; k < 9; ++k) outv[k] = 0.0;
-    } else {
-        grad_finalize(C, A, groups[face_group[f]], fdir, outv);
+    double outv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (active && any) {
+        double v[kFarTerms];
+#pragma unroll
+        for (int k = 0; k < kFarTerms; ++k) v[k] = __shfl_sync(0xffffffffu, tot, k);
+        if (lane == 0) {
+            double C[NGC];
+#pragma unroll
+            for (int k = 0; k < NGC; ++k) C[k] = __ldcg(&gc[(size_t)k * T + f]);
+            const double nz = C[GC_ZZ], L0 = C[GC_L0], cx = C[GC_CX], cy = C[GC_CY];
+            const double Ar = 0.5 * L0 * cy, q0 = v[0];
+            // dA/da = (-cy, cx - L0, 0)/2, dA/db = (cy, -cx, 0)/2, dA/dc = (0, L0, 0)/2
+            GradAcc A;
+            grad_acc_zero(A);
+            A.va = mk3(nz * (-0.5 * cy * q0 - Ar * v[1]) + v[10], nz * (0.5 * (cx - L0) * q0 - Ar * v[2]) + v[11],
+                       nz * (-Ar * v[3]) + v[12]);
+            A.vb = mk3(nz * (0.5 * cy * q0 - Ar * v[4]) + v[13], nz * (-0.5 * cx * q0 - Ar * v[5]) + v[14],
+                       nz * (-Ar * v[6]) + v[15]);
+            A.vc = mk3(nz * (-Ar * v[7]) + v[16], nz * (0.5 * L0 * q0 - Ar * v[8]) + v[17], nz * (-Ar * v[9]) + v[18]);
+            A.ai = Ar * q0;
+            A.amf = v[19];
+            A.amt[0] = v[20]; A.amt[1] = v[21]; A.amt[2] = v[22];
+            grad_finalize(C, A, groups[face_group[f]], fdir, outv);
+        }
     }
-    for (int k = 0; k < 9; ++k) part[((size_t)chunk * 9 + k) * T + f] = outv[k];
+    if (lane == 0)
+        for (int k = 0; k < 9; ++k) part[(size_t)k * T + f] = outv[k];
 }
 
 // Per station: sum of chunk partials (facet scales are already applied).
