@@ -11,6 +11,11 @@ to every DOF (analytic vertex derivatives contracted with the weighted
 residuals; the Jacobian is never formed).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--precision mixed|fp64]
+
+Precision: `mixed` (default) evaluates far and mid-field station-facet
+pairs in FP32 and near ones in FP64 (gz/TMI within 1e-6, gradient within
+1e-5 of the FP64 path); `fp64` evaluates every pair in FP64.
 
 Prints one JSON line on rank 0.  `value` is whole-job evaluations/s with the
 parameter vector resident in HBM; `e2e` is the same through the C ABI with
@@ -43,8 +48,23 @@ L2_FLUSH_BYTES = 256 << 20
 #   3 log, 1 atan2.
 FLOPS_FWD_PAIR = 137
 FLOPS_GRAD_PAIR = 331
-# FP64 CUDA-core peak of a B200 (nominal): 148 SMs x 64 FP64 FMA/clk x 2 x 1.965 GHz.
-FP64_PEAK_TFLOPS_NOMINAL = 148 * 64 * 2 * 1.965e9 / 1e12
+SFU_FWD_PAIR = 16   # 3 sqrt + 9 div + 3 log + 1 atan2, one special-function op each
+SFU_GRAD_PAIR = 16
+# Nominal B200 CUDA-core rates at the 1.965 GHz boost clock (no measured
+# figure for these pipes exists in MEASURED_PEAKS.json): FP32 148 SMs x 128
+# lanes x 2 flop; special-function unit 148 x 16 ops; FP64 148 x 64 x 2 flop.
+CLOCK_HZ = 1.965e9
+FP32_PEAK_FLOPS = 148 * 128 * 2 * CLOCK_HZ
+SFU_PEAK_OPS = 148 * 16 * CLOCK_HZ
+FP64_PEAK_FLOPS = 148 * 64 * 2 * CLOCK_HZ
+
+
+def pair_roofline(flops: int, sfu: int, precision: str) -> float:
+    """Roofline of one station-facet pair in pairs/s: the FP32 pipe or the
+    special-function unit, whichever binds (FP64 pipe in FP64 mode)."""
+    if precision == "fp64":
+        return FP64_PEAK_FLOPS / flops
+    return min(FP32_PEAK_FLOPS / flops, SFU_PEAK_OPS / sfu)
 
 
 def parse():
@@ -53,7 +73,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-stations", type=int, default=48)
     return ap.parse_args()
@@ -365,21 +385,27 @@ def main():
     value = world * args.steps / (total_ms / 1e3)
     e2e_value = world * args.steps / (e2e_ms / 1e3)
 
-    # dominant kernel roofline (FP64 CUDA-core pipe)
+    # dominant kernel roofline: pairs/s against the pipe that binds the
+    # algorithmic per-pair work (FP32 or special-function unit in mixed mode,
+    # FP64 in FP64 mode), reported as flop-equivalents
     grad_per_launch_ms = grad_ms / max(grad_n, 1)
     fwd_per_launch_ms = fwd_ms / max(fwd_n, 1)
+    pps_fwd = pairs_fwd / max(fwd_ms / 1e3, 1e-12)
+    pps_grad = pairs_grad / max(grad_ms / 1e3, 1e-12)
     if grad_ms >= fwd_ms:
-        kname, kms, kflops = "k_gradient_fp64", grad_per_launch_ms, FLOPS_GRAD_PAIR * pairs_grad / max(grad_n, 1)
+        kname = "k_gradient_warp_fp64 + k_gradient_warp_far32" if args.precision == "mixed" else "k_gradient_warp_fp64"
+        kms, pps, flops, sfu = grad_per_launch_ms, pps_grad, FLOPS_GRAD_PAIR, SFU_GRAD_PAIR
     else:
-        kname, kms, kflops = "k_forward_fp64", fwd_per_launch_ms, FLOPS_FWD_PAIR * pairs_fwd / max(fwd_n, 1)
-    achieved = kflops / (kms / 1e3) / 1e12
-    roofline = {"bound": "fp64", "kernel": kname, "achieved": achieved, "peak": FP64_PEAK_TFLOPS_NOMINAL,
-                "unit": "TFLOP/s", "frac": achieved / FP64_PEAK_TFLOPS_NOMINAL, "traffic": None,
-                "peak_source": "nominal FP64 CUDA-core rate (148 SMs x 64 FMA/clk x 1.965 GHz); "
-                               "no measured FP64 peak in MEASURED_PEAKS.json",
-                "kernel_ms_per_launch": kms,
-                "pairs_per_s": {"forward": pairs_fwd / max(fwd_ms / 1e3, 1e-12),
-                                "gradient": pairs_grad / max(grad_ms / 1e3, 1e-12)}}
+        kname = "k_forward_mixed" if args.precision == "mixed" else "k_forward_fp64"
+        kms, pps, flops, sfu = fwd_per_launch_ms, pps_fwd, FLOPS_FWD_PAIR, SFU_FWD_PAIR
+    peak_pps = pair_roofline(flops, sfu, args.precision)
+    roofline = {"bound": "fp64" if args.precision == "fp64" else "fp32+sfu", "kernel": kname,
+                "achieved": pps * flops / 1e12, "peak": peak_pps * flops / 1e12, "unit": "TFLOP/s",
+                "frac": pps / peak_pps, "traffic": None,
+                "peak_source": ("nominal CUDA-core rates at 1.965 GHz (FP32 74.4 TFLOP/s, SFU 4.65 Tops/s, "
+                                "FP64 37.2 TFLOP/s); MEASURED_PEAKS.json holds only HBM and bf16 GEMM figures"),
+                "flops_per_pair": flops, "sfu_ops_per_pair": sfu, "kernel_ms_per_launch": kms,
+                "pairs_per_s": {"forward": pps_fwd, "gradient": pps_grad}}
 
     line = {"metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",

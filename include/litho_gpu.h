@@ -232,8 +232,10 @@ lf_status lf_lbfgsb_minimize(lf_ctx* ctx, const double* x0, const double* lower,
                              const double* upper, const lf_lbfgsb_options* opt, double* x_out,
                              lf_lbfgsb_result* result);
 
-/* Work counters: station-facet pairs evaluated by the forward and gradient
- * kernels since the last reset, and kernel launches. */
+/* Work counters since the last reset: station-facet pairs evaluated by the
+ * forward (every facet) and by the gradient (facets with at least one
+ * DOF-referenced vertex; the others have no derivative to contribute), and
+ * kernel launches. */
 typedef struct {
     uint64_t forward_pairs, gradient_pairs, launches;
 } lf_counters;

@@ -91,7 +91,7 @@ struct lf_ctx {
     DevBuf<double> d_refScale, d_interpW;
     DevBuf<int16_t> d_faceGroup;
     DevBuf<GroupConst> d_groups;
-    int nInterpRows = 0, nSync = 0, nGradVerts = 0;
+    int nInterpRows = 0, nSync = 0, nGradVerts = 0, nGradFacets = 0;
 
     // forward chunking
     std::vector<int32_t> chunkBegin, chunkEnd, chunkGroup;
@@ -506,6 +506,8 @@ extern "C" lf_status lf_set_model_tables(lf_ctx* c, int G, const double* density
     for (int f = 0; f < nt; ++f)
         fneed[f] = vneed[tri[3 * f]] | vneed[tri[3 * f + 1]] | vneed[tri[3 * f + 2]];
     c->nGradVerts = static_cast<int>(gverts.size());
+    c->nGradFacets = 0;
+    for (int f = 0; f < nt; ++f) c->nGradFacets += fneed[f];
     LF_TRY_CUDA(c, upload(c->d_gradVerts, gverts.data(), gverts.size(), c->stream));
     LF_TRY_CUDA(c, upload(c->d_faceNeeds, fneed.data(), fneed.size(), c->stream));
     LF_TRY_CUDA(c, c->d_fc.reserve((size_t)NFC * nt));
@@ -844,7 +846,7 @@ static int gradient_set(lf_ctx* c, const StationSet& s, const double* gcoef, con
         prof_end(c, c->evGrad, ev2);
         c->counters.launches++;
     }
-    c->counters.gradient_pairs += (uint64_t)s.n * (uint64_t)c->T;
+    c->counters.gradient_pairs += (uint64_t)s.n * (uint64_t)c->nGradFacets;
     return mixed ? 2 : 1;
 }
 

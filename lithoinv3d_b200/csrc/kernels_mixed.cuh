@@ -54,6 +54,26 @@ __constant__ float kRadonBc[7] = {0.3333333333333333f, 0.1012865073234563f, 0.10
 __constant__ float kRadonW[7] = {0.225f, 0.1259391805448271f, 0.1259391805448271f, 0.1259391805448271f,
                                  0.1323941527885062f, 0.1323941527885062f, 0.1323941527885062f};
 
+// The same rule on the four midpoint sub-triangles (a, ab, ca), (ab, b, bc),
+// (ca, bc, c), (ab, bc, ca): 28 points in the parent's barycentric (beta_b,
+// beta_c), weights kRadonW[q % 7] / 4.  Its error at distance ratio tau/2
+// matches the 7-point rule's at tau (degree-5 error ~ (size / distance)^6),
+// so it takes the mid field tau/2 <= distance / size < tau in FP32.
+__constant__ float kRadon4Bb[28] = {
+    0.1666666666666667f, 0.0506432536617282f, 0.3987134926765437f, 0.0506432536617282f, 0.2350710320525576f,
+    0.0298579358948849f, 0.2350710320525576f, 0.6666666666666666f, 0.5506432536617281f, 0.8987134926765437f,
+    0.5506432536617281f, 0.7350710320525575f, 0.5298579358948849f, 0.7350710320525576f, 0.1666666666666667f,
+    0.0506432536617282f, 0.3987134926765437f, 0.0506432536617282f, 0.2350710320525576f, 0.0298579358948849f,
+    0.2350710320525576f, 0.3333333333333334f, 0.4493567463382718f, 0.4493567463382718f, 0.1012865073234563f,
+    0.2649289679474425f, 0.2649289679474425f, 0.4701420641051152f};
+__constant__ float kRadon4Bc[28] = {
+    0.1666666666666667f, 0.0506432536617282f, 0.0506432536617282f, 0.3987134926765437f, 0.2350710320525576f,
+    0.2350710320525576f, 0.0298579358948849f, 0.1666666666666667f, 0.0506432536617282f, 0.0506432536617282f,
+    0.3987134926765437f, 0.2350710320525576f, 0.2350710320525576f, 0.0298579358948849f, 0.6666666666666667f,
+    0.5506432536617282f, 0.5506432536617282f, 0.8987134926765437f, 0.7350710320525575f, 0.7350710320525575f,
+    0.5298579358948849f, 0.3333333333333333f, 0.1012865073234563f, 0.4493567463382718f, 0.4493567463382718f,
+    0.4701420641051151f, 0.2649289679474425f, 0.2649289679474425f};
+
 __global__ void k_face_prep_mixed(int T, const int32_t* __restrict__ tri, const double* __restrict__ pos,
                                   const int16_t* __restrict__ face_group, const GroupConst* __restrict__ groups, d3 fdir,
                                   double* __restrict__ mc) {
@@ -122,53 +142,112 @@ __global__ void k_face_prep_mixed(int T, const int32_t* __restrict__ tri, const 
 }
 
 // ----------------------------------------------------------- FP32 pieces --
+// sqrt for arguments known to be positive and normal (far-field distances):
+// r2 * rsqrt(r2), within 2 ulp.
+__device__ __forceinline__ float sqrt_pos(float r2) { return r2 * rsqrtf(r2); }
+
 // Lambda in the orientation without the d + s cancellation:
 // forward  log((s2+d2)/(s1+d1)) = log1p((L + sigma)/(s1 + d1)),
 // reverse  log((d1-s1)/(d2-s2)) = log1p((L - sigma)/(d2 - s2)),
-// sigma = d2 - d1 = L (s1 + s2) / (d1 + d2).
+// sigma = d2 - d1 = L (s1 + s2) / (d1 + d2).  log1p(u) = 2 atanh(v) with
+// v = u / (2 + u) = delta / (2 den + delta); for v <= 0.2 (every far pair:
+// u <= 0.5) the series 2 (v + v^3/3 + ... + v^9/9) (Abramowitz & Stegun
+// 4.1.28), whose first omitted term is below 2e-9 v, else log1pf.  Far-field
+// arguments are bounded away from zero and overflow, so 2-ulp quotients are
+// used.
 __device__ __forceinline__ float lam_f32(float s1, float s2, float d1, float d2, float L) {
     float ss = s1 + s2;
-    float sig = L * ss / (d1 + d2);
+    float sig = __fdividef(L * ss, d1 + d2);
     float delta, den;
     if (ss >= 0.f) { delta = L + sig; den = s1 + d1; }
     else           { delta = L - sig; den = d2 - s2; }
-    return log1pf(delta / den);
+    const float v = __fdividef(delta, fmaf(2.f, den, delta));
+    if (v <= 0.2f) {
+        const float v2 = v * v;
+        const float p = fmaf(v2, fmaf(v2, fmaf(v2, fmaf(v2, 1.f / 9.f, 1.f / 7.f), 1.f / 5.f), 1.f / 3.f), 1.f);
+        return 2.f * v * p;
+    }
+    return log1pf(__fdividef(delta, den));
 }
 
-struct FaceF32 {
-    float rx[3], ry[3], rz[3];  // rows of the local frame
-    float L0, cx, cy, e1x, e1y, L1, e2x, e2y, L2;
-    float gq;                   // n_z * gscale * area (quadrature scale)
-    float mf, mt0, mt1, mt2;
-    float qx[7], qy[7];         // quadrature points in the local frame
-};
+// atan2(y, x); for x > 0 and |y| <= x / 8 (every far pair's solid angle) the
+// Maclaurin series of atan(t), t = y / x, through t^9 (Abramowitz & Stegun
+// 4.4.42; first omitted term below 1e-10 t), else atan2f.
+__device__ __forceinline__ float atan2_far(float y, float x) {
+    if (x > 0.f && fabsf(y) <= 0.125f * x) {
+        const float t = __fdividef(y, x), t2 = t * t;
+        const float p = fmaf(t2, fmaf(t2, fmaf(t2, fmaf(t2, 1.f / 9.f, -1.f / 7.f), 1.f / 5.f), -1.f / 3.f), 1.f);
+        return t * p;
+    }
+    return atan2f(y, x);
+}
 
-// Far pair: gz by quadrature, TMI analytic, both FP32.  (x, y, z): station
-// in the facet's local frame.
-__device__ __forceinline__ void pair_far_f32(const FaceF32& F, float x, float y, float z, float* gz, float* tmi) {
-    float z2 = z * z;
+// FP32 facet record of the far-field forward, staged in shared memory and
+// read with 128-bit loads (12 per pair).  The origin and the unit normal stay
+// FP64: the height above the facet plane can be tiny next to |o - a| (a far
+// top facet seen from 1 m above it).
+struct __align__(16) FaceF32 {
+    float rx0, rx1, rx2, L0;   // local x axis, |ab|
+    float ry0, ry1, ry2, cx;   // local y axis, c.x
+    float cy, e1x, e1y, L1;    // c.y, edge b->c
+    float e2x, e2y, L2, gq;    // edge c->a, n_z * gz scale * area
+    float mf, mt0, mt1, mt2;   // TMI facet scales
+    float qx[8], qy[8];        // Radon points in the local frame (7 + pad)
+    double ax, ay, az, zx, zy, zz;
+};
+static_assert(sizeof(FaceF32) == 192, "FaceF32 layout");
+
+// Far pair: gz by quadrature (7 points; MID: 28 points on the midpoint
+// subdivision), TMI analytic, both FP32; o = station (FP64).
+template <bool MID>
+__device__ __forceinline__ void pair_far_f32(const FaceF32* Fp, double ox, double oy, double oz, float* gz,
+                                             float* tmi) {
+    const float4* v = reinterpret_cast<const float4*>(Fp);
+    const double2* w = reinterpret_cast<const double2*>(Fp);
+    const float4 v0 = v[0], v1 = v[1], v2 = v[2], v3 = v[3], v4 = v[4];
+    const double2 w0 = w[9], w1 = w[10], w2 = w[11];
+    const double ddx = ox - w0.x, ddy = oy - w0.y, ddz = oz - w1.x;
+    const float dx = (float)ddx, dy = (float)ddy, dz = (float)ddz;
+    const float x = fmaf(dx, v0.x, fmaf(dy, v0.y, dz * v0.z));
+    const float y = fmaf(dx, v1.x, fmaf(dy, v1.y, dz * v1.z));
+    const float z = (float)(ddx * w1.y + ddy * w2.x + ddz * w2.y);
+    const float L0 = v0.w, cx = v1.w, cy = v2.x, e1x = v2.y, e1y = v2.z, L1 = v2.w;
+    const float e2x = v3.x, e2y = v3.y, L2 = v3.z, gq = v3.w;
+    const float z2 = z * z;
     // gz: n_z * gscale * A * sum_q w_q / r_q
     float acc = 0.f;
+    if (MID) {
 #pragma unroll
-    for (int q = 0; q < 7; ++q) {
-        float dx = F.qx[q] - x, dy = F.qy[q] - y;
-        acc = fmaf(kRadonW[q], rsqrtf(fmaf(dx, dx, fmaf(dy, dy, z2))), acc);
+        for (int q = 0; q < 28; ++q) {
+            float px = fmaf(kRadon4Bb[q], L0, fmaf(kRadon4Bc[q], cx, -x)), py = fmaf(kRadon4Bc[q], cy, -y);
+            acc = fmaf(kRadonW[q % 7], rsqrtf(fmaf(px, px, fmaf(py, py, z2))), acc);
+        }
+        acc *= 0.25f;
+    } else {
+        const float4 qa = v[5], qb = v[6], qc = v[7], qd = v[8];
+        const float qx[7] = {qa.x, qa.y, qa.z, qa.w, qb.x, qb.y, qb.z};
+        const float qy[7] = {qc.x, qc.y, qc.z, qc.w, qd.x, qd.y, qd.z};
+#pragma unroll
+        for (int q = 0; q < 7; ++q) {
+            float px = qx[q] - x, py = qy[q] - y;
+            acc = fmaf(kRadonW[q], rsqrtf(fmaf(px, px, fmaf(py, py, z2))), acc);
+        }
     }
-    *gz += F.gq * acc;
+    *gz += gq * acc;
     // TMI: MF * Omega + sum_i MT_i Lambda_i
-    float rbx = F.L0 - x, rcx = F.cx - x, rcy = F.cy - y;
-    float la = sqrtf(fmaf(x, x, fmaf(y, y, z2)));
-    float lb = sqrtf(fmaf(rbx, rbx, fmaf(y, y, z2)));
-    float lc = sqrtf(fmaf(rcx, rcx, fmaf(rcy, rcy, z2)));
+    float rbx = L0 - x, rcx = cx - x, rcy = cy - y;
+    float la = sqrt_pos(fmaf(x, x, fmaf(y, y, z2)));
+    float lb = sqrt_pos(fmaf(rbx, rbx, fmaf(y, y, z2)));
+    float lc = sqrt_pos(fmaf(rcx, rcx, fmaf(rcy, rcy, z2)));
     float dab = fmaf(-x, rbx, fmaf(y, y, z2));
     float dac = fmaf(-x, rcx, fmaf(-y, rcy, z2));
     float dbc = fmaf(rbx, rcx, fmaf(-y, rcy, z2));
     float den = la * lb * lc + dab * lc + dac * lb + dbc * la;
-    float om = 2.f * atan2f(-z * (F.L0 * F.cy), den);
-    float l0 = lam_f32(-x, rbx, la, lb, F.L0);
-    float l1 = lam_f32(fmaf(rbx, F.e1x, -y * F.e1y), fmaf(rcx, F.e1x, rcy * F.e1y), lb, lc, F.L1);
-    float l2 = lam_f32(fmaf(rcx, F.e2x, rcy * F.e2y), fmaf(-x, F.e2x, -y * F.e2y), lc, la, F.L2);
-    *tmi += F.mf * om + F.mt0 * l0 + F.mt1 * l1 + F.mt2 * l2;
+    float om = 2.f * atan2_far(-z * (L0 * cy), den);
+    float l0 = lam_f32(-x, rbx, la, lb, L0);
+    float l1 = lam_f32(fmaf(rbx, e1x, -y * e1y), fmaf(rcx, e1x, rcy * e1y), lb, lc, L1);
+    float l2 = lam_f32(fmaf(rcx, e2x, rcy * e2y), fmaf(-x, e2x, -y * e2y), lc, la, L2);
+    *tmi += v4.x * om + v4.y * l0 + v4.z * l1 + v4.w * l2;
 }
 
 // Near pair in FP64, local frame, with the reference's lineIntegralTerm and
@@ -204,45 +283,40 @@ __device__ __forceinline__ void pair_near_f64(const double* __restrict__ s, int 
 #undef M
 }
 
-// Station tiles of 128 (stations pre-ordered along a Morton curve so a tile
-// is spatially compact) x facet chunks.  A facet is far for the whole tile
-// when its centroid is at least tau x size from the tile's bounding box.
+// Station-per-thread forward: CTAs of 128 stations (pre-ordered along a
+// Morton curve, so a warp's 32 stations are spatially compact) x facet
+// chunks, facets staged 32 at a time in shared memory.  The precision class
+// is decided per (warp, facet): lane j tests facet j of the stage against the
+// warp's station bounding box -- centroid at least tau x size away: far
+// (FP32, 7-point gz); at least tau/2 x size: mid (FP32, 28-point gz); else
+// near (FP64 analytic) -- and the warp walks each class warp-uniformly.
 template <bool GZ, bool TMI, int FT>
 __global__ void __launch_bounds__(128) k_forward_mixed(int S, const double* __restrict__ sta, int T,
                                                        const double* __restrict__ mc, const int32_t* __restrict__ chunk_begin,
                                                        const int32_t* __restrict__ chunk_end, float tau,
                                                        double* __restrict__ part_gz, double* __restrict__ part_tmi,
                                                        unsigned long long* __restrict__ near_pairs) {
+    static_assert(FT == 32, "one facet per lane in the near/far test");
     __shared__ double smd[NMC * FT];
     __shared__ FaceF32 smf[FT];
-    __shared__ float bbox[6];
-    __shared__ float red[6][4];
-    int s = blockIdx.x * blockDim.x + threadIdx.x;
-    int chunk = blockIdx.y;
-    int fb = chunk_begin[chunk], fe = chunk_end[chunk];
-    d3 o = mk3(0, 0, 0);
-    bool act = s < S;
-    if (act) o = mk3(sta[3 * s], sta[3 * s + 1], sta[3 * s + 2]);
-    // tile bounding box (warp shuffles, then across the 4 warps)
-    {
-        float v[6] = {act ? (float)o.x : 3e38f, act ? (float)o.y : 3e38f, act ? (float)o.z : 3e38f,
-                      act ? -(float)o.x : 3e38f, act ? -(float)o.y : 3e38f, act ? -(float)o.z : 3e38f};
-        for (int k = 0; k < 6; ++k)
-            for (int off = 16; off > 0; off >>= 1) v[k] = fminf(v[k], __shfl_xor_sync(0xffffffffu, v[k], off));
-        int w = threadIdx.x >> 5;
-        if ((threadIdx.x & 31) == 0)
-            for (int k = 0; k < 6; ++k) red[k][w] = v[k];
-        __syncthreads();
-        if (threadIdx.x < 6) {
-            float m = red[threadIdx.x][0];
-            for (int q = 1; q < (int)(blockDim.x >> 5); ++q) m = fminf(m, red[threadIdx.x][q]);
-            bbox[threadIdx.x] = threadIdx.x < 3 ? m : -m;
-        }
-    }
+    const int lane = threadIdx.x & 31;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const int chunk = blockIdx.y;
+    const int fb = chunk_begin[chunk], fe = chunk_end[chunk];
+    const bool act = s < S;
+    double ox = 0.0, oy = 0.0, oz = 0.0;
+    if (act) { ox = sta[3 * s]; oy = sta[3 * s + 1]; oz = sta[3 * s + 2]; }
+    // the warp's station bounding box: lo = min, hi = -min(-x)
+    float bb[6] = {act ? (float)ox : 3e38f, act ? (float)oy : 3e38f, act ? (float)oz : 3e38f,
+                   act ? -(float)ox : 3e38f, act ? -(float)oy : 3e38f, act ? -(float)oz : 3e38f};
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) bb[k] = fminf(bb[k], __shfl_xor_sync(0xffffffffu, bb[k], off));
     double gz = 0.0, tmi = 0.0;
     unsigned long long nearCount = 0;
     for (int f0 = fb; f0 < fe; f0 += FT) {
-        int nf = min(FT, fe - f0);
+        const int nf = min(FT, fe - f0);
         __syncthreads();
         for (int idx = threadIdx.x; idx < NMC * FT; idx += blockDim.x) {
             int k = idx / FT, j = idx % FT;
@@ -252,57 +326,61 @@ __global__ void __launch_bounds__(128) k_forward_mixed(int S, const double* __re
         for (int j = threadIdx.x; j < nf; j += blockDim.x) {
             FaceF32& F = smf[j];
 #define M(k) smd[(k) * FT + j]
-            F.rx[0] = (float)M(MC_XX); F.rx[1] = (float)M(MC_XY); F.rx[2] = (float)M(MC_XZ);
-            F.ry[0] = (float)M(MC_YX); F.ry[1] = (float)M(MC_YY); F.ry[2] = (float)M(MC_YZ);
-            F.rz[0] = (float)M(MC_ZX); F.rz[1] = (float)M(MC_ZY); F.rz[2] = (float)M(MC_ZZ);
+            F.rx0 = (float)M(MC_XX); F.rx1 = (float)M(MC_XY); F.rx2 = (float)M(MC_XZ);
+            F.ry0 = (float)M(MC_YX); F.ry1 = (float)M(MC_YY); F.ry2 = (float)M(MC_YZ);
             F.L0 = (float)M(MC_L0); F.cx = (float)M(MC_CX); F.cy = (float)M(MC_CY);
             F.e1x = (float)M(MC_E1X); F.e1y = (float)M(MC_E1Y); F.L1 = (float)M(MC_L1);
             F.e2x = (float)M(MC_E2X); F.e2y = (float)M(MC_E2Y); F.L2 = (float)M(MC_L2);
             F.gq = (float)(M(MC_SGZ) * 0.5 * M(MC_L0) * M(MC_CY));
             F.mf = (float)M(MC_MF); F.mt0 = (float)M(MC_MT0); F.mt1 = (float)M(MC_MT1); F.mt2 = (float)M(MC_MT2);
+#pragma unroll
             for (int q = 0; q < 7; ++q) {
                 F.qx[q] = kRadonBb[q] * F.L0 + kRadonBc[q] * F.cx;
                 F.qy[q] = kRadonBc[q] * F.cy;
             }
+            F.qx[7] = F.qy[7] = 0.f;
+            F.ax = M(MC_AX); F.ay = M(MC_AY); F.az = M(MC_AZ);
+            F.zx = M(MC_ZX); F.zy = M(MC_ZY); F.zz = M(MC_ZZ);
 #undef M
         }
         __syncthreads();
+        // lane j: facet j of the stage against this warp's box
+        bool valid = false, far = false, mid = false;
+        if (lane < nf && smd[MC_VALID * FT + lane] != 0.0) {
+            valid = true;
+            const float cxw = (float)smd[MC_CENX * FT + lane], cyw = (float)smd[MC_CENY * FT + lane],
+                        czw = (float)smd[MC_CENZ * FT + lane];
+            const float ddx = fmaxf(0.f, fmaxf(bb[0] - cxw, cxw + bb[3]));
+            const float ddy = fmaxf(0.f, fmaxf(bb[1] - cyw, cyw + bb[4]));
+            const float ddz = fmaxf(0.f, fmaxf(bb[2] - czw, czw + bb[5]));
+            const float d2 = ddx * ddx + ddy * ddy + ddz * ddz;
+            const float lim = tau * (float)smd[MC_SIZE * FT + lane], limMid = 0.5f * lim;
+            far = d2 >= lim * lim;
+            mid = !far && d2 >= limMid * limMid;
+        }
+        const unsigned farMask = __ballot_sync(0xffffffffu, valid && far);
+        const unsigned midMask = __ballot_sync(0xffffffffu, valid && mid);
+        const unsigned nearMask = __ballot_sync(0xffffffffu, valid && !far && !mid);
         if (act) {
             float gacc = 0.f, tacc = 0.f;
-            for (int j = 0; j < nf; ++j) {
-                if (smd[MC_VALID * FT + j] == 0.0) continue;
-                // uniform over the CTA: centroid vs tile bounding box
-                float cxw = (float)smd[MC_CENX * FT + j], cyw = (float)smd[MC_CENY * FT + j],
-                      czw = (float)smd[MC_CENZ * FT + j];
-                float ddx = fmaxf(0.f, fmaxf(bbox[0] - cxw, cxw - bbox[3]));
-                float ddy = fmaxf(0.f, fmaxf(bbox[1] - cyw, cyw - bbox[4]));
-                float ddz = fmaxf(0.f, fmaxf(bbox[2] - czw, czw - bbox[5]));
-                float lim = tau * (float)smd[MC_SIZE * FT + j];
-                bool far = ddx * ddx + ddy * ddy + ddz * ddz >= lim * lim;
-                if (far) {
-                    const FaceF32& F = smf[j];
-                    double ddx = o.x - smd[MC_AX * FT + j], ddy = o.y - smd[MC_AY * FT + j],
-                           ddz = o.z - smd[MC_AZ * FT + j];
-                    float dx = (float)ddx, dy = (float)ddy, dz = (float)ddz;
-                    float x = fmaf(dx, F.rx[0], fmaf(dy, F.rx[1], dz * F.rx[2]));
-                    float y = fmaf(dx, F.ry[0], fmaf(dy, F.ry[1], dz * F.ry[2]));
-                    // the height above the facet plane can be tiny next to |o - a|
-                    // (a far top facet seen from 1 m above it): FP64
-                    float z = (float)(ddx * smd[MC_ZX * FT + j] + ddy * smd[MC_ZY * FT + j] + ddz * smd[MC_ZZ * FT + j]);
-                    float g1 = 0.f, t1 = 0.f;
-                    pair_far_f32(F, x, y, z, &g1, &t1);
-                    if (GZ) gacc += g1;
-                    if (TMI) tacc += t1;
-                } else {
-                    double g1 = 0.0, t1 = 0.0;
-                    pair_near_f64(smd, j, FT, o, &g1, &t1);
-                    if (GZ) gz += g1;
-                    if (TMI) tmi += t1;
-                    ++nearCount;
-                }
+            for (unsigned m = farMask; m; m &= m - 1) {
+                const int j = __ffs(m) - 1;
+                pair_far_f32<false>(&smf[j], ox, oy, oz, &gacc, &tacc);
             }
-            gz += gacc;
-            tmi += tacc;
+            for (unsigned m = midMask; m; m &= m - 1) {
+                const int j = __ffs(m) - 1;
+                pair_far_f32<true>(&smf[j], ox, oy, oz, &gacc, &tacc);
+            }
+            if (GZ) gz += gacc;
+            if (TMI) tmi += tacc;
+            for (unsigned m = nearMask; m; m &= m - 1) {
+                const int j = __ffs(m) - 1;
+                double g1 = 0.0, t1 = 0.0;
+                pair_near_f64(smd, j, FT, mk3(ox, oy, oz), &g1, &t1);
+                if (GZ) gz += g1;
+                if (TMI) tmi += t1;
+            }
+            nearCount += __popc(nearMask);
         }
     }
     if (act) {
@@ -462,27 +540,27 @@ __global__ void __launch_bounds__(128) k_gradient_warp_far32(int T, const double
                         }
                         if (Ts != 0.f) {
                             const float rbx = L0 - x, rcx = cx - x, rcy = cy - y;
-                            const float la = sqrtf(fmaf(x, x, fmaf(y, y, z2)));
-                            const float lb = sqrtf(fmaf(rbx, rbx, fmaf(y, y, z2)));
-                            const float lc = sqrtf(fmaf(rcx, rcx, fmaf(rcy, rcy, z2)));
+                            const float la = sqrt_pos(fmaf(x, x, fmaf(y, y, z2)));
+                            const float lb = sqrt_pos(fmaf(rbx, rbx, fmaf(y, y, z2)));
+                            const float lc = sqrt_pos(fmaf(rcx, rcx, fmaf(rcy, rcy, z2)));
                             const float dab = fmaf(-x, rbx, fmaf(y, y, z2));
                             const float dac = fmaf(-x, rcx, fmaf(-y, rcy, z2));
                             const float dbc = fmaf(rbx, rcx, fmaf(-y, rcy, z2));
                             const float den = la * lb * lc + dab * lc + dac * lb + dbc * la;
-                            const float om = 2.f * atan2f(-z * A2, den);
+                            const float om = 2.f * atan2_far(-z * A2, den);
                             const float s11 = fmaf(rbx, e1x, -y * e1y), s12 = fmaf(rcx, e1x, rcy * e1y);
                             const float s21 = fmaf(rcx, e2x, rcy * e2y), s22 = fmaf(-x, e2x, -y * e2y);
                             const float l0 = lam_f32(-x, rbx, la, lb, L0);
                             const float l1 = lam_f32(s11, s12, lb, lc, L1);
                             const float l2 = lam_f32(s21, s22, lc, la, L2);
-                            const float ia = 1.f / la, ib = 1.f / lb, ic = 1.f / lc;
+                            const float ia = __fdividef(1.f, la), ib = __fdividef(1.f, lb), ic = __fdividef(1.f, lc);
                             const float kom = Ts * mf;
                             // edge (p1 -> p2): W = L / (d1 d2 + r1.r2), q = r1 - s1 e, Z = e x r1,
                             // P = W (kom Z - kl q); p1 += (P - kl e)/d1, p2 += (P + kl e)/d2
                             auto edge = [&](float r1x, float r1y, float r2x, float r2y, float d1, float d2, float ex,
                                             float ey, float L, float s1, float kl, float i1, float i2, float& g1x,
                                             float& g1y, float& g1z, float& g2x, float& g2y, float& g2z) {
-                                const float W = L / fmaf(d1, d2, fmaf(r1x, r2x, fmaf(r1y, r2y, z2)));
+                                const float W = __fdividef(L, fmaf(d1, d2, fmaf(r1x, r2x, fmaf(r1y, r2y, z2))));
                                 const float qxv = fmaf(-s1, ex, r1x), qyv = fmaf(-s1, ey, r1y), qzv = -z;
                                 const float Zx = -ey * z, Zy = ex * z, Zz = fmaf(ex, r1y, -ey * r1x);  // e x r1
                                 const float Px = W * fmaf(kom, Zx, -kl * qxv), Py = W * fmaf(kom, Zy, -kl * qyv),
