@@ -190,6 +190,24 @@ lf_status lf_objective(lf_ctx* ctx, const double* params, double* out5);
  * formed): *f = total objective, grad[n_dofs]. */
 lf_status lf_objective_grad(lf_ctx* ctx, const double* params, double* f, double* grad);
 
+/* Per-group unit responses at params (positions as after lf_forward), for
+ * property inversion: the forward of group `group` alone with
+ *  LF_UNIT_GRAVITY    unit density (mGal per g/cc) at the gravity stations
+ *                     (GravityForward::computeGroupUnitResponse,
+ *                     gravity_forward.cpp:132-146);
+ *  LF_UNIT_INDUCED    unit susceptibility under the inducing field (nT per SI)
+ *                     at the magnetic stations (MagneticForward::
+ *                     computeGroupUnitResponse, magnetic_forward.cpp:148-162);
+ *  LF_UNIT_DIRECTION  unit magnetisation along dir[3] (as given, not
+ *                     normalised) (computeGroupUnitResponseDirection :164-178);
+ *  LF_UNIT_REMANENCE  unit magnetisation along the group's remanence
+ *                     inclination/declination (computeGroupUnitRemanenceResponse
+ *                     :180-190).
+ * out[n_stations] in caller station order. */
+enum { LF_UNIT_GRAVITY = 0, LF_UNIT_INDUCED = 1, LF_UNIT_DIRECTION = 2, LF_UNIT_REMANENCE = 3 };
+lf_status lf_unit_response(lf_ctx* ctx, const double* params, int kind, int group, const double* dir,
+                           double* out);
+
 /* Dense Jacobian J[n_data x n_dofs] (row-major) of gravity (which = LF_GRAVITY)
  * or TMI (LF_MAGNETIC) at params, with the reference's DOF gather semantics:
  * each DOF collects its control-point vertices' own derivative times the axis

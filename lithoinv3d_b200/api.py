@@ -19,6 +19,7 @@ from ._native import Counters, LbfgsbOptions, LbfgsbResult, ModelInfo
 FIXED, Z_ONLY, X_ONLY, Y_ONLY, ALONG_VECTOR, XY_FREE, XZ_FREE, YZ_FREE, XYZ_FREE = range(9)
 GRAVITY, MAGNETIC = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
+UNIT_GRAVITY, UNIT_INDUCED, UNIT_DIRECTION, UNIT_REMANENCE = range(4)
 
 
 class LithoError(RuntimeError):
@@ -267,6 +268,15 @@ class Context:
         J = np.zeros((n, self.n_dofs))
         self._check(self.lib.lf_jacobian(self.h, _d(p), which, _d(J)), "jacobian")
         return J
+
+    def unit_response(self, params, kind: int, group: int, direction=None) -> np.ndarray:
+        """Forward of one group alone with unit properties (lf_unit_response)."""
+        p = f64(params)
+        n = self.n_grav if kind == UNIT_GRAVITY else self.n_mag
+        out = np.zeros(n)
+        d = f64(direction) if direction is not None else None
+        self._check(self.lib.lf_unit_response(self.h, _d(p), kind, group, _d(d), _d(out)), "unit_response")
+        return out
 
     def positions(self, n_vertices: int) -> np.ndarray:
         out = np.zeros((n_vertices, 3))

@@ -93,9 +93,12 @@ struct lf_ctx {
     DevBuf<GroupConst> d_groups;
     int nInterpRows = 0, nSync = 0, nGradVerts = 0, nGradFacets = 0;
 
-    // forward chunking
+    // forward chunking (plan cached per station count and group filter;
+    // uploaded only when it changes)
     std::vector<int32_t> chunkBegin, chunkEnd, chunkGroup;
-    int chunkCapacityS = 0;
+    int chunkCapacityS = 0, chunkFilter = -1, groupFilter = -1;
+    int64_t chunkFacets = 0;
+    bool chunksDirty = true;
 
     // data
     StationSet grav, mag;
@@ -678,25 +681,37 @@ static constexpr int kTargetBlocks = 148 * 4;
 
 // Facet chunks for the forward: contiguous ranges inside one group, sized so
 // that station tiles x chunks fill the GPU.
+// With c->groupFilter >= 0 only that group's facets are planned (unit
+// responses).
 static void plan_chunks(lf_ctx* c, int S) {
-    if (c->chunkCapacityS == S && !c->chunkBegin.empty()) return;
+    if (c->chunkCapacityS == S && c->chunkFilter == c->groupFilter && !c->chunksDirty && !c->chunkBegin.empty())
+        return;
+    const int g0 = c->groupFilter >= 0 ? c->groupFilter : 0, g1 = c->groupFilter >= 0 ? c->groupFilter + 1 : c->G;
+    const int nf = c->grpTriOff[g1] - c->grpTriOff[g0];
     int sBlocks = std::max(1, cdiv(S, kFwdThreads));
     int want = std::max(1, cdiv(kTargetBlocks, sBlocks));
-    int chunkSize = std::max(64, cdiv(c->T, want));
+    int chunkSize = std::max(64, cdiv(std::max(nf, 1), want));
     c->chunkBegin.clear(); c->chunkEnd.clear(); c->chunkGroup.clear();
-    for (int g = 0; g < c->G; ++g)
+    for (int g = g0; g < g1; ++g)
         for (int f = c->grpTriOff[g]; f < c->grpTriOff[g + 1]; f += chunkSize) {
             c->chunkBegin.push_back(f);
             c->chunkEnd.push_back(std::min(f + chunkSize, c->grpTriOff[g + 1]));
             c->chunkGroup.push_back(g);
         }
     c->chunkCapacityS = S;
+    c->chunkFilter = c->groupFilter;
+    c->chunkFacets = nf;
+    c->chunksDirty = true;
 }
 
 static lf_status upload_chunks(lf_ctx* c) {
-    LF_TRY_CUDA(c, upload(c->d_chunkBegin, c->chunkBegin.data(), c->chunkBegin.size(), c->stream));
-    LF_TRY_CUDA(c, upload(c->d_chunkEnd, c->chunkEnd.data(), c->chunkEnd.size(), c->stream));
-    LF_TRY_CUDA(c, upload(c->d_chunkGroup, c->chunkGroup.data(), c->chunkGroup.size(), c->stream));
+    if (!c->chunksDirty) return LF_OK;
+    if (!c->chunkBegin.empty()) {
+        LF_TRY_CUDA(c, upload(c->d_chunkBegin, c->chunkBegin.data(), c->chunkBegin.size(), c->stream));
+        LF_TRY_CUDA(c, upload(c->d_chunkEnd, c->chunkEnd.data(), c->chunkEnd.size(), c->stream));
+        LF_TRY_CUDA(c, upload(c->d_chunkGroup, c->chunkGroup.data(), c->chunkGroup.size(), c->stream));
+    }
+    c->chunksDirty = false;
     return LF_OK;
 }
 
@@ -731,17 +746,19 @@ static lf_status forward_set(lf_ctx* c, const StationSet& s, double* d_gz, doubl
     int nch = static_cast<int>(c->chunkBegin.size());
     if (GZ) LF_TRY_CUDA(c, c->d_partG.reserve((size_t)nch * S));
     if (TMI) LF_TRY_CUDA(c, c->d_partM.reserve((size_t)nch * S));
-    dim3 grid(cdiv(S, kFwdThreads), nch);
-    int slot = prof_begin(c, c->evFwd, c->nFwd);
-    k_forward_fp64<GZ, TMI, kFwdFacetTile><<<grid, kFwdThreads, 0, c->stream>>>(
-        S, s.d_xyz.p, c->T, c->d_fc.p, c->d_chunkBegin.p, c->d_chunkEnd.p, GZ ? c->d_partG.p : nullptr,
-        TMI ? c->d_partM.p : nullptr);
-    prof_end(c, c->evFwd, slot);
+    if (nch > 0) {
+        dim3 grid(cdiv(S, kFwdThreads), nch);
+        int slot = prof_begin(c, c->evFwd, c->nFwd);
+        k_forward_fp64<GZ, TMI, kFwdFacetTile><<<grid, kFwdThreads, 0, c->stream>>>(
+            S, s.d_xyz.p, c->T, c->d_fc.p, c->d_chunkBegin.p, c->d_chunkEnd.p, GZ ? c->d_partG.p : nullptr,
+            TMI ? c->d_partM.p : nullptr);
+        prof_end(c, c->evFwd, slot);
+    }
     k_forward_reduce<<<cdiv(S, 256), 256, 0, c->stream>>>(S, nch, c->d_chunkGroup.p, c->d_groups.p,
                                                           GZ ? c->d_partG.p : nullptr, TMI ? c->d_partM.p : nullptr,
                                                           GZ ? d_gz : nullptr, TMI ? d_tmi : nullptr);
     c->counters.launches += 2;
-    c->counters.forward_pairs += (uint64_t)S * (uint64_t)c->T;
+    c->counters.forward_pairs += (uint64_t)S * (uint64_t)c->chunkFacets;
     LF_CHECK_LAUNCH(c);
     return LF_OK;
 }
@@ -756,17 +773,19 @@ static lf_status forward_set_mixed(lf_ctx* c, const StationSet& s, double* d_gz,
     int nch = static_cast<int>(c->chunkBegin.size());
     if (GZ) LF_TRY_CUDA(c, c->d_partG.reserve((size_t)nch * S));
     if (TMI) LF_TRY_CUDA(c, c->d_partM.reserve((size_t)nch * S));
-    dim3 grid(cdiv(S, kFwdThreads), nch);
-    int slot = prof_begin(c, c->evFwd, c->nFwd);
-    k_forward_mixed<GZ, TMI, kFwdFacetTile><<<grid, kFwdThreads, 0, c->stream>>>(
-        S, s.d_xyz.p, c->T, c->d_mc.p, c->d_chunkBegin.p, c->d_chunkEnd.p, c->tau, GZ ? c->d_partG.p : nullptr,
-        TMI ? c->d_partM.p : nullptr, c->d_nearPairs.p);
-    prof_end(c, c->evFwd, slot);
+    if (nch > 0) {
+        dim3 grid(cdiv(S, kFwdThreads), nch);
+        int slot = prof_begin(c, c->evFwd, c->nFwd);
+        k_forward_mixed<GZ, TMI, kFwdFacetTile><<<grid, kFwdThreads, 0, c->stream>>>(
+            S, s.d_xyz.p, c->T, c->d_mc.p, c->d_chunkBegin.p, c->d_chunkEnd.p, c->tau, GZ ? c->d_partG.p : nullptr,
+            TMI ? c->d_partM.p : nullptr, c->d_nearPairs.p);
+        prof_end(c, c->evFwd, slot);
+    }
     k_forward_reduce_mixed<<<cdiv(S, 256), 256, 0, c->stream>>>(S, nch, GZ ? c->d_partG.p : nullptr,
                                                                 TMI ? c->d_partM.p : nullptr, GZ ? d_gz : nullptr,
                                                                 TMI ? d_tmi : nullptr);
     c->counters.launches += 2;
-    c->counters.forward_pairs += (uint64_t)S * (uint64_t)c->T;
+    c->counters.forward_pairs += (uint64_t)S * (uint64_t)c->chunkFacets;
     LF_CHECK_LAUNCH(c);
     return LF_OK;
 }
@@ -984,6 +1003,87 @@ extern "C" lf_status lf_objective_grad(lf_ctx* c, const double* params, double* 
         LF_TRY_CUDA(c, cudaMemcpyAsync(grad, c->d_grad.p, sizeof(double) * c->np, cudaMemcpyDeviceToHost, c->stream));
     LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
     if (f && !std::isfinite(*f)) return fail(c, LF_ENUMERIC, "non-finite objective");
+    return LF_OK;
+}
+
+// Forward of one group alone with unit properties (GravityForward::
+// computeGroupUnitResponse gravity_forward.cpp:132-146; MagneticForward::
+// computeGroupUnitResponse / computeGroupUnitResponseDirection /
+// computeGroupUnitRemanenceResponse magnetic_forward.cpp:148-190): the group
+// table is swapped for one where every other group has zero scales, the
+// chunk plan covers only the group's facets, and both are restored after.
+extern "C" lf_status lf_unit_response(lf_ctx* c, const double* params, int kind, int group, const double* dir,
+                                      double* out) {
+    LF_RET_IF(check_ready(c));
+    if (!out || kind < LF_UNIT_GRAVITY || kind > LF_UNIT_REMANENCE || group < 0 || group >= c->G ||
+        (kind == LF_UNIT_DIRECTION && (!dir || !finite_all(dir, 3))))
+        return fail(c, LF_EINVAL, "lf_unit_response: bad kind, group or direction");
+    StationSet& s = kind == LF_UNIT_GRAVITY ? c->grav : c->mag;
+    if (s.n == 0) return fail(c, LF_ESTATE, "no stations of the requested type");
+    LF_RET_IF(params_to_device(c, params));
+    LF_RET_IF(scatter(c, c->d_params.p));
+    std::vector<GroupConst> unit(c->gconst);
+    for (GroupConst& k : unit) {
+        k.gscale_fwd = k.gscale_jac = 0.0;
+        k.mscale = 0.0;
+        k.mag_active = 0;
+    }
+    GroupConst& k = unit[group];
+    double m[3] = {c->fdir.x, c->fdir.y, c->fdir.z}, amp = 1.0;
+    switch (kind) {
+    case LF_UNIT_GRAVITY:
+        k.gscale_fwd = kGSI * 1.0 * kDensityScale * kMs2ToMgal;
+        k.gscale_jac = (kGSI * kDensityScale * kMs2ToMgal) * 1.0;
+        break;
+    case LF_UNIT_INDUCED:  // magneticClosedMesh(obs, mesh, 1.0, F_hat, F): amp = F / 100 along F_hat
+        amp = 1.0 * c->fieldNT / 100.0;
+        break;
+    case LF_UNIT_DIRECTION:  // magneticClosedMeshVector(obs, mesh, 1.0, dir, F_hat)
+        for (int i = 0; i < 3; ++i) m[i] = dir[i];
+        break;
+    case LF_UNIT_REMANENCE: {  // unit magnetisation along the group's remanence direction
+        const GroupProps& gp = c->groups[group];
+        double I = gp.remInc * kPi / 180.0, D = gp.remDec * kPi / 180.0, cI = std::cos(I);
+        m[0] = cI * std::cos(D); m[1] = cI * std::sin(D); m[2] = -std::sin(I);
+        break;
+    }
+    }
+    if (kind != LF_UNIT_GRAVITY) {
+        for (int i = 0; i < 3; ++i) k.mdir[i] = m[i];
+        k.mscale = amp * 100.0 / (4.0 * kPi);
+        k.mag_active = 1;
+    }
+    lf_status st = LF_OK;
+    if (cudaMemcpyAsync(c->d_groups.p, unit.data(), sizeof(GroupConst) * unit.size(), cudaMemcpyHostToDevice,
+                        c->stream) != cudaSuccess)
+        st = fail(c, LF_ECUDA, "group table upload failed");
+    double* d_g = kind == LF_UNIT_GRAVITY ? s.d_pred.p : nullptr;
+    double* d_t = kind == LF_UNIT_GRAVITY ? nullptr : s.d_pred.p;
+    if (st == LF_OK) {
+        c->groupFilter = group;
+        if (c->precision == LF_PREC_MIXED) {
+            k_face_prep_mixed<<<cdiv(c->T, 128), 128, 0, c->stream>>>(c->T, c->d_tri.p, c->d_pos.p, c->d_faceGroup.p,
+                                                                      c->d_groups.p, c->fdir, c->d_mc.p);
+            c->counters.launches++;
+            st = kind == LF_UNIT_GRAVITY ? forward_set_mixed<true, false>(c, s, d_g, d_t)
+                                         : forward_set_mixed<false, true>(c, s, d_g, d_t);
+        } else {
+            k_face_prep_fwd<<<cdiv(c->T, 128), 128, 0, c->stream>>>(c->T, c->d_tri.p, c->d_pos.p, c->d_faceGroup.p,
+                                                                    c->d_groups.p, c->fdir, c->d_fc.p);
+            c->counters.launches++;
+            st = kind == LF_UNIT_GRAVITY ? forward_set<true, false>(c, s, d_g, d_t)
+                                         : forward_set<false, true>(c, s, d_g, d_t);
+        }
+        c->groupFilter = -1;
+    }
+    // restore the model's group table whatever happened above
+    if (cudaMemcpyAsync(c->d_groups.p, c->gconst.data(), sizeof(GroupConst) * c->gconst.size(),
+                        cudaMemcpyHostToDevice, c->stream) != cudaSuccess && st == LF_OK)
+        st = fail(c, LF_ECUDA, "group table restore failed");
+    LF_RET_IF(st);
+    LF_RET_IF(unpermute_device(c, s, s.d_pred.p, s.d_out.p));
+    LF_TRY_CUDA(c, cudaMemcpyAsync(out, s.d_out.p, sizeof(double) * s.n, cudaMemcpyDeviceToHost, c->stream));
+    LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
     return LF_OK;
 }
 

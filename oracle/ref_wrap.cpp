@@ -250,6 +250,19 @@ void ref_forward_tmi(void* h, const double* params, double* out) {
     fromVec(c->mf->compute(toVec(static_cast<int>(c->mf->parameterCount()), params)), out);
 }
 
+// Unit responses at params (kind 0 gravity, 1 induced, 2 direction, 3 remanence).
+void ref_unit_response(void* h, const double* params, int kind, int group, const double* dir, double* out) {
+    auto* c = static_cast<RefCtx*>(h);
+    c->ensure();
+    c->model->applyParameterVector(toVec(static_cast<int>(c->gf->parameterCount()), params));
+    VectorXd r;
+    if (kind == 0) r = c->gf->computeGroupUnitResponse(group);
+    else if (kind == 1) r = c->mf->computeGroupUnitResponse(group);
+    else if (kind == 2) r = c->mf->computeGroupUnitResponseDirection(group, Vector3d(dir[0], dir[1], dir[2]));
+    else r = c->mf->computeGroupUnitRemanenceResponse(group);
+    fromVec(r, out);
+}
+
 void ref_jacobian_gz(void* h, const double* params, double* J) {
     auto* c = static_cast<RefCtx*>(h);
     c->ensure();

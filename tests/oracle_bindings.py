@@ -107,6 +107,7 @@ def ref() -> C.CDLL:
             "ref_group_magnetization": (None, [V, C.c_int, _dp, _dp]),
             "ref_forward_gz": (None, [V, _dp, _dp]), "ref_forward_tmi": (None, [V, _dp, _dp]),
             "ref_jacobian_gz": (None, [V, _dp, _dp]), "ref_jacobian_tmi": (None, [V, _dp, _dp]),
+            "ref_unit_response": (None, [V, _dp, C.c_int, C.c_int, _dp, _dp]),
             "ref_objective": (None, [V, _dp, _dp]), "ref_gradient": (None, [V, _dp, _dp]),
             "ref_lbfgsb": (C.c_int, [V, _dp, _dp, _dp, C.c_int, C.c_double, C.c_int, _dp, _dp]),
         }
@@ -201,6 +202,12 @@ class RefModel:
         self.lib.ref_forward_tmi(self.h, _d(params), out.ctypes.data_as(_dp))
         return out
 
+    def unit_response(self, params, kind, group, direction=None):
+        out = np.zeros(self.Sg if kind == 0 else self.Sm)
+        d = np.ascontiguousarray(direction, np.float64) if direction is not None else np.zeros(3)
+        self.lib.ref_unit_response(self.h, _d(params), kind, group, d.ctypes.data_as(_dp), out.ctypes.data_as(_dp))
+        return out
+
     def jacobian_gz(self, params):
         J = np.zeros((self.Sg, self.np))
         self.lib.ref_jacobian_gz(self.h, _d(params), J.ctypes.data_as(_dp))
@@ -282,6 +289,31 @@ class OracleModel:
         self.o.lo_forward_tmi(len(sta), sta.ctypes.data_as(_dp), self.G, self._ip("grp_tri_off"), self._ip("tri"),
                               self.pos.ctypes.data_as(_dp), self.amp.ctypes.data_as(_dp),
                               self.mdir.ctypes.data_as(_dp), self.fdir.ctypes.data_as(_dp), out.ctypes.data_as(_dp))
+        return out
+
+    def forward_unit(self, sta, kind, group, direction=None, field_nt=55000.0):
+        """Group `group` alone with a unit property: kind 0 density (gz), 1
+        susceptibility under the inducing field, 2 magnetisation along
+        `direction`, 3 the same for a remanence direction (TMI)."""
+        sta = np.ascontiguousarray(sta, np.float64)
+        out = np.zeros(len(sta))
+        if kind == 0:
+            rho = np.zeros(self.G)
+            rho[group] = 1.0
+            self.o.lo_forward_gz(len(sta), sta.ctypes.data_as(_dp), self.G, self._ip("grp_tri_off"),
+                                 self._ip("tri"), self.pos.ctypes.data_as(_dp), rho.ctypes.data_as(_dp),
+                                 out.ctypes.data_as(_dp))
+            return out
+        amp = np.zeros(self.G)
+        mdir = np.ascontiguousarray(np.tile(self.fdir, (self.G, 1)))
+        if kind == 1:
+            amp[group] = field_nt / 100.0
+        else:
+            amp[group] = 1.0
+            mdir[group] = direction
+        self.o.lo_forward_tmi(len(sta), sta.ctypes.data_as(_dp), self.G, self._ip("grp_tri_off"), self._ip("tri"),
+                              self.pos.ctypes.data_as(_dp), amp.ctypes.data_as(_dp), mdir.ctypes.data_as(_dp),
+                              self.fdir.ctypes.data_as(_dp), out.ctypes.data_as(_dp))
         return out
 
     def jacobian(self, sta, kind, true_h=1e-2):

@@ -73,6 +73,19 @@ def test_forward_matches_reference(case):
     np.testing.assert_array_equal(om.forward_tmi(p.mag_xyz), rm.forward_tmi(x))
 
 
+def test_unit_responses_match_reference(case):
+    """GravityForward / MagneticForward::computeGroupUnitResponse* against the
+    oracle with a unit property on one group."""
+    p, model, rm, om = case
+    x = rm.assemble() + np.random.default_rng(6).normal(0, 3, rm.np)
+    om.scatter(x)
+    d = np.array([0.3, -0.5, 0.8])
+    for g in range(len(p.densities)):
+        np.testing.assert_array_equal(om.forward_unit(p.grav_xyz, 0, g), rm.unit_response(x, 0, g))
+        np.testing.assert_array_equal(om.forward_unit(p.mag_xyz, 1, g), rm.unit_response(x, 1, g))
+        np.testing.assert_array_equal(om.forward_unit(p.mag_xyz, 2, g, d), rm.unit_response(x, 2, g, d))
+
+
 def test_fd_jacobian_matches_reference(case):
     p, model, rm, om = case
     if p.n_triangles() > 2000:
