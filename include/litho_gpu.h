@@ -167,6 +167,17 @@ lf_status lf_set_magnetic_data(lf_ctx* ctx, int n, const double* xyz, const doub
 lf_status lf_set_objective(lf_ctx* ctx, double alpha_mag, double ref_weight,
                            const double* ref_params);
 
+/* SurfaceSmoothness regularisation (smoothness.cpp:20-390), added to the
+ * objective and its gradient ahead of the reference-model term, as the
+ * runner registers them (runner.cpp:164-179): weight * sum over non-fixed
+ * vertices of 0.5 |free axes of (p - mean of same-freedom mesh neighbours)|^2,
+ * gradient gathered to DOFs with the reference's control-point semantics.
+ * freedom[n_vertices]: VertexFreedom code per vertex in the tables' order;
+ * NULL takes the freedoms of the model given to lf_set_model.  weight 0
+ * turns it off.  LF_EINVAL for ALONG_VECTOR vertices (their move vectors are
+ * not part of the tables).  Reset by every lf_set_model*. */
+lf_status lf_set_smoothness(lf_ctx* ctx, double weight, const uint8_t* freedom);
+
 lf_status lf_set_precision(lf_ctx* ctx, int mode);
 
 /* Mixed path: a facet whose centroid lies at least tau x its longest edge

@@ -221,6 +221,12 @@ class Context:
         rp = f64(ref_params) if ref_params is not None else None
         self._check(self.lib.lf_set_objective(self.h, alpha_mag, ref_weight, _d(rp)), "set_objective")
 
+    def set_smoothness(self, weight: float, freedom=None):
+        """SurfaceSmoothness regularisation (lf_set_smoothness); freedom per
+        vertex, or None for the freedoms of the model given to set_model."""
+        fr = None if freedom is None else np.ascontiguousarray(freedom, np.uint8)
+        self._check(self.lib.lf_set_smoothness(self.h, float(weight), _u8(fr)), "set_smoothness")
+
     def set_precision(self, mode: int):
         self._check(self.lib.lf_set_precision(self.h, mode), "set_precision")
 

@@ -106,6 +106,14 @@ struct lf_ctx {
     double alphaMag = 1.0, refWeight = 0.0;
     bool hasRef = false;
 
+    // SurfaceSmoothness regularisation (off unless lf_set_smoothness)
+    std::vector<uint8_t> vertexFreedom;  // from lf_set_model's builder
+    bool smoothOn = false;
+    double smoothWeight = 0.0;
+    DevBuf<int32_t> d_smOff, d_smNbr;
+    DevBuf<uint8_t> d_freedom;
+    DevBuf<double> d_smDiff, d_smVgrad, d_blockS;
+
     // workspaces
     DevBuf<double> d_partG, d_partM, d_partGrad, d_blockG, d_blockM, d_ones, d_jac;
 
@@ -526,6 +534,8 @@ extern "C" lf_status lf_set_model_tables(lf_ctx* c, int G, const double* density
     LF_TRY_CUDA(c, c->d_f.reserve(1));
     c->chunkCapacityS = 0;
     c->hasRef = false;
+    c->smoothOn = false;
+    c->vertexFreedom.clear();
     c->hasModel = true;
     LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
     return LF_OK;
@@ -543,11 +553,82 @@ extern "C" lf_status lf_set_model(lf_ctx* c, lf_model* m) {
         rv[3 * g] = gr.remVector.x; rv[3 * g + 1] = gr.remVector.y; rv[3 * g + 2] = gr.remVector.z;
     }
     int nSync = static_cast<int>(t.syncOff.size()) - 1;
-    return lf_set_model_tables(c, G, rho.data(), chi.data(), rm.data(), ri.data(), rd.data(), rv.data(), t.nVertices,
-                               t.pos.data(), t.nTriangles, t.tri.data(), t.grpTriOff.data(), t.nDofs,
-                               t.dofOff.data(), t.refVertex.data(), t.refAxis.data(), t.refScale.data(),
-                               t.interpOff.data(), t.interpSrc.data(), t.interpW.data(), nSync,
-                               t.syncOff.data(), t.syncVertex.data());
+    lf_status st = lf_set_model_tables(c, G, rho.data(), chi.data(), rm.data(), ri.data(), rd.data(), rv.data(),
+                                       t.nVertices, t.pos.data(), t.nTriangles, t.tri.data(), t.grpTriOff.data(),
+                                       t.nDofs, t.dofOff.data(), t.refVertex.data(), t.refAxis.data(),
+                                       t.refScale.data(), t.interpOff.data(), t.interpSrc.data(), t.interpW.data(),
+                                       nSync, t.syncOff.data(), t.syncVertex.data());
+    if (st != LF_OK) return st;
+    // vertex freedoms in the tables' vertex order (meshes in group order)
+    for (int g = 0; g < m->host.meshCount(); ++g)
+        if (const Mesh* mesh = m->host.mesh(g))
+            c->vertexFreedom.insert(c->vertexFreedom.end(), mesh->freedom.begin(), mesh->freedom.end());
+    if ((int)c->vertexFreedom.size() != c->V) c->vertexFreedom.clear();
+    return LF_OK;
+}
+
+// SurfaceSmoothness (smoothness.cpp): same-freedom neighbour lists per vertex,
+// built like SurfaceMesh::buildNeighbors (surface_mesh.cpp:265-286: the other
+// vertices of every triangle holding the vertex, ascending, without
+// duplicates), filtered to the vertex's own freedom; FIXED vertices get none.
+extern "C" lf_status lf_set_smoothness(lf_ctx* c, double weight, const uint8_t* freedom) {
+    if (!c || !std::isfinite(weight) || weight < 0.0) return LF_EINVAL;
+    if (!c->hasModel) return fail(c, LF_ESTATE, "lf_set_smoothness before lf_set_model");
+    if (weight == 0.0) {
+        c->smoothOn = false;
+        c->smoothWeight = 0.0;
+        return LF_OK;
+    }
+    const uint8_t* fr = freedom ? freedom : (c->vertexFreedom.empty() ? nullptr : c->vertexFreedom.data());
+    if (!fr) return fail(c, LF_EINVAL, "lf_set_smoothness: no vertex freedoms known (pass freedom[n_vertices])");
+    const int V = c->V, T = c->T;
+    for (int v = 0; v < V; ++v) {
+        if (fr[v] > LF_XYZ_FREE) return fail(c, LF_EINVAL, "lf_set_smoothness: bad freedom code");
+        if (fr[v] == LF_ALONG_VECTOR)
+            return fail(c, LF_EINVAL, "lf_set_smoothness: ALONG_VECTOR vertices need move vectors, not supported");
+    }
+    std::vector<int32_t> tri((size_t)3 * T);
+    LF_TRY_CUDA(c, cudaMemcpyAsync(tri.data(), c->d_tri.p, sizeof(int32_t) * tri.size(), cudaMemcpyDeviceToHost,
+                                   c->stream));
+    LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
+    std::vector<std::vector<int32_t>> nb(V);
+    for (int t = 0; t < T; ++t) {
+        int a = tri[3 * t], b = tri[3 * t + 1], d = tri[3 * t + 2];
+        nb[a].push_back(b); nb[a].push_back(d);
+        nb[b].push_back(a); nb[b].push_back(d);
+        nb[d].push_back(a); nb[d].push_back(b);
+    }
+    std::vector<int32_t> off(V + 1, 0), list;
+    for (int v = 0; v < V; ++v) {
+        std::vector<int32_t>& l = nb[v];
+        std::sort(l.begin(), l.end());
+        l.erase(std::unique(l.begin(), l.end()), l.end());
+        if (fr[v] != LF_FIXED)
+            for (int32_t u : l)
+                if (fr[u] == fr[v]) list.push_back(u);
+        off[v + 1] = static_cast<int32_t>(list.size());
+    }
+    LF_TRY_CUDA(c, upload(c->d_smOff, off.data(), off.size(), c->stream));
+    LF_TRY_CUDA(c, upload(c->d_smNbr, list.empty() ? off.data() : list.data(), std::max<size_t>(list.size(), 1),
+                          c->stream));
+    LF_TRY_CUDA(c, upload(c->d_freedom, fr, (size_t)V, c->stream));
+    LF_TRY_CUDA(c, c->d_smDiff.reserve((size_t)3 * V));
+    LF_TRY_CUDA(c, c->d_smVgrad.reserve((size_t)3 * V));
+    LF_TRY_CUDA(c, c->d_blockS.reserve(cdiv(V, 256)));
+    LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->smoothOn = true;
+    c->smoothWeight = weight;
+    return LF_OK;
+}
+
+// diff and per-block penalties at the current positions.
+static lf_status smooth_diff(lf_ctx* c) {
+    if (!c->smoothOn) return LF_OK;
+    k_smooth_diff<<<cdiv(c->V, 256), 256, 0, c->stream>>>(c->V, c->d_pos.p, c->d_freedom.p, c->d_smOff.p,
+                                                          c->d_smNbr.p, c->d_smDiff.p, c->d_blockS.p);
+    c->counters.launches++;
+    LF_CHECK_LAUNCH(c);
+    return LF_OK;
 }
 
 extern "C" lf_status lf_set_field(lf_ctx* c, double inc, double dec, double field, int remMode) {
@@ -835,7 +916,9 @@ static lf_status residuals(lf_ctx* c, bool wantCoef) {
 static lf_status objective_final(lf_ctx* c, const double* d_params, double* d_f) {
     int nbg = cdiv(std::max(c->grav.n, 1), 256), nbm = cdiv(std::max(c->mag.n, 1), 256);
     k_objective_final<<<1, 256, 0, c->stream>>>(nbg, c->d_blockG.p, nbm, c->d_blockM.p, c->alphaMag, c->np, d_params,
-                                                c->hasRef ? c->d_refp.p : nullptr, c->refWeight, c->d_out5.p, d_f);
+                                                c->hasRef ? c->d_refp.p : nullptr, c->refWeight, cdiv(c->V, 256),
+                                                c->smoothOn ? c->d_blockS.p : nullptr, c->smoothWeight, c->d_out5.p,
+                                                d_f);
     c->counters.launches++;
     LF_CHECK_LAUNCH(c);
     return LF_OK;
@@ -898,10 +981,17 @@ static lf_status gradient_all(lf_ctx* c, const double* d_params, double* d_grad)
             c->counters.launches++;
         }
     }
+    if (c->smoothOn) {
+        k_smooth_vgrad<<<cdiv(c->V, 256), 256, 0, c->stream>>>(c->V, c->d_freedom.p, c->d_smOff.p, c->d_smNbr.p,
+                                                               c->d_smDiff.p, c->d_smVgrad.p);
+        c->counters.launches++;
+    }
     if (c->np > 0) {
         k_dof_gather<<<cdiv(c->np, 256), 256, 0, c->stream>>>(c->np, c->d_dofOff.p, c->d_refVertex.p, c->d_refAxis.p,
                                                               c->d_refScale.p, c->d_vgrad.p, d_params,
-                                                              c->hasRef ? c->d_refp.p : nullptr, c->refWeight, d_grad);
+                                                              c->hasRef ? c->d_refp.p : nullptr, c->refWeight,
+                                                              c->smoothOn ? c->d_smVgrad.p : nullptr,
+                                                              c->smoothWeight, d_grad);
         c->counters.launches++;
     }
     LF_CHECK_LAUNCH(c);
@@ -969,6 +1059,7 @@ extern "C" lf_status lf_forward(lf_ctx* c, const double* params, double* gz, dou
 
 static lf_status objective_device(lf_ctx* c, const double* d_params) {
     LF_RET_IF(scatter(c, d_params));
+    LF_RET_IF(smooth_diff(c));
     LF_RET_IF(forward_all(c));
     LF_RET_IF(residuals(c, false));
     return objective_final(c, d_params, c->d_f.p);
@@ -988,6 +1079,7 @@ extern "C" lf_status lf_objective(lf_ctx* c, const double* params, double* out5)
 extern "C" lf_status lf_objective_grad_device(lf_ctx* c, const double* d_params, double* d_f, double* d_grad) {
     LF_RET_IF(check_ready(c));
     LF_RET_IF(scatter(c, d_params));
+    LF_RET_IF(smooth_diff(c));
     LF_RET_IF(forward_all(c));
     LF_RET_IF(residuals(c, true));
     LF_RET_IF(objective_final(c, d_params, d_f ? d_f : c->d_f.p));

@@ -699,11 +699,19 @@ __global__ void k_vertex_reduce(int nverts, const int32_t* __restrict__ verts, c
 __global__ void k_dof_gather(int np, const int32_t* __restrict__ dof_off, const int32_t* __restrict__ ref_vertex,
                              const uint8_t* __restrict__ ref_axis, const double* __restrict__ ref_scale,
                              const double* __restrict__ vgrad, const double* __restrict__ params,
-                             const double* __restrict__ ref_params, double ref_weight, double* __restrict__ grad) {
+                             const double* __restrict__ ref_params, double ref_weight,
+                             const double* __restrict__ vgrad_smooth, double smooth_weight,
+                             double* __restrict__ grad) {
     int d = blockIdx.x * blockDim.x + threadIdx.x;
     if (d >= np) return;
     double acc = 0.0;
     for (int r = dof_off[d]; r < dof_off[d + 1]; ++r) acc += vgrad[3 * ref_vertex[r] + ref_axis[r]] * ref_scale[r];
+    if (vgrad_smooth) {  // SurfaceSmoothness::gradient gather (smoothness.cpp:231-242), times its weight
+        double s = 0.0;
+        for (int r = dof_off[d]; r < dof_off[d + 1]; ++r)
+            s += vgrad_smooth[3 * ref_vertex[r] + ref_axis[r]] * ref_scale[r];
+        acc += smooth_weight * s;
+    }
     if (ref_params) acc += ref_weight * (params[d] - ref_params[d]);
     grad[d] = acc;
 }
@@ -735,9 +743,101 @@ __global__ void k_jacobian_gather(int nst, int np, const int32_t* __restrict__ d
 
 // Final deterministic reduction of block partials and objective assembly:
 // out = {grav misfit, mag misfit, reg, 0, total}.
+// ---------------------------------------------------------- smoothness ----
+// SurfaceSmoothness (modules/litho-regularization/src/regularization/
+// smoothness.cpp): every non-fixed vertex against the mean of its
+// same-freedom mesh neighbours (nbr: CSR, ascending, built on the host like
+// SurfaceMesh::buildNeighbors surface_mesh.cpp:265-286).
+
+// Free axes of a VertexFreedom code (surface_mesh.h:9-19); ALONG_VECTOR is
+// rejected on the host.
+__device__ __forceinline__ void freedom_mask(int fr, bool m[3]) {
+    m[0] = fr == 2 || fr == 5 || fr == 6 || fr == 8;
+    m[1] = fr == 3 || fr == 5 || fr == 7 || fr == 8;
+    m[2] = fr == 1 || fr == 6 || fr == 7 || fr == 8;
+}
+
+// diff_v = p_v - mean_v (evaluate :29-49) and the per-vertex penalty
+// 0.5 |mask diff|^2 (:51-99), summed per block; same operation order as the
+// reference.
+__global__ void k_smooth_diff(int V, const double* __restrict__ pos, const uint8_t* __restrict__ freedom,
+                              const int32_t* __restrict__ off, const int32_t* __restrict__ nbr,
+                              double* __restrict__ diff, double* __restrict__ block_pen) {
+    __shared__ double red[256];
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    double pen = 0.0;
+    if (v < V) {
+        const int b = off[v], e = off[v + 1];
+        double d0 = 0.0, d1 = 0.0, d2 = 0.0;
+        if (e > b) {
+            double m0 = 0.0, m1 = 0.0, m2 = 0.0;
+            for (int i = b; i < e; ++i) {
+                const double* q = pos + 3 * (size_t)nbr[i];
+                m0 = __dadd_rn(m0, q[0]); m1 = __dadd_rn(m1, q[1]); m2 = __dadd_rn(m2, q[2]);
+            }
+            const double n = static_cast<double>(e - b);
+            m0 = __ddiv_rn(m0, n); m1 = __ddiv_rn(m1, n); m2 = __ddiv_rn(m2, n);
+            d0 = __dsub_rn(pos[3 * (size_t)v], m0);
+            d1 = __dsub_rn(pos[3 * (size_t)v + 1], m1);
+            d2 = __dsub_rn(pos[3 * (size_t)v + 2], m2);
+            auto sq = [](double d) { return __dmul_rn(d, d); };
+            switch (freedom[v]) {
+            case 1: pen = __dmul_rn(__dmul_rn(0.5, d2), d2); break;
+            case 2: pen = __dmul_rn(__dmul_rn(0.5, d0), d0); break;
+            case 3: pen = __dmul_rn(__dmul_rn(0.5, d1), d1); break;
+            case 5: pen = __dmul_rn(0.5, __dadd_rn(sq(d0), sq(d1))); break;
+            case 6: pen = __dmul_rn(0.5, __dadd_rn(sq(d0), sq(d2))); break;
+            case 7: pen = __dmul_rn(0.5, __dadd_rn(sq(d1), sq(d2))); break;
+            case 8: pen = __dmul_rn(0.5, __dadd_rn(__dadd_rn(sq(d0), sq(d1)), sq(d2))); break;
+            default: break;
+            }
+        }
+        diff[3 * (size_t)v] = d0; diff[3 * (size_t)v + 1] = d1; diff[3 * (size_t)v + 2] = d2;
+    }
+    red[threadIdx.x] = pen;
+    __syncthreads();
+    for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+        if (threadIdx.x < k) red[threadIdx.x] += red[threadIdx.x + k];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) block_pen[blockIdx.x] = red[0];
+}
+
+// Per-vertex smoothness gradient (gradient :152-242): own term mask(diff_v),
+// then -mask(diff_u) / n_u for every same-freedom neighbour u in ascending
+// order (the neighbour relation and the freedom filter are symmetric, so the
+// vertices that add to v are exactly v's own list).
+__global__ void k_smooth_vgrad(int V, const uint8_t* __restrict__ freedom, const int32_t* __restrict__ off,
+                               const int32_t* __restrict__ nbr, const double* __restrict__ diff,
+                               double* __restrict__ vg) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= V) return;
+    double g0 = 0.0, g1 = 0.0, g2 = 0.0;
+    const int b = off[v], e = off[v + 1];
+    if (e > b) {
+        bool m[3];
+        freedom_mask(freedom[v], m);
+        if (m[0]) g0 = diff[3 * (size_t)v];
+        if (m[1]) g1 = diff[3 * (size_t)v + 1];
+        if (m[2]) g2 = diff[3 * (size_t)v + 2];
+        for (int i = b; i < e; ++i) {
+            const int u = nbr[i];
+            const double nu = static_cast<double>(off[u + 1] - off[u]);
+            if (m[0]) g0 = __dadd_rn(g0, __ddiv_rn(-diff[3 * (size_t)u], nu));
+            if (m[1]) g1 = __dadd_rn(g1, __ddiv_rn(-diff[3 * (size_t)u + 1], nu));
+            if (m[2]) g2 = __dadd_rn(g2, __ddiv_rn(-diff[3 * (size_t)u + 2], nu));
+        }
+    }
+    vg[3 * (size_t)v] = g0; vg[3 * (size_t)v + 1] = g1; vg[3 * (size_t)v + 2] = g2;
+}
+
+// Objective components: misfits from the residual block sums; regularisation
+// = smoothness (weight x block penalty sums) + reference-model term, in the
+// order the runner registers them (runner.cpp:164-179).
 __global__ void k_objective_final(int nbg, const double* __restrict__ bg, int nbm, const double* __restrict__ bm,
                                   double alpha, int np, const double* __restrict__ params,
-                                  const double* __restrict__ ref_params, double ref_weight, double* __restrict__ out5,
+                                  const double* __restrict__ ref_params, double ref_weight, int nbs,
+                                  const double* __restrict__ bs, double smooth_weight, double* __restrict__ out5,
                                   double* __restrict__ f_out) {
     __shared__ double red[256];
     double reg = 0.0;
@@ -757,6 +857,11 @@ __global__ void k_objective_final(int nbg, const double* __restrict__ bg, int nb
         for (int i = 0; i < nbg; ++i) g += bg[i];
         for (int i = 0; i < nbm; ++i) m += bm[i];
         double r = ref_params ? 0.5 * ref_weight * red[0] : 0.0;
+        if (bs) {
+            double sp = 0.0;
+            for (int i = 0; i < nbs; ++i) sp += bs[i];
+            r = smooth_weight * sp + r;
+        }
         double total = g + alpha * m + r;
         out5[0] = g; out5[1] = m; out5[2] = r; out5[3] = 0.0; out5[4] = total;
         if (f_out) *f_out = total;

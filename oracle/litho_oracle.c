@@ -454,3 +454,133 @@ void lo_misfit_gradient(int S, int np, const double *J, const double *pred, cons
         for (int d = 0; d < np; ++d) grad_accum[d] += -alpha * row[d] * wr;
     }
 }
+
+/* ------------------------------------------------------------------------
+ * SurfaceSmoothness (modules/litho-regularization/src/regularization/
+ * smoothness.cpp:20-105 evaluate, :107-390 gradient).
+ *
+ * Neighbours: SurfaceMesh::buildNeighbors (modules/litho-surface/src/surface/
+ * surface_mesh.cpp:265-286) -- every other vertex of every triangle that
+ * contains the vertex, sorted ascending, duplicates removed.  Only neighbours
+ * with the vertex's own freedom count; FIXED vertices take no part.
+ * penalty_v = 0.5 |mask_v(p_v - mean_v)|^2, mask_v = the vertex's free axes
+ * (ALONG_VECTOR is not represented here).  Value = weight * sum_v penalty_v,
+ * summed over vertices in order.  Gradient per vertex (the CP-stride branch,
+ * :152-242; the plain branch :243-384 gives the same numbers for axis
+ * freedoms): own term mask_v(diff_v), then, for every same-freedom neighbour
+ * u in ascending order, -mask_u(diff_u) / n_u; gathered to DOFs as
+ * weight * sum_refs vgrad[v][axis] * scale.
+ * ------------------------------------------------------------------------ */
+static int lo_cmp_i32(const void *a, const void *b) {
+    int32_t x = *(const int32_t *)a, y = *(const int32_t *)b;
+    return (x > y) - (x < y);
+}
+
+/* free axes of a VertexFreedom (surface_mesh.h:9-19) */
+static void lo_axis_mask(int freedom, int m[3]) {
+    m[0] = m[1] = m[2] = 0;
+    switch (freedom) {
+    case 1: m[2] = 1; break;            /* Z_ONLY */
+    case 2: m[0] = 1; break;            /* X_ONLY */
+    case 3: m[1] = 1; break;            /* Y_ONLY */
+    case 5: m[0] = m[1] = 1; break;     /* XY_FREE */
+    case 6: m[0] = m[2] = 1; break;     /* XZ_FREE */
+    case 7: m[1] = m[2] = 1; break;     /* YZ_FREE */
+    case 8: m[0] = m[1] = m[2] = 1; break; /* XYZ_FREE */
+    default: break;
+    }
+}
+
+/* Same-freedom neighbour CSR (caller frees *off and *nbr). */
+static void lo_same_neighbours(int V, int T, const int32_t *tri, const uint8_t *freedom, int32_t **off_out,
+                               int32_t **nbr_out) {
+    int32_t *cnt = (int32_t *)calloc((size_t)V + 1, sizeof(int32_t));
+    for (int t = 0; t < T; ++t)
+        for (int k = 0; k < 3; ++k) cnt[tri[3 * t + k] + 1] += 2;
+    for (int v = 0; v < V; ++v) cnt[v + 1] += cnt[v];
+    int32_t *raw = (int32_t *)malloc(sizeof(int32_t) * ((size_t)cnt[V] + 1));
+    int32_t *fill = (int32_t *)malloc(sizeof(int32_t) * ((size_t)V + 1));
+    memcpy(fill, cnt, sizeof(int32_t) * (size_t)V);
+    for (int t = 0; t < T; ++t) {
+        int32_t a = tri[3 * t], b = tri[3 * t + 1], c = tri[3 * t + 2];
+        raw[fill[a]++] = b; raw[fill[a]++] = c;
+        raw[fill[b]++] = a; raw[fill[b]++] = c;
+        raw[fill[c]++] = a; raw[fill[c]++] = b;
+    }
+    int32_t *off = (int32_t *)calloc((size_t)V + 1, sizeof(int32_t));
+    int32_t *nbr = (int32_t *)malloc(sizeof(int32_t) * ((size_t)cnt[V] + 1));
+    int k = 0;
+    for (int v = 0; v < V; ++v) {
+        int32_t *l = raw + cnt[v];
+        int n = cnt[v + 1] - cnt[v];
+        qsort(l, (size_t)n, sizeof(int32_t), lo_cmp_i32);
+        off[v] = k;
+        if (freedom[v] != 0)
+            for (int i = 0; i < n; ++i) {
+                if (i > 0 && l[i] == l[i - 1]) continue;
+                if (freedom[l[i]] == freedom[v]) nbr[k++] = l[i];
+            }
+    }
+    off[V] = k;
+    free(cnt); free(raw); free(fill);
+    *off_out = off;
+    *nbr_out = nbr;
+}
+
+/* Value (weight * penalty) and DOF gradient of the smoothness term at the
+ * positions pos[V*3] (after the scatter).  Either output may be NULL. */
+void lo_smoothness(int V, const double *pos, const uint8_t *freedom, int T, const int32_t *tri, double weight,
+                   int np, const int32_t *dof_off, const int32_t *ref_vertex, const uint8_t *ref_axis,
+                   const double *ref_scale, double *value, double *grad) {
+    int32_t *off, *nbr;
+    lo_same_neighbours(V, T, tri, freedom, &off, &nbr);
+    double *diff = (double *)calloc((size_t)V * 3, sizeof(double));
+    double *vg = (double *)calloc((size_t)V * 3, sizeof(double));
+    double pen = 0.0;
+    for (int v = 0; v < V; ++v) {
+        int n = off[v + 1] - off[v];
+        if (n == 0) continue;
+        double mean[3] = {0.0, 0.0, 0.0};
+        for (int i = off[v]; i < off[v + 1]; ++i)
+            for (int k = 0; k < 3; ++k) mean[k] += pos[3 * nbr[i] + k];
+        for (int k = 0; k < 3; ++k) mean[k] /= (double)n;
+        for (int k = 0; k < 3; ++k) diff[3 * v + k] = pos[3 * v + k] - mean[k];
+        double d0 = diff[3 * v], d1 = diff[3 * v + 1], d2 = diff[3 * v + 2];
+        switch (freedom[v]) {
+        case 1: pen += 0.5 * d2 * d2; break;
+        case 2: pen += 0.5 * d0 * d0; break;
+        case 3: pen += 0.5 * d1 * d1; break;
+        case 5: pen += 0.5 * (d0 * d0 + d1 * d1); break;
+        case 6: pen += 0.5 * (d0 * d0 + d2 * d2); break;
+        case 7: pen += 0.5 * (d1 * d1 + d2 * d2); break;
+        case 8: pen += 0.5 * (d0 * d0 + d1 * d1 + d2 * d2); break;
+        default: break;
+        }
+    }
+    if (value) *value = weight * pen;
+    if (grad) {
+        for (int v = 0; v < V; ++v) {
+            if (off[v + 1] == off[v]) continue;
+            int m[3];
+            lo_axis_mask(freedom[v], m);
+            for (int k = 0; k < 3; ++k)
+                if (m[k]) vg[3 * v + k] = diff[3 * v + k];
+        }
+        for (int u = 0; u < V; ++u) {
+            int n = off[u + 1] - off[u];
+            if (n == 0) continue;
+            int m[3];
+            double contrib[3];
+            lo_axis_mask(freedom[u], m);
+            for (int k = 0; k < 3; ++k) contrib[k] = m[k] ? -diff[3 * u + k] / (double)n : 0.0;
+            for (int i = off[u]; i < off[u + 1]; ++i)
+                for (int k = 0; k < 3; ++k) vg[3 * nbr[i] + k] += contrib[k];
+        }
+        for (int d = 0; d < np; ++d) {
+            double g = 0.0;
+            for (int r = dof_off[d]; r < dof_off[d + 1]; ++r) g += vg[3 * ref_vertex[r] + ref_axis[r]] * ref_scale[r];
+            grad[d] = weight * g;
+        }
+    }
+    free(off); free(nbr); free(diff); free(vg);
+}

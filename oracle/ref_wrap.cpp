@@ -41,6 +41,8 @@ struct RefCtx {
     std::shared_ptr<ReferenceModelRegularization> refReg;
     double alphaMag = 1.0;
     double refWeight = 0.0;
+    double smoothWeight = 0.0;
+    std::shared_ptr<SurfaceSmoothness> smooth;
     VectorXd refParams;
     bool built = false;
 
@@ -49,6 +51,11 @@ struct RefCtx {
         mf = std::make_shared<MagneticForward>(model, mag, inc, dec, field);
         mf->setRemanenceMode(static_cast<RemanentMagnetizationMode>(remMode));
         gobj = std::make_shared<ObjectiveFunction>(gf, grav);
+        // the runner registers the smoothness first, then the reference model
+        // (runner.cpp:164-179)
+        smooth = std::make_shared<SurfaceSmoothness>(model);
+        smooth->setWeight(smoothWeight);
+        if (smoothWeight > 0.0) gobj->addRegularization(smooth);
         if (refWeight > 0.0 && refParams.size() > 0) {
             refReg = std::make_shared<ReferenceModelRegularization>(model);
             refReg->setWeight(refWeight);
@@ -228,6 +235,25 @@ void ref_set_objective(void* h, double alpha_mag, double ref_weight, const doubl
     c->refWeight = ref_weight;
     if (ref_params) c->refParams = toVec(static_cast<int>(c->model->totalDofCount()), ref_params);
     c->built = false;
+}
+
+void ref_set_smoothness(void* h, double weight) {
+    auto* c = static_cast<RefCtx*>(h);
+    c->smoothWeight = weight;
+    c->built = false;
+}
+
+// SurfaceSmoothness::evaluate / gradient (smoothness.cpp:20-390) with the
+// weight set by ref_set_smoothness.
+double ref_smoothness_value(void* h, const double* params) {
+    auto* c = static_cast<RefCtx*>(h);
+    c->ensure();
+    return c->smooth->evaluate(toVec(static_cast<int>(c->model->totalDofCount()), params));
+}
+void ref_smoothness_gradient(void* h, const double* params, double* grad) {
+    auto* c = static_cast<RefCtx*>(h);
+    c->ensure();
+    fromVec(c->smooth->gradient(toVec(static_cast<int>(c->model->totalDofCount()), params)), grad);
 }
 
 void ref_group_magnetization(void* h, int g, double* amp, double* dir3) {

@@ -73,6 +73,9 @@ def oracle() -> C.CDLL:
         lib.lo_misfit.argtypes = [C.c_int, _dp, _dp, _dp]
         lib.lo_misfit_gradient.restype = None
         lib.lo_misfit_gradient.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp, _dp, C.c_double, _dp]
+        lib.lo_smoothness.restype = None
+        lib.lo_smoothness.argtypes = [C.c_int, _dp, _u8p, C.c_int, _ip, C.c_double, C.c_int, _ip, _ip, _u8p, _dp,
+                                      _dp, _dp]
         _ORACLE = lib
     return _ORACLE
 
@@ -108,6 +111,9 @@ def ref() -> C.CDLL:
             "ref_forward_gz": (None, [V, _dp, _dp]), "ref_forward_tmi": (None, [V, _dp, _dp]),
             "ref_jacobian_gz": (None, [V, _dp, _dp]), "ref_jacobian_tmi": (None, [V, _dp, _dp]),
             "ref_unit_response": (None, [V, _dp, C.c_int, C.c_int, _dp, _dp]),
+            "ref_set_smoothness": (None, [V, C.c_double]),
+            "ref_smoothness_value": (C.c_double, [V, _dp]),
+            "ref_smoothness_gradient": (None, [V, _dp, _dp]),
             "ref_objective": (None, [V, _dp, _dp]), "ref_gradient": (None, [V, _dp, _dp]),
             "ref_lbfgsb": (C.c_int, [V, _dp, _dp, _dp, C.c_int, C.c_double, C.c_int, _dp, _dp]),
         }
@@ -124,7 +130,7 @@ class RefModel:
     synth.Problem (test harness over oracle/_ref)."""
 
     def __init__(self, problem, grav_obs=None, grav_std=None, mag_obs=None, mag_std=None, alpha_mag=1.0,
-                 ref_weight=0.0, ref_params=None, remanence_mode=0):
+                 ref_weight=0.0, ref_params=None, remanence_mode=0, smooth_weight=0.0):
         self.lib = ref()
         self.h = self.lib.ref_new()
         for g, (rho, chi) in enumerate(zip(problem.densities, problem.susceptibilities)):
@@ -149,6 +155,7 @@ class RefModel:
             self.lib.ref_set_magnetic(self.h, len(problem.mag_xyz), _d(problem.mag_xyz), _d(mag_obs), _d(mag_std),
                                       inc, dec, F0, remanence_mode)
         self.lib.ref_set_objective(self.h, alpha_mag, ref_weight, _d(ref_params))
+        self.lib.ref_set_smoothness(self.h, smooth_weight)
         self.np = self.lib.ref_dof_count(self.h)
         self.nv = self.lib.ref_vertex_count(self.h)
         self.Sg = Sg
@@ -201,6 +208,13 @@ class RefModel:
         out = np.zeros(self.Sm)
         self.lib.ref_forward_tmi(self.h, _d(params), out.ctypes.data_as(_dp))
         return out
+
+    def smoothness(self, params):
+        """SurfaceSmoothness value and DOF gradient at params."""
+        g = np.zeros(self.np)
+        v = self.lib.ref_smoothness_value(self.h, _d(params))
+        self.lib.ref_smoothness_gradient(self.h, _d(params), g.ctypes.data_as(_dp))
+        return v, g
 
     def unit_response(self, params, kind, group, direction=None):
         out = np.zeros(self.Sg if kind == 0 else self.Sm)
@@ -290,6 +304,21 @@ class OracleModel:
                               self.pos.ctypes.data_as(_dp), self.amp.ctypes.data_as(_dp),
                               self.mdir.ctypes.data_as(_dp), self.fdir.ctypes.data_as(_dp), out.ctypes.data_as(_dp))
         return out
+
+    def smoothness(self, freedom, weight):
+        """SurfaceSmoothness value and DOF gradient at the current positions
+        (freedom: VertexFreedom code per global vertex)."""
+        t = self.t
+        fr = np.ascontiguousarray(freedom, np.uint8)
+        V = self.pos.size // 3
+        T = t["tri"].size // 3
+        g = np.zeros(self.np)
+        val = np.zeros(1)
+        self.o.lo_smoothness(V, self.pos.ctypes.data_as(_dp), fr.ctypes.data_as(_u8p), T, self._ip("tri"), weight,
+                             self.np, self._ip("dof_off"), self._ip("ref_vertex"),
+                             t["ref_axis"].ctypes.data_as(_u8p), t["ref_scale"].ctypes.data_as(_dp),
+                             val.ctypes.data_as(_dp), g.ctypes.data_as(_dp))
+        return float(val[0]), g
 
     def forward_unit(self, sta, kind, group, direction=None, field_nt=55000.0):
         """Group `group` alone with a unit property: kind 0 density (gz), 1

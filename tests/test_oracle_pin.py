@@ -86,6 +86,20 @@ def test_unit_responses_match_reference(case):
         np.testing.assert_array_equal(om.forward_unit(p.mag_xyz, 2, g, d), rm.unit_response(x, 2, g, d))
 
 
+def test_smoothness_matches_reference(case):
+    """SurfaceSmoothness::evaluate / gradient against the C restatement:
+    value and DOF gradient bit for bit."""
+    p, model, rm, om = case
+    rs = ob.RefModel(p, smooth_weight=0.7)
+    x = rs.assemble() + np.random.default_rng(8).normal(0, 3, rs.np)
+    om.scatter(x)
+    fr = np.concatenate([np.broadcast_to(np.asarray(f, np.uint8), (len(V),)) for V, F, f in p.meshes])
+    v_o, g_o = om.smoothness(fr, 0.7)
+    v_r, g_r = rs.smoothness(x)
+    assert v_o == v_r
+    np.testing.assert_array_equal(g_o, g_r)
+
+
 def test_fd_jacobian_matches_reference(case):
     p, model, rm, om = case
     if p.n_triangles() > 2000:
