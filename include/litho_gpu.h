@@ -192,6 +192,17 @@ lf_status lf_get_near_pairs(lf_ctx* ctx, unsigned long long* n);
  * output may be NULL. */
 lf_status lf_forward(lf_ctx* ctx, const double* params, double* gz, double* tmi);
 
+/* Graph mode (no reference counterpart: the reference evaluates on one CPU
+ * thread).  When enabled, lf_objective, lf_objective_grad and
+ * lf_objective_grad_device replay a CUDA graph of the whole evaluation
+ * (scatter, forward, residuals, objective, gradient) instead of launching its
+ * kernels one by one: the first call with a given set of buffers runs
+ * normally and captures the sequence, later calls replay it.  Any setter,
+ * and any call that grows a device buffer, invalidates the graph.  Results
+ * are identical to the direct launches.  Profiling (lf_set_profiling) turns
+ * replay off while it is enabled. */
+lf_status lf_set_graph_mode(lf_ctx* ctx, int enabled);
+
 /* Objective components at params: out5 = {gravity misfit, magnetic misfit,
  * regularisation, constraint penalty (0), total} (JointComponents,
  * joint_objective.h:55-63). */

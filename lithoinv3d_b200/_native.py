@@ -71,6 +71,7 @@ SIGNATURES = {
     "lf_objective_grad": (C.c_int, [_vp, _dp, _dp, _dp]),
     "lf_jacobian": (C.c_int, [_vp, _dp, C.c_int, _dp]),
     "lf_unit_response": (C.c_int, [_vp, _dp, C.c_int, C.c_int, _dp, _dp]),
+    "lf_set_graph_mode": (C.c_int, [_vp, C.c_int]),
     "lf_set_smoothness": (C.c_int, [_vp, C.c_double, C.POINTER(C.c_uint8)]),
     "lf_get_positions": (C.c_int, [_vp, _dp]),
     "lf_forward_device": (C.c_int, [_vp, _vp, _vp, _vp]),

@@ -227,6 +227,10 @@ class Context:
         fr = None if freedom is None else np.ascontiguousarray(freedom, np.uint8)
         self._check(self.lib.lf_set_smoothness(self.h, float(weight), _u8(fr)), "set_smoothness")
 
+    def set_graph_mode(self, enabled: bool = True):
+        """Replay evaluations as a captured CUDA graph (lf_set_graph_mode)."""
+        self._check(self.lib.lf_set_graph_mode(self.h, int(bool(enabled))), "set_graph_mode")
+
     def set_precision(self, mode: int):
         self._check(self.lib.lf_set_precision(self.h, mode), "set_precision")
 

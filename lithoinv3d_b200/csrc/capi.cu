@@ -23,6 +23,13 @@ struct lf_model {
 
 namespace {
 
+// Bumped by every device (re)allocation in the process: a captured CUDA
+// graph holds raw buffer addresses and is re-captured when this moves.
+static uint64_t& reallocAll() {
+    static uint64_t n = 0;
+    return n;
+}
+
 template <typename T>
 struct DevBuf {
     T* p = nullptr;
@@ -43,6 +50,7 @@ struct DevBuf {
         cudaError_t e = cudaMalloc(&p, count * sizeof(T));
         if (e != cudaSuccess) { p = nullptr; return e; }
         n = count;
+        ++reallocAll();
         return cudaSuccess;
     }
 };
@@ -86,7 +94,7 @@ struct lf_ctx {
     DevBuf<unsigned long long> d_nearPairs;
     float tau = 3.0f;  // far-field ratio of the mixed path
     DevBuf<int32_t> d_tri, d_dofOff, d_refVertex, d_interpOff, d_interpSrc, d_interpRows, d_syncOff,
-        d_syncVertex, d_vfOff, d_vf, d_gradVerts, d_chunkBegin, d_chunkEnd, d_chunkGroup;
+        d_syncVertex, d_vfOff, d_vf, d_gradVerts, d_gradFacets, d_chunkBegin, d_chunkEnd, d_chunkGroup;
     DevBuf<uint8_t> d_refAxis, d_faceNeeds;
     DevBuf<double> d_refScale, d_interpW;
     DevBuf<int16_t> d_faceGroup;
@@ -118,6 +126,26 @@ struct lf_ctx {
     DevBuf<double> d_partG, d_partM, d_partGrad, d_blockG, d_blockM, d_ones, d_jac;
 
     lf_counters counters{0, 0, 0};
+
+    // CUDA graph replay of whole evaluations (lf_set_graph_mode).  epoch is
+    // bumped by every setter; a cached graph is valid for one (epoch,
+    // allocation count, buffer addresses) and is re-captured otherwise.
+    struct GraphCache {
+        cudaGraphExec_t exec = nullptr;
+        uint64_t epoch = ~0ull, reallocs = ~0ull;
+        const double* params = nullptr;
+        double *f = nullptr, *grad = nullptr;
+        lf_counters delta{0, 0, 0};
+    };
+    static constexpr int kGraphSlots = 4;  // buffer sets replayed without re-capture (e.g. ping-pong params)
+    struct GraphSet {
+        GraphCache slot[kGraphSlots];
+        int next = 0;
+        uint64_t failedEpoch = ~0ull;
+    };
+    bool graphMode = false;
+    uint64_t epoch = 0;
+    GraphSet gObjGrad, gObj;
 
     // optional per-kernel timing (events on `stream`)
     bool profiling = false;
@@ -362,10 +390,21 @@ extern "C" lf_status lf_create(lf_ctx** out, int device) {
     return LF_OK;
 }
 
+static void drop_graph(lf_ctx::GraphSet& set) {
+    for (auto& g : set.slot) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        g = lf_ctx::GraphCache{};
+    }
+    set.next = 0;
+    set.failedEpoch = ~0ull;
+}
+
 extern "C" void lf_destroy(lf_ctx* c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    drop_graph(c->gObjGrad);
+    drop_graph(c->gObj);
     clear_events(c->evFwd);
     clear_events(c->evGrad);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -421,6 +460,7 @@ extern "C" lf_status lf_set_model_tables(lf_ctx* c, int G, const double* density
                                          const int32_t* interpOff, const int32_t* interpSrc, const double* interpW,
                                          int nSync, const int32_t* syncOff, const int32_t* syncVertex) {
     if (!c) return LF_EINVAL;
+    c->epoch++;
     if (G <= 0 || G > 32000 || nv <= 0 || nt <= 0 || np < 0 || !density || !xyz || !tri || !grpTriOff ||
         (np > 0 && (!dofOff || !refVertex || !refAxis || !refScale)))
         return fail(c, LF_EINVAL, "lf_set_model_tables: bad sizes or null arrays");
@@ -517,8 +557,11 @@ extern "C" lf_status lf_set_model_tables(lf_ctx* c, int G, const double* density
     for (int f = 0; f < nt; ++f)
         fneed[f] = vneed[tri[3 * f]] | vneed[tri[3 * f + 1]] | vneed[tri[3 * f + 2]];
     c->nGradVerts = static_cast<int>(gverts.size());
-    c->nGradFacets = 0;
-    for (int f = 0; f < nt; ++f) c->nGradFacets += fneed[f];
+    std::vector<int32_t> gfacets;
+    for (int f = 0; f < nt; ++f)
+        if (fneed[f]) gfacets.push_back(f);
+    c->nGradFacets = static_cast<int>(gfacets.size());
+    if (!gfacets.empty()) LF_TRY_CUDA(c, upload(c->d_gradFacets, gfacets.data(), gfacets.size(), c->stream));
     LF_TRY_CUDA(c, upload(c->d_gradVerts, gverts.data(), gverts.size(), c->stream));
     LF_TRY_CUDA(c, upload(c->d_faceNeeds, fneed.data(), fneed.size(), c->stream));
     LF_TRY_CUDA(c, c->d_fc.reserve((size_t)NFC * nt));
@@ -573,6 +616,7 @@ extern "C" lf_status lf_set_model(lf_ctx* c, lf_model* m) {
 // duplicates), filtered to the vertex's own freedom; FIXED vertices get none.
 extern "C" lf_status lf_set_smoothness(lf_ctx* c, double weight, const uint8_t* freedom) {
     if (!c || !std::isfinite(weight) || weight < 0.0) return LF_EINVAL;
+    c->epoch++;
     if (!c->hasModel) return fail(c, LF_ESTATE, "lf_set_smoothness before lf_set_model");
     if (weight == 0.0) {
         c->smoothOn = false;
@@ -634,6 +678,7 @@ static lf_status smooth_diff(lf_ctx* c) {
 extern "C" lf_status lf_set_field(lf_ctx* c, double inc, double dec, double field, int remMode) {
     if (!c || !std::isfinite(inc) || !std::isfinite(dec) || !std::isfinite(field) || remMode < 0 || remMode > 2)
         return LF_EINVAL;
+    c->epoch++;
     c->inc = inc; c->dec = dec; c->fieldNT = field; c->remMode = remMode;
     if (c->hasModel) return upload_groups(c);
     return LF_OK;
@@ -641,6 +686,7 @@ extern "C" lf_status lf_set_field(lf_ctx* c, double inc, double dec, double fiel
 
 static lf_status set_stations(lf_ctx* c, StationSet& s, int n, const double* xyz, const double* obs, const double* sd) {
     if (!c || n < 0 || (n > 0 && !xyz)) return LF_EINVAL;
+    c->epoch++;
     if (!finite_all(xyz, (size_t)n * 3)) return fail(c, LF_EINVAL, "non-finite station position");
     if (obs && !finite_all(obs, n)) return fail(c, LF_EINVAL, "non-finite observation");
     cudaSetDevice(c->device);
@@ -720,6 +766,7 @@ extern "C" lf_status lf_set_magnetic_data(lf_ctx* c, int n, const double* xyz, c
 
 extern "C" lf_status lf_set_objective(lf_ctx* c, double alpha, double refWeight, const double* refParams) {
     if (!c || !std::isfinite(alpha) || !std::isfinite(refWeight)) return LF_EINVAL;
+    c->epoch++;
     if (!c->hasModel) return fail(c, LF_ESTATE, "lf_set_objective before lf_set_model");
     c->alphaMag = alpha;
     c->refWeight = refWeight;
@@ -734,6 +781,7 @@ extern "C" lf_status lf_set_objective(lf_ctx* c, double alpha, double refWeight,
 
 extern "C" lf_status lf_set_far_field_ratio(lf_ctx* c, double tau) {
     if (!c || !std::isfinite(tau)) return LF_EINVAL;
+    c->epoch++;
     c->tau = tau <= 0.0 ? 3.0e38f : static_cast<float>(tau);
     return LF_OK;
 }
@@ -749,6 +797,7 @@ extern "C" lf_status lf_get_near_pairs(lf_ctx* c, unsigned long long* n) {
 
 extern "C" lf_status lf_set_precision(lf_ctx* c, int mode) {
     if (!c || (mode != LF_PREC_FP64 && mode != LF_PREC_MIXED)) return LF_EINVAL;
+    c->epoch++;
     c->precision = mode;
     return LF_OK;
 }
@@ -758,6 +807,7 @@ static constexpr int kFwdThreads = 128;
 static constexpr int kFwdFacetTile = 32;
 static constexpr int kGradThreads = 32;             // Jacobian rows: one warp of facets per CTA
 static constexpr int kGradWarpsPerBlock = 4;        // objective gradient: one warp per facet
+static constexpr int kTargetGradWarps = 148 * 64;   // facet warps x station chunks per gradient launch
 static constexpr int kTargetBlocks = 148 * 4;
 
 // Facet chunks for the forward: contiguous ranges inside one group, sized so
@@ -783,6 +833,7 @@ static void plan_chunks(lf_ctx* c, int S) {
     c->chunkFilter = c->groupFilter;
     c->chunkFacets = nf;
     c->chunksDirty = true;
+    c->epoch++;
 }
 
 static lf_status upload_chunks(lf_ctx* c) {
@@ -929,27 +980,41 @@ static lf_status objective_final(lf_ctx* c, const double* d_params, double* d_f)
 // FP64 kernel over every (facet, station) pair.  Mixed mode: the FP64 kernel
 // takes each facet's near station tiles and the FP32 far-field kernel the
 // rest, writing slot + 1.  Returns the number of slots written.
-static int gradient_set(lf_ctx* c, const StationSet& s, const double* gcoef, const double* mcoef, int slot) {
-    if (s.n == 0) return 0;
+// Station chunks of the gradient grid: enough warps (facets with a DOF
+// vertex x chunks) to fill the GPU several times over, whole tiles per chunk.
+static void grad_chunks(lf_ctx* c, int S, int* nchunks, int* tilesPerChunk) {
+    const int ntiles = std::max(1, cdiv(S, kStationTile));
+    const int want = std::max(1, cdiv(kTargetGradWarps, std::max(c->nGradFacets, 1)));
+    *tilesPerChunk = cdiv(ntiles, std::min(want, ntiles));
+    *nchunks = cdiv(ntiles, *tilesPerChunk);
+}
+
+// Gradient kernels over one station set with the given adjoints; writes
+// facet partial slots [slot0, slot0 + returned count) of d_partGrad
+// ([slot][9][T], one slot per (kernel, station chunk)).
+static int gradient_set(lf_ctx* c, const StationSet& s, const double* gcoef, const double* mcoef, int slot0) {
+    if (s.n == 0 || c->nGradFacets == 0) return 0;
     const bool mixed = c->precision == LF_PREC_MIXED;
     const double tau = mixed ? static_cast<double>(c->tau) : 3.0e38;
-    const int blocks = cdiv(c->T, kGradWarpsPerBlock);
+    int nch = 1, tpc = 1;
+    grad_chunks(c, s.n, &nch, &tpc);
+    const dim3 grid(cdiv(c->nGradFacets, kGradWarpsPerBlock), nch);
     int ev = prof_begin(c, c->evGrad, c->nGrad);
-    k_gradient_warp_fp64<<<blocks, 32 * kGradWarpsPerBlock, 0, c->stream>>>(
+    k_gradient_warp_fp64<<<grid, 32 * kGradWarpsPerBlock, 0, c->stream>>>(
         c->T, c->d_gc.p, s.n, s.d_xyz.p, gcoef, mcoef, s.d_tileBox.p, c->d_faceGroup.p, c->d_groups.p, c->fdir, tau,
-        c->d_partGrad.p + (size_t)slot * 9 * c->T);
+        c->d_gradFacets.p, c->nGradFacets, tpc, c->d_partGrad.p + (size_t)slot0 * 9 * c->T);
     prof_end(c, c->evGrad, ev);
     c->counters.launches++;
     if (mixed) {
         int ev2 = prof_begin(c, c->evGrad, c->nGrad);
-        k_gradient_warp_far32<<<blocks, 32 * kGradWarpsPerBlock, 0, c->stream>>>(
+        k_gradient_warp_far32<<<grid, 32 * kGradWarpsPerBlock, 0, c->stream>>>(
             c->T, c->d_gc.p, s.n, s.d_xyz.p, gcoef, mcoef, s.d_tileBox.p, c->d_faceGroup.p, c->d_groups.p, c->fdir,
-            tau, c->d_partGrad.p + (size_t)(slot + 1) * 9 * c->T);
+            tau, c->d_gradFacets.p, c->nGradFacets, tpc, c->d_partGrad.p + (size_t)(slot0 + nch) * 9 * c->T);
         prof_end(c, c->evGrad, ev2);
         c->counters.launches++;
     }
     c->counters.gradient_pairs += (uint64_t)s.n * (uint64_t)c->nGradFacets;
-    return mixed ? 2 : 1;
+    return mixed ? 2 * nch : nch;
 }
 
 static lf_status gradient_all(lf_ctx* c, const double* d_params, double* d_grad) {
@@ -959,9 +1024,16 @@ static lf_status gradient_all(lf_ctx* c, const double* d_params, double* d_grad)
                                                              c->d_gc.p);
     c->counters.launches++;
     LF_CHECK_LAUNCH(c);
-    const int perSet = c->precision == LF_PREC_MIXED ? 2 : 1;
-    const int sets = (c->sameStations && gOn) ? 1 : (int)gOn + (int)mOn;
-    const int slots = sets * perSet;
+    const int perKernel = c->precision == LF_PREC_MIXED ? 2 : 1;
+    int slots = 0, nch = 1, tpc = 1;
+    if (c->sameStations && gOn) {
+        grad_chunks(c, c->grav.n, &nch, &tpc);
+        slots = perKernel * nch;
+    } else {
+        if (gOn) { grad_chunks(c, c->grav.n, &nch, &tpc); slots += perKernel * nch; }
+        if (mOn) { grad_chunks(c, c->mag.n, &nch, &tpc); slots += perKernel * nch; }
+    }
+    if (c->nGradFacets == 0) slots = 0;
     if (slots == 0) {
         LF_TRY_CUDA(c, cudaMemsetAsync(c->d_vgrad.p, 0, sizeof(double) * 3 * c->V, c->stream));
     } else {
@@ -1057,6 +1129,79 @@ extern "C" lf_status lf_forward(lf_ctx* c, const double* params, double* gz, dou
     return LF_OK;
 }
 
+// Runs `body` (a whole evaluation enqueued on c->stream) directly, or, in
+// graph mode, replays a CUDA graph of it.  A cache miss runs the body eagerly
+// -- which also sizes every buffer and uploads every table -- and then
+// captures the same launch sequence for the next call.  A capture that fails
+// is not an error (the eager run already produced the result); it is not
+// retried until a setter changes the context.
+template <class Body>
+static lf_status run_cached(lf_ctx* c, lf_ctx::GraphSet& set, const double* p, double* f, double* grad, Body body) {
+    if (!c->graphMode || c->profiling) return body();
+    for (auto& g : set.slot)
+        if (g.exec && g.epoch == c->epoch && g.reallocs == reallocAll() && g.params == p && g.f == f &&
+            g.grad == grad) {
+            LF_TRY_CUDA(c, cudaGraphLaunch(g.exec, c->stream));
+            c->counters.forward_pairs += g.delta.forward_pairs;
+            c->counters.gradient_pairs += g.delta.gradient_pairs;
+            c->counters.launches += g.delta.launches;
+            return LF_OK;
+        }
+    LF_RET_IF(body());
+    if (set.failedEpoch == c->epoch) return LF_OK;
+    // slots captured under an older epoch or allocation state are stale
+    for (auto& g : set.slot)
+        if (g.exec && (g.epoch != c->epoch || g.reallocs != reallocAll())) {
+            cudaGraphExecDestroy(g.exec);
+            g = lf_ctx::GraphCache{};
+        }
+    lf_ctx::GraphCache& g = set.slot[set.next];
+    set.next = (set.next + 1) % lf_ctx::kGraphSlots;
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    g = lf_ctx::GraphCache{};
+    const lf_counters before = c->counters;
+    const uint64_t epoch0 = c->epoch, realloc0 = reallocAll();
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        set.failedEpoch = c->epoch;
+        return LF_OK;
+    }
+    const lf_status cst = body();
+    const cudaError_t ee = cudaStreamEndCapture(c->stream, &graph);
+    const lf_counters after = c->counters;
+    c->counters = before;  // a capture executes nothing
+    bool ok = cst == LF_OK && ee == cudaSuccess && graph && c->epoch == epoch0 && reallocAll() == realloc0;
+    cudaGraphExec_t exec = nullptr;
+    if (ok && cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) ok = false;
+    if (graph) cudaGraphDestroy(graph);
+    if (!ok) {
+        if (exec) cudaGraphExecDestroy(exec);
+        cudaGetLastError();
+        set.failedEpoch = c->epoch;
+        return LF_OK;
+    }
+    g.exec = exec;
+    g.epoch = c->epoch;
+    g.reallocs = reallocAll();
+    g.params = p;
+    g.f = f;
+    g.grad = grad;
+    g.delta = {after.forward_pairs - before.forward_pairs, after.gradient_pairs - before.gradient_pairs,
+               after.launches - before.launches};
+    return LF_OK;
+}
+
+extern "C" lf_status lf_set_graph_mode(lf_ctx* c, int enabled) {
+    if (!c) return LF_EINVAL;
+    cudaSetDevice(c->device);
+    LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->graphMode = enabled != 0;
+    drop_graph(c->gObjGrad);
+    drop_graph(c->gObj);
+    return LF_OK;
+}
+
 static lf_status objective_device(lf_ctx* c, const double* d_params) {
     LF_RET_IF(scatter(c, d_params));
     LF_RET_IF(smooth_diff(c));
@@ -1069,7 +1214,8 @@ extern "C" lf_status lf_objective(lf_ctx* c, const double* params, double* out5)
     LF_RET_IF(check_ready(c));
     if (!out5) return LF_EINVAL;
     LF_RET_IF(params_to_device(c, params));
-    LF_RET_IF(objective_device(c, c->d_params.p));
+    LF_RET_IF(run_cached(c, c->gObj, c->d_params.p, c->d_out5.p, nullptr,
+                         [&] { return objective_device(c, c->d_params.p); }));
     LF_TRY_CUDA(c, cudaMemcpyAsync(out5, c->d_out5.p, sizeof(double) * 5, cudaMemcpyDeviceToHost, c->stream));
     LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
     if (!std::isfinite(out5[4])) return fail(c, LF_ENUMERIC, "non-finite objective");
@@ -1078,12 +1224,16 @@ extern "C" lf_status lf_objective(lf_ctx* c, const double* params, double* out5)
 
 extern "C" lf_status lf_objective_grad_device(lf_ctx* c, const double* d_params, double* d_f, double* d_grad) {
     LF_RET_IF(check_ready(c));
-    LF_RET_IF(scatter(c, d_params));
-    LF_RET_IF(smooth_diff(c));
-    LF_RET_IF(forward_all(c));
-    LF_RET_IF(residuals(c, true));
-    LF_RET_IF(objective_final(c, d_params, d_f ? d_f : c->d_f.p));
-    return gradient_all(c, d_params, d_grad ? d_grad : c->d_grad.p);
+    double* f = d_f ? d_f : c->d_f.p;
+    double* g = d_grad ? d_grad : c->d_grad.p;
+    return run_cached(c, c->gObjGrad, d_params, f, g, [&]() -> lf_status {
+        LF_RET_IF(scatter(c, d_params));
+        LF_RET_IF(smooth_diff(c));
+        LF_RET_IF(forward_all(c));
+        LF_RET_IF(residuals(c, true));
+        LF_RET_IF(objective_final(c, d_params, f));
+        return gradient_all(c, d_params, g);
+    });
 }
 
 extern "C" lf_status lf_objective_grad(lf_ctx* c, const double* params, double* f, double* grad) {
@@ -1309,6 +1459,7 @@ extern "C" lf_status lf_get_counters(lf_ctx* c, lf_counters* out) {
 }
 extern "C" lf_status lf_set_profiling(lf_ctx* c, int enabled) {
     if (!c) return LF_EINVAL;
+    c->epoch++;
     cudaSetDevice(c->device);
     LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
     c->profiling = enabled != 0;

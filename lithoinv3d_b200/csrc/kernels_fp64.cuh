@@ -622,7 +622,9 @@ __device__ __forceinline__ void grad_acc_warp_sum(GradAcc& A) {
 // the tile's stations in turn; per-lane sums are reduced across the warp
 // once per facet and lane 0 finalises.  The work of a facet is spread over
 // 32 lanes, so facets with many near tiles leave no long tail behind.
-// part layout [9][T].
+// Warps run over `facets` (those with a DOF vertex); grid.y splits the
+// station tiles into chunks of tiles_per_chunk so that a model with few such
+// facets still fills the GPU.  part layout [chunk][9][T].
 __global__ void __launch_bounds__(128) k_gradient_warp_fp64(int T, const double* __restrict__ gc, int S,
                                                             const double* __restrict__ sta,
                                                             const double* __restrict__ gcoef,
@@ -630,10 +632,16 @@ __global__ void __launch_bounds__(128) k_gradient_warp_fp64(int T, const double*
                                                             const double* __restrict__ tile_box,
                                                             const int16_t* __restrict__ face_group,
                                                             const GroupConst* __restrict__ groups, d3 fdir, double tau,
-                                                            double* __restrict__ part) {
+                                                            const int32_t* __restrict__ facets, int nfacets,
+        int tiles_per_chunk, double* __restrict__ part) {
     const int lane = threadIdx.x & 31;
-    const int f = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
-    if (f >= T) return;  // warp-uniform
+    const int w = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+    if (w >= nfacets) return;  // warp-uniform
+    const int f = facets[w];
+    // this chunk's station tiles
+    const int ntiles_all = (S + kStationTile - 1) / kStationTile;
+    const int tbeg = blockIdx.y * tiles_per_chunk, ntiles = min(ntiles_all, tbeg + tiles_per_chunk);
+    part += (size_t)blockIdx.y * 9 * T;
     double C[NGC];
 #pragma unroll
     for (int k = 0; k < NGC; ++k) C[k] = gc[(size_t)k * T + f];
@@ -642,10 +650,9 @@ __global__ void __launch_bounds__(128) k_gradient_warp_fp64(int T, const double*
         GradAcc A;
         grad_acc_zero(A);
         const double gsn = C[GC_GS], ms = C[GC_MS];
-        const int ntiles = (S + kStationTile - 1) / kStationTile;
         const FarKey key = facet_far_key(C, tau);
         bool any = false;
-        for (int t0 = 0; t0 < ntiles; t0 += 32) {
+        for (int t0 = tbeg; t0 < ntiles; t0 += 32) {
             const int t = t0 + lane;
             const bool nearT = t < ntiles && !tile_far(key, tile_box + 6 * (size_t)t);
             unsigned m = __ballot_sync(0xffffffffu, nearT);

@@ -424,7 +424,8 @@ constexpr int kFarFlushTiles = 4;  // far tiles summed per lane in FP32 between 
 // Each lane sums up to kFarFlushTiles tiles (8 stations) in FP32; the 23
 // sums are then reduced across the warp in one transposed pass and lane k
 // adds sum k to its FP64 total.  Lane 0 gathers the totals, forms the facet
-// accumulators in FP64 and finalises.  part layout [9][T].
+// accumulators in FP64 and finalises.  Facet list and station chunks as in
+// k_gradient_warp_fp64; part layout [chunk][9][T].
 // Sums: 0 Q0; 1-3, 4-6, 7-9 sum_q beta_q{a,b,c} D_q; 10-12, 13-15, 16-18 TMI
 // vertex terms of a, b, c; 19 sum Ts Omega; 20-22 sum Ts Lambda_i.
 __global__ void __launch_bounds__(128) k_gradient_warp_far32(int T, const double* __restrict__ gc, int S,
@@ -434,10 +435,16 @@ __global__ void __launch_bounds__(128) k_gradient_warp_far32(int T, const double
                                                              const double* __restrict__ tile_box,
                                                              const int16_t* __restrict__ face_group,
                                                              const GroupConst* __restrict__ groups, d3 fdir,
-                                                             double tau, double* __restrict__ part) {
+                                                             double tau, const int32_t* __restrict__ facets, int nfacets,
+        int tiles_per_chunk, double* __restrict__ part) {
     const int lane = threadIdx.x & 31;
-    const int f = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
-    if (f >= T) return;  // warp-uniform
+    const int w = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+    if (w >= nfacets) return;  // warp-uniform
+    const int f = facets[w];
+    // this chunk's station tiles
+    const int ntiles_all = (S + kStationTile - 1) / kStationTile;
+    const int tbeg = blockIdx.y * tiles_per_chunk, ntiles = min(ntiles_all, tbeg + tiles_per_chunk);
+    part += (size_t)blockIdx.y * 9 * T;
     bool active, any = false;
     double tot = 0.0;
     {
@@ -495,9 +502,8 @@ __global__ void __launch_bounds__(128) k_gradient_warp_far32(int T, const double
                 vax = vay = vaz = vbx = vby = vbz = vcx = vcy = vcz = 0.f;
                 amf = amt0 = amt1 = amt2 = 0.f;
             };
-            const int ntiles = (S + kStationTile - 1) / kStationTile;
             const FarKey key = facet_far_key(C, tau);
-            for (int t0 = 0; t0 < ntiles; t0 += 32) {
+            for (int t0 = tbeg; t0 < ntiles; t0 += 32) {
                 const int t = t0 + lane;
                 const bool farT = t < ntiles && tile_far(key, tile_box + 6 * (size_t)t);
                 unsigned m = __ballot_sync(0xffffffffu, farT);
