@@ -307,6 +307,7 @@ def main():
     ctx = p.make_context(model, device=local, grav_obs=gobs, grav_std=gstd, mag_obs=mobs, mag_std=mstd)
     ctx.set_precision(PREC_MIXED if args.precision == "mixed" else PREC_FP64)
     ctx.set_graph_mode(True)
+    tuned, _ = ctx.autotune(x0, repeats=3)
     np_ = model.n_dofs
     dev = torch.device("cuda", local)
     stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
@@ -423,7 +424,10 @@ def main():
             "config": {"workload": WORKLOAD, "triangles": p.n_triangles(), "stations": len(p.grav_xyz),
                        "dofs": np_, "parallelism": f"replicas x{world}", "l2": "flushed between steps (256 MiB write)",
                        "precision": args.precision, "fp64_near_pair_fraction": round(near_frac, 4),
-                       "cuda_graph": True},
+                       "cuda_graph": True,
+                       "tuning": {"fwd_target_blocks": tuned.fwd_target_blocks,
+                                  "grad_target_warps": tuned.grad_target_warps,
+                                  "near_tiles_per_chunk": tuned.near_tiles_per_chunk}},
             "e2e": {"value": e2e_value, "unit": "evals/s", "h2d_bytes_per_step": 8 * np_,
                     "d2h_bytes_per_step": 8 * (np_ + 1)},
             "gpu_launches": launches, "roofline": roofline}

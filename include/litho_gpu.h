@@ -192,6 +192,28 @@ lf_status lf_get_near_pairs(lf_ctx* ctx, unsigned long long* n);
  * output may be NULL. */
 lf_status lf_forward(lf_ctx* ctx, const double* params, double* gz, double* tmi);
 
+/* Launch shapes of the hot kernels (no reference counterpart).
+ *  fwd_target_blocks     forward CTAs per launch: stations/128 x facet chunks;
+ *                        more chunks = more CTAs, each over fewer facets
+ *  grad_target_warps     gradient warps per launch: DOF facets x station chunks
+ *  near_tiles_per_chunk  mixed near-field gradient: 64-station tiles per warp
+ *                        (0: the grad_target_warps split)
+ * lf_autotune measures candidates on the context's own model, stations and
+ * precision, at params, and keeps the fastest; lf_set_tuning / lf_get_tuning
+ * set and read them directly.  Results do not depend on the shapes beyond
+ * the summation order of partial sums. */
+typedef struct {
+    int fwd_target_blocks;
+    int grad_target_warps;
+    int near_tiles_per_chunk;
+} lf_tuning;
+lf_status lf_set_tuning(lf_ctx* ctx, const lf_tuning* t);
+lf_status lf_get_tuning(lf_ctx* ctx, lf_tuning* t);
+/* Times each candidate over `repeats` objective+gradient evaluations (device
+ * events) and keeps the fastest; *best_ms (may be NULL) = its time per
+ * evaluation.  Needs the model and the data set. */
+lf_status lf_autotune(lf_ctx* ctx, const double* params, int repeats, lf_tuning* chosen, double* best_ms);
+
 /* Graph mode (no reference counterpart: the reference evaluates on one CPU
  * thread).  When enabled, lf_objective, lf_objective_grad and
  * lf_objective_grad_device replay a CUDA graph of the whole evaluation

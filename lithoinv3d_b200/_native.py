@@ -28,6 +28,10 @@ class LbfgsbResult(C.Structure):
                 ("gradients", C.c_int), ("final_value", C.c_double), ("message", C.c_char * 96)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("fwd_target_blocks", C.c_int), ("grad_target_warps", C.c_int), ("near_tiles_per_chunk", C.c_int)]
+
+
 class Counters(C.Structure):
     _fields_ = [("forward_pairs", C.c_uint64), ("gradient_pairs", C.c_uint64), ("launches", C.c_uint64)]
 
@@ -72,6 +76,9 @@ SIGNATURES = {
     "lf_jacobian": (C.c_int, [_vp, _dp, C.c_int, _dp]),
     "lf_unit_response": (C.c_int, [_vp, _dp, C.c_int, C.c_int, _dp, _dp]),
     "lf_set_graph_mode": (C.c_int, [_vp, C.c_int]),
+    "lf_set_tuning": (C.c_int, [_vp, C.c_void_p]),
+    "lf_get_tuning": (C.c_int, [_vp, C.c_void_p]),
+    "lf_autotune": (C.c_int, [_vp, _dp, C.c_int, C.c_void_p, _dp]),
     "lf_set_smoothness": (C.c_int, [_vp, C.c_double, C.POINTER(C.c_uint8)]),
     "lf_get_positions": (C.c_int, [_vp, _dp]),
     "lf_forward_device": (C.c_int, [_vp, _vp, _vp, _vp]),

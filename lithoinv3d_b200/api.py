@@ -13,7 +13,7 @@ from typing import Optional, Sequence
 import numpy as np
 
 from . import _native
-from ._native import Counters, LbfgsbOptions, LbfgsbResult, ModelInfo
+from ._native import Counters, LbfgsbOptions, LbfgsbResult, ModelInfo, Tuning
 
 # VertexFreedom numbering (surface_mesh.h:9-19)
 FIXED, Z_ONLY, X_ONLY, Y_ONLY, ALONG_VECTOR, XY_FREE, XZ_FREE, YZ_FREE, XYZ_FREE = range(9)
@@ -226,6 +226,23 @@ class Context:
         vertex, or None for the freedoms of the model given to set_model."""
         fr = None if freedom is None else np.ascontiguousarray(freedom, np.uint8)
         self._check(self.lib.lf_set_smoothness(self.h, float(weight), _u8(fr)), "set_smoothness")
+
+    def tuning(self) -> Tuning:
+        t = Tuning()
+        self._check(self.lib.lf_get_tuning(self.h, C.byref(t)), "get_tuning")
+        return t
+
+    def set_tuning(self, fwd_target_blocks: int, grad_target_warps: int, near_tiles_per_chunk: int = 0):
+        t = Tuning(fwd_target_blocks, grad_target_warps, near_tiles_per_chunk)
+        self._check(self.lib.lf_set_tuning(self.h, C.byref(t)), "set_tuning")
+
+    def autotune(self, params, repeats: int = 3):
+        """Times candidate launch shapes on this context's problem and keeps
+        the fastest (lf_autotune); returns (Tuning, ms per evaluation)."""
+        t = Tuning()
+        ms = np.zeros(1)
+        self._check(self.lib.lf_autotune(self.h, _d(f64(params)), repeats, C.byref(t), _d(ms)), "autotune")
+        return t, float(ms[0])
 
     def set_graph_mode(self, enabled: bool = True):
         """Replay evaluations as a captured CUDA graph (lf_set_graph_mode)."""

@@ -147,6 +147,10 @@ struct lf_ctx {
     uint64_t epoch = 0;
     GraphSet gObjGrad, gObj;
 
+    // launch shapes chosen by lf_autotune (defaults: measured on the
+    // 19k-facet, 4096-station contact model)
+    lf_tuning tune{148 * 4, 148 * 64, 0};
+
     // optional per-kernel timing (events on `stream`)
     bool profiling = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> evFwd, evGrad;
@@ -807,8 +811,6 @@ static constexpr int kFwdThreads = 128;
 static constexpr int kFwdFacetTile = 32;
 static constexpr int kGradThreads = 32;             // Jacobian rows: one warp of facets per CTA
 static constexpr int kGradWarpsPerBlock = 4;        // objective gradient: one warp per facet
-static constexpr int kTargetGradWarps = 148 * 64;   // facet warps x station chunks per gradient launch
-static constexpr int kTargetBlocks = 148 * 4;
 
 // Facet chunks for the forward: contiguous ranges inside one group, sized so
 // that station tiles x chunks fill the GPU.
@@ -820,7 +822,7 @@ static void plan_chunks(lf_ctx* c, int S) {
     const int g0 = c->groupFilter >= 0 ? c->groupFilter : 0, g1 = c->groupFilter >= 0 ? c->groupFilter + 1 : c->G;
     const int nf = c->grpTriOff[g1] - c->grpTriOff[g0];
     int sBlocks = std::max(1, cdiv(S, kFwdThreads));
-    int want = std::max(1, cdiv(kTargetBlocks, sBlocks));
+    int want = std::max(1, cdiv(c->tune.fwd_target_blocks, sBlocks));
     int chunkSize = std::max(64, cdiv(std::max(nf, 1), want));
     c->chunkBegin.clear(); c->chunkEnd.clear(); c->chunkGroup.clear();
     for (int g = g0; g < g1; ++g)
@@ -980,13 +982,31 @@ static lf_status objective_final(lf_ctx* c, const double* d_params, double* d_f)
 // FP64 kernel over every (facet, station) pair.  Mixed mode: the FP64 kernel
 // takes each facet's near station tiles and the FP32 far-field kernel the
 // rest, writing slot + 1.  Returns the number of slots written.
-// Station chunks of the gradient grid: enough warps (facets with a DOF
-// vertex x chunks) to fill the GPU several times over, whole tiles per chunk.
-static void grad_chunks(lf_ctx* c, int S, int* nchunks, int* tilesPerChunk) {
+// Station chunks of a gradient grid, whole tiles per chunk: enough chunks
+// for tune.grad_target_warps warps (facets with a DOF vertex x chunks).  The
+// mixed near-field kernel, whose work sits in few (facet, tile) places, may
+// instead take tune.near_tiles_per_chunk tiles per chunk (0: as above).
+static void grad_chunks(lf_ctx* c, int S, bool nearOnly, int* nchunks, int* tilesPerChunk) {
     const int ntiles = std::max(1, cdiv(S, kStationTile));
-    const int want = std::max(1, cdiv(kTargetGradWarps, std::max(c->nGradFacets, 1)));
-    *tilesPerChunk = cdiv(ntiles, std::min(want, ntiles));
+    if (nearOnly && c->tune.near_tiles_per_chunk > 0) {
+        *tilesPerChunk = std::min(c->tune.near_tiles_per_chunk, ntiles);
+    } else {
+        const int want = std::max(1, cdiv(c->tune.grad_target_warps, std::max(c->nGradFacets, 1)));
+        *tilesPerChunk = cdiv(ntiles, std::min(want, ntiles));
+    }
     *nchunks = cdiv(ntiles, *tilesPerChunk);
+}
+
+// Partial slots one station set takes (see gradient_set).
+static int grad_slots(lf_ctx* c, int S) {
+    int n1 = 1, n2 = 1, t = 1;
+    if (c->precision == LF_PREC_MIXED) {
+        grad_chunks(c, S, true, &n1, &t);
+        grad_chunks(c, S, false, &n2, &t);
+        return n1 + n2;
+    }
+    grad_chunks(c, S, false, &n1, &t);
+    return n1;
 }
 
 // Gradient kernels over one station set with the given adjoints; writes
@@ -997,24 +1017,28 @@ static int gradient_set(lf_ctx* c, const StationSet& s, const double* gcoef, con
     const bool mixed = c->precision == LF_PREC_MIXED;
     const double tau = mixed ? static_cast<double>(c->tau) : 3.0e38;
     int nch = 1, tpc = 1;
-    grad_chunks(c, s.n, &nch, &tpc);
-    const dim3 grid(cdiv(c->nGradFacets, kGradWarpsPerBlock), nch);
+    grad_chunks(c, s.n, mixed, &nch, &tpc);
+    const int fblocks = cdiv(c->nGradFacets, kGradWarpsPerBlock);
     int ev = prof_begin(c, c->evGrad, c->nGrad);
-    k_gradient_warp_fp64<<<grid, 32 * kGradWarpsPerBlock, 0, c->stream>>>(
+    k_gradient_warp_fp64<<<dim3(fblocks, nch), 32 * kGradWarpsPerBlock, 0, c->stream>>>(
         c->T, c->d_gc.p, s.n, s.d_xyz.p, gcoef, mcoef, s.d_tileBox.p, c->d_faceGroup.p, c->d_groups.p, c->fdir, tau,
         c->d_gradFacets.p, c->nGradFacets, tpc, c->d_partGrad.p + (size_t)slot0 * 9 * c->T);
     prof_end(c, c->evGrad, ev);
     c->counters.launches++;
+    int used = nch;
     if (mixed) {
+        int nch2 = 1, tpc2 = 1;
+        grad_chunks(c, s.n, false, &nch2, &tpc2);
         int ev2 = prof_begin(c, c->evGrad, c->nGrad);
-        k_gradient_warp_far32<<<grid, 32 * kGradWarpsPerBlock, 0, c->stream>>>(
+        k_gradient_warp_far32<<<dim3(fblocks, nch2), 32 * kGradWarpsPerBlock, 0, c->stream>>>(
             c->T, c->d_gc.p, s.n, s.d_xyz.p, gcoef, mcoef, s.d_tileBox.p, c->d_faceGroup.p, c->d_groups.p, c->fdir,
-            tau, c->d_gradFacets.p, c->nGradFacets, tpc, c->d_partGrad.p + (size_t)(slot0 + nch) * 9 * c->T);
+            tau, c->d_gradFacets.p, c->nGradFacets, tpc2, c->d_partGrad.p + (size_t)(slot0 + nch) * 9 * c->T);
         prof_end(c, c->evGrad, ev2);
         c->counters.launches++;
+        used += nch2;
     }
     c->counters.gradient_pairs += (uint64_t)s.n * (uint64_t)c->nGradFacets;
-    return mixed ? 2 * nch : nch;
+    return used;
 }
 
 static lf_status gradient_all(lf_ctx* c, const double* d_params, double* d_grad) {
@@ -1024,14 +1048,12 @@ static lf_status gradient_all(lf_ctx* c, const double* d_params, double* d_grad)
                                                              c->d_gc.p);
     c->counters.launches++;
     LF_CHECK_LAUNCH(c);
-    const int perKernel = c->precision == LF_PREC_MIXED ? 2 : 1;
-    int slots = 0, nch = 1, tpc = 1;
+    int slots = 0;
     if (c->sameStations && gOn) {
-        grad_chunks(c, c->grav.n, &nch, &tpc);
-        slots = perKernel * nch;
+        slots = grad_slots(c, c->grav.n);
     } else {
-        if (gOn) { grad_chunks(c, c->grav.n, &nch, &tpc); slots += perKernel * nch; }
-        if (mOn) { grad_chunks(c, c->mag.n, &nch, &tpc); slots += perKernel * nch; }
+        if (gOn) slots += grad_slots(c, c->grav.n);
+        if (mOn) slots += grad_slots(c, c->mag.n);
     }
     if (c->nGradFacets == 0) slots = 0;
     if (slots == 0) {
@@ -1047,7 +1069,7 @@ static lf_status gradient_all(lf_ctx* c, const double* d_params, double* d_grad)
         }
         LF_CHECK_LAUNCH(c);
         if (c->nGradVerts > 0) {
-            k_vertex_reduce<<<cdiv(c->nGradVerts, 128), 128, 0, c->stream>>>(c->nGradVerts, c->d_gradVerts.p,
+            k_vertex_reduce<<<cdiv(c->nGradVerts, 4), 128, 0, c->stream>>>(c->nGradVerts, c->d_gradVerts.p,
                                                                               c->d_vfOff.p, c->d_vf.p, c->T, used,
                                                                               c->d_partGrad.p, c->d_vgrad.p);
             c->counters.launches++;
@@ -1189,6 +1211,82 @@ static lf_status run_cached(lf_ctx* c, lf_ctx::GraphSet& set, const double* p, d
     g.grad = grad;
     g.delta = {after.forward_pairs - before.forward_pairs, after.gradient_pairs - before.gradient_pairs,
                after.launches - before.launches};
+    return LF_OK;
+}
+
+extern "C" lf_status lf_set_tuning(lf_ctx* c, const lf_tuning* t) {
+    if (!c || !t || t->fwd_target_blocks < 1 || t->grad_target_warps < 1 || t->near_tiles_per_chunk < 0)
+        return LF_EINVAL;
+    c->epoch++;
+    c->tune = *t;
+    c->chunkCapacityS = 0;  // re-plan the forward chunks
+    return LF_OK;
+}
+
+extern "C" lf_status lf_get_tuning(lf_ctx* c, lf_tuning* t) {
+    if (!c || !t) return LF_EINVAL;
+    *t = c->tune;
+    return LF_OK;
+}
+
+// Coordinate search over the launch shapes, each candidate timed with device
+// events over `repeats` direct (not replayed) objective+gradient evaluations
+// after one untimed evaluation that sizes buffers and uploads its plan.
+extern "C" lf_status lf_autotune(lf_ctx* c, const double* params, int repeats, lf_tuning* chosen, double* best_ms) {
+    LF_RET_IF(check_ready(c));
+    if (repeats <= 0) repeats = 3;
+    LF_RET_IF(params_to_device(c, params));
+    const bool graph = c->graphMode;
+    c->graphMode = false;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        if (e0) cudaEventDestroy(e0);
+        c->graphMode = graph;
+        return fail(c, LF_ECUDA, "event creation failed");
+    }
+    auto timeit = [&](const lf_tuning& t, double* ms) -> lf_status {
+        LF_RET_IF(lf_set_tuning(c, &t));
+        LF_RET_IF(lf_objective_grad_device(c, c->d_params.p, c->d_f.p, c->d_grad.p));
+        LF_TRY_CUDA(c, cudaEventRecord(e0, c->stream));
+        for (int r = 0; r < repeats; ++r) LF_RET_IF(lf_objective_grad_device(c, c->d_params.p, c->d_f.p, c->d_grad.p));
+        LF_TRY_CUDA(c, cudaEventRecord(e1, c->stream));
+        LF_TRY_CUDA(c, cudaEventSynchronize(e1));
+        float t_ms = 0.f;
+        LF_TRY_CUDA(c, cudaEventElapsedTime(&t_ms, e0, e1));
+        *ms = t_ms / repeats;
+        return LF_OK;
+    };
+    lf_tuning best = c->tune;
+    double bestMs = 0.0;
+    lf_status st = timeit(best, &bestMs);
+    const int fwdC[] = {148 * 2, 148 * 4, 148 * 8, 148 * 16};
+    const int gradC[] = {148 * 16, 148 * 32, 148 * 64, 148 * 128};
+    const int nearC[] = {0, 1, 2, 4, 8};
+    for (int dim = 0; dim < 3 && st == LF_OK; ++dim) {
+        const int* cand = dim == 0 ? fwdC : (dim == 1 ? gradC : nearC);
+        const int nc = dim == 2 ? 5 : 4;
+        if (dim == 2 && c->precision != LF_PREC_MIXED) break;
+        for (int k = 0; k < nc && st == LF_OK; ++k) {
+            lf_tuning t = best;
+            int& field = dim == 0 ? t.fwd_target_blocks : (dim == 1 ? t.grad_target_warps : t.near_tiles_per_chunk);
+            if (field == cand[k]) continue;
+            field = cand[k];
+            double ms = 0.0;
+            st = timeit(t, &ms);
+            if (st == LF_OK && ms < bestMs) {
+                bestMs = ms;
+                best = t;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->graphMode = graph;
+    lf_status st2 = lf_set_tuning(c, &best);
+    LF_RET_IF(st);
+    LF_RET_IF(st2);
+    if (chosen) *chosen = best;
+    if (best_ms) *best_ms = bestMs;
     return LF_OK;
 }
 

@@ -679,26 +679,35 @@ __global__ void __launch_bounds__(128) k_gradient_warp_fp64(int T, const double*
         for (int k = 0; k < 9; ++k) part[(size_t)k * T + f] = outv[k];
 }
 
-// Sums facet partials into vertex gradients (deterministic order: chunks,
-// then the vertex's incident (facet, corner) list), for the vertices listed.
+// Sums facet partials into vertex gradients: one warp per listed vertex,
+// lanes over its (chunk, incident facet corner) items, then a fixed warp
+// reduction (deterministic).
 __global__ void k_vertex_reduce(int nverts, const int32_t* __restrict__ verts, const int32_t* __restrict__ vf_off,
                                 const int32_t* __restrict__ vf, int T, int nchunks, const double* __restrict__ part,
                                 double* __restrict__ vgrad) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nverts) return;
-    int v = verts[i];
+    const int i = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (i >= nverts) return;  // warp-uniform
+    const int v = verts[i];
+    const int b = vf_off[v], ninc = vf_off[v + 1] - b;
+    const int items = nchunks * ninc;
     double gx = 0, gy = 0, gz = 0;
-    for (int c = 0; c < nchunks; ++c)
-        for (int k = vf_off[v]; k < vf_off[v + 1]; ++k) {
-            int f = vf[k] / 3, corner = vf[k] % 3;
-            const double* p = part + ((size_t)c * 9 + 3 * corner) * T + f;
-            gx += p[0];
-            gy += p[(size_t)T];
-            gz += p[(size_t)2 * T];
-        }
-    vgrad[3 * v] = gx;
-    vgrad[3 * v + 1] = gy;
-    vgrad[3 * v + 2] = gz;
+    for (int it = lane; it < items; it += 32) {
+        const int c = it / ninc, k = b + it % ninc;
+        const int f = vf[k] / 3, corner = vf[k] % 3;
+        const double* p = part + ((size_t)c * 9 + 3 * corner) * T + f;
+        gx += p[0];
+        gy += p[(size_t)T];
+        gz += p[(size_t)2 * T];
+    }
+    gx = warp_sum(gx);
+    gy = warp_sum(gy);
+    gz = warp_sum(gz);
+    if (lane == 0) {
+        vgrad[3 * v] = gx;
+        vgrad[3 * v + 1] = gy;
+        vgrad[3 * v + 2] = gz;
+    }
 }
 
 // grad[d] = sum_refs vgrad[vertex][axis] * axis scale + reference-model term

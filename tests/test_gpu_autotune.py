@@ -1,0 +1,47 @@
+"""Autotuner (lf_autotune): the chosen launch shapes come from the candidate
+sets, and the objective and gradient under any shape agree with the default
+shapes up to the summation order of partial sums: 1e-12 relative in FP64;
+1e-6 in mixed precision, where chunk boundaries regroup the FP32 far-field
+partial sums (the mixed gradient's own tolerance is 1e-5)."""
+import numpy as np
+import pytest
+
+from lithoinv3d_b200 import PREC_MIXED, LithoError, synth
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.max(np.abs(np.asarray(a) - np.asarray(b))) / max(np.max(np.abs(b)), 1e-300))
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_autotune_keeps_results(mixed):
+    p = synth.voxel_contact_model(shape=(12, 12, 6), n_side=24, cp_stride=2)
+    m = p.build_model()
+    x0 = m.assemble_parameters()
+    gen = p.make_context(m)
+    gobs, mobs = gen.forward(x0 + np.random.default_rng(3).normal(0, 4, len(x0)))
+    gen.close()
+    ctx = p.make_context(m, grav_obs=gobs, mag_obs=mobs)
+    if mixed:
+        ctx.set_precision(PREC_MIXED)
+    tol = 1e-6 if mixed else 1e-12
+    f0, g0 = ctx.objective_and_gradient(x0)
+    t, ms = ctx.autotune(x0, repeats=2)
+    assert ms > 0
+    assert t.fwd_target_blocks in (148 * 2, 148 * 4, 148 * 8, 148 * 16)
+    assert t.grad_target_warps in (148 * 16, 148 * 32, 148 * 64, 148 * 128)
+    assert t.near_tiles_per_chunk in (0, 1, 2, 4, 8)
+    got = ctx.tuning()
+    assert (got.fwd_target_blocks, got.grad_target_warps, got.near_tiles_per_chunk) == \
+        (t.fwd_target_blocks, t.grad_target_warps, t.near_tiles_per_chunk)
+    f1, g1 = ctx.objective_and_gradient(x0)
+    assert abs(f1 - f0) <= tol * abs(f0) and rel(g1, g0) < tol
+    # extreme shapes give the same numbers too
+    for shape in ((148, 148, 1), (148 * 32, 148 * 256, 3)):
+        ctx.set_tuning(*shape)
+        f2, g2 = ctx.objective_and_gradient(x0)
+        assert abs(f2 - f0) <= tol * abs(f0) and rel(g2, g0) < tol
+    with pytest.raises(LithoError):
+        ctx.set_tuning(0, 1, 0)
