@@ -888,7 +888,7 @@ static lf_status forward_set(lf_ctx* c, const StationSet& s, double* d_gz, doubl
             TMI ? c->d_partM.p : nullptr);
         prof_end(c, c->evFwd, slot);
     }
-    k_forward_reduce<<<cdiv(S, 256), 256, 0, c->stream>>>(S, nch, c->d_chunkGroup.p, c->d_groups.p,
+    k_forward_reduce<<<cdiv(S, 32), 256, 0, c->stream>>>(S, nch, c->d_chunkGroup.p, c->d_groups.p,
                                                           GZ ? c->d_partG.p : nullptr, TMI ? c->d_partM.p : nullptr,
                                                           GZ ? d_gz : nullptr, TMI ? d_tmi : nullptr);
     c->counters.launches += 2;
@@ -915,7 +915,7 @@ static lf_status forward_set_mixed(lf_ctx* c, const StationSet& s, double* d_gz,
             TMI ? c->d_partM.p : nullptr, c->d_nearPairs.p);
         prof_end(c, c->evFwd, slot);
     }
-    k_forward_reduce_mixed<<<cdiv(S, 256), 256, 0, c->stream>>>(S, nch, GZ ? c->d_partG.p : nullptr,
+    k_forward_reduce_mixed<<<cdiv(S, 32), 256, 0, c->stream>>>(S, nch, GZ ? c->d_partG.p : nullptr,
                                                                 TMI ? c->d_partM.p : nullptr, GZ ? d_gz : nullptr,
                                                                 TMI ? d_tmi : nullptr);
     c->counters.launches += 2;
@@ -1259,12 +1259,12 @@ extern "C" lf_status lf_autotune(lf_ctx* c, const double* params, int repeats, l
     lf_tuning best = c->tune;
     double bestMs = 0.0;
     lf_status st = timeit(best, &bestMs);
-    const int fwdC[] = {148 * 2, 148 * 4, 148 * 8, 148 * 16};
+    const int fwdC[] = {148 * 4, 148 * 8, 148 * 16, 148 * 32, 148 * 64};
     const int gradC[] = {148 * 16, 148 * 32, 148 * 64, 148 * 128};
     const int nearC[] = {0, 1, 2, 4, 8};
     for (int dim = 0; dim < 3 && st == LF_OK; ++dim) {
         const int* cand = dim == 0 ? fwdC : (dim == 1 ? gradC : nearC);
-        const int nc = dim == 2 ? 5 : 4;
+        const int nc = dim == 1 ? 4 : 5;
         if (dim == 2 && c->precision != LF_PREC_MIXED) break;
         for (int k = 0; k < nc && st == LF_OK; ++k) {
             lf_tuning t = best;

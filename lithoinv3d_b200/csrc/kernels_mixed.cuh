@@ -629,18 +629,33 @@ __global__ void __launch_bounds__(128) k_gradient_warp_far32(int T, const double
 }
 
 // Per station: sum of chunk partials (facet scales are already applied).
-__global__ void k_forward_reduce_mixed(int S, int nchunks, const double* __restrict__ part_gz,
-                                       const double* __restrict__ part_tmi, double* __restrict__ gz,
-                                       double* __restrict__ tmi) {
-    int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= S) return;
+// Blocks of 32 stations x 8 chunk lanes: lane y sums chunks y, y+8, ...
+// (coalesced over stations), then the 8 lane sums are added in lane order.
+__global__ void __launch_bounds__(256) k_forward_reduce_mixed(int S, int nchunks, const double* __restrict__ part_gz,
+                                                              const double* __restrict__ part_tmi,
+                                                              double* __restrict__ gz, double* __restrict__ tmi) {
+    __shared__ double sg[8][33], st[8][33];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int s = blockIdx.x * 32 + tx;
     double g = 0.0, t = 0.0;
-    for (int c = 0; c < nchunks; ++c) {
-        if (part_gz) g += part_gz[(size_t)c * S + s];
-        if (part_tmi) t += part_tmi[(size_t)c * S + s];
+    if (s < S)
+        for (int c = ty; c < nchunks; c += 8) {
+            if (part_gz) g += part_gz[(size_t)c * S + s];
+            if (part_tmi) t += part_tmi[(size_t)c * S + s];
+        }
+    sg[ty][tx] = g;
+    st[ty][tx] = t;
+    __syncthreads();
+    if (ty == 0 && s < S) {
+        double G = 0.0, Tm = 0.0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            G += sg[k][tx];
+            Tm += st[k][tx];
+        }
+        if (gz) gz[s] = G;
+        if (tmi) tmi[s] = Tm;
     }
-    if (gz) gz[s] = g;
-    if (tmi) tmi[s] = t;
 }
 
 }  // namespace litho_b200
