@@ -195,9 +195,11 @@ lf_status lf_forward(lf_ctx* ctx, const double* params, double* gz, double* tmi)
 /* Launch shapes of the hot kernels (no reference counterpart).
  *  fwd_target_blocks     forward CTAs per launch: stations/128 x facet chunks;
  *                        more chunks = more CTAs, each over fewer facets
+ *                        (candidates 148 x {4, 8, 16, 32, 64})
  *  grad_target_warps     gradient warps per launch: DOF facets x station chunks
+ *                        (148 x {16, 32, 64, 128})
  *  near_tiles_per_chunk  mixed near-field gradient: 64-station tiles per warp
- *                        (0: the grad_target_warps split)
+ *                        (0: the grad_target_warps split; candidates 0, 1, 2, 4, 8)
  * lf_autotune measures candidates on the context's own model, stations and
  * precision, at params, and keeps the fastest; lf_set_tuning / lf_get_tuning
  * set and read them directly.  Results do not depend on the shapes beyond
@@ -213,6 +215,22 @@ lf_status lf_get_tuning(lf_ctx* ctx, lf_tuning* t);
  * events) and keeps the fastest; *best_ms (may be NULL) = its time per
  * evaluation.  Needs the model and the data set. */
 lf_status lf_autotune(lf_ctx* ctx, const double* params, int repeats, lf_tuning* chosen, double* best_ms);
+
+/* Batched bodies (no reference counterpart: the reference inverts one model
+ * at a time).  Many independent closed bodies are given as the groups of one
+ * model (lf_set_model / lf_set_model_tables, one group per body), and their
+ * station grids as one concatenated list: counts[g] stations of body g, in
+ * group order, in both data sets.  Each body's facets then see only its own
+ * stations; the forward runs as one persistent launch over (body, station
+ * block, facet chunk) items ordered largest first, and the gradient as one
+ * launch over every body's facets.  The objective is the sum of the bodies'
+ * objectives (the gradient is separable: each body's DOFs see only its own
+ * misfit); lf_get_group_objectives returns the per-body data misfits of the
+ * last evaluation.  Call before setting the station data (it clears them);
+ * counts = NULL turns batching off.  Dense Jacobian rows and unit responses
+ * are not available in this mode (LF_ESTATE). */
+lf_status lf_set_station_groups(lf_ctx* ctx, int n_groups, const int32_t* counts);
+lf_status lf_get_group_objectives(lf_ctx* ctx, double* out);
 
 /* Graph mode (no reference counterpart: the reference evaluates on one CPU
  * thread).  When enabled, lf_objective, lf_objective_grad and

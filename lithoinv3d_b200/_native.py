@@ -76,6 +76,8 @@ SIGNATURES = {
     "lf_jacobian": (C.c_int, [_vp, _dp, C.c_int, _dp]),
     "lf_unit_response": (C.c_int, [_vp, _dp, C.c_int, C.c_int, _dp, _dp]),
     "lf_set_graph_mode": (C.c_int, [_vp, C.c_int]),
+    "lf_set_station_groups": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_int32)]),
+    "lf_get_group_objectives": (C.c_int, [_vp, _dp]),
     "lf_set_tuning": (C.c_int, [_vp, C.c_void_p]),
     "lf_get_tuning": (C.c_int, [_vp, C.c_void_p]),
     "lf_autotune": (C.c_int, [_vp, _dp, C.c_int, C.c_void_p, _dp]),

@@ -244,6 +244,20 @@ class Context:
         self._check(self.lib.lf_autotune(self.h, _d(f64(params)), repeats, C.byref(t), _d(ms)), "autotune")
         return t, float(ms[0])
 
+    def set_station_groups(self, counts):
+        """Batched bodies (lf_set_station_groups): counts[g] stations of group g;
+        None turns batching off.  Set station data afterwards."""
+        if counts is None:
+            self._check(self.lib.lf_set_station_groups(self.h, 0, None), "set_station_groups")
+            return
+        c = i32(counts)
+        self._check(self.lib.lf_set_station_groups(self.h, len(c), _i(c)), "set_station_groups")
+
+    def group_objectives(self, n_groups: int) -> np.ndarray:
+        out = np.zeros(n_groups)
+        self._check(self.lib.lf_get_group_objectives(self.h, _d(out)), "group_objectives")
+        return out
+
     def set_graph_mode(self, enabled: bool = True):
         """Replay evaluations as a captured CUDA graph (lf_set_graph_mode)."""
         self._check(self.lib.lf_set_graph_mode(self.h, int(bool(enabled))), "set_graph_mode")

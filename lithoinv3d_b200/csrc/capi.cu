@@ -100,6 +100,7 @@ struct lf_ctx {
     DevBuf<int16_t> d_faceGroup;
     DevBuf<GroupConst> d_groups;
     int nInterpRows = 0, nSync = 0, nGradVerts = 0, nGradFacets = 0;
+    std::vector<int32_t> hGradFacets;
 
     // forward chunking (plan cached per station count and group filter;
     // uploaded only when it changes)
@@ -150,6 +151,20 @@ struct lf_ctx {
     // launch shapes chosen by lf_autotune (defaults: measured on the
     // 19k-facet, 4096-station contact model)
     lf_tuning tune{148 * 4, 148 * 64, 0};
+
+    // Batched bodies (lf_set_station_groups): each group is one body and
+    // sees only its own station range [grpStaOff[g], grpStaOff[g+1]) of both
+    // data sets.  The forward runs a persistent item list (body, station
+    // block, facet chunk), planned when planEpoch moves.
+    bool partitioned = false;
+    std::vector<int32_t> grpStaOff, grpTileOff;
+    DevBuf<int32_t> d_grpStaOff, d_grpTileOff, d_staGroup, d_grpNch;
+    DevBuf<int64_t> d_grpPartOff;
+    DevBuf<FwdItem> d_items;
+    DevBuf<double> d_grpF;
+    int nItems = 0, maxGroupStations = 0;
+    int64_t partTotal = 0, itemPairs = 0;
+    uint64_t planEpoch = 0, itemsEpoch = ~0ull;
 
     // optional per-kernel timing (events on `stream`)
     bool profiling = false;
@@ -565,6 +580,7 @@ extern "C" lf_status lf_set_model_tables(lf_ctx* c, int G, const double* density
     for (int f = 0; f < nt; ++f)
         if (fneed[f]) gfacets.push_back(f);
     c->nGradFacets = static_cast<int>(gfacets.size());
+    c->hGradFacets = gfacets;
     if (!gfacets.empty()) LF_TRY_CUDA(c, upload(c->d_gradFacets, gfacets.data(), gfacets.size(), c->stream));
     LF_TRY_CUDA(c, upload(c->d_gradVerts, gverts.data(), gverts.size(), c->stream));
     LF_TRY_CUDA(c, upload(c->d_faceNeeds, fneed.data(), fneed.size(), c->stream));
@@ -583,6 +599,8 @@ extern "C" lf_status lf_set_model_tables(lf_ctx* c, int G, const double* density
     c->hasRef = false;
     c->smoothOn = false;
     c->vertexFreedom.clear();
+    c->partitioned = false;
+    c->planEpoch++;
     c->hasModel = true;
     LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
     return LF_OK;
@@ -702,28 +720,38 @@ static lf_status set_stations(lf_ctx* c, StationSet& s, int n, const double* xyz
         if (obs) s.obs[i] = obs[i];
         if (sd && sd[i] > 0) s.w[i] = 1.0 / sd[i];  // objective.cpp:26
     }
-    // Morton order of (x, y) quantised to 16 bits over the set's extent
+    // Segments: the whole set, or each group's stations when the stations
+    // are partitioned among batched bodies (lf_set_station_groups).
+    std::vector<int32_t> seg = {0, n};
+    if (c->partitioned) {
+        if (n != c->grpStaOff.back())
+            return fail(c, LF_EINVAL, "station count differs from the sum of lf_set_station_groups counts");
+        seg = c->grpStaOff;
+    }
+    // Morton order of (x, y) quantised to 16 bits over each segment's extent
     s.perm.resize(n);
-    {
+    for (size_t g = 0; g + 1 < seg.size(); ++g) {
+        const int b = seg[g], e = seg[g + 1];
         double lo[2] = {1e300, 1e300}, hi[2] = {-1e300, -1e300};
-        for (int i = 0; i < n; ++i)
+        for (int i = b; i < e; ++i)
             for (int k = 0; k < 2; ++k) {
                 lo[k] = std::min(lo[k], s.xyz[3 * i + k]);
                 hi[k] = std::max(hi[k], s.xyz[3 * i + k]);
             }
-        std::vector<std::pair<uint32_t, int32_t>> key(n);
-        for (int i = 0; i < n; ++i) {
+        std::vector<std::pair<uint32_t, int32_t>> key(e - b);
+        for (int i = b; i < e; ++i) {
             uint32_t q[2];
             for (int k = 0; k < 2; ++k) {
                 double span = hi[k] - lo[k];
                 q[k] = span > 0 ? static_cast<uint32_t>((s.xyz[3 * i + k] - lo[k]) / span * 65535.0) : 0u;
             }
             uint32_t m = 0;
-            for (int b = 0; b < 16; ++b) m |= ((q[0] >> b) & 1u) << (2 * b) | ((q[1] >> b) & 1u) << (2 * b + 1);
-            key[i] = {m, i};
+            for (int bit = 0; bit < 16; ++bit)
+                m |= ((q[0] >> bit) & 1u) << (2 * bit) | ((q[1] >> bit) & 1u) << (2 * bit + 1);
+            key[i - b] = {m, i};
         }
         std::stable_sort(key.begin(), key.end());
-        for (int i = 0; i < n; ++i) s.perm[i] = key[i].second;
+        for (int i = b; i < e; ++i) s.perm[i] = key[i - b].second;
     }
     std::vector<double> px(3 * (size_t)n), po(n), pw(n);
     for (int i = 0; i < n; ++i) {
@@ -736,20 +764,30 @@ static lf_status set_stations(lf_ctx* c, StationSet& s, int n, const double* xyz
     LF_TRY_CUDA(c, upload(s.d_obs, po.data(), po.size(), c->stream));
     LF_TRY_CUDA(c, upload(s.d_w, pw.data(), pw.size(), c->stream));
     LF_TRY_CUDA(c, upload(s.d_perm, s.perm.data(), s.perm.size(), c->stream));
-    // bounding box of every tile of kStationTile consecutive (Morton-ordered) stations
+    // bounding box of every tile of kStationTile consecutive (Morton-ordered)
+    // stations; tiles never straddle segments
     {
-        int nt = cdiv(std::max(n, 1), kStationTile);
-        std::vector<double> box(6 * (size_t)nt);
-        for (int t = 0; t < nt; ++t) {
-            double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-            for (int i = t * kStationTile; i < std::min(n, (t + 1) * kStationTile); ++i)
-                for (int k = 0; k < 3; ++k) {
-                    lo[k] = std::min(lo[k], px[3 * i + k]);
-                    hi[k] = std::max(hi[k], px[3 * i + k]);
-                }
-            for (int k = 0; k < 3; ++k) { box[6 * t + k] = lo[k]; box[6 * t + 3 + k] = hi[k]; }
+        std::vector<double> box;
+        std::vector<int32_t> tileOff(1, 0);
+        for (size_t g = 0; g + 1 < seg.size(); ++g) {
+            for (int t0 = seg[g]; t0 < seg[g + 1]; t0 += kStationTile) {
+                double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+                for (int i = t0; i < std::min(seg[g + 1], t0 + kStationTile); ++i)
+                    for (int k = 0; k < 3; ++k) {
+                        lo[k] = std::min(lo[k], px[3 * i + k]);
+                        hi[k] = std::max(hi[k], px[3 * i + k]);
+                    }
+                for (int k = 0; k < 3; ++k) box.push_back(lo[k]);
+                for (int k = 0; k < 3; ++k) box.push_back(hi[k]);
+            }
+            tileOff.push_back(static_cast<int32_t>(box.size() / 6));
         }
+        if (box.empty()) box.assign(6, 0.0);
         LF_TRY_CUDA(c, upload(s.d_tileBox, box.data(), box.size(), c->stream));
+        if (c->partitioned) {
+            c->grpTileOff = tileOff;
+            LF_TRY_CUDA(c, upload(c->d_grpTileOff, tileOff.data(), tileOff.size(), c->stream));
+        }
     }
     LF_TRY_CUDA(c, s.d_pred.reserve(std::max(n, 1)));
     LF_TRY_CUDA(c, s.d_coef.reserve(std::max(n, 1)));
@@ -757,6 +795,7 @@ static lf_status set_stations(lf_ctx* c, StationSet& s, int n, const double* xyz
     c->sameStations = c->grav.n > 0 && c->grav.n == c->mag.n && c->grav.xyz == c->mag.xyz &&
                       c->grav.perm == c->mag.perm;
     c->chunkCapacityS = 0;
+    c->planEpoch++;
     LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
     return LF_OK;
 }
@@ -870,8 +909,125 @@ static lf_status scatter(lf_ctx* c, const double* d_params) {
     return LF_OK;
 }
 
+// Batched bodies: the stations of both data sets are the concatenation of
+// per-group station lists (counts[g] stations for group g, in group order);
+// each group's facets then see only their own group's stations.  Station
+// data must be (re)set after this call.  counts == NULL turns it off.
+extern "C" lf_status lf_set_station_groups(lf_ctx* c, int G, const int32_t* counts) {
+    if (!c) return LF_EINVAL;
+    if (!c->hasModel) return fail(c, LF_ESTATE, "lf_set_station_groups before lf_set_model");
+    c->epoch++;
+    c->planEpoch++;
+    c->grav.n = c->mag.n = 0;
+    c->sameStations = false;
+    if (!counts) {
+        c->partitioned = false;
+        return LF_OK;
+    }
+    if (G != c->G) return fail(c, LF_EINVAL, "lf_set_station_groups: one count per group");
+    std::vector<int32_t> off(G + 1, 0);
+    int mx = 0;
+    for (int g = 0; g < G; ++g) {
+        if (counts[g] < 0) return fail(c, LF_EINVAL, "lf_set_station_groups: negative count");
+        off[g + 1] = off[g] + counts[g];
+        mx = std::max(mx, counts[g]);
+    }
+    std::vector<int32_t> sg(std::max(off[G], 1), 0);
+    for (int g = 0; g < G; ++g)
+        for (int i = off[g]; i < off[g + 1]; ++i) sg[i] = g;
+    LF_TRY_CUDA(c, upload(c->d_grpStaOff, off.data(), off.size(), c->stream));
+    LF_TRY_CUDA(c, upload(c->d_staGroup, sg.data(), sg.size(), c->stream));
+    LF_TRY_CUDA(c, c->d_grpF.reserve(G));
+    LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->grpStaOff = off;
+    c->maxGroupStations = mx;
+    c->partitioned = true;
+    return LF_OK;
+}
+
+extern "C" lf_status lf_get_group_objectives(lf_ctx* c, double* out) {
+    if (!c || !out) return LF_EINVAL;
+    if (!c->partitioned) return fail(c, LF_ESTATE, "no station groups set");
+    LF_TRY_CUDA(c, cudaMemcpyAsync(out, c->d_grpF.p, sizeof(double) * c->G, cudaMemcpyDeviceToHost, c->stream));
+    LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
+    return LF_OK;
+}
+
+// Item list of the batched forward: every (group, 128-station block, facet
+// chunk), chunk length chosen from the total own-group pairs so that the
+// list holds ~4 items per persistent CTA; ordered by cost, largest first.
+static lf_status plan_items(lf_ctx* c) {
+    if (c->itemsEpoch == c->planEpoch) return LF_OK;
+    const int G = c->G;
+    int64_t pairs = 0;
+    for (int g = 0; g < G; ++g)
+        pairs += (int64_t)(c->grpStaOff[g + 1] - c->grpStaOff[g]) * (c->grpTriOff[g + 1] - c->grpTriOff[g]);
+    const int64_t targetItems = 4 * (int64_t)c->tune.fwd_target_blocks;
+    const int64_t F64 = std::max<int64_t>(kFwdFacetTile, (pairs / (128 * targetItems) + 31) / 32 * 32);
+    const int F = static_cast<int>(std::min<int64_t>(F64, 1 << 30));
+    std::vector<FwdItem> items;
+    std::vector<int64_t> partOff(G + 1, 0);
+    std::vector<int32_t> nch(G, 0);
+    int64_t off = 0;
+    for (int g = 0; g < G; ++g) {
+        const int sb = c->grpStaOff[g], se = c->grpStaOff[g + 1], Sg = se - sb;
+        const int fb = c->grpTriOff[g], Tg = c->grpTriOff[g + 1] - fb;
+        partOff[g] = off;
+        if (Sg == 0 || Tg == 0) continue;
+        nch[g] = cdiv(Tg, F);
+        for (int k = 0; k < nch[g]; ++k)
+            for (int s0 = sb; s0 < se; s0 += kFwdThreads)
+                items.push_back({s0, std::min(se, s0 + kFwdThreads), fb + k * F, std::min(fb + Tg, fb + (k + 1) * F),
+                                 off + (int64_t)k * Sg - sb});
+        off += (int64_t)nch[g] * Sg;
+    }
+    partOff[G] = off;
+    std::stable_sort(items.begin(), items.end(), [](const FwdItem& a, const FwdItem& b) {
+        return (int64_t)(a.s_end - a.s0) * (a.fe - a.fb) > (int64_t)(b.s_end - b.s0) * (b.fe - b.fb);
+    });
+    if (!items.empty()) LF_TRY_CUDA(c, upload(c->d_items, items.data(), items.size(), c->stream));
+    LF_TRY_CUDA(c, upload(c->d_grpPartOff, partOff.data(), partOff.size(), c->stream));
+    LF_TRY_CUDA(c, upload(c->d_grpNch, nch.data(), nch.size(), c->stream));
+    c->nItems = static_cast<int>(items.size());
+    c->partTotal = std::max<int64_t>(off, 1);
+    c->itemPairs = pairs;
+    c->itemsEpoch = c->planEpoch;
+    return LF_OK;
+}
+
+// Batched forward over one station set (both data types share the groups).
+template <bool GZ, bool TMI, bool MIXED>
+static lf_status forward_set_items(lf_ctx* c, const StationSet& s, double* d_gz, double* d_tmi) {
+    const int S = s.n;
+    if (S == 0) return LF_OK;
+    LF_RET_IF(plan_items(c));
+    if (GZ) LF_TRY_CUDA(c, c->d_partG.reserve((size_t)c->partTotal));
+    if (TMI) LF_TRY_CUDA(c, c->d_partM.reserve((size_t)c->partTotal));
+    if (c->nItems > 0) {
+        const int grid = std::min(c->nItems, c->tune.fwd_target_blocks);
+        int slot = prof_begin(c, c->evFwd, c->nFwd);
+        if (MIXED)
+            k_forward_mixed_items<GZ, TMI, kFwdFacetTile><<<grid, kFwdThreads, 0, c->stream>>>(
+                c->d_items.p, c->nItems, s.d_xyz.p, c->T, c->d_mc.p, c->tau, GZ ? c->d_partG.p : nullptr,
+                TMI ? c->d_partM.p : nullptr, c->d_nearPairs.p);
+        else
+            k_forward_fp64_items<GZ, TMI, kFwdFacetTile><<<grid, kFwdThreads, 0, c->stream>>>(
+                c->d_items.p, c->nItems, s.d_xyz.p, c->T, c->d_fc.p, GZ ? c->d_partG.p : nullptr,
+                TMI ? c->d_partM.p : nullptr);
+        prof_end(c, c->evFwd, slot);
+    }
+    k_forward_reduce_groups<<<cdiv(S, 32), 256, 0, c->stream>>>(
+        S, c->d_staGroup.p, c->d_grpStaOff.p, c->d_grpPartOff.p, c->d_grpNch.p, MIXED ? nullptr : c->d_groups.p,
+        GZ ? c->d_partG.p : nullptr, TMI ? c->d_partM.p : nullptr, GZ ? d_gz : nullptr, TMI ? d_tmi : nullptr);
+    c->counters.launches += 2;
+    c->counters.forward_pairs += (uint64_t)c->itemPairs;
+    LF_CHECK_LAUNCH(c);
+    return LF_OK;
+}
+
 template <bool GZ, bool TMI>
 static lf_status forward_set(lf_ctx* c, const StationSet& s, double* d_gz, double* d_tmi) {
+    if (c->partitioned) return forward_set_items<GZ, TMI, false>(c, s, d_gz, d_tmi);
     int S = s.n;
     if (S == 0) return LF_OK;
     plan_chunks(c, S);
@@ -899,6 +1055,7 @@ static lf_status forward_set(lf_ctx* c, const StationSet& s, double* d_gz, doubl
 
 template <bool GZ, bool TMI>
 static lf_status forward_set_mixed(lf_ctx* c, const StationSet& s, double* d_gz, double* d_tmi) {
+    if (c->partitioned) return forward_set_items<GZ, TMI, true>(c, s, d_gz, d_tmi);
     int S = s.n;
     if (S == 0) return LF_OK;
     plan_chunks(c, S);
@@ -962,6 +1119,15 @@ static lf_status residuals(lf_ctx* c, bool wantCoef) {
     else
         LF_TRY_CUDA(c, cudaMemsetAsync(c->d_blockM.p, 0, sizeof(double) * nbm, c->stream));
     c->counters.launches += 2;
+    if (c->partitioned) {  // per-body data misfit (lf_get_group_objectives)
+        const bool g = c->grav.n > 0;
+        k_group_misfit<<<c->G, 256, 0, c->stream>>>(c->G, c->d_grpStaOff.p, g ? c->grav.d_pred.p : nullptr,
+                                                     g ? c->grav.d_obs.p : nullptr, g ? c->grav.d_w.p : nullptr,
+                                                     magOn ? c->mag.d_pred.p : nullptr,
+                                                     magOn ? c->mag.d_obs.p : nullptr,
+                                                     magOn ? c->mag.d_w.p : nullptr, c->alphaMag, c->d_grpF.p);
+        c->counters.launches++;
+    }
     LF_CHECK_LAUNCH(c);
     return LF_OK;
 }
@@ -988,6 +1154,11 @@ static lf_status objective_final(lf_ctx* c, const double* d_params, double* d_f)
 // instead take tune.near_tiles_per_chunk tiles per chunk (0: as above).
 static void grad_chunks(lf_ctx* c, int S, bool nearOnly, int* nchunks, int* tilesPerChunk) {
     const int ntiles = std::max(1, cdiv(S, kStationTile));
+    if (c->partitioned) {  // batched bodies: one chunk covering the largest body's tiles
+        *tilesPerChunk = std::max(1, cdiv(c->maxGroupStations, kStationTile));
+        *nchunks = 1;
+        return;
+    }
     if (nearOnly && c->tune.near_tiles_per_chunk > 0) {
         *tilesPerChunk = std::min(c->tune.near_tiles_per_chunk, ntiles);
     } else {
@@ -1018,11 +1189,13 @@ static int gradient_set(lf_ctx* c, const StationSet& s, const double* gcoef, con
     const double tau = mixed ? static_cast<double>(c->tau) : 3.0e38;
     int nch = 1, tpc = 1;
     grad_chunks(c, s.n, mixed, &nch, &tpc);
+    const int32_t* grpSta = c->partitioned ? c->d_grpStaOff.p : nullptr;
+    const int32_t* grpTile = c->partitioned ? c->d_grpTileOff.p : nullptr;
     const int fblocks = cdiv(c->nGradFacets, kGradWarpsPerBlock);
     int ev = prof_begin(c, c->evGrad, c->nGrad);
     k_gradient_warp_fp64<<<dim3(fblocks, nch), 32 * kGradWarpsPerBlock, 0, c->stream>>>(
         c->T, c->d_gc.p, s.n, s.d_xyz.p, gcoef, mcoef, s.d_tileBox.p, c->d_faceGroup.p, c->d_groups.p, c->fdir, tau,
-        c->d_gradFacets.p, c->nGradFacets, tpc, c->d_partGrad.p + (size_t)slot0 * 9 * c->T);
+        c->d_gradFacets.p, c->nGradFacets, tpc, grpSta, grpTile, c->d_partGrad.p + (size_t)slot0 * 9 * c->T);
     prof_end(c, c->evGrad, ev);
     c->counters.launches++;
     int used = nch;
@@ -1032,12 +1205,21 @@ static int gradient_set(lf_ctx* c, const StationSet& s, const double* gcoef, con
         int ev2 = prof_begin(c, c->evGrad, c->nGrad);
         k_gradient_warp_far32<<<dim3(fblocks, nch2), 32 * kGradWarpsPerBlock, 0, c->stream>>>(
             c->T, c->d_gc.p, s.n, s.d_xyz.p, gcoef, mcoef, s.d_tileBox.p, c->d_faceGroup.p, c->d_groups.p, c->fdir,
-            tau, c->d_gradFacets.p, c->nGradFacets, tpc2, c->d_partGrad.p + (size_t)(slot0 + nch) * 9 * c->T);
+            tau, c->d_gradFacets.p, c->nGradFacets, tpc2, grpSta, grpTile,
+            c->d_partGrad.p + (size_t)(slot0 + nch) * 9 * c->T);
         prof_end(c, c->evGrad, ev2);
         c->counters.launches++;
         used += nch2;
     }
-    c->counters.gradient_pairs += (uint64_t)s.n * (uint64_t)c->nGradFacets;
+    if (c->partitioned) {
+        for (int32_t f : c->hGradFacets) {
+            const int g = static_cast<int>(std::upper_bound(c->grpTriOff.begin(), c->grpTriOff.end(), f) -
+                                           c->grpTriOff.begin()) - 1;
+            c->counters.gradient_pairs += (uint64_t)(c->grpStaOff[g + 1] - c->grpStaOff[g]);
+        }
+    } else {
+        c->counters.gradient_pairs += (uint64_t)s.n * (uint64_t)c->nGradFacets;
+    }
     return used;
 }
 
@@ -1220,6 +1402,7 @@ extern "C" lf_status lf_set_tuning(lf_ctx* c, const lf_tuning* t) {
     c->epoch++;
     c->tune = *t;
     c->chunkCapacityS = 0;  // re-plan the forward chunks
+    c->planEpoch++;
     return LF_OK;
 }
 
@@ -1360,6 +1543,7 @@ extern "C" lf_status lf_unit_response(lf_ctx* c, const double* params, int kind,
         return fail(c, LF_EINVAL, "lf_unit_response: bad kind, group or direction");
     StationSet& s = kind == LF_UNIT_GRAVITY ? c->grav : c->mag;
     if (s.n == 0) return fail(c, LF_ESTATE, "no stations of the requested type");
+    if (c->partitioned) return fail(c, LF_ESTATE, "unit responses are not available for batched bodies");
     LF_RET_IF(params_to_device(c, params));
     LF_RET_IF(scatter(c, c->d_params.p));
     std::vector<GroupConst> unit(c->gconst);
@@ -1432,6 +1616,7 @@ extern "C" lf_status lf_jacobian(lf_ctx* c, const double* params, int which, dou
     if (!J || (which != LF_GRAVITY && which != LF_MAGNETIC)) return LF_EINVAL;
     StationSet& s = which == LF_GRAVITY ? c->grav : c->mag;
     if (s.n == 0) return fail(c, LF_ESTATE, "no stations of the requested type");
+    if (c->partitioned) return fail(c, LF_ESTATE, "dense Jacobian rows are not available for batched bodies");
     LF_RET_IF(params_to_device(c, params));
     LF_RET_IF(scatter(c, c->d_params.p));
     k_face_prep_grad<<<cdiv(c->T, 128), 128, 0, c->stream>>>(c->T, c->d_tri.p, c->d_pos.p, c->d_faceGroup.p,

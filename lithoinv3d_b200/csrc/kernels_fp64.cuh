@@ -297,17 +297,15 @@ __device__ __forceinline__ void pair_forward_fp64(const double* __restrict__ s, 
 
 // Grid: x = station tiles of blockDim.x, y = facet chunks (each inside one
 // group).  Writes the chunk's unscaled facet sums per station.
+// One CTA's work: station s (act = s is a station of the block) against
+// facets [fb, fe); out_gz[s] / out_tmi[s] receive the unscaled sums.
 template <bool GZ, bool TMI, int FT>
-__global__ void __launch_bounds__(128) k_forward_fp64(int S, const double* __restrict__ sta, int T,
-                                                      const double* __restrict__ fc, const int32_t* __restrict__ chunk_begin,
-                                                      const int32_t* __restrict__ chunk_end, double* __restrict__ part_gz,
-                                                      double* __restrict__ part_tmi) {
-    __shared__ double sm[NFC * FT];
-    int s = blockIdx.x * blockDim.x + threadIdx.x;
-    int chunk = blockIdx.y;
-    int fb = chunk_begin[chunk], fe = chunk_end[chunk];
+__device__ __forceinline__ void forward_fp64_block(double* __restrict__ sm, int s, bool act,
+                                                   const double* __restrict__ sta, int T,
+                                                   const double* __restrict__ fc, int fb, int fe,
+                                                   double* __restrict__ out_gz, double* __restrict__ out_tmi) {
     d3 o = mk3(0, 0, 0);
-    if (s < S) o = mk3(sta[3 * s], sta[3 * s + 1], sta[3 * s + 2]);
+    if (act) o = mk3(sta[3 * s], sta[3 * s + 1], sta[3 * s + 2]);
     double gz = 0.0, tmi = 0.0;
     for (int f0 = fb; f0 < fe; f0 += FT) {
         int nf = min(FT, fe - f0);
@@ -317,13 +315,123 @@ __global__ void __launch_bounds__(128) k_forward_fp64(int S, const double* __res
             sm[idx] = (j < nf) ? fc[(size_t)k * T + f0 + j] : 0.0;
         }
         __syncthreads();
-        if (s < S)
+        if (act)
             for (int j = 0; j < nf; ++j) pair_forward_fp64<GZ, TMI>(sm, j, FT, o, &gz, &tmi);
     }
-    if (s < S) {
-        if (GZ) part_gz[(size_t)chunk * S + s] = gz;
-        if (TMI) part_tmi[(size_t)chunk * S + s] = tmi;
+    if (act) {
+        if (GZ) out_gz[s] = gz;
+        if (TMI) out_tmi[s] = tmi;
     }
+}
+
+template <bool GZ, bool TMI, int FT>
+__global__ void __launch_bounds__(128) k_forward_fp64(int S, const double* __restrict__ sta, int T,
+                                                      const double* __restrict__ fc, const int32_t* __restrict__ chunk_begin,
+                                                      const int32_t* __restrict__ chunk_end, double* __restrict__ part_gz,
+                                                      double* __restrict__ part_tmi) {
+    __shared__ double sm[NFC * FT];
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const int chunk = blockIdx.y;
+    forward_fp64_block<GZ, TMI, FT>(sm, s, s < S, sta, T, fc, chunk_begin[chunk], chunk_end[chunk],
+                                    GZ ? part_gz + (size_t)chunk * S : nullptr,
+                                    TMI ? part_tmi + (size_t)chunk * S : nullptr);
+}
+
+// Batched bodies: a persistent grid walks a list of (station block, facet
+// range) items -- one body's stations against one chunk of that body's
+// facets -- in the order given (largest first).  Item out: offset added to
+// the global station index to address the item's partial slot.
+struct FwdItem {
+    int32_t s0, s_end, fb, fe;
+    int64_t out;
+};
+
+template <bool GZ, bool TMI, int FT>
+__global__ void __launch_bounds__(128) k_forward_fp64_items(const FwdItem* __restrict__ items, int nitems,
+                                                            const double* __restrict__ sta, int T,
+                                                            const double* __restrict__ fc,
+                                                            double* __restrict__ part_gz, double* __restrict__ part_tmi) {
+    __shared__ double sm[NFC * FT];
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const FwdItem w = items[it];
+        const int s = w.s0 + (int)threadIdx.x;
+        forward_fp64_block<GZ, TMI, FT>(sm, s, s < w.s_end, sta, T, fc, w.fb, w.fe,
+                                        GZ ? part_gz + w.out : nullptr, TMI ? part_tmi + w.out : nullptr);
+    }
+}
+
+// Per station of a batch of bodies: sum of its body's chunk partials
+// (grp_part_off[g] + c * n_g + local index, c < grp_nch[g]), times the body's
+// group scales when `groups` is given (FP64 path; the mixed partials carry
+// their scales).  Lane sums over chunks as in k_forward_reduce.
+__global__ void __launch_bounds__(256) k_forward_reduce_groups(int S, const int32_t* __restrict__ sta_group,
+                                                               const int32_t* __restrict__ grp_sta_off,
+                                                               const int64_t* __restrict__ grp_part_off,
+                                                               const int32_t* __restrict__ grp_nch,
+                                                               const GroupConst* __restrict__ groups,
+                                                               const double* __restrict__ part_gz,
+                                                               const double* __restrict__ part_tmi,
+                                                               double* __restrict__ gz, double* __restrict__ tmi) {
+    __shared__ double sg[8][33], st[8][33];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int s = blockIdx.x * 32 + tx;
+    double g = 0.0, t = 0.0;
+    int grp = 0;
+    if (s < S) {
+        grp = sta_group[s];
+        const int n = grp_sta_off[grp + 1] - grp_sta_off[grp], loc = s - grp_sta_off[grp];
+        const int64_t base = grp_part_off[grp] + loc;
+        for (int c = ty; c < grp_nch[grp]; c += 8) {
+            if (part_gz) g += part_gz[base + (int64_t)c * n];
+            if (part_tmi) t += part_tmi[base + (int64_t)c * n];
+        }
+    }
+    sg[ty][tx] = g;
+    st[ty][tx] = t;
+    __syncthreads();
+    if (ty == 0 && s < S) {
+        double G = 0.0, Tm = 0.0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            G += sg[k][tx];
+            Tm += st[k][tx];
+        }
+        if (groups) {
+            G = G * groups[grp].gscale_fwd;
+            Tm = -groups[grp].mscale * Tm;
+        }
+        if (gz) gz[s] = G;
+        if (tmi) tmi[s] = Tm;
+    }
+}
+
+// Per body (group) of a batch: data misfit of its stations, gravity + alpha
+// x magnetic, from the residual definition of k_residual.
+__global__ void k_group_misfit(int G, const int32_t* __restrict__ grp_sta_off, const double* __restrict__ gpred,
+                               const double* __restrict__ gobs, const double* __restrict__ gw,
+                               const double* __restrict__ mpred, const double* __restrict__ mobs,
+                               const double* __restrict__ mw, double alpha, double* __restrict__ out) {
+    __shared__ double red[256];
+    const int g = blockIdx.x;
+    if (g >= G) return;
+    double acc = 0.0;
+    for (int s = grp_sta_off[g] + threadIdx.x; s < grp_sta_off[g + 1]; s += blockDim.x) {
+        if (gpred) {
+            const double r = gw[s] * (gobs[s] - gpred[s]);
+            acc += 0.5 * r * r;
+        }
+        if (mpred) {
+            const double r = mw[s] * (mobs[s] - mpred[s]);
+            acc += alpha * (0.5 * r * r);
+        }
+    }
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+        if (threadIdx.x < k) red[threadIdx.x] += red[threadIdx.x + k];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[g] = red[0];
 }
 
 // Sums chunk partials with the group scales applied chunk by chunk (a chunk
@@ -644,11 +752,20 @@ __global__ void __launch_bounds__(128) k_gradient_warp_fp64(int T, const double*
                                                             const int16_t* __restrict__ face_group,
                                                             const GroupConst* __restrict__ groups, d3 fdir, double tau,
                                                             const int32_t* __restrict__ facets, int nfacets,
-        int tiles_per_chunk, double* __restrict__ part) {
+        int tiles_per_chunk, const int32_t* __restrict__ grp_sta_off,
+        const int32_t* __restrict__ grp_tile_off, double* __restrict__ part) {
     const int lane = threadIdx.x & 31;
     const int w = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
     if (w >= nfacets) return;  // warp-uniform
     const int f = facets[w];
+    if (grp_sta_off) {  // batched bodies: only the facet's own body's stations
+        const int g = face_group[f], sb = grp_sta_off[g];
+        S = grp_sta_off[g + 1] - sb;
+        sta += 3 * (size_t)sb;
+        if (gcoef) gcoef += sb;
+        if (mcoef) mcoef += sb;
+        tile_box += 6 * (size_t)grp_tile_off[g];
+    }
     // this chunk's station tiles
     const int ntiles_all = (S + kStationTile - 1) / kStationTile;
     const int tbeg = blockIdx.y * tiles_per_chunk, ntiles = min(ntiles_all, tbeg + tiles_per_chunk);

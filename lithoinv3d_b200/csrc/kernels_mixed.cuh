@@ -290,20 +290,16 @@ __device__ __forceinline__ void pair_near_f64(const double* __restrict__ s, int 
 // warp's station bounding box -- centroid at least tau x size away: far
 // (FP32, 7-point gz); at least tau/2 x size: mid (FP32, 28-point gz); else
 // near (FP64 analytic) -- and the warp walks each class warp-uniformly.
+// One CTA's work: station s (this thread; act = s is a station of the
+// block) against facets [fb, fe); out_gz[s] / out_tmi[s] receive the sums.
 template <bool GZ, bool TMI, int FT>
-__global__ void __launch_bounds__(128) k_forward_mixed(int S, const double* __restrict__ sta, int T,
-                                                       const double* __restrict__ mc, const int32_t* __restrict__ chunk_begin,
-                                                       const int32_t* __restrict__ chunk_end, float tau,
-                                                       double* __restrict__ part_gz, double* __restrict__ part_tmi,
-                                                       unsigned long long* __restrict__ near_pairs) {
+__device__ __forceinline__ void forward_mixed_block(double* __restrict__ smd, FaceF32* __restrict__ smf, int s,
+                                                    bool act, const double* __restrict__ sta, int T,
+                                                    const double* __restrict__ mc, int fb, int fe, float tau,
+                                                    double* __restrict__ out_gz, double* __restrict__ out_tmi,
+                                                    unsigned long long* __restrict__ near_pairs) {
     static_assert(FT == 32, "one facet per lane in the near/far test");
-    __shared__ double smd[NMC * FT];
-    __shared__ FaceF32 smf[FT];
     const int lane = threadIdx.x & 31;
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    const int chunk = blockIdx.y;
-    const int fb = chunk_begin[chunk], fe = chunk_end[chunk];
-    const bool act = s < S;
     double ox = 0.0, oy = 0.0, oz = 0.0;
     if (act) { ox = sta[3 * s]; oy = sta[3 * s + 1]; oz = sta[3 * s + 2]; }
     // the warp's station bounding box: lo = min, hi = -min(-x)
@@ -384,9 +380,42 @@ __global__ void __launch_bounds__(128) k_forward_mixed(int S, const double* __re
         }
     }
     if (act) {
-        if (GZ) part_gz[(size_t)chunk * S + s] = gz;
-        if (TMI) part_tmi[(size_t)chunk * S + s] = tmi;
+        if (GZ) out_gz[s] = gz;
+        if (TMI) out_tmi[s] = tmi;
         if (near_pairs && nearCount) atomicAdd(near_pairs, nearCount);
+    }
+}
+
+template <bool GZ, bool TMI, int FT>
+__global__ void __launch_bounds__(128) k_forward_mixed(int S, const double* __restrict__ sta, int T,
+                                                       const double* __restrict__ mc, const int32_t* __restrict__ chunk_begin,
+                                                       const int32_t* __restrict__ chunk_end, float tau,
+                                                       double* __restrict__ part_gz, double* __restrict__ part_tmi,
+                                                       unsigned long long* __restrict__ near_pairs) {
+    __shared__ double smd[NMC * FT];
+    __shared__ FaceF32 smf[FT];
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const int chunk = blockIdx.y;
+    forward_mixed_block<GZ, TMI, FT>(smd, smf, s, s < S, sta, T, mc, chunk_begin[chunk], chunk_end[chunk], tau,
+                                     GZ ? part_gz + (size_t)chunk * S : nullptr,
+                                     TMI ? part_tmi + (size_t)chunk * S : nullptr, near_pairs);
+}
+
+// Batched bodies (item list as for k_forward_fp64_items).
+template <bool GZ, bool TMI, int FT>
+__global__ void __launch_bounds__(128) k_forward_mixed_items(const FwdItem* __restrict__ items, int nitems,
+                                                             const double* __restrict__ sta, int T,
+                                                             const double* __restrict__ mc, float tau,
+                                                             double* __restrict__ part_gz, double* __restrict__ part_tmi,
+                                                             unsigned long long* __restrict__ near_pairs) {
+    __shared__ double smd[NMC * FT];
+    __shared__ FaceF32 smf[FT];
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const FwdItem w = items[it];
+        const int s = w.s0 + (int)threadIdx.x;
+        forward_mixed_block<GZ, TMI, FT>(smd, smf, s, s < w.s_end, sta, T, mc, w.fb, w.fe, tau,
+                                         GZ ? part_gz + w.out : nullptr, TMI ? part_tmi + w.out : nullptr,
+                                         near_pairs);
     }
 }
 
@@ -436,11 +465,20 @@ __global__ void __launch_bounds__(128) k_gradient_warp_far32(int T, const double
                                                              const int16_t* __restrict__ face_group,
                                                              const GroupConst* __restrict__ groups, d3 fdir,
                                                              double tau, const int32_t* __restrict__ facets, int nfacets,
-        int tiles_per_chunk, double* __restrict__ part) {
+        int tiles_per_chunk, const int32_t* __restrict__ grp_sta_off,
+        const int32_t* __restrict__ grp_tile_off, double* __restrict__ part) {
     const int lane = threadIdx.x & 31;
     const int w = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
     if (w >= nfacets) return;  // warp-uniform
     const int f = facets[w];
+    if (grp_sta_off) {  // batched bodies: only the facet's own body's stations
+        const int g = face_group[f], sb = grp_sta_off[g];
+        S = grp_sta_off[g + 1] - sb;
+        sta += 3 * (size_t)sb;
+        if (gcoef) gcoef += sb;
+        if (mcoef) mcoef += sb;
+        tile_box += 6 * (size_t)grp_tile_off[g];
+    }
     // this chunk's station tiles
     const int ntiles_all = (S + kStationTile - 1) / kStationTile;
     const int tbeg = blockIdx.y * tiles_per_chunk, ntiles = min(ntiles_all, tbeg + tiles_per_chunk);

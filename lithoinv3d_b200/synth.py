@@ -166,6 +166,7 @@ class Problem:
     cp_stride: int = 0
     depth_bounds: Optional[tuple] = None
     extra: dict = field(default_factory=dict)
+    station_groups: Optional[List[int]] = None  # batched bodies: stations per group, in group order
 
     def build_model(self) -> Model:
         m = Model()
@@ -180,7 +181,7 @@ class Problem:
             m.set_depth_bounds(*self.depth_bounds)
         if self.cp_stride > 0:
             m.set_control_point_stride(self.cp_stride)
-        if len(self.meshes) > 1:
+        if len(self.meshes) > 1 and self.station_groups is None:
             m.build_shared_vertex_sync()
         return m
 
@@ -191,6 +192,8 @@ class Problem:
                      mag_std=None) -> Context:
         ctx = Context(device)
         ctx.set_model(model)
+        if self.station_groups is not None:
+            ctx.set_station_groups(self.station_groups)
         ctx.set_field(*self.inducing)
         ctx.set_gravity_data(self.grav_xyz, grav_obs, grav_std)
         if self.mag_xyz is not None:
@@ -237,3 +240,105 @@ def voxel_contact_model(shape=(24, 24, 12), cell=100.0, n_groups=4, n_blobs=6, s
     p = Problem("voxel", rho, chi, meshes, st, st if joint else None, cp_stride=cp_stride, axis_scale=axis_scale)
     p.extra["labels"] = labels
     return p
+
+
+# ------------------------------------------------------------ batched bodies --
+
+
+def latlong_sphere(n_lat: int, n_lon: int):
+    """Closed unit sphere: two poles and (n_lat - 1) rings of n_lon vertices;
+    2 n_lon (n_lat - 1) triangles, outward."""
+    V = [(0.0, 0.0, 1.0)]
+    for i in range(1, n_lat):
+        th = np.pi * i / n_lat
+        for j in range(n_lon):
+            ph = 2 * np.pi * j / n_lon
+            V.append((np.sin(th) * np.cos(ph), np.sin(th) * np.sin(ph), np.cos(th)))
+    V.append((0.0, 0.0, -1.0))
+    V = np.array(V)
+    south = len(V) - 1
+
+    def ring(i, j):
+        return 1 + (i - 1) * n_lon + (j % n_lon)
+
+    F = []
+    for j in range(n_lon):
+        F.append((0, ring(1, j), ring(1, j + 1)))
+    for i in range(1, n_lat - 1):
+        for j in range(n_lon):
+            a, b, c, d = ring(i, j), ring(i, j + 1), ring(i + 1, j), ring(i + 1, j + 1)
+            F.append((a, c, d))
+            F.append((a, d, b))
+    for j in range(n_lon):
+        F.append((south, ring(n_lat - 1, j + 1), ring(n_lat - 1, j)))
+    F = np.array(F, dtype=np.int32)
+    if signed_volume(V, F) < 0:
+        F = F[:, [0, 2, 1]].copy()
+    return V, F
+
+
+def star_prism(n_poly: int, n_layers: int, rng: np.random.Generator):
+    """Closed prism over a random star-shaped polygon (radius 0.6-1.0 at
+    n_poly sorted angles), n_layers side layers of height 2 / n_layers, caps
+    fanned from their centres: 2 n_poly n_layers + 2 n_poly triangles."""
+    ang = np.sort(rng.uniform(0, 2 * np.pi, n_poly))
+    rad = rng.uniform(0.6, 1.0, n_poly)
+    zs = np.linspace(1.0, -1.0, n_layers + 1)
+    V = [(r * np.cos(a), r * np.sin(a), z) for z in zs for a, r in zip(ang, rad)]
+    top, bot = len(V), len(V) + 1
+    V += [(0.0, 0.0, 1.0), (0.0, 0.0, -1.0)]
+    V = np.array(V)
+    F = []
+    for l in range(n_layers):
+        for j in range(n_poly):
+            a, b = l * n_poly + j, l * n_poly + (j + 1) % n_poly
+            c, d = a + n_poly, b + n_poly
+            F.append((a, c, d))
+            F.append((a, d, b))
+    for j in range(n_poly):
+        F.append((top, j, (j + 1) % n_poly))
+        F.append((bot, n_layers * n_poly + (j + 1) % n_poly, n_layers * n_poly + j))
+    F = np.array(F, dtype=np.int32)
+    if signed_volume(V, F) < 0:
+        F = F[:, [0, 2, 1]].copy()
+    return V, F
+
+
+def batch_bodies_model(n_bodies=256, t_range=(500, 50000), side_range=(16, 128), spacing_range=(25.0, 100.0),
+                       seed=21, height=1.0, offset=1.0e5, joint=True) -> Problem:
+    """Batched independent closed bodies: perturbed lat-long spheres and
+    extruded star-shaped prisms (alternating), triangle counts log-uniform in
+    t_range, each body with its own square station grid (side uniform in
+    side_range, spacing uniform in spacing_range) `height` above the ground,
+    body b shifted by b x `offset` in x so that no two bodies share a
+    position.  Densities U(0.1, 0.5) g/cc, susceptibilities U(0, 0.05) SI;
+    z-free vertices, one group per body."""
+    rng = np.random.default_rng(seed)
+    meshes, rho, chi, grids = [], [], [], []
+    for b in range(n_bodies):
+        T = float(np.exp(rng.uniform(np.log(t_range[0]), np.log(t_range[1]))))
+        side = int(rng.integers(side_range[0], side_range[1] + 1))
+        spacing = float(rng.uniform(*spacing_range))
+        extent = side * spacing
+        radius = rng.uniform(0.1, 0.3) * extent
+        depth = radius * rng.uniform(1.3, 2.5)
+        if b % 2 == 0:
+            n_lon = max(4, int(round(np.sqrt(T))))
+            n_lat = max(3, int(round(T / (2 * n_lon))) + 1)
+            U, F = latlong_sphere(n_lat, n_lon)
+            U = U * (1.0 + rng.normal(0, 0.03, (len(U), 1)))
+            V = U * radius
+        else:
+            n_poly = max(6, int(round(np.sqrt(T / 2))))
+            n_layers = max(1, int(round((T - 2 * n_poly) / (2 * n_poly))))
+            U, F = star_prism(n_poly, n_layers, rng)
+            V = U * np.array([radius, radius, 0.5 * radius])
+        cx = b * offset
+        V = V + np.array([cx, 0.0, -depth])
+        meshes.append((V, F, Z_ONLY))
+        rho.append(float(rng.uniform(0.1, 0.5)))
+        chi.append(float(rng.uniform(0.0, 0.05)))
+        grids.append(station_grid(side, spacing, height, center=(cx, 0.0)))
+    st = np.concatenate(grids)
+    return Problem("batch", rho, chi, meshes, st, st if joint else None,
+                   station_groups=[len(g) for g in grids])
