@@ -38,6 +38,9 @@ sys.path.insert(0, ROOT)
 
 METRIC = "fwd+grad evals/s (joint gz+TMI forward and objective gradient)"
 WORKLOAD = "multi-unit contact model: 4 groups, 24x24x12 voxels of 100 m, 64x64 stations at 1 m, CP stride 4"
+WORKLOAD_BATCH = ("batched bodies: 256 closed bodies (perturbed lat-long spheres and star-shaped prisms), "
+                  "triangles log-uniform in [500, 50000], per-body square station grids of side U[16, 128] "
+                  "at U[25, 100] m, one persistent forward launch")
 L2_FLUSH_BYTES = 256 << 20
 
 # Algorithmic work per station-facet pair (frozen; derived from the FP64
@@ -76,15 +79,15 @@ def parse():
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-stations", type=int, default=48)
+    ap.add_argument("--workload", choices=["contact", "batch"], default="contact",
+                    help="contact: the 4-group contact model (headline); batch: 256 batched bodies")
     return ap.parse_args()
 
 
-def make_problem():
-    import numpy as np
-
+def make_problem(workload: str = "contact"):
     from lithoinv3d_b200 import synth
 
-    p = synth.voxel_contact_model()
+    p = synth.batch_bodies_model() if workload == "batch" else synth.voxel_contact_model()
     model = p.build_model()
     return p, model
 
@@ -302,7 +305,7 @@ def main():
 
     from lithoinv3d_b200 import PREC_FP64, PREC_MIXED
 
-    p, model = make_problem()
+    p, model = make_problem(args.workload)
     x0, gobs, gstd, mobs, mstd = synthetic_data(p, model)
     ctx = p.make_context(model, device=local, grav_obs=gobs, grav_std=gstd, mag_obs=mobs, mag_std=mstd)
     ctx.set_precision(PREC_MIXED if args.precision == "mixed" else PREC_FP64)
@@ -421,7 +424,8 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
             "data": "synthetic (seeded voxel model and observations)",
-            "config": {"workload": WORKLOAD, "triangles": p.n_triangles(), "stations": len(p.grav_xyz),
+            "config": {"workload": WORKLOAD_BATCH if args.workload == "batch" else WORKLOAD,
+                       "triangles": p.n_triangles(), "stations": len(p.grav_xyz),
                        "dofs": np_, "parallelism": f"replicas x{world}", "l2": "flushed between steps (256 MiB write)",
                        "precision": args.precision, "fp64_near_pair_fraction": round(near_frac, 4),
                        "cuda_graph": True,
@@ -433,7 +437,7 @@ def main():
             "gpu_launches": launches, "roofline": roofline}
     clk = clocks.summary()
     line["clocks"] = clk
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "contact":
         try:
             line["cpu_baseline"] = cpu_baseline(p, x0, gobs, gstd, mobs, mstd, args.cpu_stations)
         except Exception as e:  # the baseline is reported, never the target

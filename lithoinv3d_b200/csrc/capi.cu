@@ -955,14 +955,15 @@ extern "C" lf_status lf_get_group_objectives(lf_ctx* c, double* out) {
 
 // Item list of the batched forward: every (group, 128-station block, facet
 // chunk), chunk length chosen from the total own-group pairs so that the
-// list holds ~4 items per persistent CTA; ordered by cost, largest first.
+// list holds ~32 items per persistent CTA (no item is a large share of a
+// CTA's work); ordered by cost, largest first.
 static lf_status plan_items(lf_ctx* c) {
     if (c->itemsEpoch == c->planEpoch) return LF_OK;
     const int G = c->G;
     int64_t pairs = 0;
     for (int g = 0; g < G; ++g)
         pairs += (int64_t)(c->grpStaOff[g + 1] - c->grpStaOff[g]) * (c->grpTriOff[g + 1] - c->grpTriOff[g]);
-    const int64_t targetItems = 4 * (int64_t)c->tune.fwd_target_blocks;
+    const int64_t targetItems = 32 * (int64_t)c->tune.fwd_target_blocks;
     const int64_t F64 = std::max<int64_t>(kFwdFacetTile, (pairs / (128 * targetItems) + 31) / 32 * 32);
     const int F = static_cast<int>(std::min<int64_t>(F64, 1 << 30));
     std::vector<FwdItem> items;
