@@ -232,6 +232,26 @@ lf_status lf_autotune(lf_ctx* ctx, const double* params, int repeats, lf_tuning*
 lf_status lf_set_station_groups(lf_ctx* ctx, int n_groups, const int32_t* counts);
 lf_status lf_get_group_objectives(lf_ctx* ctx, double* out);
 
+/* Warm-start MLP (no reference counterpart: the reference has no learned
+ * component).  A ReLU network n_in -> width x depth -> n_out trained and run
+ * on the device with hand-written BF16 tensor-core GEMMs (FP32 accumulate),
+ * Adam on FP32 master weights.  width and batch must be multiples of 128.
+ * Inputs and targets are device fp32 arrays [rows][n_in] / [rows][n_out];
+ * the loss is 0.5 x mean squared error over the batch and the n_out
+ * outputs.  Parameters (get/set/gradients) in the order: for every layer W
+ * [out][in] row-major, then b [out]. */
+typedef struct lf_mlp lf_mlp;
+lf_status lf_mlp_create(int device, int n_in, int width, int depth, int n_out, int batch, unsigned seed,
+                        lf_mlp** out);
+void lf_mlp_destroy(lf_mlp* m);
+const char* lf_mlp_last_error(lf_mlp* m);
+lf_status lf_mlp_train_step(lf_mlp* m, const float* d_x, const float* d_y, float lr, float* loss);
+lf_status lf_mlp_predict(lf_mlp* m, const float* d_x, int rows, float* d_y);
+lf_status lf_mlp_param_count(lf_mlp* m, size_t* n);
+lf_status lf_mlp_get_params(lf_mlp* m, float* host);
+lf_status lf_mlp_set_params(lf_mlp* m, const float* host);
+lf_status lf_mlp_gradients(lf_mlp* m, const float* d_x, const float* d_y, float* loss, float* host_grads);
+
 /* Graph mode (no reference counterpart: the reference evaluates on one CPU
  * thread).  When enabled, lf_objective, lf_objective_grad and
  * lf_objective_grad_device replay a CUDA graph of the whole evaluation

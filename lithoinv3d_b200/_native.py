@@ -76,6 +76,15 @@ SIGNATURES = {
     "lf_jacobian": (C.c_int, [_vp, _dp, C.c_int, _dp]),
     "lf_unit_response": (C.c_int, [_vp, _dp, C.c_int, C.c_int, _dp, _dp]),
     "lf_set_graph_mode": (C.c_int, [_vp, C.c_int]),
+    "lf_mlp_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint, C.POINTER(_vp)]),
+    "lf_mlp_destroy": (None, [_vp]),
+    "lf_mlp_last_error": (C.c_char_p, [_vp]),
+    "lf_mlp_train_step": (C.c_int, [_vp, C.c_void_p, C.c_void_p, C.c_float, C.POINTER(C.c_float)]),
+    "lf_mlp_predict": (C.c_int, [_vp, C.c_void_p, C.c_int, C.c_void_p]),
+    "lf_mlp_param_count": (C.c_int, [_vp, C.POINTER(C.c_size_t)]),
+    "lf_mlp_get_params": (C.c_int, [_vp, C.c_void_p]),
+    "lf_mlp_set_params": (C.c_int, [_vp, C.c_void_p]),
+    "lf_mlp_gradients": (C.c_int, [_vp, C.c_void_p, C.c_void_p, C.POINTER(C.c_float), C.c_void_p]),
     "lf_set_station_groups": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_int32)]),
     "lf_get_group_objectives": (C.c_int, [_vp, _dp]),
     "lf_set_tuning": (C.c_int, [_vp, C.c_void_p]),
