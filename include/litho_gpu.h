@@ -318,6 +318,8 @@ typedef struct {
     int line_search_max_iter;/* default 50 */
     int disable_line_search; /* default 0 */
     double initial_gamma;    /* > 0: H0 = gamma*I for the first step (warm start); 0 = steepest descent */
+    double target_value;     /* > 0: stop once the objective is at or below it (no reference
+                                counterpart; e.g. the chi^2 = N data misfit); 0 = off */
 } lf_lbfgsb_options;
 typedef struct {
     int iterations;

@@ -20,7 +20,7 @@ class ModelInfo(C.Structure):
 class LbfgsbOptions(C.Structure):
     _fields_ = [("max_iterations", C.c_int), ("tolerance", C.c_double), ("history_size", C.c_int),
                 ("armijo_c1", C.c_double), ("line_search_max_iter", C.c_int),
-                ("disable_line_search", C.c_int), ("initial_gamma", C.c_double)]
+                ("disable_line_search", C.c_int), ("initial_gamma", C.c_double), ("target_value", C.c_double)]
 
 
 class LbfgsbResult(C.Structure):

@@ -331,7 +331,7 @@ class Context:
         self._check(self.lib.lf_objective_grad_device(self.h, d_params, d_f, d_grad), "objective_grad_device")
 
     def lbfgsb(self, x0, lower, upper, max_iterations=500, tolerance=1e-6, history_size=10, armijo_c1=1e-4,
-               line_search_max_iter=50, disable_line_search=False, initial_gamma=0.0):
+               line_search_max_iter=50, disable_line_search=False, initial_gamma=0.0, target_value=0.0):
         opt = LbfgsbOptions()
         self.lib.lf_lbfgsb_default_options(C.byref(opt))
         opt.max_iterations = max_iterations
@@ -341,6 +341,7 @@ class Context:
         opt.line_search_max_iter = line_search_max_iter
         opt.disable_line_search = int(disable_line_search)
         opt.initial_gamma = initial_gamma
+        opt.target_value = target_value
         x0 = f64(x0)
         lo, hi = f64(lower), f64(upper)
         xo = np.zeros_like(x0)

@@ -1678,6 +1678,7 @@ extern "C" void lf_lbfgsb_default_options(lf_lbfgsb_options* o) {
     o->line_search_max_iter = 50;
     o->disable_line_search = 0;
     o->initial_gamma = 0.0;
+    o->target_value = 0.0;
 }
 
 extern "C" lf_status lf_lbfgsb_minimize(lf_ctx* c, const double* x0, const double* lo, const double* hi,
@@ -1695,6 +1696,7 @@ extern "C" lf_status lf_lbfgsb_minimize(lf_ctx* c, const double* x0, const doubl
     lo2.lineSearchMaxIter = o.line_search_max_iter;
     lo2.disableLineSearch = o.disable_line_search != 0;
     lo2.initialGamma = o.initial_gamma;
+    lo2.targetValue = o.target_value;
     int n = c->np;
     lf_status status = LF_OK;
     int nEval = 0, nGrad = 0;

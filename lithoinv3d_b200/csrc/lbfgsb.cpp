@@ -120,6 +120,11 @@ LbfgsbResult LbfgsbOptimizer::minimize(const Objective& f, const Gradient& grad,
         }
         pg = std::sqrt(pg);
         if (k == 0) pg0 = pg;
+        if (opt_.targetValue > 0.0 && f(x_) <= opt_.targetValue) {
+            res.converged = true;
+            res.message = "Reached the target objective value";
+            break;
+        }
         if (k > 0 && pg < opt_.tolerance * std::max(1.0, pg0)) {
             res.converged = true;
             res.message = "Converged: projected gradient below tolerance";

@@ -17,6 +17,7 @@ struct LbfgsbOptions {
     int lineSearchMaxIter = 50;
     bool disableLineSearch = false;
     double initialGamma = 0.0;  // > 0: H0 = gamma * I when the history is empty
+    double targetValue = 0.0;   // > 0: stop once f <= targetValue (e.g. chi^2 = N)
 };
 
 struct LbfgsbResult {
