@@ -272,6 +272,17 @@ lf_status lf_objective(lf_ctx* ctx, const double* params, double* out5);
  * formed): *f = total objective, grad[n_dofs]. */
 lf_status lf_objective_grad(lf_ctx* ctx, const double* params, double* f, double* grad);
 
+/* Data-weight calibration (JointObjective::calibrateDataWeights,
+ * joint_objective.cpp:281-393), matrix-free: power iteration for the largest
+ * eigenvalue of J^T W^2 J of each data type with J v from a central
+ * difference of the FP64 forward and J^T w from the gradient kernels (the
+ * reference forms both dense Jacobians); alpha_mag *= clip(lambda_grav /
+ * lambda_mag, 1e-6, 1e6), or the gradient-norm ratio when degenerate.  Updates
+ * the context's alpha_mag like the reference; no-op without magnetic data or
+ * with alpha_mag <= 0.  seed: start vector.  Any output pointer may be NULL. */
+lf_status lf_calibrate_data_weights(lf_ctx* ctx, const double* params, unsigned seed, double* alpha_mag,
+                                    double* eig_grav, double* eig_mag);
+
 /* Per-group unit responses at params (positions as after lf_forward), for
  * property inversion: the forward of group `group` alone with
  *  LF_UNIT_GRAVITY    unit density (mGal per g/cc) at the gravity stations

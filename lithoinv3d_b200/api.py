@@ -258,6 +258,13 @@ class Context:
         self._check(self.lib.lf_get_group_objectives(self.h, _d(out)), "group_objectives")
         return out
 
+    def calibrate_data_weights(self, params, seed: int = 0):
+        """lf_calibrate_data_weights: returns (alpha_mag, lambda_grav, lambda_mag)."""
+        a, eg, em = np.zeros(1), np.zeros(1), np.zeros(1)
+        self._check(self.lib.lf_calibrate_data_weights(self.h, _d(f64(params)), seed, _d(a), _d(eg), _d(em)),
+                    "calibrate_data_weights")
+        return float(a[0]), float(eg[0]), float(em[0])
+
     def set_graph_mode(self, enabled: bool = True):
         """Replay evaluations as a captured CUDA graph (lf_set_graph_mode)."""
         self._check(self.lib.lf_set_graph_mode(self.h, int(bool(enabled))), "set_graph_mode")

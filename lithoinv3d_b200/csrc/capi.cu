@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <random>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -100,6 +101,8 @@ struct lf_ctx {
     DevBuf<int16_t> d_faceGroup;
     DevBuf<GroupConst> d_groups;
     int nInterpRows = 0, nSync = 0, nGradVerts = 0, nGradFacets = 0;
+    double maxRefScale = 0.0;
+    DevBuf<double> d_vel, d_posSave, d_tmpP, d_tmpS;  // matrix-free products (calibration)
     std::vector<int32_t> hGradFacets;
 
     // forward chunking (plan cached per station count and group filter;
@@ -543,6 +546,8 @@ extern "C" lf_status lf_set_model_tables(lf_ctx* c, int G, const double* density
     LF_TRY_CUDA(c, upload(c->d_refVertex, refVertex, (size_t)nref, c->stream));
     LF_TRY_CUDA(c, upload(c->d_refAxis, refAxis, (size_t)nref, c->stream));
     LF_TRY_CUDA(c, upload(c->d_refScale, refScale, (size_t)nref, c->stream));
+    c->maxRefScale = 0.0;
+    for (int r = 0; r < nref; ++r) c->maxRefScale = std::max(c->maxRefScale, std::fabs(refScale[r]));
     std::vector<int32_t> rows;
     if (interpOff) {
         for (int v = 0; v < nv; ++v)
@@ -1527,6 +1532,189 @@ extern "C" lf_status lf_objective_grad(lf_ctx* c, const double* params, double* 
         LF_TRY_CUDA(c, cudaMemcpyAsync(grad, c->d_grad.p, sizeof(double) * c->np, cudaMemcpyDeviceToHost, c->stream));
     LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
     if (f && !std::isfinite(*f)) return fail(c, LF_ENUMERIC, "non-finite objective");
+    return LF_OK;
+}
+
+// ---------------------------------------------------- data-weight calibration --
+// Matrix-free J v and J^T w for one data set, with the Jacobian semantics of
+// the reference's computeJacobian (the derivative of a DOF is its own
+// vertices' positional derivative times the axis scale, gravity_forward.cpp:
+// 269-289).  FP64 throughout, whatever the context's precision.
+__global__ void k_pos_shift(int n, const double* __restrict__ base, const double* __restrict__ vel, double eps,
+                            double* __restrict__ pos) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) pos[i] = base[i] + eps * vel[i];
+}
+
+// FP64 forward of one set at the current positions into s.d_pred.
+static lf_status forward_one_fp64(lf_ctx* c, StationSet& s, bool grav) {
+    k_face_prep_fwd<<<cdiv(c->T, 128), 128, 0, c->stream>>>(c->T, c->d_tri.p, c->d_pos.p, c->d_faceGroup.p,
+                                                            c->d_groups.p, c->fdir, c->d_fc.p);
+    c->counters.launches++;
+    return grav ? forward_set<true, false>(c, s, s.d_pred.p, nullptr) : forward_set<false, true>(c, s, nullptr, s.d_pred.p);
+}
+
+// out[n_stations] (device order) = J v, by a central difference along the
+// vertex velocity u = v scattered through the DOF refs, displacement
+// max |eps u| = 1e-3 m (truncation ~1e-10 relative, rounding ~1e-12).
+static lf_status jv_product(lf_ctx* c, StationSet& s, bool grav, const std::vector<double>& v, std::vector<double>& out) {
+    const int n3 = 3 * c->V;
+    double vmax = 0.0;
+    for (double x : v) vmax = std::max(vmax, std::fabs(x));
+    out.assign(s.n, 0.0);
+    if (vmax == 0.0 || c->maxRefScale == 0.0) return LF_OK;
+    const double eps = 1e-3 / (vmax * c->maxRefScale);
+    LF_TRY_CUDA(c, c->d_vel.reserve(n3));
+    LF_TRY_CUDA(c, c->d_posSave.reserve(n3));
+    LF_TRY_CUDA(c, c->d_tmpS.reserve(std::max(s.n, 1)));
+    LF_TRY_CUDA(c, upload(c->d_tmpP, v.data(), v.size(), c->stream));
+    LF_TRY_CUDA(c, cudaMemsetAsync(c->d_vel.p, 0, sizeof(double) * n3, c->stream));
+    k_scatter_dofs<<<cdiv(c->np, 256), 256, 0, c->stream>>>(c->np, c->d_tmpP.p, c->d_dofOff.p, c->d_refVertex.p,
+                                                              c->d_refAxis.p, c->d_refScale.p, c->d_vel.p);
+    LF_TRY_CUDA(c, cudaMemcpyAsync(c->d_posSave.p, c->d_pos.p, sizeof(double) * n3, cudaMemcpyDeviceToDevice, c->stream));
+    std::vector<double> plus(s.n), minus(s.n);
+    lf_status st = LF_OK;
+    for (int sign = 1; sign >= -1 && st == LF_OK; sign -= 2) {
+        k_pos_shift<<<cdiv(n3, 256), 256, 0, c->stream>>>(n3, c->d_posSave.p, c->d_vel.p, sign * eps, c->d_pos.p);
+        st = forward_one_fp64(c, s, grav);
+        if (st == LF_OK && cudaMemcpyAsync(sign > 0 ? plus.data() : minus.data(), s.d_pred.p, sizeof(double) * s.n,
+                                           cudaMemcpyDeviceToHost, c->stream) != cudaSuccess)
+            st = fail(c, LF_ECUDA, "copy failed");
+    }
+    // restore the positions whatever happened
+    if (cudaMemcpyAsync(c->d_pos.p, c->d_posSave.p, sizeof(double) * n3, cudaMemcpyDeviceToDevice, c->stream) !=
+            cudaSuccess && st == LF_OK)
+        st = fail(c, LF_ECUDA, "position restore failed");
+    LF_RET_IF(st);
+    LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (int i = 0; i < s.n; ++i) out[i] = (plus[i] - minus[i]) / (2.0 * eps);
+    return LF_OK;
+}
+
+// out[np] = J^T w, w[n_stations] in device order: the gradient kernels with
+// w as the station coefficients, no regularisation terms.
+static lf_status jtw_product(lf_ctx* c, StationSet& s, bool grav, const std::vector<double>& w, std::vector<double>& out) {
+    LF_TRY_CUDA(c, upload(c->d_tmpS, w.data(), w.size(), c->stream));
+    k_face_prep_grad<<<cdiv(c->T, 128), 128, 0, c->stream>>>(c->T, c->d_tri.p, c->d_pos.p, c->d_faceGroup.p,
+                                                             c->d_groups.p, c->d_faceNeeds.p, 1, 1, c->fdir,
+                                                             c->d_gc.p);
+    LF_TRY_CUDA(c, c->d_partGrad.reserve((size_t)std::max(grad_slots(c, s.n), 1) * 9 * c->T));
+    const int used = gradient_set(c, s, grav ? c->d_tmpS.p : nullptr, grav ? nullptr : c->d_tmpS.p, 0);
+    if (used > 0 && c->nGradVerts > 0)
+        k_vertex_reduce<<<cdiv(c->nGradVerts, 4), 128, 0, c->stream>>>(c->nGradVerts, c->d_gradVerts.p, c->d_vfOff.p,
+                                                                        c->d_vf.p, c->T, used, c->d_partGrad.p,
+                                                                        c->d_vgrad.p);
+    else
+        LF_TRY_CUDA(c, cudaMemsetAsync(c->d_vgrad.p, 0, sizeof(double) * 3 * c->V, c->stream));
+    LF_TRY_CUDA(c, c->d_tmpP.reserve(std::max(c->np, 1)));
+    if (c->np > 0)
+        k_dof_gather<<<cdiv(c->np, 256), 256, 0, c->stream>>>(c->np, c->d_dofOff.p, c->d_refVertex.p, c->d_refAxis.p,
+                                                              c->d_refScale.p, c->d_vgrad.p, nullptr, nullptr, 0.0,
+                                                              nullptr, 0.0, c->d_tmpP.p);
+    LF_CHECK_LAUNCH(c);
+    out.assign(c->np, 0.0);
+    if (c->np > 0)
+        LF_TRY_CUDA(c, cudaMemcpyAsync(out.data(), c->d_tmpP.p, sizeof(double) * c->np, cudaMemcpyDeviceToHost,
+                                       c->stream));
+    LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
+    return LF_OK;
+}
+
+// JointObjective::calibrateDataWeights (joint_objective.cpp:281-393),
+// matrix-free: power iteration (at most 50 iterations, relative tolerance
+// 1e-8) for the largest eigenvalue of J^T W^2 J of each data type, W^2 =
+// 1/sigma^2; alpha_mag *= clip(lambda_grav / lambda_mag, 1e-6, 1e6); when the
+// ratio is not finite and positive, the gradient-norm ratio
+// |J_g^T W^2 r_g| / |J_m^T W^2 r_m| instead.  The start vector is seeded
+// uniform [-1, 1) (the reference draws it from Eigen's Random).
+extern "C" lf_status lf_calibrate_data_weights(lf_ctx* c, const double* params, unsigned seed, double* alpha_out,
+                                               double* eig_grav, double* eig_mag) {
+    LF_RET_IF(check_ready(c));
+    if (eig_grav) *eig_grav = 0.0;
+    if (eig_mag) *eig_mag = 0.0;
+    if (c->mag.n == 0 || c->grav.n == 0 || c->alphaMag <= 0.0) {
+        if (alpha_out) *alpha_out = c->alphaMag;
+        return LF_OK;  // joint_objective.cpp:282
+    }
+    if (c->partitioned) return fail(c, LF_ESTATE, "calibration is not available for batched bodies");
+    LF_RET_IF(params_to_device(c, params));
+    LF_RET_IF(scatter(c, c->d_params.p));
+    const int prec = c->precision;
+    c->precision = LF_PREC_FP64;
+    auto w2_of = [&](StationSet& s, std::vector<double>& w2) -> lf_status {
+        std::vector<double> w(s.n);
+        LF_TRY_CUDA(c, cudaMemcpy(w.data(), s.d_w.p, sizeof(double) * s.n, cudaMemcpyDeviceToHost));
+        w2.resize(s.n);
+        for (int i = 0; i < s.n; ++i) w2[i] = w[i] * w[i];
+        return LF_OK;
+    };
+    std::mt19937_64 rng(seed);
+    std::uniform_real_distribution<double> uni(-1.0, 1.0);
+    auto power = [&](StationSet& s, bool grav, double* eig) -> lf_status {
+        std::vector<double> w2, v(c->np), jv, jtw;
+        LF_RET_IF(w2_of(s, w2));
+        for (double& x : v) x = uni(rng);
+        double nv = 0.0;
+        for (double x : v) nv += x * x;
+        nv = std::sqrt(nv);
+        for (double& x : v) x /= nv;
+        double lambdaOld = 0.0;
+        *eig = 0.0;
+        for (int it = 0; it < 50; ++it) {
+            LF_RET_IF(jv_product(c, s, grav, v, jv));
+            for (int i = 0; i < s.n; ++i) jv[i] *= w2[i];
+            LF_RET_IF(jtw_product(c, s, grav, jv, jtw));
+            double lam = 0.0;
+            for (double x : jtw) lam += x * x;
+            lam = std::sqrt(lam);
+            if (lam < 1e-60) return LF_OK;
+            for (int d = 0; d < c->np; ++d) v[d] = jtw[d] / lam;
+            if (std::fabs(lam - lambdaOld) / lam < 1e-8) break;
+            lambdaOld = lam;
+        }
+        LF_RET_IF(jv_product(c, s, grav, v, jv));
+        for (int i = 0; i < s.n; ++i) jv[i] *= w2[i];
+        LF_RET_IF(jtw_product(c, s, grav, jv, jtw));
+        double vh = 0.0;
+        for (int d = 0; d < c->np; ++d) vh += v[d] * jtw[d];
+        *eig = std::max(vh, 0.0);
+        return LF_OK;
+    };
+    double eg = 0.0, em = 0.0;
+    lf_status st = power(c->grav, true, &eg);
+    if (st == LF_OK) st = power(c->mag, false, &em);
+    double ratio = em > 1e-60 ? eg / em : 0.0;
+    if (st == LF_OK) {
+        c->epoch++;
+        if (std::isfinite(ratio) && ratio > 0.0) {
+            c->alphaMag *= std::max(1e-6, std::min(ratio, 1e6));
+        } else {
+            // gradient-norm fallback (joint_objective.cpp:357-392)
+            double norms[2] = {0.0, 0.0};
+            for (int k = 0; k < 2 && st == LF_OK; ++k) {
+                StationSet& s = k == 0 ? c->grav : c->mag;
+                std::vector<double> w2, pred(s.n), obs(s.n), coef(s.n), jtw;
+                st = w2_of(s, w2);
+                if (st == LF_OK) st = forward_one_fp64(c, s, k == 0);
+                if (st == LF_OK && (cudaMemcpy(pred.data(), s.d_pred.p, sizeof(double) * s.n, cudaMemcpyDeviceToHost) !=
+                                        cudaSuccess ||
+                                    cudaMemcpy(obs.data(), s.d_obs.p, sizeof(double) * s.n, cudaMemcpyDeviceToHost) !=
+                                        cudaSuccess))
+                    st = fail(c, LF_ECUDA, "copy failed");
+                if (st != LF_OK) break;
+                for (int i = 0; i < s.n; ++i) coef[i] = w2[i] * (obs[i] - pred[i]);
+                st = jtw_product(c, s, k == 0, coef, jtw);
+                for (double x : jtw) norms[k] += x * x;
+                norms[k] = std::sqrt(norms[k]);
+            }
+            if (st == LF_OK && norms[0] >= 1e-60 && norms[1] > 1e-60) c->alphaMag *= norms[0] / norms[1];
+        }
+    }
+    c->precision = prec;
+    LF_RET_IF(st);
+    if (alpha_out) *alpha_out = c->alphaMag;
+    if (eig_grav) *eig_grav = eg;
+    if (eig_mag) *eig_mag = em;
     return LF_OK;
 }
 

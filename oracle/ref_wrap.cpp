@@ -237,6 +237,15 @@ void ref_set_objective(void* h, double alpha_mag, double ref_weight, const doubl
     c->built = false;
 }
 
+// JointObjective::calibrateDataWeights (joint_objective.cpp:281-393) at
+// params; returns the new magnetic weight.
+double ref_calibrate(void* h, const double* params) {
+    auto* c = static_cast<RefCtx*>(h);
+    c->ensure();
+    c->jobj->calibrateDataWeights(toVec(static_cast<int>(c->jobj->parameterCount()), params));
+    return c->jobj->magneticWeight();
+}
+
 void ref_set_smoothness(void* h, double weight) {
     auto* c = static_cast<RefCtx*>(h);
     c->smoothWeight = weight;

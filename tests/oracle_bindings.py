@@ -112,6 +112,7 @@ def ref() -> C.CDLL:
             "ref_jacobian_gz": (None, [V, _dp, _dp]), "ref_jacobian_tmi": (None, [V, _dp, _dp]),
             "ref_unit_response": (None, [V, _dp, C.c_int, C.c_int, _dp, _dp]),
             "ref_set_smoothness": (None, [V, C.c_double]),
+            "ref_calibrate": (C.c_double, [V, _dp]),
             "ref_smoothness_value": (C.c_double, [V, _dp]),
             "ref_smoothness_gradient": (None, [V, _dp, _dp]),
             "ref_objective": (None, [V, _dp, _dp]), "ref_gradient": (None, [V, _dp, _dp]),
@@ -208,6 +209,10 @@ class RefModel:
         out = np.zeros(self.Sm)
         self.lib.ref_forward_tmi(self.h, _d(params), out.ctypes.data_as(_dp))
         return out
+
+    def calibrate(self, params):
+        """JointObjective::calibrateDataWeights; returns the new alpha_mag."""
+        return float(self.lib.ref_calibrate(self.h, _d(params)))
 
     def smoothness(self, params):
         """SurfaceSmoothness value and DOF gradient at params."""
