@@ -38,6 +38,9 @@ sys.path.insert(0, ROOT)
 
 METRIC = "fwd+grad evals/s (joint gz+TMI forward and objective gradient)"
 WORKLOAD = "multi-unit contact model: 4 groups, 24x24x12 voxels of 100 m, 64x64 stations at 1 m, CP stride 4"
+WORKLOAD_LARGE = ("large single inversion: 6 units on a 60x60x30 grid of 100 m voxels (~194k triangles), "
+                  "x/y/z-free vertices, 200x200 stations on a seeded 8-sinusoid topography, joint gz+TMI with "
+                  "reference-model regularisation")
 WORKLOAD_BATCH = ("batched bodies: 256 closed bodies (perturbed lat-long spheres and star-shaped prisms), "
                   "triangles log-uniform in [500, 50000], per-body square station grids of side U[16, 128] "
                   "at U[25, 100] m, one persistent forward launch")
@@ -79,15 +82,23 @@ def parse():
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-stations", type=int, default=48)
-    ap.add_argument("--workload", choices=["contact", "batch"], default="contact",
-                    help="contact: the 4-group contact model (headline); batch: 256 batched bodies")
+    ap.add_argument("--workload", choices=["contact", "batch", "large"], default="contact",
+                    help="contact: the 4-group contact model (headline); batch: 256 batched bodies; "
+                         "large: the 194k-facet single inversion")
+    ap.add_argument("--lbfgs-iters", type=int, default=0,
+                    help="after timing, run this many L-BFGS-B iterations and report their wall time")
     return ap.parse_args()
 
 
 def make_problem(workload: str = "contact"):
     from lithoinv3d_b200 import synth
 
-    p = synth.batch_bodies_model() if workload == "batch" else synth.voxel_contact_model()
+    if workload == "batch":
+        p = synth.batch_bodies_model()
+    elif workload == "large":
+        p = synth.large_model()
+    else:
+        p = synth.voxel_contact_model()
     model = p.build_model()
     return p, model
 
@@ -309,6 +320,9 @@ def main():
     x0, gobs, gstd, mobs, mstd = synthetic_data(p, model)
     ctx = p.make_context(model, device=local, grav_obs=gobs, grav_std=gstd, mag_obs=mobs, mag_std=mstd)
     ctx.set_precision(PREC_MIXED if args.precision == "mixed" else PREC_FP64)
+    if args.workload == "large":  # reference-model regularisation around the start (reference_model.cpp:16-25)
+        ctx.set_objective(alpha_mag=1.0, ref_weight=1e-3, ref_params=x0)
+        ctx.set_scatter_stateless(True)
     ctx.set_graph_mode(True)
     tuned, _ = ctx.autotune(x0, repeats=3)
     np_ = model.n_dofs
@@ -424,7 +438,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
             "data": "synthetic (seeded voxel model and observations)",
-            "config": {"workload": WORKLOAD_BATCH if args.workload == "batch" else WORKLOAD,
+            "config": {"workload": {"batch": WORKLOAD_BATCH, "large": WORKLOAD_LARGE}.get(args.workload, WORKLOAD),
                        "triangles": p.n_triangles(), "stations": len(p.grav_xyz),
                        "dofs": np_, "parallelism": f"replicas x{world}", "l2": "flushed between steps (256 MiB write)",
                        "precision": args.precision, "fp64_near_pair_fraction": round(near_frac, 4),
@@ -437,6 +451,18 @@ def main():
             "gpu_launches": launches, "roofline": roofline}
     clk = clocks.summary()
     line["clocks"] = clk
+    if args.lbfgs_iters > 0:  # the inversion itself (untimed by the events above; host wall clock)
+        lo, hi = model.bounds()
+        if args.workload == "large":  # +-50 m around the start in every free axis
+            lo, hi = np.maximum(lo, x0 - 50.0), np.minimum(hi, x0 + 50.0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _, res = ctx.lbfgsb(x0, lo, hi, max_iterations=args.lbfgs_iters)
+        wall = time.perf_counter() - t0
+        f0 = ctx.objective(x0)
+        line["config"]["lbfgsb"] = {"iterations": res.iterations, "evaluations": res.evaluations,
+                                    "gradients": res.gradients, "wall_s": wall, "objective_start": f0,
+                                    "objective_final": res.final_value}
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "contact":
         try:
             line["cpu_baseline"] = cpu_baseline(p, x0, gobs, gstd, mobs, mstd, args.cpu_stations)

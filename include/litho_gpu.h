@@ -252,6 +252,17 @@ lf_status lf_mlp_get_params(lf_mlp* m, float* host);
 lf_status lf_mlp_set_params(lf_mlp* m, const float* host);
 lf_status lf_mlp_gradients(lf_mlp* m, const float* d_x, const float* d_y, float* loss, float* host_grads);
 
+/* Stateless parameter scatter (off by default).  The reference's
+ * applyParameterVector averages shared vertices from their current positions
+ * (lithology_model.cpp:235-247), and vertices that the DOFs and the
+ * control-point interpolation do not rewrite keep what earlier calls left,
+ * so the model after evaluating p depends on the parameters evaluated before
+ * (reproduced bit for bit by default; on x/y-free models a line-search trial
+ * far away can displace such vertices by hundreds of metres for every later
+ * evaluation).  Enabled, every scatter starts from the model's positions as
+ * given to lf_set_model, so the evaluation at p depends on p alone. */
+lf_status lf_set_scatter_stateless(lf_ctx* ctx, int enabled);
+
 /* Graph mode (no reference counterpart: the reference evaluates on one CPU
  * thread).  When enabled, lf_objective, lf_objective_grad and
  * lf_objective_grad_device replay a CUDA graph of the whole evaluation

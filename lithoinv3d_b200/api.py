@@ -265,6 +265,10 @@ class Context:
                     "calibrate_data_weights")
         return float(a[0]), float(eg[0]), float(em[0])
 
+    def set_scatter_stateless(self, enabled: bool = True):
+        """Every scatter from the model's given positions (lf_set_scatter_stateless)."""
+        self._check(self.lib.lf_set_scatter_stateless(self.h, int(bool(enabled))), "set_scatter_stateless")
+
     def set_graph_mode(self, enabled: bool = True):
         """Replay evaluations as a captured CUDA graph (lf_set_graph_mode)."""
         self._check(self.lib.lf_set_graph_mode(self.h, int(bool(enabled))), "set_graph_mode")

@@ -102,6 +102,8 @@ struct lf_ctx {
     DevBuf<GroupConst> d_groups;
     int nInterpRows = 0, nSync = 0, nGradVerts = 0, nGradFacets = 0;
     double maxRefScale = 0.0;
+    bool statelessScatter = false;  // lf_set_scatter_stateless
+    DevBuf<double> d_pos0;          // the model's positions as given
     DevBuf<double> d_vel, d_posSave, d_tmpP, d_tmpS;  // matrix-free products (calibration)
     std::vector<int32_t> hGradFacets;
 
@@ -535,6 +537,7 @@ extern "C" lf_status lf_set_model_tables(lf_ctx* c, int G, const double* density
 
     // geometry + tables
     LF_TRY_CUDA(c, upload(c->d_pos, xyz, (size_t)nv * 3, c->stream));
+    LF_TRY_CUDA(c, upload(c->d_pos0, xyz, (size_t)nv * 3, c->stream));
     LF_TRY_CUDA(c, upload(c->d_tri, tri, (size_t)nt * 3, c->stream));
     std::vector<int16_t> faceGroup(nt);
     for (int g = 0; g < G; ++g)
@@ -894,6 +897,9 @@ static lf_status upload_chunks(lf_ctx* c) {
 }
 
 static lf_status scatter(lf_ctx* c, const double* d_params) {
+    if (c->statelessScatter)
+        LF_TRY_CUDA(c, cudaMemcpyAsync(c->d_pos.p, c->d_pos0.p, sizeof(double) * 3 * c->V, cudaMemcpyDeviceToDevice,
+                                       c->stream));
     if (c->np > 0) {
         k_scatter_dofs<<<cdiv(c->np, 256), 256, 0, c->stream>>>(c->np, d_params, c->d_dofOff.p, c->d_refVertex.p,
                                                                   c->d_refAxis.p, c->d_refScale.p, c->d_pos.p);
@@ -1476,6 +1482,13 @@ extern "C" lf_status lf_autotune(lf_ctx* c, const double* params, int repeats, l
     LF_RET_IF(st2);
     if (chosen) *chosen = best;
     if (best_ms) *best_ms = bestMs;
+    return LF_OK;
+}
+
+extern "C" lf_status lf_set_scatter_stateless(lf_ctx* c, int enabled) {
+    if (!c) return LF_EINVAL;
+    c->epoch++;
+    c->statelessScatter = enabled != 0;
     return LF_OK;
 }
 

@@ -217,14 +217,15 @@ def icosphere_model(subdiv=3, radius=200.0, center=(0.0, 0.0, -500.0), sigma=20.
 
 
 def voxel_contact_model(shape=(24, 24, 12), cell=100.0, n_groups=4, n_blobs=6, seed=3, n_side=64, height=1.0,
-                        cp_stride=4, freedom_interior=Z_ONLY, joint=True, axis_scale=1.0) -> Problem:
+                        cp_stride=4, freedom_interior=Z_ONLY, joint=True, axis_scale=1.0,
+                        blob_width=(0.1, 0.3)) -> Problem:
     """Multi-unit contact model: groups labelled on a voxel grid by
     thresholding a sum of seeded Gaussian blobs; voxel-face closed volumes;
     densities U(-0.3, 0.5) g/cc, susceptibilities U(0, 0.05) SI; an
     n_side x n_side station grid over the footprint at `height`.  Vertices on
     the flat top (z = 0) and the base are fixed, every other vertex moves in z."""
     rng = np.random.default_rng(seed)
-    labels = blob_labels(shape, n_groups, n_blobs, rng)
+    labels = blob_labels(shape, n_groups, n_blobs, rng, width=blob_width)
     nx, ny, nz = shape
     origin = (-nx * cell / 2.0, -ny * cell / 2.0, 0.0)
     vols = voxel_group_volumes(labels, cell, origin)
@@ -239,6 +240,35 @@ def voxel_contact_model(shape=(24, 24, 12), cell=100.0, n_groups=4, n_blobs=6, s
     st = station_grid(n_side, spacing, height, ny=int(round(ny * cell / spacing)))
     p = Problem("voxel", rho, chi, meshes, st, st if joint else None, cp_stride=cp_stride, axis_scale=axis_scale)
     p.extra["labels"] = labels
+    return p
+
+
+def topography(xy: np.ndarray, rng: np.random.Generator, n_waves: int = 8, amplitude: float = 80.0) -> np.ndarray:
+    """Seeded sum of n_waves plane sinusoids, scaled into [0, amplitude] m."""
+    z = np.zeros(len(xy))
+    span = float(np.max(xy.max(0) - xy.min(0)))
+    for _ in range(n_waves):
+        k = rng.uniform(1.0, 6.0) * 2 * np.pi / span
+        th = rng.uniform(0, 2 * np.pi)
+        z += rng.uniform(0.3, 1.0) * np.sin(k * (xy[:, 0] * np.cos(th) + xy[:, 1] * np.sin(th)) + rng.uniform(0, 2 * np.pi))
+    z -= z.min()
+    return amplitude * z / max(z.max(), 1e-30)
+
+
+def large_model(shape=(60, 60, 30), cell=100.0, n_groups=6, n_blobs=20, seed=5, n_side=200, cp_stride=4,
+                blob_width=(0.05, 0.15)) -> Problem:
+    """Large single inversion: the contact-model construction on a 60x60x30
+    grid of 100 m voxels with 6 units (~194k triangles), x/y/z-free interior
+    vertices, and an
+    n_side^2 station grid whose heights follow a seeded topography (sum of 8
+    sinusoids, 0-80 m above the flat top, plus 1 m)."""
+    p = voxel_contact_model(shape=shape, cell=cell, n_groups=n_groups, n_blobs=n_blobs, seed=seed, n_side=n_side,
+                            cp_stride=cp_stride, freedom_interior=XYZ_FREE, blob_width=blob_width)
+    st = p.grav_xyz.copy()
+    st[:, 2] = 1.0 + topography(st[:, :2], np.random.default_rng(seed + 100))
+    p.grav_xyz = st
+    p.mag_xyz = st
+    p.name = "large"
     return p
 
 
