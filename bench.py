@@ -56,6 +56,11 @@ FLOPS_FWD_PAIR = 137
 FLOPS_GRAD_PAIR = 331
 SFU_FWD_PAIR = 16   # 3 sqrt + 9 div + 3 log + 1 atan2, one special-function op each
 SFU_GRAD_PAIR = 16
+# DRAM bytes (read + write) of one k_forward_mixed launch on this workload,
+# from an ncu capture (dram__bytes_read.sum + dram__bytes_write.sum; launch
+# shape 148 x 32 CTAs): the facet records are read once per CTA and reused
+# by its 128 stations, so the kernel moves ~5 MB per 78 M pairs.
+FORWARD_DRAM_BYTES_PER_LAUNCH = 4.875e6
 # Nominal B200 CUDA-core rates at the 1.965 GHz boost clock (no measured
 # figure for these pipes exists in MEASURED_PEAKS.json): FP32 148 SMs x 128
 # lanes x 2 flop; special-function unit 148 x 16 ops; FP64 148 x 64 x 2 flop.
@@ -428,7 +433,9 @@ def main():
     peak_pps = pair_roofline(flops, sfu, args.precision)
     roofline = {"bound": "fp64" if args.precision == "fp64" else "fp32+sfu", "kernel": kname,
                 "achieved": pps * flops / 1e12, "peak": peak_pps * flops / 1e12, "unit": "TFLOP/s",
-                "frac": pps / peak_pps, "traffic": None,
+                "frac": pps / peak_pps,
+                "traffic": (FORWARD_DRAM_BYTES_PER_LAUNCH if kname == "k_forward_mixed" and args.workload == "contact"
+                            else None),
                 "peak_source": ("nominal CUDA-core rates at 1.965 GHz (FP32 74.4 TFLOP/s, SFU 4.65 Tops/s, "
                                 "FP64 37.2 TFLOP/s); MEASURED_PEAKS.json holds only HBM and bf16 GEMM figures"),
                 "flops_per_pair": flops, "sfu_ops_per_pair": sfu, "kernel_ms_per_launch": kms,

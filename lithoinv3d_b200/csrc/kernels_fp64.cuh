@@ -744,7 +744,7 @@ __device__ __forceinline__ void grad_acc_warp_sum(GradAcc& A) {
 // Warps run over `facets` (those with a DOF vertex); grid.y splits the
 // station tiles into chunks of tiles_per_chunk so that a model with few such
 // facets still fills the GPU.  part layout [chunk][9][T].
-__global__ void __launch_bounds__(128) k_gradient_warp_fp64(int T, const double* __restrict__ gc, int S,
+__global__ void __launch_bounds__(128, 3) k_gradient_warp_fp64(int T, const double* __restrict__ gc, int S,
                                                             const double* __restrict__ sta,
                                                             const double* __restrict__ gcoef,
                                                             const double* __restrict__ mcoef,
@@ -770,9 +770,12 @@ __global__ void __launch_bounds__(128) k_gradient_warp_fp64(int T, const double*
     const int ntiles_all = (S + kStationTile - 1) / kStationTile;
     const int tbeg = blockIdx.y * tiles_per_chunk, ntiles = min(ntiles_all, tbeg + tiles_per_chunk);
     part += (size_t)blockIdx.y * 9 * T;
-    double C[NGC];
-#pragma unroll
-    for (int k = 0; k < NGC; ++k) C[k] = gc[(size_t)k * T + f];
+    // the facet's constants live in shared memory (one row per warp): the
+    // per-lane FP64 sums and pair temporaries need the registers
+    __shared__ double Csh[4][NGC];
+    double* C = Csh[threadIdx.x >> 5];
+    if (lane < NGC) C[lane] = gc[(size_t)lane * T + f];
+    __syncwarp();
     double outv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     if (facet_grad_active(C)) {
         GradAcc A;
