@@ -78,6 +78,22 @@ def pair_roofline(flops: int, sfu: int, precision: str) -> float:
     return min(FP32_PEAK_FLOPS / flops, SFU_PEAK_OPS / sfu)
 
 
+def max_over_ranks(values, dist=None, device="cpu"):
+    """Element-wise maximum over ranks: every replica times its own steps and
+    the job takes as long as its slowest rank."""
+    import torch
+
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.cpu()]
+
+
+def job_rate(world: int, steps: int, slowest_ms: float) -> float:
+    """Whole-job evaluations/s: every rank evaluated `steps` times."""
+    return world * steps / (slowest_ms / 1e3)
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -409,13 +425,10 @@ def main():
     e2e_ms = sum(a.elapsed_time(b) for a, b in e2e_ev)
 
     # max over ranks (replicas)
-    tot = torch.tensor([total_ms, e2e_ms], dtype=torch.float64, device=dev)
-    if dist:
-        dist.all_reduce(tot, op=dist.ReduceOp.MAX)
-    total_ms, e2e_ms = float(tot[0]), float(tot[1])
+    total_ms, e2e_ms = max_over_ranks([total_ms, e2e_ms], dist, dev)
     ms_per_step = total_ms / args.steps
-    value = world * args.steps / (total_ms / 1e3)
-    e2e_value = world * args.steps / (e2e_ms / 1e3)
+    value = job_rate(world, args.steps, total_ms)
+    e2e_value = job_rate(world, args.steps, e2e_ms)
 
     # dominant kernel roofline: pairs/s against the pipe that binds the
     # algorithmic per-pair work (FP32 or special-function unit in mixed mode,
