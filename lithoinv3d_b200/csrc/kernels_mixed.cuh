@@ -150,24 +150,26 @@ __device__ __forceinline__ float sqrt_pos(float r2) { return r2 * rsqrtf(r2); }
 // forward  log((s2+d2)/(s1+d1)) = log1p((L + sigma)/(s1 + d1)),
 // reverse  log((d1-s1)/(d2-s2)) = log1p((L - sigma)/(d2 - s2)),
 // sigma = d2 - d1 = L (s1 + s2) / (d1 + d2).  log1p(u) = 2 atanh(v) with
-// v = u / (2 + u) = delta / (2 den + delta); for v <= 0.2 (every far pair:
-// u <= 0.5) the series 2 (v + v^3/3 + ... + v^9/9) (Abramowitz & Stegun
-// 4.1.28), whose first omitted term is below 2e-9 v, else log1pf.  Far-field
-// arguments are bounded away from zero and overflow, so 2-ulp quotients are
-// used.
+// v = u / (2 + u) = delta / (2 den + delta); with D = d1 + d2 and
+// ss = s1 + s2 the two quotients fold into one:
+//   v = L (D +- ss) / ((2 den + L) D +- L ss)   (+ forward, - reverse),
+// every term positive in the orientation chosen.  For v <= 0.2 (every far
+// pair: u <= 0.5) the series 2 (v + v^3/3 + ... + v^9/9) (Abramowitz &
+// Stegun 4.1.28), whose first omitted term is below 2e-9 v, else
+// log1pf(2v / (1 - v)).  Far-field arguments are bounded away from zero
+// and overflow, so the 2-ulp quotient is used.
 __device__ __forceinline__ float lam_f32(float s1, float s2, float d1, float d2, float L) {
-    float ss = s1 + s2;
-    float sig = __fdividef(L * ss, d1 + d2);
-    float delta, den;
-    if (ss >= 0.f) { delta = L + sig; den = s1 + d1; }
-    else           { delta = L - sig; den = d2 - s2; }
-    const float v = __fdividef(delta, fmaf(2.f, den, delta));
+    const float ss = s1 + s2, D = d1 + d2;
+    const bool fwd = ss >= 0.f;
+    const float den = fwd ? s1 + d1 : d2 - s2;
+    const float sgn = fwd ? ss : -ss;  // |ss|
+    const float v = __fdividef(L * (D + sgn), fmaf(fmaf(2.f, den, L), D, L * sgn));
     if (v <= 0.2f) {
         const float v2 = v * v;
         const float p = fmaf(v2, fmaf(v2, fmaf(v2, fmaf(v2, 1.f / 9.f, 1.f / 7.f), 1.f / 5.f), 1.f / 3.f), 1.f);
         return 2.f * v * p;
     }
-    return log1pf(__fdividef(delta, den));
+    return log1pf(__fdividef(2.f * v, 1.f - v));
 }
 
 // atan2(y, x); for x > 0 and |y| <= x / 8 (every far pair's solid angle) the
