@@ -383,6 +383,7 @@ def main():
     step_ms = [a.elapsed_time(b) for a, b in evs]
     total_ms = sum(step_ms)
     cnt = ctx.counters()
+    near_pairs = ctx.near_pairs() if args.precision == "mixed" else 0
     # ---- per-kernel device times for the roofline: a separate pass with
     # events around every pair kernel (direct launches, not graph replay) ----
     ctx.set_profiling(True)
@@ -393,7 +394,7 @@ def main():
     torch.cuda.synchronize()
     fwd_ms, fwd_n, grad_ms, grad_n = ctx.kernel_times()
     ctx.set_profiling(False)
-    near_frac = ctx.near_pairs() / max(cnt.forward_pairs, 1) if args.precision == "mixed" else 1.0
+    near_frac = near_pairs / max(cnt.forward_pairs, 1) if args.precision == "mixed" else 1.0
     launches = int(cnt.launches)
     pairs_fwd = int(cnt.forward_pairs)
     pairs_grad = int(cnt.gradient_pairs)

@@ -185,7 +185,8 @@ lf_status lf_set_precision(lf_ctx* ctx, int mode);
  * analytic TMI); nearer facets in FP64.  Default 3.  tau <= 0: every facet in
  * FP64 (local frame). */
 lf_status lf_set_far_field_ratio(lf_ctx* ctx, double tau);
-/* Station-facet pairs the mixed forward evaluated in FP64 since lf_set_model. */
+/* Station-facet pairs the mixed forward evaluated in FP64 since lf_set_model
+ * or the last lf_reset_counters. */
 lf_status lf_get_near_pairs(lf_ctx* ctx, unsigned long long* n);
 
 /* Forward at params (host arrays): gz[n_grav] mGal, tmi[n_mag] nT; either
@@ -364,6 +365,7 @@ typedef struct {
     uint64_t forward_pairs, gradient_pairs, launches;
 } lf_counters;
 lf_status lf_get_counters(lf_ctx* ctx, lf_counters* c);
+/* Zeroes the counters and the near-pair count (lf_get_near_pairs). */
 lf_status lf_reset_counters(lf_ctx* ctx);
 
 /* Kernel timing on the context's stream: when enabled, every launch of the

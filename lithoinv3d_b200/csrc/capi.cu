@@ -1980,5 +1980,9 @@ extern "C" lf_status lf_get_kernel_times(lf_ctx* c, double* fwdMs, int* fwdN, do
 extern "C" lf_status lf_reset_counters(lf_ctx* c) {
     if (!c) return LF_EINVAL;
     c->counters = {0, 0, 0};
+    if (c->d_nearPairs.p) {
+        cudaSetDevice(c->device);
+        LF_TRY_CUDA(c, cudaMemsetAsync(c->d_nearPairs.p, 0, sizeof(unsigned long long), c->stream));
+    }
     return LF_OK;
 }

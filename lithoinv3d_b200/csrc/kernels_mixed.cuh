@@ -146,24 +146,17 @@ __global__ void k_face_prep_mixed(int T, const int32_t* __restrict__ tri, const 
 // r2 * rsqrt(r2), within 2 ulp.
 __device__ __forceinline__ float sqrt_pos(float r2) { return r2 * rsqrtf(r2); }
 
-// Lambda in the orientation without the d + s cancellation:
-// forward  log((s2+d2)/(s1+d1)) = log1p((L + sigma)/(s1 + d1)),
-// reverse  log((d1-s1)/(d2-s2)) = log1p((L - sigma)/(d2 - s2)),
-// sigma = d2 - d1 = L (s1 + s2) / (d1 + d2).  log1p(u) = 2 atanh(v) with
-// v = u / (2 + u) = delta / (2 den + delta); with D = d1 + d2 and
-// ss = s1 + s2 the two quotients fold into one:
-//   v = L (D +- ss) / ((2 den + L) D +- L ss)   (+ forward, - reverse),
-// every term positive in the orientation chosen.  For v <= 0.2 (every far
-// pair: u <= 0.5) the series 2 (v + v^3/3 + ... + v^9/9) (Abramowitz &
-// Stegun 4.1.28), whose first omitted term is below 2e-9 v, else
-// log1pf(2v / (1 - v)).  Far-field arguments are bounded away from zero
-// and overflow, so the 2-ulp quotient is used.
-__device__ __forceinline__ float lam_f32(float s1, float s2, float d1, float d2, float L) {
-    const float ss = s1 + s2, D = d1 + d2;
-    const bool fwd = ss >= 0.f;
-    const float den = fwd ? s1 + d1 : d2 - s2;
-    const float sgn = fwd ? ss : -ss;  // |ss|
-    const float v = __fdividef(L * (D + sgn), fmaf(fmaf(2.f, den, L), D, L * sgn));
+// Lambda of an edge of length L whose end points lie at distances d1, d2
+// from the station: the line integral of 1/r along the edge,
+//   Lambda = log((d1 + d2 + L) / (d1 + d2 - L)) = 2 atanh(v),  v = L / (d1 + d2),
+// equal to the reference's oriented form log((s2 + d2) / (s1 + d1)) because
+// d2^2 - d1^2 = s2^2 - s1^2 along the edge's line.  Away from the edge (every
+// FP32 pair) d1 + d2 - L does not cancel.  For v <= 0.2 the series
+// 2 (v + v^3/3 + ... + v^9/9) (Abramowitz & Stegun 4.1.28), whose first
+// omitted term is below 2e-9 v, else log1pf(2v / (1 - v)).  The arguments are
+// bounded away from zero and overflow, so the 2-ulp quotient is used.
+__device__ __forceinline__ float lam_f32(float d1, float d2, float L) {
+    const float v = __fdividef(L, d1 + d2);
     if (v <= 0.2f) {
         const float v2 = v * v;
         const float p = fmaf(v2, fmaf(v2, fmaf(v2, fmaf(v2, 1.f / 9.f, 1.f / 7.f), 1.f / 5.f), 1.f / 3.f), 1.f);
@@ -185,19 +178,18 @@ __device__ __forceinline__ float atan2_far(float y, float x) {
 }
 
 // FP32 facet record of the far-field forward, staged in shared memory and
-// read with 128-bit loads (12 per pair).  The origin and the unit normal stay
+// read with 128-bit loads (11 per pair).  The origin and the unit normal stay
 // FP64: the height above the facet plane can be tiny next to |o - a| (a far
 // top facet seen from 1 m above it).
 struct __align__(16) FaceF32 {
     float rx0, rx1, rx2, L0;   // local x axis, |ab|
     float ry0, ry1, ry2, cx;   // local y axis, c.x
-    float cy, e1x, e1y, L1;    // c.y, edge b->c
-    float e2x, e2y, L2, gq;    // edge c->a, n_z * gz scale * area
+    float cy, L1, L2, gq;      // c.y, |bc|, |ca|, n_z * gz scale * area
     float mf, mt0, mt1, mt2;   // TMI facet scales
     float qx[8], qy[8];        // Radon points in the local frame (7 + pad)
     double ax, ay, az, zx, zy, zz;
 };
-static_assert(sizeof(FaceF32) == 192, "FaceF32 layout");
+static_assert(sizeof(FaceF32) == 176, "FaceF32 layout");
 
 // Far pair: gz by quadrature (7 points; MID: 28 points on the midpoint
 // subdivision), TMI analytic, both FP32; o = station (FP64).
@@ -206,15 +198,14 @@ __device__ __forceinline__ void pair_far_f32(const FaceF32* Fp, double ox, doubl
                                              float* tmi) {
     const float4* v = reinterpret_cast<const float4*>(Fp);
     const double2* w = reinterpret_cast<const double2*>(Fp);
-    const float4 v0 = v[0], v1 = v[1], v2 = v[2], v3 = v[3], v4 = v[4];
-    const double2 w0 = w[9], w1 = w[10], w2 = w[11];
+    const float4 v0 = v[0], v1 = v[1], v2 = v[2], v3 = v[3];
+    const double2 w0 = w[8], w1 = w[9], w2 = w[10];
     const double ddx = ox - w0.x, ddy = oy - w0.y, ddz = oz - w1.x;
     const float dx = (float)ddx, dy = (float)ddy, dz = (float)ddz;
     const float x = fmaf(dx, v0.x, fmaf(dy, v0.y, dz * v0.z));
     const float y = fmaf(dx, v1.x, fmaf(dy, v1.y, dz * v1.z));
     const float z = (float)(ddx * w1.y + ddy * w2.x + ddz * w2.y);
-    const float L0 = v0.w, cx = v1.w, cy = v2.x, e1x = v2.y, e1y = v2.z, L1 = v2.w;
-    const float e2x = v3.x, e2y = v3.y, L2 = v3.z, gq = v3.w;
+    const float L0 = v0.w, cx = v1.w, cy = v2.x, L1 = v2.y, L2 = v2.z, gq = v2.w;
     const float z2 = z * z;
     // gz: n_z * gscale * A * sum_q w_q / r_q
     float acc = 0.f;
@@ -226,7 +217,7 @@ __device__ __forceinline__ void pair_far_f32(const FaceF32* Fp, double ox, doubl
         }
         acc *= 0.25f;
     } else {
-        const float4 qa = v[5], qb = v[6], qc = v[7], qd = v[8];
+        const float4 qa = v[4], qb = v[5], qc = v[6], qd = v[7];
         const float qx[7] = {qa.x, qa.y, qa.z, qa.w, qb.x, qb.y, qb.z};
         const float qy[7] = {qc.x, qc.y, qc.z, qc.w, qd.x, qd.y, qd.z};
 #pragma unroll
@@ -246,10 +237,10 @@ __device__ __forceinline__ void pair_far_f32(const FaceF32* Fp, double ox, doubl
     float dbc = fmaf(rbx, rcx, fmaf(-y, rcy, z2));
     float den = la * lb * lc + dab * lc + dac * lb + dbc * la;
     float om = 2.f * atan2_far(-z * (L0 * cy), den);
-    float l0 = lam_f32(-x, rbx, la, lb, L0);
-    float l1 = lam_f32(fmaf(rbx, e1x, -y * e1y), fmaf(rcx, e1x, rcy * e1y), lb, lc, L1);
-    float l2 = lam_f32(fmaf(rcx, e2x, rcy * e2y), fmaf(-x, e2x, -y * e2y), lc, la, L2);
-    *tmi += v4.x * om + v4.y * l0 + v4.z * l1 + v4.w * l2;
+    float l0 = lam_f32(la, lb, L0);
+    float l1 = lam_f32(lb, lc, L1);
+    float l2 = lam_f32(lc, la, L2);
+    *tmi += v3.x * om + v3.y * l0 + v3.z * l1 + v3.w * l2;
 }
 
 // Near pair in FP64, local frame, with the reference's lineIntegralTerm and
@@ -327,8 +318,7 @@ __device__ __forceinline__ void forward_mixed_block(double* __restrict__ smd, Fa
             F.rx0 = (float)M(MC_XX); F.rx1 = (float)M(MC_XY); F.rx2 = (float)M(MC_XZ);
             F.ry0 = (float)M(MC_YX); F.ry1 = (float)M(MC_YY); F.ry2 = (float)M(MC_YZ);
             F.L0 = (float)M(MC_L0); F.cx = (float)M(MC_CX); F.cy = (float)M(MC_CY);
-            F.e1x = (float)M(MC_E1X); F.e1y = (float)M(MC_E1Y); F.L1 = (float)M(MC_L1);
-            F.e2x = (float)M(MC_E2X); F.e2y = (float)M(MC_E2Y); F.L2 = (float)M(MC_L2);
+            F.L1 = (float)M(MC_L1); F.L2 = (float)M(MC_L2);
             F.gq = (float)(M(MC_SGZ) * 0.5 * M(MC_L0) * M(MC_CY));
             F.mf = (float)M(MC_MF); F.mt0 = (float)M(MC_MT0); F.mt1 = (float)M(MC_MT1); F.mt2 = (float)M(MC_MT2);
 #pragma unroll
@@ -594,11 +584,10 @@ __global__ void __launch_bounds__(128) k_gradient_warp_far32(int T, const double
                             const float dbc = fmaf(rbx, rcx, fmaf(-y, rcy, z2));
                             const float den = la * lb * lc + dab * lc + dac * lb + dbc * la;
                             const float om = 2.f * atan2_far(-z * A2, den);
-                            const float s11 = fmaf(rbx, e1x, -y * e1y), s12 = fmaf(rcx, e1x, rcy * e1y);
-                            const float s21 = fmaf(rcx, e2x, rcy * e2y), s22 = fmaf(-x, e2x, -y * e2y);
-                            const float l0 = lam_f32(-x, rbx, la, lb, L0);
-                            const float l1 = lam_f32(s11, s12, lb, lc, L1);
-                            const float l2 = lam_f32(s21, s22, lc, la, L2);
+                            const float s11 = fmaf(rbx, e1x, -y * e1y), s21 = fmaf(rcx, e2x, rcy * e2y);
+                            const float l0 = lam_f32(la, lb, L0);
+                            const float l1 = lam_f32(lb, lc, L1);
+                            const float l2 = lam_f32(lc, la, L2);
                             const float ia = __fdividef(1.f, la), ib = __fdividef(1.f, lb), ic = __fdividef(1.f, lc);
                             const float kom = Ts * mf;
                             // edge (p1 -> p2): W = L / (d1 d2 + r1.r2), q = r1 - s1 e, Z = e x r1,
