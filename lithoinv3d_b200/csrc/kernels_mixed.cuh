@@ -7,15 +7,15 @@
 // coefficients alone costs 1e-6..5e-6 relative in gz.  Two facts fix it:
 //  * a facet far from a station tile (centroid distance >= tau x facet size)
 //    is integrated directly: gz facet = n_z * integral of 1/r over the facet,
-//    evaluated with Radon's 7-point degree-5 rule in FP32 (positive terms, no
-//    cancellation);
+//    evaluated by quadrature in FP32 (positive terms, no cancellation):
+//    Dunavant's 6-point degree-4 rule in the forward (3 points beyond
+//    4 tau), Radon's 7-point degree-5 rule in the gradient;
 //  * a facet near the tile uses the analytic formula in FP64, in the facet's
 //    local frame (origin at a vertex, x along the longest edge, z along the
 //    unit normal).
 // The TMI facet term of the reference (magneticFacet magnetic_forward.cpp:
 // 312-347) has no such cancellation; far facets evaluate it analytically in
-// FP32, with Lambda formed in the orientation that avoids the d + s
-// cancellation and taken as log1p of an accurately formed ratio.
+// FP32, with Lambda from the symmetric form 2 atanh(L / (d1 + d2)).
 #pragma once
 #include "kernels_fp64.cuh"
 
@@ -54,7 +54,25 @@ __constant__ float kRadonBc[7] = {0.3333333333333333f, 0.1012865073234563f, 0.10
 __constant__ float kRadonW[7] = {0.225f, 0.1259391805448271f, 0.1259391805448271f, 0.1259391805448271f,
                                  0.1323941527885062f, 0.1323941527885062f, 0.1323941527885062f};
 
-// The same rule on the four midpoint sub-triangles (a, ab, ca), (ab, b, bc),
+// Dunavant's 6-point degree-4 rule (D. A. Dunavant, "High degree efficient
+// symmetrical Gaussian quadrature rules for the triangle", IJNME 21, 1985):
+// (a, b, b) permutations with a = 0.108103018168070, b = 0.445948490915965,
+// weight 0.223381589678011, and a = 0.816847572980459, b = 0.091576213509771,
+// weight 0.109951743655322.  Its degree-6 error term, which sets the error at
+// the far-field distances, is as small as the 7-point rule's; one point fewer.
+__constant__ float kDun6Bb[6] = {0.445948490915965f, 0.108103018168070f, 0.445948490915965f,
+                                 0.091576213509771f, 0.816847572980459f, 0.091576213509771f};
+__constant__ float kDun6Bc[6] = {0.445948490915965f, 0.445948490915965f, 0.108103018168070f,
+                                 0.091576213509771f, 0.091576213509771f, 0.816847572980459f};
+__constant__ float kDun6W[6] = {0.223381589678011f, 0.223381589678011f, 0.223381589678011f,
+                                0.109951743655322f, 0.109951743655322f, 0.109951743655322f};
+// 3-point degree-2 rule: (2/3, 1/6, 1/6) permutations, weights 1/3 (Strang &
+// Fix).  Taken beyond 4 tau x size, where its (size / distance)^3 error term
+// is below 1e-7 of the station total.
+__constant__ float kTri3Bb[3] = {0.1666666666666667f, 0.6666666666666667f, 0.1666666666666667f};
+__constant__ float kTri3Bc[3] = {0.1666666666666667f, 0.1666666666666667f, 0.6666666666666667f};
+
+// Radon's rule on the four midpoint sub-triangles (a, ab, ca), (ab, b, bc),
 // (ca, bc, c), (ab, bc, ca): 28 points in the parent's barycentric (beta_b,
 // beta_c), weights kRadonW[q % 7] / 4.  Its error at distance ratio tau/2
 // matches the 7-point rule's at tau (degree-5 error ~ (size / distance)^6),
@@ -178,7 +196,7 @@ __device__ __forceinline__ float atan2_far(float y, float x) {
 }
 
 // FP32 facet record of the far-field forward, staged in shared memory and
-// read with 128-bit loads (11 per pair).  The origin and the unit normal stay
+// read with 128-bit loads (10 per far pair, 9 beyond 4 tau).  The origin and the unit normal stay
 // FP64: the height above the facet plane can be tiny next to |o - a| (a far
 // top facet seen from 1 m above it).
 struct __align__(16) FaceF32 {
@@ -186,20 +204,24 @@ struct __align__(16) FaceF32 {
     float ry0, ry1, ry2, cx;   // local y axis, c.x
     float cy, L1, L2, gq;      // c.y, |bc|, |ca|, n_z * gz scale * area
     float mf, mt0, mt1, mt2;   // TMI facet scales
-    float qx[8], qy[8];        // Radon points in the local frame (7 + pad)
+    float q6[12];              // (x, y) of the 6-point rule's points in the local frame
+    float q3[8];               // (x, y) of the 3-point rule's points, pad
     double ax, ay, az, zx, zy, zz;
 };
-static_assert(sizeof(FaceF32) == 176, "FaceF32 layout");
+static_assert(sizeof(FaceF32) == 192, "FaceF32 layout");
 
-// Far pair: gz by quadrature (7 points; MID: 28 points on the midpoint
-// subdivision), TMI analytic, both FP32; o = station (FP64).
-template <bool MID>
+enum { RULE_TRI3 = 0, RULE_DUN6 = 1, RULE_MID28 = 2 };
+
+// Far pair: gz by quadrature (RULE_TRI3 beyond 4 tau, RULE_DUN6 beyond tau,
+// RULE_MID28: Radon's rule on the midpoint subdivision beyond tau/2), TMI
+// analytic, both FP32; o = station (FP64).
+template <int RULE>
 __device__ __forceinline__ void pair_far_f32(const FaceF32* Fp, double ox, double oy, double oz, float* gz,
                                              float* tmi) {
     const float4* v = reinterpret_cast<const float4*>(Fp);
     const double2* w = reinterpret_cast<const double2*>(Fp);
     const float4 v0 = v[0], v1 = v[1], v2 = v[2], v3 = v[3];
-    const double2 w0 = w[8], w1 = w[9], w2 = w[10];
+    const double2 w0 = w[9], w1 = w[10], w2 = w[11];
     const double ddx = ox - w0.x, ddy = oy - w0.y, ddz = oz - w1.x;
     const float dx = (float)ddx, dy = (float)ddy, dz = (float)ddz;
     const float x = fmaf(dx, v0.x, fmaf(dy, v0.y, dz * v0.z));
@@ -209,22 +231,30 @@ __device__ __forceinline__ void pair_far_f32(const FaceF32* Fp, double ox, doubl
     const float z2 = z * z;
     // gz: n_z * gscale * A * sum_q w_q / r_q
     float acc = 0.f;
-    if (MID) {
+    if (RULE == RULE_MID28) {
 #pragma unroll
         for (int q = 0; q < 28; ++q) {
             float px = fmaf(kRadon4Bb[q], L0, fmaf(kRadon4Bc[q], cx, -x)), py = fmaf(kRadon4Bc[q], cy, -y);
             acc = fmaf(kRadonW[q % 7], rsqrtf(fmaf(px, px, fmaf(py, py, z2))), acc);
         }
         acc *= 0.25f;
-    } else {
-        const float4 qa = v[4], qb = v[5], qc = v[6], qd = v[7];
-        const float qx[7] = {qa.x, qa.y, qa.z, qa.w, qb.x, qb.y, qb.z};
-        const float qy[7] = {qc.x, qc.y, qc.z, qc.w, qd.x, qd.y, qd.z};
+    } else if (RULE == RULE_DUN6) {
+        const float4 qa = v[4], qb = v[5], qc = v[6];
+        const float q[12] = {qa.x, qa.y, qa.z, qa.w, qb.x, qb.y, qb.z, qb.w, qc.x, qc.y, qc.z, qc.w};
 #pragma unroll
-        for (int q = 0; q < 7; ++q) {
-            float px = qx[q] - x, py = qy[q] - y;
-            acc = fmaf(kRadonW[q], rsqrtf(fmaf(px, px, fmaf(py, py, z2))), acc);
+        for (int k = 0; k < 6; ++k) {
+            float px = q[2 * k] - x, py = q[2 * k + 1] - y;
+            acc = fmaf(kDun6W[k], rsqrtf(fmaf(px, px, fmaf(py, py, z2))), acc);
         }
+    } else {
+        const float4 qa = v[7], qb = v[8];
+        const float q[6] = {qa.x, qa.y, qa.z, qa.w, qb.x, qb.y};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            float px = q[2 * k] - x, py = q[2 * k + 1] - y;
+            acc += rsqrtf(fmaf(px, px, fmaf(py, py, z2)));
+        }
+        acc *= (1.f / 3.f);
     }
     *gz += gq * acc;
     // TMI: MF * Omega + sum_i MT_i Lambda_i
@@ -280,9 +310,10 @@ __device__ __forceinline__ void pair_near_f64(const double* __restrict__ s, int 
 // Morton curve, so a warp's 32 stations are spatially compact) x facet
 // chunks, facets staged 32 at a time in shared memory.  The precision class
 // is decided per (warp, facet): lane j tests facet j of the stage against the
-// warp's station bounding box -- centroid at least tau x size away: far
-// (FP32, 7-point gz); at least tau/2 x size: mid (FP32, 28-point gz); else
-// near (FP64 analytic) -- and the warp walks each class warp-uniformly.
+// warp's station bounding box -- centroid at least 4 tau x size away: very
+// far (FP32, 3-point gz); at least tau x size: far (FP32, 6-point gz); at
+// least tau/2 x size: mid (FP32, 28-point gz); else near (FP64 analytic) --
+// and the warp walks each class warp-uniformly.
 // One CTA's work: station s (this thread; act = s is a station of the
 // block) against facets [fb, fe); out_gz[s] / out_tmi[s] receive the sums.
 template <bool GZ, bool TMI, int FT>
@@ -322,18 +353,23 @@ __device__ __forceinline__ void forward_mixed_block(double* __restrict__ smd, Fa
             F.gq = (float)(M(MC_SGZ) * 0.5 * M(MC_L0) * M(MC_CY));
             F.mf = (float)M(MC_MF); F.mt0 = (float)M(MC_MT0); F.mt1 = (float)M(MC_MT1); F.mt2 = (float)M(MC_MT2);
 #pragma unroll
-            for (int q = 0; q < 7; ++q) {
-                F.qx[q] = kRadonBb[q] * F.L0 + kRadonBc[q] * F.cx;
-                F.qy[q] = kRadonBc[q] * F.cy;
+            for (int q = 0; q < 6; ++q) {
+                F.q6[2 * q] = kDun6Bb[q] * F.L0 + kDun6Bc[q] * F.cx;
+                F.q6[2 * q + 1] = kDun6Bc[q] * F.cy;
             }
-            F.qx[7] = F.qy[7] = 0.f;
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                F.q3[2 * q] = kTri3Bb[q] * F.L0 + kTri3Bc[q] * F.cx;
+                F.q3[2 * q + 1] = kTri3Bc[q] * F.cy;
+            }
+            F.q3[6] = F.q3[7] = 0.f;
             F.ax = M(MC_AX); F.ay = M(MC_AY); F.az = M(MC_AZ);
             F.zx = M(MC_ZX); F.zy = M(MC_ZY); F.zz = M(MC_ZZ);
 #undef M
         }
         __syncthreads();
         // lane j: facet j of the stage against this warp's box
-        bool valid = false, far = false, mid = false;
+        bool valid = false, vfar = false, far = false, mid = false;
         if (lane < nf && smd[MC_VALID * FT + lane] != 0.0) {
             valid = true;
             const float cxw = (float)smd[MC_CENX * FT + lane], cyw = (float)smd[MC_CENY * FT + lane],
@@ -343,21 +379,27 @@ __device__ __forceinline__ void forward_mixed_block(double* __restrict__ smd, Fa
             const float ddz = fmaxf(0.f, fmaxf(bb[2] - czw, czw + bb[5]));
             const float d2 = ddx * ddx + ddy * ddy + ddz * ddz;
             const float lim = tau * (float)smd[MC_SIZE * FT + lane], limMid = 0.5f * lim;
-            far = d2 >= lim * lim;
-            mid = !far && d2 >= limMid * limMid;
+            vfar = d2 >= 16.f * (lim * lim);
+            far = !vfar && d2 >= lim * lim;
+            mid = !vfar && !far && d2 >= limMid * limMid;
         }
+        const unsigned vfarMask = __ballot_sync(0xffffffffu, valid && vfar);
         const unsigned farMask = __ballot_sync(0xffffffffu, valid && far);
         const unsigned midMask = __ballot_sync(0xffffffffu, valid && mid);
-        const unsigned nearMask = __ballot_sync(0xffffffffu, valid && !far && !mid);
+        const unsigned nearMask = __ballot_sync(0xffffffffu, valid && !vfar && !far && !mid);
         if (act) {
             float gacc = 0.f, tacc = 0.f;
+            for (unsigned m = vfarMask; m; m &= m - 1) {
+                const int j = __ffs(m) - 1;
+                pair_far_f32<RULE_TRI3>(&smf[j], ox, oy, oz, &gacc, &tacc);
+            }
             for (unsigned m = farMask; m; m &= m - 1) {
                 const int j = __ffs(m) - 1;
-                pair_far_f32<false>(&smf[j], ox, oy, oz, &gacc, &tacc);
+                pair_far_f32<RULE_DUN6>(&smf[j], ox, oy, oz, &gacc, &tacc);
             }
             for (unsigned m = midMask; m; m &= m - 1) {
                 const int j = __ffs(m) - 1;
-                pair_far_f32<true>(&smf[j], ox, oy, oz, &gacc, &tacc);
+                pair_far_f32<RULE_MID28>(&smf[j], ox, oy, oz, &gacc, &tacc);
             }
             if (GZ) gz += gacc;
             if (TMI) tmi += tacc;
@@ -434,7 +476,8 @@ constexpr int kFarFlushTiles = 4;  // far tiles summed per lane in FP32 between 
 
 // Far-field objective gradient in FP32: one warp per facet, lanes over the
 // stations of the facet's far tiles (exactly the tiles k_gradient_warp_fp64
-// leaves out: both classify with facet_far_key / tile_far).
+// leaves out: both classify with facet_far_key / tile_far).  gz by Dunavant's
+// 6-point rule.
 //  * gz: I = A sum_q w_q / r_q, so
 //      sum_s G0 dI/dv = (dA/dv) Q0 - A sum_q beta_qv D_q,
 //    Q0 = sum_s G0 sum_q w_q / r_q, D_q = sum_s G0 w_q (p_q - o) / r_q^3
@@ -494,24 +537,24 @@ __global__ void __launch_bounds__(128) k_gradient_warp_far32(int T, const double
             const double ax = C[GC_AX], ay = C[GC_AY], az = C[GC_AZ];
             const double zx = C[GC_ZX], zy = C[GC_ZY], zz = C[GC_ZZ];
             const double gsn = C[GC_GS], ms = C[GC_MS];
-            float qx[7], qy[7];
+            float qx[6], qy[6];
 #pragma unroll
-            for (int q = 0; q < 7; ++q) {
-                qx[q] = kRadonBb[q] * L0 + kRadonBc[q] * cx;
-                qy[q] = kRadonBc[q] * cy;
+            for (int q = 0; q < 6; ++q) {
+                qx[q] = kDun6Bb[q] * L0 + kDun6Bc[q] * cx;
+                qy[q] = kDun6Bc[q] * cy;
             }
-            float q0 = 0.f, dqx[7], dqy[7], dqz[7];
+            float q0 = 0.f, dqx[6], dqy[6], dqz[6];
             float vax = 0.f, vay = 0.f, vaz = 0.f, vbx = 0.f, vby = 0.f, vbz = 0.f, vcx = 0.f, vcy = 0.f, vcz = 0.f;
             float amf = 0.f, amt0 = 0.f, amt1 = 0.f, amt2 = 0.f;
 #pragma unroll
-            for (int q = 0; q < 7; ++q) dqx[q] = dqy[q] = dqz[q] = 0.f;
+            for (int q = 0; q < 6; ++q) dqx[q] = dqy[q] = dqz[q] = 0.f;
             int pending = 0;
             auto flush = [&]() {
                 float v[32];
                 float sa0 = 0.f, sa1 = 0.f, sa2 = 0.f, sb0 = 0.f, sb1 = 0.f, sb2 = 0.f, sc0 = 0.f, sc1 = 0.f, sc2 = 0.f;
 #pragma unroll
-                for (int q = 0; q < 7; ++q) {
-                    const float bb = kRadonBb[q], bc = kRadonBc[q], ba = 1.f - bb - bc;
+                for (int q = 0; q < 6; ++q) {
+                    const float bb = kDun6Bb[q], bc = kDun6Bc[q], ba = 1.f - bb - bc;
                     sa0 = fmaf(ba, dqx[q], sa0); sa1 = fmaf(ba, dqy[q], sa1); sa2 = fmaf(ba, dqz[q], sa2);
                     sb0 = fmaf(bb, dqx[q], sb0); sb1 = fmaf(bb, dqy[q], sb1); sb2 = fmaf(bb, dqz[q], sb2);
                     sc0 = fmaf(bc, dqx[q], sc0); sc1 = fmaf(bc, dqy[q], sc1); sc2 = fmaf(bc, dqz[q], sc2);
@@ -562,10 +605,10 @@ __global__ void __launch_bounds__(128) k_gradient_warp_far32(int T, const double
                         if (G0 != 0.f) {
                             float sw = 0.f;
 #pragma unroll
-                            for (int q = 0; q < 7; ++q) {
+                            for (int q = 0; q < 6; ++q) {
                                 const float px = qx[q] - x, py = qy[q] - y;
                                 const float rs = rsqrtf(fmaf(px, px, fmaf(py, py, z2)));
-                                const float w = kRadonW[q] * rs;
+                                const float w = kDun6W[q] * rs;
                                 sw += w;
                                 const float g3 = G0 * w * rs * rs;
                                 dqx[q] = fmaf(g3, px, dqx[q]);
