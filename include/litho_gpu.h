@@ -196,9 +196,9 @@ lf_status lf_forward(lf_ctx* ctx, const double* params, double* gz, double* tmi)
 /* Launch shapes of the hot kernels (no reference counterpart).
  *  fwd_target_blocks     forward CTAs per launch: stations/128 x facet chunks;
  *                        more chunks = more CTAs, each over fewer facets
- *                        (candidates 148 x {4, 8, 16, 32, 64})
+ *                        (candidates 148 x {4, 8, 16, 32, 64, 128})
  *  grad_target_warps     gradient warps per launch: DOF facets x station chunks
- *                        (148 x {16, 32, 64, 128})
+ *                        (148 x {16, 32, 64, 128, 256})
  *  near_tiles_per_chunk  mixed near-field gradient: 64-station tiles per warp
  *                        (0: the grad_target_warps split; candidates 0, 1, 2, 4, 8)
  * lf_autotune measures candidates on the context's own model, stations and

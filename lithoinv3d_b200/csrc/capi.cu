@@ -1454,12 +1454,12 @@ extern "C" lf_status lf_autotune(lf_ctx* c, const double* params, int repeats, l
     lf_tuning best = c->tune;
     double bestMs = 0.0;
     lf_status st = timeit(best, &bestMs);
-    const int fwdC[] = {148 * 4, 148 * 8, 148 * 16, 148 * 32, 148 * 64};
-    const int gradC[] = {148 * 16, 148 * 32, 148 * 64, 148 * 128};
+    const int fwdC[] = {148 * 4, 148 * 8, 148 * 16, 148 * 32, 148 * 64, 148 * 128};
+    const int gradC[] = {148 * 16, 148 * 32, 148 * 64, 148 * 128, 148 * 256};
     const int nearC[] = {0, 1, 2, 4, 8};
     for (int dim = 0; dim < 3 && st == LF_OK; ++dim) {
         const int* cand = dim == 0 ? fwdC : (dim == 1 ? gradC : nearC);
-        const int nc = dim == 1 ? 4 : 5;
+        const int nc = dim == 0 ? 6 : 5;
         if (dim == 2 && c->precision != LF_PREC_MIXED) break;
         for (int k = 0; k < nc && st == LF_OK; ++k) {
             lf_tuning t = best;

@@ -30,8 +30,8 @@ def test_autotune_keeps_results(mixed):
     f0, g0 = ctx.objective_and_gradient(x0)
     t, ms = ctx.autotune(x0, repeats=2)
     assert ms > 0
-    assert t.fwd_target_blocks in (148 * 4, 148 * 8, 148 * 16, 148 * 32, 148 * 64)
-    assert t.grad_target_warps in (148 * 16, 148 * 32, 148 * 64, 148 * 128)
+    assert t.fwd_target_blocks in (148 * 4, 148 * 8, 148 * 16, 148 * 32, 148 * 64, 148 * 128)
+    assert t.grad_target_warps in (148 * 16, 148 * 32, 148 * 64, 148 * 128, 148 * 256)
     assert t.near_tiles_per_chunk in (0, 1, 2, 4, 8)
     got = ctx.tuning()
     assert (got.fwd_target_blocks, got.grad_target_warps, got.near_tiles_per_chunk) == \
