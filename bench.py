@@ -44,6 +44,9 @@ WORKLOAD_LARGE = ("large single inversion: 6 units on a 60x60x30 grid of 100 m v
 WORKLOAD_BATCH = ("batched bodies: 256 closed bodies (perturbed lat-long spheres and star-shaped prisms), "
                   "triangles log-uniform in [500, 50000], per-body square station grids of side U[16, 128] "
                   "at U[25, 100] m, one persistent forward launch")
+WORKLOAD_CONSTRAINTS = ("borehole-constraint gradient on the multi-unit contact model: 64 intervals (32 within "
+                        "0.3 m of control-point vertices, 32 random), 1,313 DOFs, central differences with a 1 m "
+                        "step (2 x np scatter + ray-cast classification passes per gradient)")
 L2_FLUSH_BYTES = 256 << 20
 
 # Algorithmic work per station-facet pair (frozen; derived from the FP64
@@ -103,7 +106,7 @@ def parse():
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-stations", type=int, default=48)
-    ap.add_argument("--workload", choices=["contact", "batch", "large"], default="contact",
+    ap.add_argument("--workload", choices=["contact", "batch", "large", "constraints"], default="contact",
                     help="contact: the 4-group contact model (headline); batch: 256 batched bodies; "
                          "large: the 194k-facet single inversion")
     ap.add_argument("--lbfgs-iters", type=int, default=0,
@@ -315,10 +318,89 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def constraint_intervals(pos, cp_vertices, n_group, rng, n_near=32, n_random=32):
+    """Borehole intervals for the constraint workload: midpoints 0.3 m above
+    or below control-point vertices (a 1 m DOF step flips their class) and
+    random midpoints inside the model; half-thickness U(0.5, 40) m."""
+    import numpy as np
+
+    pick = pos[rng.choice(cp_vertices, n_near, replace=False)]
+    mid = pick + np.where(rng.random(n_near) < 0.5, 0.3, -0.3)[:, None] * np.array([0.0, 0.0, 1.0])
+    mid = np.concatenate([mid, rng.uniform([-1150.0, -1150.0, -1150.0], [1150.0, 1150.0, -20.0], (n_random, 3))])
+    half = rng.uniform(0.5, 40.0, len(mid))
+    group = rng.integers(0, n_group, len(mid)).astype(np.int32)
+    return mid[:, :2].copy(), -mid[:, 2] - half, -mid[:, 2] + half, group
+
+
+def run_constraints(args):
+    """--workload constraints: ConstraintHandler::gradient (lf_constraint_gradient)
+    per second on one GPU; the CPU baseline is the compiled reference's
+    ConstraintHandler::evaluate (one scatter + classification of every
+    interval, the unit of the gradient's 2 np evaluations) on a sample."""
+    import numpy as np
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    p, model = make_problem("contact")
+    t = model.tables()
+    x0 = model.assemble_parameters()
+    cp_vertices = np.unique(t["ref_vertex"][t["ref_axis"] == 2])
+    xy, zt, zb, group = constraint_intervals(t["pos"], cp_vertices, len(p.meshes), np.random.default_rng(11))
+    ctx = p.make_context(model, device=local)
+    ctx.set_constraints(xy, zt, zb, group)
+    for _ in range(args.warmup):
+        g = ctx.constraint_gradient(x0)
+    torch.cuda.synchronize()
+    ctx.reset_counters()
+    with ClockSampler(local) as clocks:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            g = ctx.constraint_gradient(x0)  # synchronous: H2D params, 2 np passes, D2H gradient
+        dt = time.perf_counter() - t0
+    launches = int(ctx.counters().launches)
+    value = args.steps / dt
+    np_ = model.n_dofs
+    line = {"metric": "constraint-gradient evals/s (ConstraintHandler::gradient)", "value": value,
+            "unit": "evals/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded voxel model and intervals)",
+            "config": {"workload": WORKLOAD_CONSTRAINTS, "intervals": len(xy), "dofs": np_,
+                       "triangles": int(len(t["tri"])), "nonzero_gradient_entries": int(np.count_nonzero(g))},
+            "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 8 * np_,
+                    "d2h_bytes_per_step": 8 * np_},
+            "gpu_launches": launches, "launches_per_step": launches / args.steps,
+            "clocks": clocks.summary()}
+    if rank == 0 and not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import oracle_bindings as ob
+
+        if ob.ref_available():
+            rm = ob.RefModel(p)
+            rm.set_constraints(xy, zt, zb, group)
+            n_eval = 20
+            t0 = time.perf_counter()
+            for j in range(n_eval):
+                xp = x0.copy()
+                xp[j] += 1.0
+                rm.constraint_value(xp)
+            per_eval = (time.perf_counter() - t0) / n_eval
+            cpu = 1.0 / (2 * np_ * per_eval)
+            line["cpu_baseline"] = {"value": cpu, "unit": "evals/s", "cores": 1, "kind": "reference",
+                                    "sample": f"{n_eval} ConstraintHandler::evaluate calls ({per_eval * 1e3:.1f} ms "
+                                              f"each), scaled to the gradient's 2 x {np_} evaluations"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.workload == "constraints":
+        run_constraints(args)
         return
     import numpy as np
     import torch

@@ -376,6 +376,47 @@ lf_status lf_set_profiling(lf_ctx* ctx, int enabled);
 lf_status lf_get_kernel_times(lf_ctx* ctx, double* forward_ms, int* forward_launches,
                               double* gradient_ms, int* gradient_launches);
 
+/* ---------------------------------------- point classification, constraints */
+/* LithologyModel::setLabelGrid (modules/litho-model/src/litho/
+ * lithology_model.cpp:89-103): labels[(iz*ny + iy)*nx + ix] = group id of
+ * voxel (ix, iy, iz) with corner (x0, y0, z0) and spacing (dx, dy, dz); a
+ * voxel holding a negative id falls back to ray casting.  nx, ny or nz <= 0
+ * or labels == NULL removes the grid.  Spacings must be non-zero. */
+lf_status lf_set_label_grid(lf_ctx* ctx, int nx, int ny, int nz, double x0, double y0, double z0, double dx,
+                            double dy, double dz, const int32_t* labels);
+/* LithologyModel::setBottomDepth (lithology_model.cpp:856-858): points below
+ * it classify as -1.  Default -5000. */
+lf_status lf_set_bottom_depth(lf_ctx* ctx, double depth);
+/* LithologyModel::classifyPoint (lithology_model.cpp:288-363) for n points
+ * xyz[3n]: group[i] = the group whose closed mesh contains the point (label
+ * grid first, then a +x ray cast against every group mesh in group order,
+ * first odd crossing count wins), -1 outside every mesh or below the bottom
+ * depth.  With params != NULL the parameters are applied first
+ * (applyParameterVector); with NULL the positions of the last call are used.
+ * Same answers as the reference, bit for bit (the ray test is evaluated in
+ * FP64 in the reference's operation order). */
+lf_status lf_classify_points(lf_ctx* ctx, const double* params, int n, const double* xyz, int32_t* group);
+/* ConstraintHandler(model, constraints) + setWeight (modules/
+ * litho-inversion/src/inversion/constraint_handler.cpp:7-13,
+ * include/.../constraint_handler.h:16): n borehole intervals, xy[2n] column
+ * positions, z_top / z_bottom depths positive down, group = lithology known
+ * in the interval.  The reference's default weight is 1e6. */
+lf_status lf_set_constraints(lf_ctx* ctx, int n, const double* xy, const double* z_top, const double* z_bottom,
+                             const int32_t* group, double weight);
+/* ConstraintHandler::evaluate (constraint_handler.cpp:31-42): weight x sum
+ * of squared violations, a violation being |z_bottom - z_top| when the
+ * interval midpoint does not classify as its group.  Applies params. */
+lf_status lf_constraint_penalty(lf_ctx* ctx, const double* params, double* value);
+/* ConstraintHandler::gradient (constraint_handler.cpp:44-66): central
+ * differences with a 1 m step over every parameter (2 np evaluations, each a
+ * scatter + classification of every interval midpoint on the GPU), scaled
+ * by the weight as the reference does (the evaluations already carry it, so
+ * the result carries weight^2).  Leaves the positions at the last perturbed
+ * parameters, as the reference leaves its model.  The ObjectiveFunction
+ * with a constraint handler (objective.cpp:61-73, 97-101) is lf_objective /
+ * lf_objective_grad plus these two. */
+lf_status lf_constraint_gradient(lf_ctx* ctx, const double* params, double* grad);
+
 /* ------------------------------------------------------------------------ */
 /* Allocation-free forward.  No counterpart in the reference: for callers    */
 /* that cannot call cudaMalloc (a host framework owning all device memory   */

@@ -104,6 +104,13 @@ SIGNATURES = {
     "lf_forward_noalloc": (C.c_int, [C.c_int, _vp, C.c_int, _vp, C.c_int, _vp, C.c_double, C.c_double, C.c_double,
                                      C.c_double, C.c_double, _vp, _vp, _vp]),
     "lf_get_kernel_times": (C.c_int, [_vp, _dp, C.POINTER(C.c_int), _dp, C.POINTER(C.c_int)]),
+    "lf_set_label_grid": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                    C.c_double, C.c_double, _ip]),
+    "lf_set_bottom_depth": (C.c_int, [_vp, C.c_double]),
+    "lf_classify_points": (C.c_int, [_vp, _dp, C.c_int, _dp, _ip]),
+    "lf_set_constraints": (C.c_int, [_vp, C.c_int, _dp, _dp, _dp, _ip, C.c_double]),
+    "lf_constraint_penalty": (C.c_int, [_vp, _dp, _dp]),
+    "lf_constraint_gradient": (C.c_int, [_vp, _dp, _dp]),
 }
 
 STATUS = {0: "LF_OK", 1: "LF_EINVAL", 2: "LF_ECUDA", 3: "LF_ENOMEM", 4: "LF_ESTATE", 5: "LF_ETIMEOUT",

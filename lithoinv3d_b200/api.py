@@ -265,6 +265,47 @@ class Context:
                     "calibrate_data_weights")
         return float(a[0]), float(eg[0]), float(em[0])
 
+    # ---- point classification and borehole constraints ----
+    def set_label_grid(self, labels, origin, spacing):
+        """lf_set_label_grid: labels shaped (nz, ny, nx) of group ids (negative:
+        ray casting decides); labels=None removes the grid."""
+        if labels is None:
+            self._check(self.lib.lf_set_label_grid(self.h, 0, 0, 0, 0.0, 0.0, 0.0, 1.0, 1.0, 1.0, None),
+                        "set_label_grid")
+            return
+        lab = i32(labels)
+        nz, ny, nx = lab.shape
+        self._check(self.lib.lf_set_label_grid(self.h, nx, ny, nz, *map(float, origin), *map(float, spacing),
+                                               _i(lab)), "set_label_grid")
+
+    def set_bottom_depth(self, depth: float):
+        self._check(self.lib.lf_set_bottom_depth(self.h, float(depth)), "set_bottom_depth")
+
+    def classify_points(self, xyz, params=None) -> np.ndarray:
+        """lf_classify_points: group id per point (-1 outside every mesh)."""
+        x = f64(xyz).reshape(-1, 3)
+        out = np.zeros(len(x), np.int32)
+        self._check(self.lib.lf_classify_points(self.h, _d(f64(params)) if params is not None else None, len(x),
+                                                _d(x), _i(out)), "classify_points")
+        return out
+
+    def set_constraints(self, xy, z_top, z_bottom, group, weight: float = 1e6):
+        """lf_set_constraints: borehole intervals (depths positive down)."""
+        xy = f64(xy).reshape(-1, 2)
+        zt, zb, g = f64(z_top), f64(z_bottom), i32(group)
+        self._check(self.lib.lf_set_constraints(self.h, len(xy), _d(xy), _d(zt), _d(zb), _i(g), float(weight)),
+                    "set_constraints")
+
+    def constraint_penalty(self, params) -> float:
+        v = np.zeros(1)
+        self._check(self.lib.lf_constraint_penalty(self.h, _d(f64(params)), _d(v)), "constraint_penalty")
+        return float(v[0])
+
+    def constraint_gradient(self, params) -> np.ndarray:
+        g = np.zeros(self.n_dofs)
+        self._check(self.lib.lf_constraint_gradient(self.h, _d(f64(params)), _d(g)), "constraint_gradient")
+        return g
+
     def set_scatter_stateless(self, enabled: bool = True):
         """Every scatter from the model's given positions (lf_set_scatter_stateless)."""
         self._check(self.lib.lf_set_scatter_stateless(self.h, int(bool(enabled))), "set_scatter_stateless")

@@ -1,6 +1,7 @@
 // C ABI implementation: contexts, device buffers and the launch sequence of
 // one forward / objective / objective+gradient evaluation.
 #include "../../include/litho_gpu.h"
+#include "kernels_classify.cuh"
 #include "kernels_mixed.cuh"
 #include "lbfgsb.hpp"
 #include "model_builder.hpp"
@@ -131,6 +132,16 @@ struct lf_ctx {
     // workspaces
     DevBuf<double> d_partG, d_partM, d_partGrad, d_blockG, d_blockM, d_ones, d_jac;
 
+    // point classification and the constraint penalty (lf_set_label_grid,
+    // lf_set_bottom_depth, lf_set_constraints)
+    double bottomDepth = -5000.0;  // LithologyModel's default
+    LabelGridDev labelGrid;        // labels -> d_labels.p when a grid is set
+    DevBuf<int32_t> d_labels, d_grpTriOffDev, d_cGroup, d_cCls, d_ptCls;
+    DevBuf<unsigned long long> d_clsMask;  // per-point crossing parities (one bit per group)
+    DevBuf<double> d_cMid, d_cThick, d_cPar, d_cPar0, d_cFp, d_cFm, d_cGrad, d_cOut, d_pts;
+    int nCons = 0;
+    double consWeight = 1e6;  // ConstraintHandler's default weight
+
     lf_counters counters{0, 0, 0};
 
     // CUDA graph replay of whole evaluations (lf_set_graph_mode).  epoch is
@@ -151,7 +162,7 @@ struct lf_ctx {
     };
     bool graphMode = false;
     uint64_t epoch = 0;
-    GraphSet gObjGrad, gObj;
+    GraphSet gObjGrad, gObj, gCons;
 
     // launch shapes chosen by lf_autotune (defaults: measured on the
     // 19k-facet, 4096-station contact model)
@@ -429,6 +440,7 @@ extern "C" void lf_destroy(lf_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     drop_graph(c->gObjGrad);
     drop_graph(c->gObj);
+    drop_graph(c->gCons);
     clear_events(c->evFwd);
     clear_events(c->evGrad);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -1352,8 +1364,9 @@ extern "C" lf_status lf_forward(lf_ctx* c, const double* params, double* gz, dou
 // is not an error (the eager run already produced the result); it is not
 // retried until a setter changes the context.
 template <class Body>
-static lf_status run_cached(lf_ctx* c, lf_ctx::GraphSet& set, const double* p, double* f, double* grad, Body body) {
-    if (!c->graphMode || c->profiling) return body();
+static lf_status run_cached(lf_ctx* c, lf_ctx::GraphSet& set, const double* p, double* f, double* grad, Body body,
+                            bool always = false) {
+    if ((!c->graphMode && !always) || c->profiling) return body();
     for (auto& g : set.slot)
         if (g.exec && g.epoch == c->epoch && g.reallocs == reallocAll() && g.params == p && g.f == f &&
             g.grad == grad) {
@@ -1984,5 +1997,188 @@ extern "C" lf_status lf_reset_counters(lf_ctx* c) {
         cudaSetDevice(c->device);
         LF_TRY_CUDA(c, cudaMemsetAsync(c->d_nearPairs.p, 0, sizeof(unsigned long long), c->stream));
     }
+    return LF_OK;
+}
+
+// ------------------------------------------- classification and constraints --
+// LithologyModel::setLabelGrid / setBottomDepth / classifyPoint
+// (lithology_model.cpp:89-103, 856-858, 288-363) and ConstraintHandler
+// (constraint_handler.cpp:7-66) over the context's device positions.
+
+static lf_status model_ready(lf_ctx* c) {
+    if (!c) return LF_EINVAL;
+    if (!c->hasModel) return fail(c, LF_ESTATE, "no model set");
+    cudaSetDevice(c->device);
+    return LF_OK;
+}
+
+// Classifies n device points (xyz rows) into d_out against the current
+// device positions (the group triangle ranges must be on the device).
+// With at most 64 groups the crossings of one point are split over several
+// CTAs (parities combine by XOR); d_clsMask must hold n masks.
+static lf_status classify_launch(lf_ctx* c, int n, const double* d_pts, int32_t* d_out) {
+    if (n <= 0) return LF_OK;
+    if (c->G > 64 || c->d_clsMask.n < (size_t)n) {
+        k_classify_points<<<n, kClassifyThreads, 0, c->stream>>>(n, d_pts, c->G, c->d_grpTriOffDev.p, c->d_tri.p,
+                                                                 c->d_pos.p, c->bottomDepth, c->labelGrid, d_out);
+        c->counters.launches++;
+        LF_CHECK_LAUNCH(c);
+        return LF_OK;
+    }
+    const int slices = std::max(1, std::min(cdiv(c->T, 2 * kCrossThreads), cdiv(148 * 8, n)));
+    const int slice = cdiv(c->T, slices);
+    k_classify_prep<<<cdiv(n, 128), 128, 0, c->stream>>>(n, d_pts, c->G, c->bottomDepth, c->labelGrid, d_out,
+                                                         c->d_clsMask.p);
+    k_classify_cross<<<dim3(n, slices), kCrossThreads, 0, c->stream>>>(n, d_pts, c->T, slice, c->d_faceGroup.p,
+                                                                        c->d_tri.p, c->d_pos.p, d_out,
+                                                                        c->d_clsMask.p);
+    k_classify_finish<<<cdiv(n, 128), 128, 0, c->stream>>>(n, c->d_clsMask.p, d_out);
+    c->counters.launches += 3;
+    LF_CHECK_LAUNCH(c);
+    return LF_OK;
+}
+
+static lf_status classify_dev(lf_ctx* c, int n, const double* d_pts, int32_t* d_out) {
+    if (n <= 0) return LF_OK;
+    LF_TRY_CUDA(c, upload(c->d_grpTriOffDev, c->grpTriOff.data(), c->grpTriOff.size(), c->stream));
+    return classify_launch(c, n, d_pts, d_out);
+}
+
+// Scatter of the context's constraint parameter buffer, classification of
+// the interval midpoints and the penalty into *d_out (device).
+static lf_status constraint_eval_dev(lf_ctx* c, double* d_out) {
+    LF_RET_IF(scatter(c, c->d_cPar.p));
+    LF_RET_IF(classify_launch(c, c->nCons, c->d_cMid.p, c->d_cCls.p));
+    k_constraint_penalty<<<1, kPenaltyThreads, 0, c->stream>>>(c->nCons, c->d_cCls.p, c->d_cGroup.p, c->d_cThick.p,
+                                                               c->consWeight, d_out);
+    c->counters.launches++;
+    LF_CHECK_LAUNCH(c);
+    return LF_OK;
+}
+
+static lf_status constraint_params(lf_ctx* c, const double* params) {
+    if (c->np > 0 && !params) return fail(c, LF_EINVAL, "null params");
+    if (!finite_all(params, c->np)) return fail(c, LF_EINVAL, "non-finite parameter");
+    LF_TRY_CUDA(c, upload(c->d_cPar, params, c->np, c->stream));
+    return LF_OK;
+}
+
+extern "C" lf_status lf_set_label_grid(lf_ctx* c, int nx, int ny, int nz, double x0, double y0, double z0, double dx,
+                                       double dy, double dz, const int32_t* labels) {
+    LF_RET_IF(model_ready(c));
+    c->epoch++;  // cached constraint sweeps bake the grid in
+    if (nx <= 0 || ny <= 0 || nz <= 0 || !labels) {  // no grid: ray casting only
+        c->labelGrid = LabelGridDev{};
+        return LF_OK;
+    }
+    const double g[6] = {x0, y0, z0, dx, dy, dz};
+    if (!finite_all(g, 6) || dx == 0.0 || dy == 0.0 || dz == 0.0 ||
+        (long long)nx * ny * nz > (long long)1 << 31)
+        return fail(c, LF_EINVAL, "lf_set_label_grid: bad origin, spacing or size");
+    const size_t n = (size_t)nx * ny * nz;
+    LF_TRY_CUDA(c, upload(c->d_labels, labels, n, c->stream));
+    LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->labelGrid = LabelGridDev{nx, ny, nz, x0, y0, z0, dx, dy, dz, c->d_labels.p};
+    return LF_OK;
+}
+
+extern "C" lf_status lf_set_bottom_depth(lf_ctx* c, double depth) {
+    if (!c || std::isnan(depth)) return LF_EINVAL;
+    c->epoch++;
+    c->bottomDepth = depth;
+    return LF_OK;
+}
+
+extern "C" lf_status lf_classify_points(lf_ctx* c, const double* params, int n, const double* xyz, int32_t* group) {
+    LF_RET_IF(model_ready(c));
+    if (n < 0 || (n > 0 && (!xyz || !group))) return fail(c, LF_EINVAL, "lf_classify_points: bad point arrays");
+    if (params) {
+        LF_RET_IF(constraint_params(c, params));
+        LF_RET_IF(scatter(c, c->d_cPar.p));
+    }
+    if (n == 0) return LF_OK;
+    if (!finite_all(xyz, 3 * (size_t)n)) return fail(c, LF_EINVAL, "lf_classify_points: non-finite point");
+    LF_TRY_CUDA(c, upload(c->d_pts, xyz, 3 * (size_t)n, c->stream));
+    LF_TRY_CUDA(c, c->d_ptCls.reserve(n));
+    LF_TRY_CUDA(c, c->d_clsMask.reserve(std::max<size_t>(c->d_clsMask.n, n)));
+    LF_RET_IF(classify_dev(c, n, c->d_pts.p, c->d_ptCls.p));
+    LF_TRY_CUDA(c, cudaMemcpyAsync(group, c->d_ptCls.p, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, c->stream));
+    LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
+    return LF_OK;
+}
+
+extern "C" lf_status lf_set_constraints(lf_ctx* c, int n, const double* xy, const double* z_top,
+                                        const double* z_bottom, const int32_t* group, double weight) {
+    LF_RET_IF(model_ready(c));
+    if (n < 0 || (n > 0 && (!xy || !z_top || !z_bottom || !group)) || !std::isfinite(weight))
+        return fail(c, LF_EINVAL, "lf_set_constraints: bad arrays or weight");
+    if (n > 0 && (!finite_all(xy, 2 * (size_t)n) || !finite_all(z_top, n) || !finite_all(z_bottom, n)))
+        return fail(c, LF_EINVAL, "lf_set_constraints: non-finite constraint");
+    std::vector<double> mid(3 * (size_t)n), thick(n);
+    for (int k = 0; k < n; ++k) {
+        // computeViolation (constraint_handler.cpp:16-29): depth positive down
+        mid[3 * k] = xy[2 * k];
+        mid[3 * k + 1] = xy[2 * k + 1];
+        mid[3 * k + 2] = -(z_top[k] + z_bottom[k]) / 2.0;
+        thick[k] = std::abs(z_bottom[k] - z_top[k]);
+    }
+    LF_TRY_CUDA(c, upload(c->d_cMid, mid.data(), mid.size(), c->stream));
+    LF_TRY_CUDA(c, upload(c->d_cThick, thick.data(), thick.size(), c->stream));
+    LF_TRY_CUDA(c, upload(c->d_cGroup, group, (size_t)n, c->stream));
+    LF_TRY_CUDA(c, c->d_cCls.reserve(n));
+    LF_TRY_CUDA(c, c->d_cOut.reserve(1));
+    LF_TRY_CUDA(c, c->d_clsMask.reserve(std::max<size_t>(c->d_clsMask.n, n)));
+    LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->epoch++;
+    c->nCons = n;
+    c->consWeight = weight;
+    return LF_OK;
+}
+
+extern "C" lf_status lf_constraint_penalty(lf_ctx* c, const double* params, double* value) {
+    LF_RET_IF(model_ready(c));
+    if (!value) return fail(c, LF_EINVAL, "null value");
+    LF_RET_IF(constraint_params(c, params));
+    LF_TRY_CUDA(c, c->d_cOut.reserve(1));
+    LF_TRY_CUDA(c, upload(c->d_grpTriOffDev, c->grpTriOff.data(), c->grpTriOff.size(), c->stream));
+    LF_RET_IF(constraint_eval_dev(c, c->d_cOut.p));
+    LF_TRY_CUDA(c, cudaMemcpyAsync(value, c->d_cOut.p, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
+    return LF_OK;
+}
+
+extern "C" lf_status lf_constraint_gradient(lf_ctx* c, const double* params, double* grad) {
+    LF_RET_IF(model_ready(c));
+    if (c->np > 0 && !grad) return fail(c, LF_EINVAL, "null grad");
+    LF_RET_IF(constraint_params(c, params));
+    if (c->np == 0) return LF_OK;
+    LF_TRY_CUDA(c, upload(c->d_cPar0, params, c->np, c->stream));
+    LF_TRY_CUDA(c, c->d_cFp.reserve(c->np));
+    LF_TRY_CUDA(c, c->d_cFm.reserve(c->np));
+    LF_TRY_CUDA(c, c->d_cGrad.reserve(c->np));
+    LF_TRY_CUDA(c, upload(c->d_grpTriOffDev, c->grpTriOff.data(), c->grpTriOff.size(), c->stream));
+    // The 2 np passes are sequential (each scatter starts from the positions
+    // the previous one left, as the reference's model does) and each is a
+    // handful of short launches, so the sweep is replayed as one CUDA graph
+    // after its first direct run.
+    auto sweep = [c]() -> lf_status {
+        const double h = 1.0;  // constraint_handler.cpp:54
+        for (int j = 0; j < c->np; ++j) {
+            k_constraint_step<<<1, 32, 0, c->stream>>>(c->d_cPar.p, c->d_cPar0.p, j, h, 0);
+            LF_RET_IF(constraint_eval_dev(c, c->d_cFp.p + j));
+            k_constraint_step<<<1, 32, 0, c->stream>>>(c->d_cPar.p, c->d_cPar0.p, j, h, 1);
+            LF_RET_IF(constraint_eval_dev(c, c->d_cFm.p + j));
+            k_constraint_step<<<1, 32, 0, c->stream>>>(c->d_cPar.p, c->d_cPar0.p, j, h, 2);
+            c->counters.launches += 3;
+        }
+        k_constraint_fd<<<cdiv(c->np, 256), 256, 0, c->stream>>>(c->np, c->d_cFp.p, c->d_cFm.p, h,
+                                                                  c->consWeight, c->d_cGrad.p);
+        c->counters.launches++;
+        LF_CHECK_LAUNCH(c);
+        return LF_OK;
+    };
+    LF_RET_IF(run_cached(c, c->gCons, c->d_cPar0.p, c->d_cFp.p, c->d_cGrad.p, sweep, true));
+    LF_TRY_CUDA(c, cudaMemcpyAsync(grad, c->d_cGrad.p, sizeof(double) * c->np, cudaMemcpyDeviceToHost, c->stream));
+    LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
     return LF_OK;
 }

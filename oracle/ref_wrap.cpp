@@ -10,6 +10,7 @@
 // product library links or loads it.
 #include <litho_invert/forward/gravity_forward.h>
 #include <litho_invert/forward/magnetic_forward.h>
+#include <litho_invert/inversion/constraint_handler.h>
 #include <litho_invert/inversion/joint_objective.h>
 #include <litho_invert/inversion/lbfgsb_optimizer.h>
 #include <litho_invert/inversion/objective.h>
@@ -44,6 +45,7 @@ struct RefCtx {
     double smoothWeight = 0.0;
     std::shared_ptr<SurfaceSmoothness> smooth;
     VectorXd refParams;
+    std::shared_ptr<ConstraintHandler> cons;
     bool built = false;
 
     void build() {
@@ -235,6 +237,43 @@ void ref_set_objective(void* h, double alpha_mag, double ref_weight, const doubl
     c->refWeight = ref_weight;
     if (ref_params) c->refParams = toVec(static_cast<int>(c->model->totalDofCount()), ref_params);
     c->built = false;
+}
+
+// LithologyModel::setLabelGrid / setBottomDepth / classifyPoint
+// (lithology_model.cpp:89-103, 856-858, 288-363) on the current positions.
+void ref_set_label_grid(void* h, int nx, int ny, int nz, double x0, double y0, double z0, double dx, double dy,
+                        double dz, const int32_t* labels) {
+    std::vector<int> lab(labels ? static_cast<size_t>(nx) * ny * nz : 0);
+    for (size_t i = 0; i < lab.size(); ++i) lab[i] = labels[i];
+    static_cast<RefCtx*>(h)->model->setLabelGrid(lab, nx, ny, nz, x0, y0, z0, dx, dy, dz);
+}
+void ref_set_bottom_depth(void* h, double depth) { static_cast<RefCtx*>(h)->model->setBottomDepth(depth); }
+void ref_classify(void* h, int n, const double* xyz, int32_t* out) {
+    auto* c = static_cast<RefCtx*>(h);
+    for (int i = 0; i < n; ++i) out[i] = c->model->classifyPoint(Vector3d(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]));
+}
+
+// ConstraintHandler (constraint_handler.cpp:7-66).
+void ref_set_constraints(void* h, int n, const double* xy, const double* z_top, const double* z_bottom,
+                         const int32_t* group, double weight) {
+    auto* c = static_cast<RefCtx*>(h);
+    std::vector<Constraint> cs(n);
+    for (int k = 0; k < n; ++k) {
+        cs[k].position = Vector3d(xy[2 * k], xy[2 * k + 1], 0.0);
+        cs[k].z_top = z_top[k];
+        cs[k].z_bottom = z_bottom[k];
+        cs[k].litho_group_id = group[k];
+    }
+    c->cons = std::make_shared<ConstraintHandler>(c->model, cs);
+    c->cons->setWeight(weight);
+}
+double ref_constraint_value(void* h, const double* params) {
+    auto* c = static_cast<RefCtx*>(h);
+    return c->cons->evaluate(toVec(static_cast<int>(c->model->totalDofCount()), params));
+}
+void ref_constraint_gradient(void* h, const double* params, double* grad) {
+    auto* c = static_cast<RefCtx*>(h);
+    fromVec(c->cons->gradient(toVec(static_cast<int>(c->model->totalDofCount()), params)), grad);
 }
 
 // JointObjective::calibrateDataWeights (joint_objective.cpp:281-393) at

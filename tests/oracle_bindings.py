@@ -117,6 +117,13 @@ def ref() -> C.CDLL:
             "ref_smoothness_gradient": (None, [V, _dp, _dp]),
             "ref_objective": (None, [V, _dp, _dp]), "ref_gradient": (None, [V, _dp, _dp]),
             "ref_lbfgsb": (C.c_int, [V, _dp, _dp, _dp, C.c_int, C.c_double, C.c_int, _dp, _dp]),
+            "ref_set_label_grid": (None, [V, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                          C.c_double, C.c_double, C.c_double, _ip]),
+            "ref_set_bottom_depth": (None, [V, C.c_double]),
+            "ref_classify": (None, [V, C.c_int, _dp, _ip]),
+            "ref_set_constraints": (None, [V, C.c_int, _dp, _dp, _dp, _ip, C.c_double]),
+            "ref_constraint_value": (C.c_double, [V, _dp]),
+            "ref_constraint_gradient": (None, [V, _dp, _dp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -220,6 +227,36 @@ class RefModel:
         v = self.lib.ref_smoothness_value(self.h, _d(params))
         self.lib.ref_smoothness_gradient(self.h, _d(params), g.ctypes.data_as(_dp))
         return v, g
+
+    def set_label_grid(self, labels, origin, spacing):
+        lab = np.ascontiguousarray(labels, np.int32)
+        nz, ny, nx = lab.shape
+        self.lib.ref_set_label_grid(self.h, nx, ny, nz, *map(float, origin), *map(float, spacing),
+                                    lab.ctypes.data_as(_ip))
+
+    def set_bottom_depth(self, depth):
+        self.lib.ref_set_bottom_depth(self.h, float(depth))
+
+    def classify(self, xyz):
+        """classifyPoint for each row of xyz at the current positions."""
+        x = np.ascontiguousarray(xyz, np.float64).reshape(-1, 3)
+        out = np.zeros(len(x), np.int32)
+        self.lib.ref_classify(self.h, len(x), _d(x), out.ctypes.data_as(_ip))
+        return out
+
+    def set_constraints(self, xy, z_top, z_bottom, group, weight=1e6):
+        xy = np.ascontiguousarray(xy, np.float64).reshape(-1, 2)
+        zt, zb = np.ascontiguousarray(z_top, np.float64), np.ascontiguousarray(z_bottom, np.float64)
+        g = np.ascontiguousarray(group, np.int32)
+        self.lib.ref_set_constraints(self.h, len(xy), _d(xy), _d(zt), _d(zb), g.ctypes.data_as(_ip), float(weight))
+
+    def constraint_value(self, params):
+        return self.lib.ref_constraint_value(self.h, _d(params))
+
+    def constraint_gradient(self, params):
+        g = np.zeros(self.np)
+        self.lib.ref_constraint_gradient(self.h, _d(params), g.ctypes.data_as(_dp))
+        return g
 
     def unit_response(self, params, kind, group, direction=None):
         out = np.zeros(self.Sg if kind == 0 else self.Sm)
