@@ -313,6 +313,33 @@ enum { LF_UNIT_GRAVITY = 0, LF_UNIT_INDUCED = 1, LF_UNIT_DIRECTION = 2, LF_UNIT_
 lf_status lf_unit_response(lf_ctx* ctx, const double* params, int kind, int group, const double* dir,
                            double* out);
 
+/* Property step of the alternating inversion (InversionRunner::
+ * runPropertyInversion, modules/litho-inversion/src/inversion/
+ * runner.cpp:708-917, parts A and B): at the geometry `params`, the
+ * per-group unit responses (one lf_unit_response column each) form U, and
+ * the small bounded least-squares problem
+ *   min_d 0.5 sum_i (w_i (obs_i - (U d)_i))^2 / rms^2 + 0.5 damping |d - d0|^2,
+ *   rms = sqrt(max(mean(obs^2), 1)),
+ * is solved on the host by the projected L-BFGS of lf_lbfgsb_minimize
+ * (history min(5, n), the given iteration limit and tolerance).  Part A:
+ * densities from the gravity data; part B (when magnetic data are set):
+ * per group chi, plus the remanence magnitude (LF_REM_FIXED_VECTOR) or the
+ * remanence vector (LF_REM_VECTOR), bounds as the runner's options.  The
+ * results are written back into the context's groups (as the reference
+ * writes them into its model) and returned: density[G], magnetic[p G] with
+ * p = 1, 2 or 4 parameters per group (NULL to skip). */
+typedef struct {
+    double density_min, density_max;                            /* propertyDensityMin / Max */
+    double susceptibility_min, susceptibility_max;              /* propertySusceptibilityMin / Max */
+    double remanence_min, remanence_max;                        /* propertyRemanenceMin / Max */
+    double remanence_component_min, remanence_component_max;    /* propertyRemanenceComponentMin / Max */
+    double damping;                                             /* propertyDamping */
+    int max_iterations;                                         /* propertyInversionMaxIter */
+    double tolerance;                                           /* tolerance */
+} lf_property_options;
+lf_status lf_property_inversion(lf_ctx* ctx, const double* params, const lf_property_options* opt, double* density,
+                                double* magnetic);
+
 /* Dense Jacobian J[n_data x n_dofs] (row-major) of gravity (which = LF_GRAVITY)
  * or TMI (LF_MAGNETIC) at params, with the reference's DOF gather semantics:
  * each DOF collects its control-point vertices' own derivative times the axis

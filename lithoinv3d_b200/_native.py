@@ -32,6 +32,13 @@ class Tuning(C.Structure):
     _fields_ = [("fwd_target_blocks", C.c_int), ("grad_target_warps", C.c_int), ("near_tiles_per_chunk", C.c_int)]
 
 
+class PropertyOptions(C.Structure):
+    _fields_ = [(n, C.c_double) for n in (
+        "density_min", "density_max", "susceptibility_min", "susceptibility_max", "remanence_min",
+        "remanence_max", "remanence_component_min", "remanence_component_max", "damping")] + [
+        ("max_iterations", C.c_int), ("tolerance", C.c_double)]
+
+
 class Counters(C.Structure):
     _fields_ = [("forward_pairs", C.c_uint64), ("gradient_pairs", C.c_uint64), ("launches", C.c_uint64)]
 
@@ -104,6 +111,7 @@ SIGNATURES = {
     "lf_forward_noalloc": (C.c_int, [C.c_int, _vp, C.c_int, _vp, C.c_int, _vp, C.c_double, C.c_double, C.c_double,
                                      C.c_double, C.c_double, _vp, _vp, _vp]),
     "lf_get_kernel_times": (C.c_int, [_vp, _dp, C.POINTER(C.c_int), _dp, C.POINTER(C.c_int)]),
+    "lf_property_inversion": (C.c_int, [_vp, _dp, C.c_void_p, _dp, _dp]),
     "lf_set_label_grid": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                     C.c_double, C.c_double, _ip]),
     "lf_set_bottom_depth": (C.c_int, [_vp, C.c_double]),

@@ -176,6 +176,7 @@ class Context:
             raise LithoError(st, "lf_create (a CUDA device is required)")
         self.h = h
         self.n_dofs = 0
+        self.n_groups = 0
         self.n_grav = 0
         self.n_mag = 0
 
@@ -199,6 +200,7 @@ class Context:
     def set_model(self, model: Model) -> None:
         self._check(self.lib.lf_set_model(self.h, model.h), "set_model")
         self.n_dofs = model.n_dofs
+        self.n_groups = model.info().n_groups
 
     def set_field(self, inclination: float, declination: float, field_nt: float, remanence_mode: int = 0):
         self._check(self.lib.lf_set_field(self.h, inclination, declination, field_nt, remanence_mode), "set_field")
@@ -264,6 +266,20 @@ class Context:
         self._check(self.lib.lf_calibrate_data_weights(self.h, _d(f64(params)), seed, _d(a), _d(eg), _d(em)),
                     "calibrate_data_weights")
         return float(a[0]), float(eg[0]), float(em[0])
+
+    def property_inversion(self, params, density_range=(-1.0, 1.0), susceptibility_range=(0.0, 1.0),
+                           remanence_range=(0.0, 100.0), remanence_component_range=(-100.0, 100.0),
+                           damping=0.0, max_iterations=50, tolerance=1e-6, magnetic_per_group=1):
+        """lf_property_inversion: returns (densities[G], magnetic[p G] or None);
+        the context's group properties are updated as the reference updates
+        its model."""
+        o = _native.PropertyOptions(*density_range, *susceptibility_range, *remanence_range,
+                                    *remanence_component_range, float(damping), int(max_iterations), float(tolerance))
+        dens = np.zeros(self.n_groups)
+        mag = np.zeros(magnetic_per_group * self.n_groups)
+        self._check(self.lib.lf_property_inversion(self.h, _d(f64(params)), C.byref(o), _d(dens), _d(mag)),
+                    "property_inversion")
+        return dens, (mag if self.n_mag else None)
 
     # ---- point classification and borehole constraints ----
     def set_label_grid(self, labels, origin, spacing):

@@ -1826,6 +1826,126 @@ extern "C" lf_status lf_unit_response(lf_ctx* c, const double* params, int kind,
     return LF_OK;
 }
 
+// One bounded least-squares property problem of runPropertyInversion
+// (runner.cpp:737-786 / 866-913): U column-major [n x m], the reference's
+// summation orders (U d by columns, U^T r by rows, squared norms in index
+// order).
+static std::vector<double> property_solve(const std::vector<double>& U, int n, int m, const std::vector<double>& obs,
+                                          const std::vector<double>& w, const std::vector<double>& x0,
+                                          const std::vector<double>& lo, const std::vector<double>& hi,
+                                          const lf_property_options& o) {
+    double var = 0.0;
+    for (int i = 0; i < n; ++i) var += obs[i] * obs[i];
+    var /= static_cast<double>(n);
+    const double rms = std::sqrt(std::max(var, 1.0));
+    const double lambda = o.damping;
+    auto predict = [&](const std::vector<double>& d) {
+        std::vector<double> y(n, 0.0);
+        for (int j = 0; j < m; ++j)
+            for (int i = 0; i < n; ++i) y[i] += U[(size_t)j * n + i] * d[j];
+        return y;
+    };
+    Objective f = [&](const std::vector<double>& d) {
+        const std::vector<double> pred = predict(d);
+        double misfit = 0.0;
+        for (int i = 0; i < n; ++i) {
+            const double res = w[i] * (obs[i] - pred[i]);
+            misfit += 0.5 * res * res;
+        }
+        misfit /= rms * rms;
+        if (lambda > 0.0) {
+            double sq = 0.0;
+            for (int j = 0; j < m; ++j) sq += (d[j] - x0[j]) * (d[j] - x0[j]);
+            misfit += 0.5 * lambda * sq;
+        }
+        return misfit;
+    };
+    Gradient g = [&](const std::vector<double>& d) {
+        const std::vector<double> pred = predict(d);
+        const double inv2 = 1.0 / (rms * rms);
+        std::vector<double> wr(n), grad(m);
+        for (int i = 0; i < n; ++i) wr[i] = inv2 * w[i] * w[i] * (obs[i] - pred[i]);
+        for (int j = 0; j < m; ++j) {
+            double acc = 0.0;
+            for (int i = 0; i < n; ++i) acc += (-1.0 * U[(size_t)j * n + i]) * wr[i];
+            grad[j] = acc;
+        }
+        if (lambda > 0.0)
+            for (int j = 0; j < m; ++j) grad[j] = grad[j] + lambda * (d[j] - x0[j]);
+        return grad;
+    };
+    LbfgsbOptions lo_opt;
+    lo_opt.maxIterations = o.max_iterations;
+    lo_opt.historySize = std::min(5, m);
+    lo_opt.tolerance = o.tolerance;
+    LbfgsbOptimizer opt(lo_opt);
+    return opt.minimize(f, g, x0, lo, hi).params;
+}
+
+extern "C" lf_status lf_property_inversion(lf_ctx* c, const double* params, const lf_property_options* o,
+                                           double* density, double* magnetic) {
+    LF_RET_IF(check_ready(c));
+    if (!o || o->max_iterations < 0 || !std::isfinite(o->damping) || !std::isfinite(o->tolerance))
+        return fail(c, LF_EINVAL, "lf_property_inversion: bad options");
+    if (c->partitioned) return fail(c, LF_ESTATE, "property inversion is not available for batched bodies");
+    const int G = c->G;
+    // Part A: densities from the gravity data (runner.cpp:716-798)
+    if (c->grav.n > 0) {
+        const int n = c->grav.n;
+        std::vector<double> U((size_t)n * G), x0(G), lo(G, o->density_min), hi(G, o->density_max);
+        for (int g = 0; g < G; ++g) {
+            LF_RET_IF(lf_unit_response(c, params, LF_UNIT_GRAVITY, g, nullptr, U.data() + (size_t)g * n));
+            x0[g] = c->groups[g].density;
+        }
+        const std::vector<double> d = property_solve(U, n, G, c->grav.obs, c->grav.w, x0, lo, hi, *o);
+        for (int g = 0; g < G; ++g) c->groups[g].density = d[g];
+    }
+    // Part B: susceptibility (+ remanence) from the magnetic data (runner.cpp:803-917)
+    const int ppg = c->remMode == LF_REM_FIXED_VECTOR ? 2 : (c->remMode == LF_REM_VECTOR ? 4 : 1);
+    if (c->mag.n > 0) {
+        const int n = c->mag.n, m = ppg * G;
+        std::vector<double> U((size_t)n * m), x0(m), lo(m), hi(m);
+        const double ex[3][3] = {{1.0, 0.0, 0.0}, {0.0, 1.0, 0.0}, {0.0, 0.0, 1.0}};
+        for (int g = 0; g < G; ++g) {
+            const int col = ppg * g;
+            LF_RET_IF(lf_unit_response(c, params, LF_UNIT_INDUCED, g, nullptr, U.data() + (size_t)col * n));
+            x0[col] = c->groups[g].chi;
+            lo[col] = o->susceptibility_min;
+            hi[col] = o->susceptibility_max;
+            if (ppg == 2) {
+                LF_RET_IF(lf_unit_response(c, params, LF_UNIT_REMANENCE, g, nullptr, U.data() + (size_t)(col + 1) * n));
+                x0[col + 1] = c->groups[g].remMag;
+                lo[col + 1] = o->remanence_min;
+                hi[col + 1] = o->remanence_max;
+            } else if (ppg == 4) {
+                for (int k = 0; k < 3; ++k) {
+                    LF_RET_IF(lf_unit_response(c, params, LF_UNIT_DIRECTION, g, ex[k],
+                                               U.data() + (size_t)(col + 1 + k) * n));
+                    x0[col + 1 + k] = c->groups[g].remVec[k];
+                    lo[col + 1 + k] = o->remanence_component_min;
+                    hi[col + 1 + k] = o->remanence_component_max;
+                }
+            }
+        }
+        const std::vector<double> d = property_solve(U, n, m, c->mag.obs, c->mag.w, x0, lo, hi, *o);
+        for (int g = 0; g < G; ++g) {
+            const int col = ppg * g;
+            c->groups[g].chi = d[col];
+            if (ppg == 2) c->groups[g].remMag = d[col + 1];
+            if (ppg == 4)
+                for (int k = 0; k < 3; ++k) c->groups[g].remVec[k] = d[col + 1 + k];
+        }
+        if (magnetic)
+            for (int j = 0; j < m; ++j) magnetic[j] = d[j];
+    }
+    if (density)
+        for (int g = 0; g < G; ++g) density[g] = c->groups[g].density;
+    c->epoch++;
+    LF_RET_IF(upload_groups(c));
+    LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
+    return LF_OK;
+}
+
 extern "C" lf_status lf_jacobian(lf_ctx* c, const double* params, int which, double* J) {
     LF_RET_IF(check_ready(c));
     if (!J || (which != LF_GRAVITY && which != LF_MAGNETIC)) return LF_EINVAL;

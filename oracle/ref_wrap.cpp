@@ -337,6 +337,116 @@ void ref_unit_response(void* h, const double* params, int kind, int group, const
     fromVec(r, out);
 }
 
+// InversionRunner::runPropertyInversion parts A and B (runner.cpp:708-917),
+// restated with the reference's own classes (GravityForward /
+// MagneticForward unit responses, LBFGSBOptimizer): runner.cpp itself needs
+// the IO and EM modules and is not compiled here.  opt = {density min, max,
+// chi min, max, remanence min, max, remanence component min, max, damping,
+// tolerance}.  Returns the new properties and writes them into the groups.
+void ref_property_inversion(void* h, const double* params, const double* opt, int max_iter, double* density,
+                            double* magnetic) {
+    auto* c = static_cast<RefCtx*>(h);
+    c->ensure();
+    c->model->applyParameterVector(toVec(static_cast<int>(c->gf->parameterCount()), params));
+    const int nGroups = c->model->groupCount();
+    const double lambda = opt[8], tol = opt[9];
+    auto solve = [&](const MatrixXd& U, const std::vector<double>& obsv, const std::vector<double>& sdv,
+                     VectorXd x0, const VectorXd& lo, const VectorXd& hi) {
+        const size_t n = obsv.size();
+        double var = 0.0;
+        for (size_t i = 0; i < n; ++i) var += obsv[i] * obsv[i];
+        var /= static_cast<double>(n);
+        const double rms = std::sqrt(std::max(var, 1.0));
+        const VectorXd ref = x0;
+        auto obj = [&](const VectorXd& d) -> double {
+            VectorXd pred = U * d;
+            double misfit = 0.0;
+            for (size_t i = 0; i < n; ++i) {
+                double w = (sdv[i] > 0) ? (1.0 / sdv[i]) : 1.0;
+                double res = w * (obsv[i] - pred[static_cast<Index>(i)]);
+                misfit += 0.5 * res * res;
+            }
+            misfit /= rms * rms;
+            if (lambda > 0.0) {
+                VectorXd diff = d - ref;
+                misfit += 0.5 * lambda * diff.squaredNorm();
+            }
+            return misfit;
+        };
+        auto grad = [&](const VectorXd& d) -> VectorXd {
+            VectorXd pred = U * d;
+            VectorXd Wr(static_cast<Index>(n));
+            double invScale2 = 1.0 / (rms * rms);
+            for (size_t i = 0; i < n; ++i) {
+                double w = (sdv[i] > 0) ? (1.0 / sdv[i]) : 1.0;
+                Wr[static_cast<Index>(i)] = invScale2 * w * w * (obsv[i] - pred[static_cast<Index>(i)]);
+            }
+            VectorXd g = -U.transpose() * Wr;
+            if (lambda > 0.0) g += lambda * (d - ref);
+            return g;
+        };
+        LBFGSBOptimizer o;
+        o.setMaxIterations(max_iter);
+        o.setHistorySize(std::min(5, static_cast<int>(x0.size())));
+        o.setTolerance(tol);
+        return o.minimize(obj, grad, x0, lo, hi).params;
+    };
+    {  // part A
+        const size_t n = c->grav.size();
+        MatrixXd U(static_cast<Index>(n), nGroups);
+        VectorXd x0(nGroups), lo(nGroups), hi(nGroups);
+        std::vector<double> obsv(n), sdv(n);
+        for (size_t i = 0; i < n; ++i) { obsv[i] = c->grav[i].g_obs; sdv[i] = c->grav[i].g_std; }
+        for (int g = 0; g < nGroups; ++g) {
+            U.col(g) = c->gf->computeGroupUnitResponse(g);
+            x0[g] = c->model->group(g).density;
+            lo[g] = opt[0];
+            hi[g] = opt[1];
+        }
+        VectorXd d = solve(U, obsv, sdv, x0, lo, hi);
+        for (int g = 0; g < nGroups; ++g) c->model->group(g).density = d[g];
+    }
+    if (!c->mag.empty()) {  // part B
+        const int ppg = c->remMode == 1 ? 2 : (c->remMode == 2 ? 4 : 1);
+        const size_t n = c->mag.size();
+        const int m = ppg * nGroups;
+        MatrixXd U(static_cast<Index>(n), m);
+        VectorXd x0(m), lo(m), hi(m);
+        std::vector<double> obsv(n), sdv(n);
+        for (size_t i = 0; i < n; ++i) { obsv[i] = c->mag[i].t_obs; sdv[i] = c->mag[i].t_std; }
+        for (int g = 0; g < nGroups; ++g) {
+            const int col = ppg * g;
+            U.col(col) = c->mf->computeGroupUnitResponse(g);
+            x0[col] = c->model->group(g).susceptibility;
+            lo[col] = opt[2];
+            hi[col] = opt[3];
+            if (ppg == 2) {
+                U.col(col + 1) = c->mf->computeGroupUnitRemanenceResponse(g);
+                x0[col + 1] = c->model->group(g).remanence_magnitude;
+                lo[col + 1] = opt[4];
+                hi[col + 1] = opt[5];
+            } else if (ppg == 4) {
+                const Vector3d e[3] = {Vector3d(1.0, 0.0, 0.0), Vector3d(0.0, 1.0, 0.0), Vector3d(0.0, 0.0, 1.0)};
+                for (int k = 0; k < 3; ++k) {
+                    U.col(col + 1 + k) = c->mf->computeGroupUnitResponseDirection(g, e[k]);
+                    x0[col + 1 + k] = c->model->group(g).magnetization[k];
+                    lo[col + 1 + k] = opt[6];
+                    hi[col + 1 + k] = opt[7];
+                }
+            }
+        }
+        VectorXd d = solve(U, obsv, sdv, x0, lo, hi);
+        for (int j = 0; j < m; ++j) magnetic[j] = d[j];
+        for (int g = 0; g < nGroups; ++g) {
+            const int col = ppg * g;
+            c->model->group(g).susceptibility = d[col];
+            if (ppg == 2) c->model->group(g).remanence_magnitude = d[col + 1];
+            if (ppg == 4) c->model->group(g).magnetization = Vector3d(d[col + 1], d[col + 2], d[col + 3]);
+        }
+    }
+    for (int g = 0; g < nGroups; ++g) density[g] = c->model->group(g).density;
+}
+
 void ref_jacobian_gz(void* h, const double* params, double* J) {
     auto* c = static_cast<RefCtx*>(h);
     c->ensure();

@@ -117,6 +117,7 @@ def ref() -> C.CDLL:
             "ref_smoothness_gradient": (None, [V, _dp, _dp]),
             "ref_objective": (None, [V, _dp, _dp]), "ref_gradient": (None, [V, _dp, _dp]),
             "ref_lbfgsb": (C.c_int, [V, _dp, _dp, _dp, C.c_int, C.c_double, C.c_int, _dp, _dp]),
+            "ref_property_inversion": (None, [V, _dp, _dp, C.c_int, _dp, _dp]),
             "ref_set_label_grid": (None, [V, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                           C.c_double, C.c_double, C.c_double, _ip]),
             "ref_set_bottom_depth": (None, [V, C.c_double]),
@@ -227,6 +228,16 @@ class RefModel:
         v = self.lib.ref_smoothness_value(self.h, _d(params))
         self.lib.ref_smoothness_gradient(self.h, _d(params), g.ctypes.data_as(_dp))
         return v, g
+
+    def property_inversion(self, params, opt, max_iter, n_groups, magnetic_per_group):
+        """runPropertyInversion parts A and B (restated with the reference's
+        classes): (densities, magnetic parameters)."""
+        o = np.ascontiguousarray(opt, np.float64)
+        dens = np.zeros(n_groups)
+        mag = np.zeros(magnetic_per_group * n_groups)
+        self.lib.ref_property_inversion(self.h, _d(params), _d(o), int(max_iter), dens.ctypes.data_as(_dp),
+                                        mag.ctypes.data_as(_dp))
+        return dens, mag
 
     def set_label_grid(self, labels, origin, spacing):
         lab = np.ascontiguousarray(labels, np.int32)
