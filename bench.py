@@ -106,6 +106,8 @@ def parse():
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-stations", type=int, default=48)
+    ap.add_argument("--bodies", type=int, default=256,
+                    help="number of bodies of the batch workload (256 is the configuration; fewer for profiling)")
     ap.add_argument("--workload", choices=["contact", "batch", "large", "constraints"], default="contact",
                     help="contact: the 4-group contact model (headline); batch: 256 batched bodies; "
                          "large: the 194k-facet single inversion")
@@ -114,11 +116,11 @@ def parse():
     return ap.parse_args()
 
 
-def make_problem(workload: str = "contact"):
+def make_problem(workload: str = "contact", bodies: int = 256):
     from lithoinv3d_b200 import synth
 
     if workload == "batch":
-        p = synth.batch_bodies_model()
+        p = synth.batch_bodies_model(n_bodies=bodies)
     elif workload == "large":
         p = synth.large_model()
     else:
@@ -419,7 +421,7 @@ def main():
 
     from lithoinv3d_b200 import PREC_FP64, PREC_MIXED
 
-    p, model = make_problem(args.workload)
+    p, model = make_problem(args.workload, args.bodies)
     x0, gobs, gstd, mobs, mstd = synthetic_data(p, model)
     ctx = p.make_context(model, device=local, grav_obs=gobs, grav_std=gstd, mag_obs=mobs, mag_std=mstd)
     ctx.set_precision(PREC_MIXED if args.precision == "mixed" else PREC_FP64)
@@ -541,7 +543,8 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
             "data": "synthetic (seeded voxel model and observations)",
-            "config": {"workload": {"batch": WORKLOAD_BATCH, "large": WORKLOAD_LARGE}.get(args.workload, WORKLOAD),
+            "config": {"workload": {"batch": WORKLOAD_BATCH.replace("256", str(args.bodies)),
+                                    "large": WORKLOAD_LARGE}.get(args.workload, WORKLOAD),
                        "triangles": p.n_triangles(), "stations": len(p.grav_xyz),
                        "dofs": np_, "parallelism": f"replicas x{world}", "l2": "flushed between steps (256 MiB write)",
                        "precision": args.precision, "fp64_near_pair_fraction": round(near_frac, 4),

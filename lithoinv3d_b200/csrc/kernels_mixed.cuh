@@ -492,7 +492,10 @@ constexpr int kFarFlushTiles = 4;  // far tiles summed per lane in FP32 between 
 // k_gradient_warp_fp64; part layout [chunk][9][T].
 // Sums: 0 Q0; 1-3, 4-6, 7-9 sum_q beta_q{a,b,c} D_q; 10-12, 13-15, 16-18 TMI
 // vertex terms of a, b, c; 19 sum Ts Omega; 20-22 sum Ts Lambda_i.
-__global__ void __launch_bounds__(128) k_gradient_warp_far32(int T, const double* __restrict__ gc, int S,
+// Four CTAs per SM (at most 128 registers, a few bytes of spill) ran faster
+// than the unconstrained 147-register, three-CTA build on every workload
+// measured (contact model -1 %, large model -3 %, 256-body batch -7 %).
+__global__ void __launch_bounds__(128, 4) k_gradient_warp_far32(int T, const double* __restrict__ gc, int S,
                                                              const double* __restrict__ sta,
                                                              const double* __restrict__ gcoef,
                                                              const double* __restrict__ mcoef,
