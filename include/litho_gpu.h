@@ -252,6 +252,24 @@ lf_status lf_mlp_param_count(lf_mlp* m, size_t* n);
 lf_status lf_mlp_get_params(lf_mlp* m, float* host);
 lf_status lf_mlp_set_params(lf_mlp* m, const float* host);
 lf_status lf_mlp_gradients(lf_mlp* m, const float* d_x, const float* d_y, float* loss, float* host_grads);
+/* GEMM engine of the network: LF_GEMM_MMA_SYNC (default: warp-level
+ * mma.sync m16n8k16 with ldmatrix, cp.async double buffering) or
+ * LF_GEMM_TCGEN05 (5th-generation tensor cores: tcgen05.mma from shared-memory
+ * descriptors, accumulator in tensor memory, 128 x 256 or 128 x 128 tiles).
+ * Both give the same results to FP32 summation order; at the network's
+ * shapes the mma.sync kernel is the faster of the two. */
+enum { LF_GEMM_TCGEN05 = 0, LF_GEMM_MMA_SYNC = 1 };
+lf_status lf_mlp_set_engine(lf_mlp* m, int engine);
+/* The network's BF16 GEMM on device buffers: C[M x N] = A[M x K] . B[K x N]
+ * with A stored [M][K] (a_trans = 0) or [K][M] (a_trans = 1), B stored
+ * [K][N] (b_trans = 0) or [N][K] (b_trans = 1), row lengths lda / ldb / ldc
+ * (multiples of 8 elements, operands 16-byte aligned), FP32 accumulation;
+ * epilogue 0: C fp32, 1: bf16 relu(C + bias[n]), 2: fp32 C + bias[n],
+ * 3: bf16 C.  M and N multiples of 128, K of 64 (tcgen05) or 32 (mma.sync).
+ * Runs on `stream` (NULL = default stream) and synchronises it; returns
+ * LF_ETIMEOUT if a tensor-core mbarrier wait expired. */
+lf_status lf_gemm_bf16(int engine, int a_trans, int b_trans, int epilogue, int M, int N, int K, const void* A,
+                       int lda, const void* B, int ldb, const float* bias, void* C, int ldc, void* stream);
 
 /* Stateless parameter scatter (off by default).  The reference's
  * applyParameterVector averages shared vertices from their current positions

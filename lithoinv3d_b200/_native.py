@@ -111,6 +111,9 @@ SIGNATURES = {
     "lf_forward_noalloc": (C.c_int, [C.c_int, _vp, C.c_int, _vp, C.c_int, _vp, C.c_double, C.c_double, C.c_double,
                                      C.c_double, C.c_double, _vp, _vp, _vp]),
     "lf_get_kernel_times": (C.c_int, [_vp, _dp, C.POINTER(C.c_int), _dp, C.POINTER(C.c_int)]),
+    "lf_mlp_set_engine": (C.c_int, [_vp, C.c_int]),
+    "lf_gemm_bf16": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _vp, C.c_int, _vp,
+                               C.c_int, _vp, _vp, C.c_int, _vp]),
     "lf_property_inversion": (C.c_int, [_vp, _dp, C.c_void_p, _dp, _dp]),
     "lf_set_label_grid": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                     C.c_double, C.c_double, _ip]),

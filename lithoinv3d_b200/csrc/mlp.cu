@@ -9,6 +9,7 @@
 // zero targets and are masked out of the loss.
 #include "../../include/litho_gpu.h"
 #include "mlp_kernels.cuh"
+#include "tc_gemm.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -68,6 +69,7 @@ struct lf_mlp {
     Buf<__nv_bfloat16> xb, dz, dh;  // input, gradient buffers (bf16)
     Buf<float> pred, loss_blocks;
     int step = 0;
+    int engine = LF_GEMM_MMA_SYNC;  // lf_mlp_set_engine (mma.sync measured faster at the network's shapes)
     std::string err;
 };
 
@@ -89,11 +91,58 @@ static lf_status mlp_check_launch(lf_mlp* m) {
     return LF_OK;
 }
 
+// One GEMM on `stream`: the tcgen05 kernel (K a multiple of 64; 128 x 256
+// tiles when N allows, else 128 x 128) or the warp-level mma.sync kernel
+// (K a multiple of 32).
+template <bool A_T, bool B_T, int EPI, int BN>
+static cudaError_t gemm_tc(cudaStream_t stream, int M, int N, int K, const __nv_bfloat16* A, int lda,
+                           const __nv_bfloat16* B, int ldb, const float* bias, float* Cf, __nv_bfloat16* Cb, int ldc) {
+    static bool attr = false;  // per instantiation, per process (the attribute is per function)
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(k_gemm_tc<A_T, B_T, EPI, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             TcShape<BN>::kSmem);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    dim3 grid(N / BN, M / kBM);
+    k_gemm_tc<A_T, B_T, EPI, BN><<<grid, kTcThreads, TcShape<BN>::kSmem, stream>>>(M, N, K, A, lda, B, ldb, bias, Cf,
+                                                                                  Cb, ldc);
+    return cudaPeekAtLastError();  // left for the caller's launch check
+}
+
+template <bool A_T, bool B_T, int EPI>
+static cudaError_t gemm_on(int engine, cudaStream_t stream, int M, int N, int K, const __nv_bfloat16* A, int lda,
+                           const __nv_bfloat16* B, int ldb, const float* bias, float* Cf, __nv_bfloat16* Cb, int ldc) {
+    if (engine == LF_GEMM_TCGEN05) {
+        if (N % 256 == 0)
+            return gemm_tc<A_T, B_T, EPI, 256>(stream, M, N, K, A, lda, B, ldb, bias, Cf, Cb, ldc);
+        return gemm_tc<A_T, B_T, EPI, 128>(stream, M, N, K, A, lda, B, ldb, bias, Cf, Cb, ldc);
+    }
+    dim3 grid(N / kBN, M / kBM);
+    k_gemm_bf16<A_T, B_T, EPI><<<grid, kGemmThreads, 0, stream>>>(M, N, K, A, lda, B, ldb, bias, Cf, Cb, ldc);
+    return cudaPeekAtLastError();  // left for the caller's launch check
+}
+
 template <bool A_T, bool B_T, int EPI>
 static void gemm(lf_mlp* m, int M, int N, int K, const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int ldb,
                  const float* bias, float* Cf, __nv_bfloat16* Cb, int ldc) {
-    dim3 grid(N / kBN, M / kBM);
-    k_gemm_bf16<A_T, B_T, EPI><<<grid, kGemmThreads, 0, m->stream>>>(M, N, K, A, lda, B, ldb, bias, Cf, Cb, ldc);
+    cudaError_t e = gemm_on<A_T, B_T, EPI>(m->engine, m->stream, M, N, K, A, lda, B, ldb, bias, Cf, Cb, ldc);
+    if (e != cudaSuccess && m->err.empty()) m->err = std::string("gemm launch: ") + cudaGetErrorString(e);
+}
+
+// Reads and clears the tensor-core GEMM error flag (an mbarrier wait that
+// expired); synchronises the stream.
+static lf_status tc_check(lf_mlp* m) {
+    unsigned int flag = 0;
+    MLP_TRY(m, cudaMemcpyFromSymbolAsync(&flag, g_tc_gemm_error, sizeof(flag), 0, cudaMemcpyDeviceToHost, m->stream));
+    MLP_TRY(m, cudaStreamSynchronize(m->stream));
+    if (flag) {
+        const unsigned int zero = 0;
+        MLP_TRY(m, cudaMemcpyToSymbol(g_tc_gemm_error, &zero, sizeof(zero)));
+        m->err = "tensor-core GEMM: an mbarrier wait expired";
+        return LF_ETIMEOUT;
+    }
+    return LF_OK;
 }
 
 extern "C" lf_status lf_mlp_create(int device, int n_in, int width, int depth, int n_out, int batch, unsigned seed,
@@ -258,7 +307,9 @@ extern "C" lf_status lf_mlp_train_step(lf_mlp* m, const float* d_x, const float*
         k_adam<<<cdiv_i(L.out, 256), 256, 0, m->stream>>>(L.out, L.b.p, L.gb.p, L.mb.p, L.vb.p, lr, b1, b2, eps, c1, c2,
                                                            nullptr);
     }
-    return mlp_check_launch(m);
+    st = mlp_check_launch(m);
+    if (st == LF_OK && m->engine == LF_GEMM_TCGEN05) st = tc_check(m);
+    return st;
 }
 
 extern "C" lf_status lf_mlp_predict(lf_mlp* m, const float* d_x, int rows, float* d_y) {
@@ -274,7 +325,7 @@ extern "C" lf_status lf_mlp_predict(lf_mlp* m, const float* d_x, int rows, float
                                      cudaMemcpyDeviceToDevice, m->stream));
     }
     MLP_TRY(m, cudaStreamSynchronize(m->stream));
-    return LF_OK;
+    return m->engine == LF_GEMM_TCGEN05 ? tc_check(m) : LF_OK;
 }
 
 // Parameters in the unpadded order: for each layer W [out][in] then b [out].
@@ -351,6 +402,60 @@ extern "C" lf_status lf_mlp_gradients(lf_mlp* m, const float* d_x, const float* 
     lf_status st = load_input(m, d_x, m->batch);
     if (st == LF_OK) st = forward(m);
     if (st == LF_OK) st = backward(m, d_y, loss);
+    if (st == LF_OK && m->engine == LF_GEMM_TCGEN05) st = tc_check(m);
     if (st == LF_OK && host_grads) st = copy_params(m, 1, host_grads);
     return st;
+}
+
+extern "C" lf_status lf_mlp_set_engine(lf_mlp* m, int engine) {
+    if (!m || (engine != LF_GEMM_TCGEN05 && engine != LF_GEMM_MMA_SYNC)) return LF_EINVAL;
+    m->engine = engine;
+    return LF_OK;
+}
+
+extern "C" lf_status lf_gemm_bf16(int engine, int a_trans, int b_trans, int epilogue, int M, int N, int K,
+                                  const void* A, int lda, const void* B, int ldb, const float* bias, void* C, int ldc,
+                                  void* stream) {
+    if ((engine != LF_GEMM_TCGEN05 && engine != LF_GEMM_MMA_SYNC) || M <= 0 || N <= 0 || K <= 0 || M % kBM ||
+        N % kBN || K % (engine == LF_GEMM_TCGEN05 ? kTcBK : kBK) || !A || !B || !C ||
+        (epilogue != EPI_F32 && epilogue != EPI_BF16 && epilogue != EPI_BIAS_RELU && epilogue != EPI_BIAS_F32) ||
+        ((epilogue == EPI_BIAS_RELU || epilogue == EPI_BIAS_F32) && !bias) || lda % 8 || ldb % 8 || ldc % 2 ||
+        (reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B)) % 16)
+        return LF_EINVAL;
+    // minimum row lengths of the stored operands
+    if (lda < (a_trans ? M : K) || ldb < (b_trans ? K : N) || ldc < N) return LF_EINVAL;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const auto* a = static_cast<const __nv_bfloat16*>(A);
+    const auto* b = static_cast<const __nv_bfloat16*>(B);
+    float* cf = static_cast<float*>(C);
+    __nv_bfloat16* cb = static_cast<__nv_bfloat16*>(C);
+    cudaError_t e = cudaSuccess;
+#define LF_GEMM_CASE(AT, BT)                                                                                          \
+    if (!!a_trans == AT && !!b_trans == BT) {                                                                        \
+        switch (epilogue) {                                                                                          \
+        case EPI_F32: e = gemm_on<AT, BT, EPI_F32>(engine, st, M, N, K, a, lda, b, ldb, bias, cf, nullptr, ldc); break; \
+        case EPI_BF16: e = gemm_on<AT, BT, EPI_BF16>(engine, st, M, N, K, a, lda, b, ldb, bias, nullptr, cb, ldc); break; \
+        case EPI_BIAS_RELU:                                                                                          \
+            e = gemm_on<AT, BT, EPI_BIAS_RELU>(engine, st, M, N, K, a, lda, b, ldb, bias, nullptr, cb, ldc);          \
+            break;                                                                                                   \
+        default: e = gemm_on<AT, BT, EPI_BIAS_F32>(engine, st, M, N, K, a, lda, b, ldb, bias, cf, nullptr, ldc); break; \
+        }                                                                                                            \
+    }
+    LF_GEMM_CASE(false, false)
+    LF_GEMM_CASE(false, true)
+    LF_GEMM_CASE(true, false)
+    LF_GEMM_CASE(true, true)
+#undef LF_GEMM_CASE
+    if (e != cudaSuccess) return LF_ECUDA;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return LF_ECUDA;
+    if (engine == LF_GEMM_TCGEN05) {
+        unsigned int flag = 0;
+        if (cudaMemcpyFromSymbol(&flag, g_tc_gemm_error, sizeof(flag)) != cudaSuccess) return LF_ECUDA;
+        if (flag) {
+            const unsigned int zero = 0;
+            cudaMemcpyToSymbol(g_tc_gemm_error, &zero, sizeof(zero));
+            return LF_ETIMEOUT;
+        }
+    }
+    return LF_OK;
 }

@@ -89,10 +89,12 @@ def rel(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
 
 
+@pytest.mark.parametrize("engine", [0, 1])  # LF_GEMM_TCGEN05, LF_GEMM_MMA_SYNC
 @pytest.mark.parametrize("n_in,width,depth,n_out", [(256, 128, 2, 70), (384, 256, 3, 200)])
-def test_mlp_gradients_match_cpu(n_in, width, depth, n_out):
+def test_mlp_gradients_match_cpu(n_in, width, depth, n_out, engine):
     batch = 128
     net = Net(n_in, width, depth, n_out, batch, seed=3)
+    assert net.lib.lf_mlp_set_engine(net.h, engine) == 0
     rng = np.random.default_rng(4)
     x = rng.normal(size=(batch, n_in)).astype(np.float32)
     y = rng.normal(size=(batch, n_out)).astype(np.float32)
