@@ -2297,7 +2297,12 @@ extern "C" lf_status lf_constraint_gradient(lf_ctx* c, const double* params, dou
         LF_CHECK_LAUNCH(c);
         return LF_OK;
     };
-    LF_RET_IF(run_cached(c, c->gCons, c->d_cPar0.p, c->d_cFp.p, c->d_cGrad.p, sweep, true));
+    // graph replay up to 4096 parameters (about 66k graph nodes); beyond that
+    // the capture itself would cost more than the launches it saves
+    if (c->np <= 4096)
+        LF_RET_IF(run_cached(c, c->gCons, c->d_cPar0.p, c->d_cFp.p, c->d_cGrad.p, sweep, true));
+    else
+        LF_RET_IF(sweep());
     LF_TRY_CUDA(c, cudaMemcpyAsync(grad, c->d_cGrad.p, sizeof(double) * c->np, cudaMemcpyDeviceToHost, c->stream));
     LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
     return LF_OK;
