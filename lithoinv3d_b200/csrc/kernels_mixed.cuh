@@ -471,13 +471,26 @@ __device__ __forceinline__ float warp_transpose_sum32(float (&v)[32]) {
     return v[0];
 }
 
+// Class of a (facet, tile) in the far-field gradient: 0 near (the FP64
+// kernel's), 1 far (6-point rule), 2 beyond 4 tau x size (3-point rule).
+// The near / far decision is tile_far's, operation for operation.
+__device__ __forceinline__ int tile_gradient_class(const FarKey& k, const double* __restrict__ bbox) {
+    if (k.th2 < 0.0) return 0;
+    const double d0 = fmax(0.0, fmax(__dadd_rn(bbox[0], -k.c0), __dadd_rn(k.c0, -bbox[3])));
+    const double d1 = fmax(0.0, fmax(__dadd_rn(bbox[1], -k.c1), __dadd_rn(k.c1, -bbox[4])));
+    const double d2 = fmax(0.0, fmax(__dadd_rn(bbox[2], -k.c2), __dadd_rn(k.c2, -bbox[5])));
+    const double dd = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2));
+    return dd >= __dmul_rn(16.0, k.th2) ? 2 : (dd >= k.th2 ? 1 : 0);
+}
+
 constexpr int kFarTerms = 23;      // far-field station sums per facet (listed below)
 constexpr int kFarFlushTiles = 4;  // far tiles summed per lane in FP32 between warp reductions
 
 // Far-field objective gradient in FP32: one warp per facet, lanes over the
 // stations of the facet's far tiles (exactly the tiles k_gradient_warp_fp64
 // leaves out: both classify with facet_far_key / tile_far).  gz by Dunavant's
-// 6-point rule.
+// 6-point rule, the 3-point rule beyond 4 tau x size (tile_gradient_class);
+// the point sums are flushed whenever the rule changes.
 //  * gz: I = A sum_q w_q / r_q, so
 //      sum_s G0 dI/dv = (dA/dv) Q0 - A sum_q beta_qv D_q,
 //    Q0 = sum_s G0 sum_q w_q / r_q, D_q = sum_s G0 w_q (p_q - o) / r_q^3
@@ -551,13 +564,16 @@ __global__ void __launch_bounds__(128, 4) k_gradient_warp_far32(int T, const dou
             float amf = 0.f, amt0 = 0.f, amt1 = 0.f, amt2 = 0.f;
 #pragma unroll
             for (int q = 0; q < 6; ++q) dqx[q] = dqy[q] = dqz[q] = 0.f;
-            int pending = 0;
+            int pending = 0, rule = 0;  // rule of the pending point sums: 0 six-point, 1 three-point
             auto flush = [&]() {
                 float v[32];
                 float sa0 = 0.f, sa1 = 0.f, sa2 = 0.f, sb0 = 0.f, sb1 = 0.f, sb2 = 0.f, sc0 = 0.f, sc1 = 0.f, sc2 = 0.f;
 #pragma unroll
                 for (int q = 0; q < 6; ++q) {
-                    const float bb = kDun6Bb[q], bc = kDun6Bc[q], ba = 1.f - bb - bc;
+                    // slots 0-2 hold the three-point rule's sums when rule == 1 (slots 3-5 are then zero)
+                    const float bb = rule ? (q < 3 ? kTri3Bb[q] : 0.f) : kDun6Bb[q];
+                    const float bc = rule ? (q < 3 ? kTri3Bc[q] : 0.f) : kDun6Bc[q];
+                    const float ba = 1.f - bb - bc;
                     sa0 = fmaf(ba, dqx[q], sa0); sa1 = fmaf(ba, dqy[q], sa1); sa2 = fmaf(ba, dqz[q], sa2);
                     sb0 = fmaf(bb, dqx[q], sb0); sb1 = fmaf(bb, dqy[q], sb1); sb2 = fmaf(bb, dqz[q], sb2);
                     sc0 = fmaf(bc, dqx[q], sc0); sc1 = fmaf(bc, dqy[q], sc1); sc2 = fmaf(bc, dqz[q], sc2);
@@ -581,12 +597,19 @@ __global__ void __launch_bounds__(128, 4) k_gradient_warp_far32(int T, const dou
             const FarKey key = facet_far_key(C, tau);
             for (int t0 = tbeg; t0 < ntiles; t0 += 32) {
                 const int t = t0 + lane;
-                const bool farT = t < ntiles && tile_far(key, tile_box + 6 * (size_t)t);
-                unsigned m = __ballot_sync(0xffffffffu, farT);
+                const int cls = t < ntiles ? tile_gradient_class(key, tile_box + 6 * (size_t)t) : 0;
+                unsigned m = __ballot_sync(0xffffffffu, cls != 0);
+                const unsigned mv = __ballot_sync(0xffffffffu, cls == 2);
                 any |= m != 0;
                 while (m) {
                     const int b = __ffs(m) - 1;
                     m &= m - 1;
+                    const int r = (mv >> b) & 1u;  // warp-uniform
+                    if (pending && r != rule) {  // the pending sums belong to the other rule
+                        flush();
+                        pending = 0;
+                    }
+                    rule = r;
                     const int s0 = (t0 + b) * kStationTile;
 #pragma unroll
                     for (int k = 0; k < kStationTile; k += 32) {
@@ -605,7 +628,22 @@ __global__ void __launch_bounds__(128, 4) k_gradient_warp_far32(int T, const dou
                         const float y = fmaf(dx, ry0, fmaf(dy, ry1, dzf * ry2));
                         const float z = (float)(ddx * zx + ddy * zy + ddz * zz);
                         const float z2 = z * z;
-                        if (G0 != 0.f) {
+                        if (G0 != 0.f && r) {  // beyond 4 tau: the 3-point rule, weights 1/3
+                            float sw = 0.f;
+#pragma unroll
+                            for (int q = 0; q < 3; ++q) {
+                                const float px = fmaf(kTri3Bb[q], L0, fmaf(kTri3Bc[q], cx, -x));
+                                const float py = fmaf(kTri3Bc[q], cy, -y);
+                                const float rs = rsqrtf(fmaf(px, px, fmaf(py, py, z2)));
+                                const float w = (1.f / 3.f) * rs;
+                                sw += w;
+                                const float g3 = G0 * w * rs * rs;
+                                dqx[q] = fmaf(g3, px, dqx[q]);
+                                dqy[q] = fmaf(g3, py, dqy[q]);
+                                dqz[q] = fmaf(g3, -z, dqz[q]);
+                            }
+                            q0 = fmaf(G0, sw, q0);
+                        } else if (G0 != 0.f) {
                             float sw = 0.f;
 #pragma unroll
                             for (int q = 0; q < 6; ++q) {
