@@ -462,6 +462,17 @@ lf_status lf_constraint_penalty(lf_ctx* ctx, const double* params, double* value
  * lf_objective_grad plus these two. */
 lf_status lf_constraint_gradient(lf_ctx* ctx, const double* params, double* grad);
 
+/* InversionRunner::smoothGradient (modules/litho-inversion/src/inversion/
+ * runner.cpp:643-706), the runner's optional gradient smoothing: every
+ * DOF-mapped vertex axis blends its gradient with the mean over its mesh
+ * neighbours carrying the same axis, (1 - weight) g + weight mean, and each
+ * DOF takes the value of its last (mesh, local DOF) reference.  weight <= 0
+ * returns the gradient unchanged.  Host arrays (lf_smooth_gradient) or device
+ * buffers on the context's stream (lf_smooth_gradient_device; in and out may
+ * be the same buffer). */
+lf_status lf_smooth_gradient(lf_ctx* ctx, double weight, const double* grad_in, double* grad_out);
+lf_status lf_smooth_gradient_device(lf_ctx* ctx, double weight, const double* d_grad_in, double* d_grad_out);
+
 /* ------------------------------------------------------------------------ */
 /* Allocation-free forward.  No counterpart in the reference: for callers    */
 /* that cannot call cudaMalloc (a host framework owning all device memory   */

@@ -281,6 +281,13 @@ class Context:
                     "property_inversion")
         return dens, (mag if self.n_mag else None)
 
+    def smooth_gradient(self, grad, weight: float) -> np.ndarray:
+        """lf_smooth_gradient: the runner's neighbour-blended gradient."""
+        g = f64(grad)
+        out = np.zeros(self.n_dofs)
+        self._check(self.lib.lf_smooth_gradient(self.h, float(weight), _d(g), _d(out)), "smooth_gradient")
+        return out
+
     # ---- point classification and borehole constraints ----
     def set_label_grid(self, labels, origin, spacing):
         """lf_set_label_grid: labels shaped (nz, ny, nx) of group ids (negative:

@@ -142,6 +142,12 @@ struct lf_ctx {
     int nCons = 0;
     double consWeight = 1e6;  // ConstraintHandler's default weight
 
+    // gradient smoothing (lf_smooth_gradient): mesh neighbour lists, built on first use
+    bool gnReady = false;
+    DevBuf<int32_t> d_gnOff, d_gnList;
+    DevBuf<double> d_gsVg, d_gsSg, d_gsIn;
+    DevBuf<uint8_t> d_gsHas;
+
     lf_counters counters{0, 0, 0};
 
     // CUDA graph replay of whole evaluations (lf_set_graph_mode).  epoch is
@@ -622,6 +628,7 @@ extern "C" lf_status lf_set_model_tables(lf_ctx* c, int G, const double* density
     c->partitioned = false;
     c->planEpoch++;
     c->hasModel = true;
+    c->gnReady = false;
     LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
     return LF_OK;
 }
@@ -2304,6 +2311,82 @@ extern "C" lf_status lf_constraint_gradient(lf_ctx* c, const double* params, dou
     else
         LF_RET_IF(sweep());
     LF_TRY_CUDA(c, cudaMemcpyAsync(grad, c->d_cGrad.p, sizeof(double) * c->np, cudaMemcpyDeviceToHost, c->stream));
+    LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
+    return LF_OK;
+}
+
+// ------------------------------------------------------ gradient smoothing --
+// InversionRunner::smoothGradient (runner.cpp:643-706) on device buffers.
+static lf_status gsmooth_tables(lf_ctx* c) {
+    if (c->gnReady) return LF_OK;
+    const int V = c->V, T = c->T;
+    std::vector<int32_t> tri((size_t)3 * T);
+    LF_TRY_CUDA(c, cudaMemcpyAsync(tri.data(), c->d_tri.p, sizeof(int32_t) * tri.size(), cudaMemcpyDeviceToHost,
+                                   c->stream));
+    LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
+    // SurfaceMesh::buildNeighbors (surface_mesh.cpp:265-286): sorted, unique
+    std::vector<std::vector<int32_t>> nb(V);
+    for (int t = 0; t < T; ++t) {
+        const int a = tri[3 * t], b = tri[3 * t + 1], d = tri[3 * t + 2];
+        nb[a].push_back(b); nb[a].push_back(d);
+        nb[b].push_back(a); nb[b].push_back(d);
+        nb[d].push_back(a); nb[d].push_back(b);
+    }
+    std::vector<int32_t> off(V + 1, 0), list;
+    for (int v = 0; v < V; ++v) {
+        std::sort(nb[v].begin(), nb[v].end());
+        nb[v].erase(std::unique(nb[v].begin(), nb[v].end()), nb[v].end());
+        list.insert(list.end(), nb[v].begin(), nb[v].end());
+        off[v + 1] = static_cast<int32_t>(list.size());
+    }
+    if (list.empty()) list.push_back(0);
+    LF_TRY_CUDA(c, upload(c->d_gnOff, off.data(), off.size(), c->stream));
+    LF_TRY_CUDA(c, upload(c->d_gnList, list.data(), list.size(), c->stream));
+    LF_TRY_CUDA(c, c->d_gsVg.reserve((size_t)3 * V));
+    LF_TRY_CUDA(c, c->d_gsSg.reserve((size_t)3 * V));
+    LF_TRY_CUDA(c, c->d_gsHas.reserve((size_t)3 * V));
+    LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->gnReady = true;
+    return LF_OK;
+}
+
+extern "C" lf_status lf_smooth_gradient_device(lf_ctx* c, double weight, const double* d_in, double* d_out) {
+    if (!c) return LF_EINVAL;
+    if (!c->hasModel) return fail(c, LF_ESTATE, "no model set");
+    if (!std::isfinite(weight)) return fail(c, LF_EINVAL, "lf_smooth_gradient: non-finite weight");
+    if (c->np == 0) return LF_OK;
+    if (!d_in || !d_out) return fail(c, LF_EINVAL, "lf_smooth_gradient: null gradient");
+    cudaSetDevice(c->device);
+    if (weight <= 0.0) {  // runner.cpp:645: the gradient unchanged
+        if (d_out != d_in)
+            LF_TRY_CUDA(c, cudaMemcpyAsync(d_out, d_in, sizeof(double) * c->np, cudaMemcpyDeviceToDevice, c->stream));
+        return LF_OK;
+    }
+    LF_RET_IF(gsmooth_tables(c));
+    LF_TRY_CUDA(c, cudaMemsetAsync(c->d_gsHas.p, 0, (size_t)3 * c->V, c->stream));
+    k_gsmooth_scatter<<<cdiv(c->np, 256), 256, 0, c->stream>>>(c->np, c->d_dofOff.p, c->d_refVertex.p, c->d_refAxis.p,
+                                                               d_in, c->d_gsVg.p, c->d_gsHas.p);
+    k_gsmooth_vertex<<<cdiv(3 * (long long)c->V, 256), 256, 0, c->stream>>>(c->V, c->d_gnOff.p, c->d_gnList.p,
+                                                                           c->d_gsVg.p, c->d_gsHas.p, weight,
+                                                                           c->d_gsSg.p);
+    k_gsmooth_gather<<<cdiv(c->np, 256), 256, 0, c->stream>>>(c->np, c->d_dofOff.p, c->d_refVertex.p, c->d_refAxis.p,
+                                                              d_in, c->d_gsSg.p, d_out);
+    c->counters.launches += 3;
+    LF_CHECK_LAUNCH(c);
+    return LF_OK;
+}
+
+extern "C" lf_status lf_smooth_gradient(lf_ctx* c, double weight, const double* grad_in, double* grad_out) {
+    if (!c) return LF_EINVAL;
+    if (!c->hasModel) return fail(c, LF_ESTATE, "no model set");
+    if (c->np == 0) return LF_OK;
+    if (!grad_in || !grad_out) return fail(c, LF_EINVAL, "lf_smooth_gradient: null gradient");
+    if (!finite_all(grad_in, c->np)) return fail(c, LF_EINVAL, "lf_smooth_gradient: non-finite gradient");
+    cudaSetDevice(c->device);
+    LF_TRY_CUDA(c, upload(c->d_gsIn, grad_in, (size_t)c->np, c->stream));
+    LF_TRY_CUDA(c, c->d_cGrad.reserve(c->np));
+    LF_RET_IF(lf_smooth_gradient_device(c, weight, c->d_gsIn.p, c->d_cGrad.p));
+    LF_TRY_CUDA(c, cudaMemcpyAsync(grad_out, c->d_cGrad.p, sizeof(double) * c->np, cudaMemcpyDeviceToHost, c->stream));
     LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
     return LF_OK;
 }

@@ -211,4 +211,58 @@ __global__ void k_constraint_fd(int np, const double* __restrict__ fp, const dou
     if (j < np) grad[j] = __dmul_rn(weight, __ddiv_rn(__dsub_rn(fp[j], fm[j]), __dmul_rn(2.0, h)));
 }
 
+// InversionRunner::smoothGradient (modules/litho-inversion/src/inversion/
+// runner.cpp:643-706): each DOF-mapped vertex axis of a mesh takes
+// (1 - w) x its gradient + w x the mean gradient of its mesh neighbours
+// (sorted neighbour order) that carry the same axis; every global DOF then
+// takes the value of its last (mesh, local DOF) reference, DOFs without
+// references keep their gradient.  Three passes: refs -> per-vertex-axis
+// values (k_gsmooth_scatter), the neighbour blend (k_gsmooth_vertex), and the
+// gather (k_gsmooth_gather); products and sums rounded explicitly in the
+// reference's order.
+__global__ void k_gsmooth_scatter(int np, const int32_t* __restrict__ dof_off, const int32_t* __restrict__ ref_vertex,
+                                  const uint8_t* __restrict__ ref_axis, const double* __restrict__ g,
+                                  double* __restrict__ vg, uint8_t* __restrict__ has) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= np) return;
+    for (int r = dof_off[j]; r < dof_off[j + 1]; ++r) {
+        const size_t idx = 3 * (size_t)ref_vertex[r] + ref_axis[r];
+        vg[idx] = g[j];
+        has[idx] = 1;
+    }
+}
+
+__global__ void k_gsmooth_vertex(int V, const int32_t* __restrict__ nb_off, const int32_t* __restrict__ nb,
+                                 const double* __restrict__ vg, const uint8_t* __restrict__ has, double w,
+                                 double* __restrict__ sg) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 3 * V) return;
+    if (!has[i]) return;
+    const int v = i / 3, a = i % 3;
+    double sum = 0.0;
+    int n = 0;
+    for (int k = nb_off[v]; k < nb_off[v + 1]; ++k) {
+        const size_t ni = 3 * (size_t)nb[k] + a;
+        if (has[ni]) {
+            sum = __dadd_rn(sum, vg[ni]);
+            ++n;
+        }
+    }
+    if (n > 0) {
+        const double mean = __ddiv_rn(sum, (double)n);
+        sg[i] = __dadd_rn(__dmul_rn(__dsub_rn(1.0, w), vg[i]), __dmul_rn(w, mean));
+    } else {
+        sg[i] = vg[i];
+    }
+}
+
+__global__ void k_gsmooth_gather(int np, const int32_t* __restrict__ dof_off, const int32_t* __restrict__ ref_vertex,
+                                 const uint8_t* __restrict__ ref_axis, const double* __restrict__ g,
+                                 const double* __restrict__ sg, double* __restrict__ out) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= np) return;
+    const int r = dof_off[j + 1] - 1;
+    out[j] = r >= dof_off[j] ? sg[3 * (size_t)ref_vertex[r] + ref_axis[r]] : g[j];
+}
+
 }  // namespace litho_b200

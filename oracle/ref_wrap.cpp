@@ -337,6 +337,67 @@ void ref_unit_response(void* h, const double* params, int kind, int group, const
     fromVec(r, out);
 }
 
+// InversionRunner::smoothGradient (runner.cpp:643-706), restated with the
+// reference model's public API (runner.cpp is not compiled here).
+void ref_smooth_gradient(void* h, double w, const double* g_in, double* g_out) {
+    auto* c = static_cast<RefCtx*>(h);
+    for (int i = 0; i < c->model->groupMeshCount(); ++i)  // as the runner does at set-up (runner.cpp:59)
+        if (c->model->groupMesh(i)) c->model->groupMesh(i)->buildNeighbors();
+    const LithologyModel* model = c->model.get();
+    const Index np = static_cast<Index>(model->totalDofCount());
+    VectorXd g = toVec(static_cast<int>(np), g_in);
+    VectorXd smoothed = g;
+    if (w > 0.0) {
+        const int nM = model->groupMeshCount();
+        for (int mi = 0; mi < nM; ++mi) {
+            const auto* mesh = model->groupMesh(mi);
+            if (!mesh || mesh->vertexCount() == 0) continue;
+            const auto& mappings = mesh->dofMappings();
+            const uint32_t nVerts = mesh->vertexCount();
+            std::vector<double> vertGrad(nVerts * 3, 0.0);
+            std::vector<int> vertHasAxis(nVerts * 3, 0);
+            for (uint32_t li = 0; li < mappings.size(); ++li) {
+                const auto& dm = mappings[li];
+                const int gi = model->globalDofIndex(mi, static_cast<int>(li));
+                if (gi < 0 || gi >= g.size()) continue;
+                const uint32_t idx = dm.vertexIndex * 3 + dm.axis;
+                vertGrad[idx] = g[gi];
+                vertHasAxis[idx] = 1;
+            }
+            std::vector<double> smoothGrad(nVerts * 3, 0.0);
+            for (uint32_t vi = 0; vi < nVerts; ++vi) {
+                const auto& neighbors = mesh->neighborVertices(vi);
+                for (int a = 0; a < 3; ++a) {
+                    const uint32_t idx = vi * 3 + a;
+                    if (!vertHasAxis[idx]) continue;
+                    double neighborSum = 0.0;
+                    int nNbr = 0;
+                    for (uint32_t ni : neighbors) {
+                        const uint32_t nidx = ni * 3 + a;
+                        if (vertHasAxis[nidx]) {
+                            neighborSum += vertGrad[nidx];
+                            ++nNbr;
+                        }
+                    }
+                    if (nNbr > 0) {
+                        const double neighborMean = neighborSum / nNbr;
+                        smoothGrad[idx] = (1.0 - w) * vertGrad[idx] + w * neighborMean;
+                    } else {
+                        smoothGrad[idx] = vertGrad[idx];
+                    }
+                }
+            }
+            for (uint32_t li = 0; li < mappings.size(); ++li) {
+                const auto& dm = mappings[li];
+                const int gi = model->globalDofIndex(mi, static_cast<int>(li));
+                if (gi < 0 || gi >= g.size()) continue;
+                smoothed[gi] = smoothGrad[dm.vertexIndex * 3 + dm.axis];
+            }
+        }
+    }
+    fromVec(smoothed, g_out);
+}
+
 // InversionRunner::runPropertyInversion parts A and B (runner.cpp:708-917),
 // restated with the reference's own classes (GravityForward /
 // MagneticForward unit responses, LBFGSBOptimizer): runner.cpp itself needs

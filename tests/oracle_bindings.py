@@ -117,6 +117,7 @@ def ref() -> C.CDLL:
             "ref_smoothness_gradient": (None, [V, _dp, _dp]),
             "ref_objective": (None, [V, _dp, _dp]), "ref_gradient": (None, [V, _dp, _dp]),
             "ref_lbfgsb": (C.c_int, [V, _dp, _dp, _dp, C.c_int, C.c_double, C.c_int, _dp, _dp]),
+            "ref_smooth_gradient": (None, [V, C.c_double, _dp, _dp]),
             "ref_property_inversion": (None, [V, _dp, _dp, C.c_int, _dp, _dp]),
             "ref_set_label_grid": (None, [V, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                           C.c_double, C.c_double, C.c_double, _ip]),
@@ -228,6 +229,13 @@ class RefModel:
         v = self.lib.ref_smoothness_value(self.h, _d(params))
         self.lib.ref_smoothness_gradient(self.h, _d(params), g.ctypes.data_as(_dp))
         return v, g
+
+    def smooth_gradient(self, grad, weight):
+        """InversionRunner::smoothGradient restated with the reference model."""
+        g = np.ascontiguousarray(grad, np.float64)
+        out = np.zeros(self.np)
+        self.lib.ref_smooth_gradient(self.h, float(weight), _d(g), out.ctypes.data_as(_dp))
+        return out
 
     def property_inversion(self, params, opt, max_iter, n_groups, magnetic_per_group):
         """runPropertyInversion parts A and B (restated with the reference's
