@@ -462,6 +462,20 @@ lf_status lf_constraint_penalty(lf_ctx* ctx, const double* params, double* value
  * lf_objective_grad plus these two. */
 lf_status lf_constraint_gradient(lf_ctx* ctx, const double* params, double* grad);
 
+/* LithologyModel::validate (modules/litho-model/src/litho/
+ * lithology_model.cpp:624-803) at params (NULL: the current positions): the
+ * shared-vertex gap, adjacent and non-adjacent overlap (every vertex
+ * classified as in lf_classify_points, on the GPU), edge-tearing, bounding
+ * box and spike checks in the reference's order; *passed = 0 with the
+ * reference's failure text in reason[reason_len] and its worst violation in
+ * *worst for the first check that fails.  freedom[n_vertices] (NULL: the
+ * builder's) marks the boundary vertices of the tearing check (not
+ * LF_XYZ_FREE).  The overlap baselines are the runner's (runner.cpp:494-516:
+ * counts of the initial model, obtainable with lf_classify_points). */
+lf_status lf_validate_model(lf_ctx* ctx, const double* params, const uint8_t* freedom,
+                            unsigned long long overlap_baseline, unsigned long long adjacent_overlap_baseline,
+                            int* passed, double* worst, char* reason, int reason_len);
+
 /* InversionRunner::smoothGradient (modules/litho-inversion/src/inversion/
  * runner.cpp:643-706), the runner's optional gradient smoothing: every
  * DOF-mapped vertex axis blends its gradient with the mean over its mesh

@@ -281,6 +281,18 @@ class Context:
                     "property_inversion")
         return dens, (mag if self.n_mag else None)
 
+    def validate_model(self, params=None, overlap_baseline: int = 0, adjacent_overlap_baseline: int = 0,
+                       freedom=None):
+        """lf_validate_model: (passed, reason, worst violation)."""
+        ok = C.c_int(0)
+        worst = np.zeros(1)
+        buf = C.create_string_buffer(256)
+        fr = np.ascontiguousarray(freedom, np.uint8) if freedom is not None else None
+        self._check(self.lib.lf_validate_model(self.h, _d(f64(params)) if params is not None else None,
+                                               _u8(fr), int(overlap_baseline), int(adjacent_overlap_baseline),
+                                               C.byref(ok), _d(worst), buf, len(buf)), "validate_model")
+        return bool(ok.value), buf.value.decode(), float(worst[0])
+
     def smooth_gradient(self, grad, weight: float) -> np.ndarray:
         """lf_smooth_gradient: the runner's neighbour-blended gradient."""
         g = f64(grad)

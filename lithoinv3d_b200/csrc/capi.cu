@@ -9,6 +9,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
+#include <map>
 #include <random>
 #include <cmath>
 #include <cstdio>
@@ -123,6 +125,7 @@ struct lf_ctx {
 
     // SurfaceSmoothness regularisation (off unless lf_set_smoothness)
     std::vector<uint8_t> vertexFreedom;  // from lf_set_model's builder
+    std::vector<int32_t> grpVertOff;     // vertex range of each group mesh (lf_set_model's builder)
     bool smoothOn = false;
     double smoothWeight = 0.0;
     DevBuf<int32_t> d_smOff, d_smNbr;
@@ -625,6 +628,7 @@ extern "C" lf_status lf_set_model_tables(lf_ctx* c, int G, const double* density
     c->hasRef = false;
     c->smoothOn = false;
     c->vertexFreedom.clear();
+    c->grpVertOff.clear();
     c->partitioned = false;
     c->planEpoch++;
     c->hasModel = true;
@@ -651,6 +655,7 @@ extern "C" lf_status lf_set_model(lf_ctx* c, lf_model* m) {
                                        t.refScale.data(), t.interpOff.data(), t.interpSrc.data(), t.interpW.data(),
                                        nSync, t.syncOff.data(), t.syncVertex.data());
     if (st != LF_OK) return st;
+    c->grpVertOff.assign(t.vertexOffset.begin(), t.vertexOffset.end());
     // vertex freedoms in the tables' vertex order (meshes in group order)
     for (int g = 0; g < m->host.meshCount(); ++g)
         if (const Mesh* mesh = m->host.mesh(g))
@@ -2389,4 +2394,199 @@ extern "C" lf_status lf_smooth_gradient(lf_ctx* c, double weight, const double* 
     LF_TRY_CUDA(c, cudaMemcpyAsync(grad_out, c->d_cGrad.p, sizeof(double) * c->np, cudaMemcpyDeviceToHost, c->stream));
     LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
     return LF_OK;
+}
+
+// ------------------------------------------------------------ validation --
+// LithologyModel::validate (lithology_model.cpp:624-803): the six quality
+// checks in the reference's order, the first failure returned.  Vertex
+// positions come from the device; the two overlap counts classify every
+// vertex with the GPU ray cast (the O(V x T) part); the rest is O(V) host
+// work over the downloaded positions.  Neighbour lists as
+// SurfaceMesh::buildNeighbors, which the runner calls at set-up.
+extern "C" lf_status lf_validate_model(lf_ctx* c, const double* params, const uint8_t* freedom,
+                                       unsigned long long overlap_baseline,
+                                       unsigned long long adjacent_overlap_baseline, int* passed, double* worst,
+                                       char* reason, int reason_len) {
+    LF_RET_IF(model_ready(c));
+    if (!passed || !worst) return fail(c, LF_EINVAL, "lf_validate_model: null result");
+    if (params) {
+        LF_RET_IF(constraint_params(c, params));
+        LF_RET_IF(scatter(c, c->d_cPar.p));
+    }
+    const uint8_t* fr = freedom ? freedom : (c->vertexFreedom.empty() ? nullptr : c->vertexFreedom.data());
+    if (!fr) return fail(c, LF_EINVAL, "lf_validate_model: no vertex freedoms known (pass freedom[n_vertices])");
+    *passed = 1;
+    *worst = 0.0;
+    std::string why;
+    auto finish = [&](lf_status st) -> lf_status {
+        if (reason && reason_len > 0) {
+            std::strncpy(reason, why.c_str(), (size_t)reason_len - 1);
+            reason[reason_len - 1] = '\0';
+        }
+        return st;
+    };
+    const int G = c->G, V = c->V, T = c->T;
+    if (G < 2) return finish(LF_OK);
+    std::vector<double> pos((size_t)3 * V);
+    std::vector<int32_t> tri((size_t)3 * T);
+    LF_TRY_CUDA(c, cudaMemcpyAsync(pos.data(), c->d_pos.p, sizeof(double) * pos.size(), cudaMemcpyDeviceToHost,
+                                   c->stream));
+    LF_TRY_CUDA(c, cudaMemcpyAsync(tri.data(), c->d_tri.p, sizeof(int32_t) * tri.size(), cudaMemcpyDeviceToHost,
+                                   c->stream));
+    std::vector<int32_t> syncOff, syncVertex;
+    if (c->nSync > 0) {
+        syncOff.resize(c->nSync + 1);
+        LF_TRY_CUDA(c, cudaMemcpyAsync(syncOff.data(), c->d_syncOff.p, sizeof(int32_t) * syncOff.size(),
+                                       cudaMemcpyDeviceToHost, c->stream));
+        LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
+        syncVertex.resize(syncOff.back());
+        if (!syncVertex.empty())
+            LF_TRY_CUDA(c, cudaMemcpyAsync(syncVertex.data(), c->d_syncVertex.p, sizeof(int32_t) * syncVertex.size(),
+                                           cudaMemcpyDeviceToHost, c->stream));
+    }
+    // classification of every vertex (checks 2 and 3)
+    LF_TRY_CUDA(c, c->d_ptCls.reserve(V));
+    LF_TRY_CUDA(c, c->d_clsMask.reserve(std::max<size_t>(c->d_clsMask.n, V)));
+    LF_RET_IF(classify_dev(c, V, c->d_pos.p, c->d_ptCls.p));
+    std::vector<int32_t> cls(V);
+    LF_TRY_CUDA(c, cudaMemcpyAsync(cls.data(), c->d_ptCls.p, sizeof(int32_t) * V, cudaMemcpyDeviceToHost, c->stream));
+    LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
+    // vertex range of each group mesh (meshes are stored one after another):
+    // the builder's offsets, else the range the group's triangles use
+    std::vector<int32_t> vlo(G, V), vhi(G, -1);
+    if ((int)c->grpVertOff.size() == G + 1) {
+        for (int g = 0; g < G; ++g) {
+            vlo[g] = c->grpVertOff[g];
+            vhi[g] = c->grpVertOff[g + 1] - 1;
+        }
+    } else {
+        for (int g = 0; g < G; ++g)
+            for (int t = c->grpTriOff[g]; t < c->grpTriOff[g + 1]; ++t)
+                for (int k = 0; k < 3; ++k) {
+                    vlo[g] = std::min(vlo[g], tri[3 * t + k]);
+                    vhi[g] = std::max(vhi[g], tri[3 * t + k]);
+                }
+    }
+    auto P = [&](int v, int k) { return pos[3 * (size_t)v + k]; };
+    auto dist = [&](int u, int v) {
+        const double dx = P(u, 0) - P(v, 0), dy = P(u, 1) - P(v, 1), dz = P(u, 2) - P(v, 2);
+        return std::sqrt(dx * dx + dy * dy + dz * dz);
+    };
+    double xmin = 1e30, xmax = -1e30, ymin = 1e30, ymax = -1e30, zmin = 1e30, zmax = -1e30;
+    for (int g = 0; g < G; ++g)
+        for (int v = vlo[g]; v <= vhi[g]; ++v) {
+            xmin = std::min(xmin, P(v, 0)); xmax = std::max(xmax, P(v, 0));
+            ymin = std::min(ymin, P(v, 1)); ymax = std::max(ymax, P(v, 1));
+            zmin = std::min(zmin, P(v, 2)); zmax = std::max(zmax, P(v, 2));
+        }
+    const double modelDim = std::max({xmax - xmin, ymax - ymin, zmax - zmin, 1.0});
+    const double aabbMargin = modelDim * 0.02;
+    // 1: shared vertex gaps
+    for (int s = 0; s < c->nSync; ++s) {
+        if (syncOff[s + 1] - syncOff[s] < 2) continue;
+        const int r = syncVertex[syncOff[s]];
+        for (int k = syncOff[s] + 1; k < syncOff[s + 1]; ++k) {
+            const double gap = dist(syncVertex[k], r);
+            if (gap > 0.1) {
+                *passed = 0;
+                *worst = std::max(*worst, gap);
+                why = "Shared vertex gap: " + std::to_string(gap) + "m";
+                return finish(LF_OK);
+            }
+        }
+    }
+    // 2 and 3: vertices of group g classified into another group
+    unsigned long long adj = 0, nonAdj = 0;
+    for (int g = 0; g < G; ++g)
+        for (int v = vlo[g]; v <= vhi[g]; ++v) {
+            const int k = cls[v];
+            if (k < 0 || k == g) continue;
+            if (std::abs(k - g) == 1) ++adj;
+            else ++nonAdj;
+        }
+    const unsigned long long adjLimit = adjacent_overlap_baseline + 20;
+    if (adj > adjLimit) {
+        *passed = 0;
+        *worst = static_cast<double>(adj - adjacent_overlap_baseline);
+        why = "Adjacent overlap: " + std::to_string(adj) + " (baseline=" + std::to_string(adjacent_overlap_baseline) +
+              ", limit=" + std::to_string(adjLimit) + ")";
+        return finish(LF_OK);
+    }
+    const unsigned long long overlapLimit = overlap_baseline + 120;
+    if (nonAdj > overlapLimit) {
+        *passed = 0;
+        *worst = static_cast<double>(nonAdj - overlap_baseline);
+        why = "Non-adjacent overlap: " + std::to_string(nonAdj) + " (baseline=" + std::to_string(overlap_baseline) +
+              ", limit=" + std::to_string(overlapLimit) + ")";
+        return finish(LF_OK);
+    }
+    // 4: boundary vertices (not XYZ-free) quantised to 0.1 mm must stay together
+    std::map<std::array<int64_t, 3>, std::vector<int>> boundary;
+    for (int g = 0; g < G; ++g)
+        for (int v = vlo[g]; v <= vhi[g]; ++v) {
+            if (fr[v] == LF_XYZ_FREE) continue;
+            const std::array<int64_t, 3> key = {static_cast<int64_t>(std::round(P(v, 0) * 1e4)),
+                                                static_cast<int64_t>(std::round(P(v, 1) * 1e4)),
+                                                static_cast<int64_t>(std::round(P(v, 2) * 1e4))};
+            boundary[key].push_back(v);
+        }
+    for (const auto& kv : boundary) {
+        const std::vector<int>& vs = kv.second;
+        for (size_t i = 1; i < vs.size(); ++i) {
+            const double gap = dist(vs[i], vs[0]);
+            if (gap > 0.1) {
+                *passed = 0;
+                *worst = std::max(*worst, gap);
+                why = "Edge tearing: boundary vertices diverged by " + std::to_string(gap) + "m";
+                return finish(LF_OK);
+            }
+        }
+    }
+    // 5: containment in the model's (own) bounding box with a 2 % margin
+    for (int g = 0; g < G; ++g)
+        for (int v = vlo[g]; v <= vhi[g]; ++v) {
+            const double x = P(v, 0), y = P(v, 1), z = P(v, 2);
+            if (x < xmin - aabbMargin || x > xmax + aabbMargin || y < ymin - aabbMargin || y > ymax + aabbMargin ||
+                z < zmin - aabbMargin || z > zmax + aabbMargin) {
+                *passed = 0;
+                *worst = std::max({xmin - aabbMargin - x, x - xmax - aabbMargin, ymin - aabbMargin - y,
+                                   y - ymax - aabbMargin, zmin - aabbMargin - z, z - zmax - aabbMargin, 0.0});
+                why = "AABB containment: vertex in group " + std::to_string(g) + " outside model envelope";
+                return finish(LF_OK);
+            }
+        }
+    // 6: spikes -- |vertex - mean of its mesh neighbours| above modelDim / 5
+    const double spikeThreshold = modelDim / 5.0;
+    std::vector<std::vector<int32_t>> nb(V);
+    for (int t = 0; t < T; ++t) {
+        const int a = tri[3 * t], b = tri[3 * t + 1], d = tri[3 * t + 2];
+        nb[a].push_back(b); nb[a].push_back(d);
+        nb[b].push_back(a); nb[b].push_back(d);
+        nb[d].push_back(a); nb[d].push_back(b);
+    }
+    for (int g = 0; g < G; ++g)
+        for (int v = vlo[g]; v <= vhi[g]; ++v) {
+            std::vector<int32_t>& l = nb[v];
+            std::sort(l.begin(), l.end());
+            l.erase(std::unique(l.begin(), l.end()), l.end());
+            if (l.empty()) continue;
+            double ax = 0.0, ay = 0.0, az = 0.0;
+            for (int32_t u : l) {
+                ax += P(u, 0);
+                ay += P(u, 1);
+                az += P(u, 2);
+            }
+            const double n = static_cast<double>(l.size());
+            ax /= n; ay /= n; az /= n;
+            const double lx = P(v, 0) - ax, ly = P(v, 1) - ay, lz = P(v, 2) - az;
+            const double mag = std::sqrt(lx * lx + ly * ly + lz * lz);
+            if (mag > spikeThreshold) {
+                *passed = 0;
+                *worst = mag;
+                why = "Spike detected: vertex in group " + std::to_string(g) + " vi=" + std::to_string(v - vlo[g]) +
+                      " Laplacian=" + std::to_string(mag) + "m (threshold=" + std::to_string(spikeThreshold) + "m)";
+                return finish(LF_OK);
+            }
+        }
+    return finish(LF_OK);
 }

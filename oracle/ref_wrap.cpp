@@ -337,6 +337,20 @@ void ref_unit_response(void* h, const double* params, int kind, int group, const
     fromVec(r, out);
 }
 
+// LithologyModel::validate (lithology_model.cpp:624-803) on the current
+// positions, neighbours built as the runner builds them (runner.cpp:59).
+int ref_validate(void* h, unsigned long long overlap_baseline, unsigned long long adjacent_baseline, double* worst,
+                 char* reason, int reason_len) {
+    auto* c = static_cast<RefCtx*>(h);
+    for (int i = 0; i < c->model->groupMeshCount(); ++i)
+        if (c->model->groupMesh(i)) c->model->groupMesh(i)->buildNeighbors();
+    const ValidationResult r = c->model->validate(overlap_baseline, adjacent_baseline);
+    *worst = r.worstViolation;
+    std::strncpy(reason, r.failureReason.c_str(), (size_t)reason_len - 1);
+    reason[reason_len - 1] = '\0';
+    return r.passed ? 1 : 0;
+}
+
 // InversionRunner::smoothGradient (runner.cpp:643-706), restated with the
 // reference model's public API (runner.cpp is not compiled here).
 void ref_smooth_gradient(void* h, double w, const double* g_in, double* g_out) {

@@ -117,6 +117,7 @@ def ref() -> C.CDLL:
             "ref_smoothness_gradient": (None, [V, _dp, _dp]),
             "ref_objective": (None, [V, _dp, _dp]), "ref_gradient": (None, [V, _dp, _dp]),
             "ref_lbfgsb": (C.c_int, [V, _dp, _dp, _dp, C.c_int, C.c_double, C.c_int, _dp, _dp]),
+            "ref_validate": (C.c_int, [V, C.c_ulonglong, C.c_ulonglong, _dp, C.c_char_p, C.c_int]),
             "ref_smooth_gradient": (None, [V, C.c_double, _dp, _dp]),
             "ref_property_inversion": (None, [V, _dp, _dp, C.c_int, _dp, _dp]),
             "ref_set_label_grid": (None, [V, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
@@ -229,6 +230,14 @@ class RefModel:
         v = self.lib.ref_smoothness_value(self.h, _d(params))
         self.lib.ref_smoothness_gradient(self.h, _d(params), g.ctypes.data_as(_dp))
         return v, g
+
+    def validate(self, overlap_baseline=0, adjacent_baseline=0):
+        """LithologyModel::validate at the current positions: (passed, reason, worst)."""
+        worst = np.zeros(1)
+        buf = C.create_string_buffer(256)
+        ok = self.lib.ref_validate(self.h, int(overlap_baseline), int(adjacent_baseline),
+                                   worst.ctypes.data_as(_dp), buf, len(buf))
+        return bool(ok), buf.value.decode(), float(worst[0])
 
     def smooth_gradient(self, grad, weight):
         """InversionRunner::smoothGradient restated with the reference model."""
