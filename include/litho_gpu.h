@@ -487,6 +487,23 @@ lf_status lf_validate_model(lf_ctx* ctx, const double* params, const uint8_t* fr
 lf_status lf_smooth_gradient(lf_ctx* ctx, double weight, const double* grad_in, double* grad_out);
 lf_status lf_smooth_gradient_device(lf_ctx* ctx, double weight, const double* d_grad_in, double* d_grad_out);
 
+/* ---------------------------------------------------------------- surfaces */
+/* loadSurfaceMesh (modules/litho-io/src/io/surface_loader.cpp:163-181):
+ * a GOCAD TSurf (.ts: VRTX / PVRTX vertices in file order, TRGL 1-based
+ * triangles, HEADER blocks, comments and GOCAD / TFACE / TRIANGLES lines
+ * skipped, END stops) or OBJ (.obj: v, f / fo with polygons fanned from the
+ * first vertex) surface.  Call with xyz = tri = NULL for the counts, then
+ * with xyz[3 n_vertices] and tri[3 n_triangles] (0-based).  LF_EINVAL for an
+ * unreadable file, another extension, a file without vertices or a triangle
+ * naming a vertex the file does not have (the reference returns that mesh
+ * unchecked). */
+lf_status lf_read_surface(const char* path, int* n_vertices, int* n_triangles, double* xyz, int32_t* tri);
+/* InversionExporter::exportTS (modules/litho-io/src/io/exporters.cpp:116-151):
+ * writes a GOCAD TSurf with header name `name`, vertices in %.8e form and
+ * 1-based triangles. */
+lf_status lf_write_tsurf(const char* path, const char* name, int n_vertices, const double* xyz, int n_triangles,
+                         const int32_t* tri);
+
 /* ------------------------------------------------------------------------ */
 /* Allocation-free forward.  No counterpart in the reference: for callers    */
 /* that cannot call cudaMalloc (a host framework owning all device memory   */

@@ -2,8 +2,8 @@
 gradient contracted into the objective gradient, DOF scatter/gather and a
 host projected L-BFGS driver, behind the C ABI of include/litho_gpu.h."""
 from .api import (FIXED, GRAVITY, MAGNETIC, PREC_FP64, PREC_MIXED, XYZ_FREE, Z_ONLY, Context, LithoError,
-                  Model)
+                  Model, read_surface, write_tsurf)
 from .build import build_library, library_path
 
 __all__ = ["Context", "Model", "LithoError", "build_library", "library_path", "FIXED", "Z_ONLY", "XYZ_FREE",
-           "GRAVITY", "MAGNETIC", "PREC_FP64", "PREC_MIXED"]
+           "GRAVITY", "MAGNETIC", "PREC_FP64", "PREC_MIXED", "read_surface", "write_tsurf"]

@@ -111,6 +111,8 @@ SIGNATURES = {
     "lf_forward_noalloc": (C.c_int, [C.c_int, _vp, C.c_int, _vp, C.c_int, _vp, C.c_double, C.c_double, C.c_double,
                                      C.c_double, C.c_double, _vp, _vp, _vp]),
     "lf_get_kernel_times": (C.c_int, [_vp, _dp, C.POINTER(C.c_int), _dp, C.POINTER(C.c_int)]),
+    "lf_read_surface": (C.c_int, [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), _dp, _ip]),
+    "lf_write_tsurf": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, _dp, C.c_int, _ip]),
     "lf_validate_model": (C.c_int, [_vp, _dp, _u8p, C.c_ulonglong, C.c_ulonglong, C.POINTER(C.c_int), _dp,
                                     C.c_char_p, C.c_int]),
     "lf_smooth_gradient": (C.c_int, [_vp, C.c_double, _dp, _dp]),

@@ -54,6 +54,32 @@ def i32(a) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.int32)
 
 
+def read_surface(path: str):
+    """lf_read_surface: (vertices [n, 3], triangles [m, 3] 0-based) of a .ts or .obj file."""
+    lib = _native.load()
+    nv, nt = C.c_int(0), C.c_int(0)
+    b = str(path).encode()
+    st = lib.lf_read_surface(b, C.byref(nv), C.byref(nt), None, None)
+    if st != 0:
+        raise LithoError(st, f"read_surface: {path}")
+    xyz = np.zeros((nv.value, 3))
+    tri = np.zeros((nt.value, 3), np.int32)
+    st = lib.lf_read_surface(b, C.byref(nv), C.byref(nt), _d(xyz), _i(tri))
+    if st != 0:
+        raise LithoError(st, f"read_surface: {path}")
+    return xyz, tri
+
+
+def write_tsurf(path: str, name: str, xyz, tri):
+    """lf_write_tsurf: a GOCAD TSurf of the given vertices and triangles."""
+    lib = _native.load()
+    x = f64(xyz).reshape(-1, 3)
+    t = i32(tri).reshape(-1, 3)
+    st = lib.lf_write_tsurf(str(path).encode(), name.encode(), len(x), _d(x), len(t), _i(t))
+    if st != 0:
+        raise LithoError(st, f"write_tsurf: {path}")
+
+
 class Model:
     """Host lithology model (LithologyModel / SurfaceMesh setup semantics)."""
 

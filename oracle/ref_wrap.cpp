@@ -11,6 +11,8 @@
 #include <litho_invert/forward/gravity_forward.h>
 #include <litho_invert/forward/magnetic_forward.h>
 #include <litho_invert/inversion/constraint_handler.h>
+#include <litho_invert/io/exporters.h>
+#include <litho_invert/io/surface_loader.h>
 #include <litho_invert/inversion/joint_objective.h>
 #include <litho_invert/inversion/lbfgsb_optimizer.h>
 #include <litho_invert/inversion/objective.h>
@@ -335,6 +337,37 @@ void ref_unit_response(void* h, const double* params, int kind, int group, const
     else if (kind == 2) r = c->mf->computeGroupUnitResponseDirection(group, Vector3d(dir[0], dir[1], dir[2]));
     else r = c->mf->computeGroupUnitRemanenceResponse(group);
     fromVec(r, out);
+}
+
+// loadSurfaceMesh (surface_loader.cpp:163-181): counts, and with non-null
+// buffers the vertices and 0-based triangles; 0 when the loader returns null.
+int ref_load_surface(const char* path, int* nv, int* nt, double* xyz, int32_t* tri) {
+    auto mesh = loadSurfaceMesh(path);
+    if (!mesh) return 0;
+    *nv = static_cast<int>(mesh->vertexCount());
+    *nt = static_cast<int>(mesh->triangleCount());
+    if (xyz)
+        for (uint32_t i = 0; i < mesh->vertexCount(); ++i)
+            for (int k = 0; k < 3; ++k) xyz[3 * i + k] = mesh->vertex(i).position[k];
+    if (tri)
+        for (uint32_t i = 0; i < mesh->triangleCount(); ++i) {
+            const Triangle& t = mesh->triangle(i);
+            tri[3 * i] = static_cast<int32_t>(t.v0);
+            tri[3 * i + 1] = static_cast<int32_t>(t.v1);
+            tri[3 * i + 2] = static_cast<int32_t>(t.v2);
+        }
+    return 1;
+}
+
+// InversionExporter(dir, base).exportTS(mesh, suffix) of the given surface.
+void ref_export_ts(const char* dir, const char* base, const char* suffix, int nv, const double* xyz, int nt,
+                   const int32_t* tri) {
+    SurfaceMesh mesh;
+    for (int i = 0; i < nv; ++i) mesh.addVertex(Vector3d(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]));
+    for (int i = 0; i < nt; ++i)
+        mesh.addTriangle(static_cast<uint32_t>(tri[3 * i]), static_cast<uint32_t>(tri[3 * i + 1]),
+                         static_cast<uint32_t>(tri[3 * i + 2]));
+    InversionExporter(dir, base).exportTS(mesh, suffix);
 }
 
 // LithologyModel::validate (lithology_model.cpp:624-803) on the current

@@ -117,6 +117,8 @@ def ref() -> C.CDLL:
             "ref_smoothness_gradient": (None, [V, _dp, _dp]),
             "ref_objective": (None, [V, _dp, _dp]), "ref_gradient": (None, [V, _dp, _dp]),
             "ref_lbfgsb": (C.c_int, [V, _dp, _dp, _dp, C.c_int, C.c_double, C.c_int, _dp, _dp]),
+            "ref_load_surface": (C.c_int, [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), _dp, _ip]),
+            "ref_export_ts": (None, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int, _dp, C.c_int, _ip]),
             "ref_validate": (C.c_int, [V, C.c_ulonglong, C.c_ulonglong, _dp, C.c_char_p, C.c_int]),
             "ref_smooth_gradient": (None, [V, C.c_double, _dp, _dp]),
             "ref_property_inversion": (None, [V, _dp, _dp, C.c_int, _dp, _dp]),
@@ -437,3 +439,24 @@ def misfit(pred, obs, std):
 def misfit_gradient(J, pred, obs, std, alpha=1.0):
     w = np.where(std > 0, 1.0 / np.where(std > 0, std, 1.0), 1.0)
     return -alpha * J.T @ (w * w * (obs - pred))
+
+
+def ref_load_surface(path):
+    """The reference's loadSurfaceMesh: (xyz [n, 3], tri [m, 3]) or None."""
+    lib = ref()
+    nv, nt = C.c_int(0), C.c_int(0)
+    if not lib.ref_load_surface(str(path).encode(), C.byref(nv), C.byref(nt), None, None):
+        return None
+    xyz = np.zeros((nv.value, 3))
+    tri = np.zeros((nt.value, 3), np.int32)
+    lib.ref_load_surface(str(path).encode(), C.byref(nv), C.byref(nt), xyz.ctypes.data_as(_dp),
+                         tri.ctypes.data_as(_ip))
+    return xyz, tri
+
+
+def ref_export_ts(directory, base, suffix, xyz, tri):
+    """The reference's InversionExporter(directory, base).exportTS(mesh, suffix)."""
+    x = np.ascontiguousarray(xyz, np.float64).reshape(-1, 3)
+    t = np.ascontiguousarray(tri, np.int32).reshape(-1, 3)
+    ref().ref_export_ts(str(directory).encode(), base.encode(), suffix.encode(), len(x), x.ctypes.data_as(_dp),
+                        len(t), t.ctypes.data_as(_ip))
