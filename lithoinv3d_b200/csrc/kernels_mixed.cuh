@@ -173,26 +173,41 @@ __device__ __forceinline__ float sqrt_pos(float r2) { return r2 * rsqrtf(r2); }
 // 2 (v + v^3/3 + ... + v^9/9) (Abramowitz & Stegun 4.1.28), whose first
 // omitted term is below 2e-9 v, else log1pf(2v / (1 - v)).  The arguments are
 // bounded away from zero and overflow, so the 2-ulp quotient is used.
+// atanh(v) for 0 <= v <= 0.2 by the series above (Lambda = 2 atanh(v)).
+__device__ __forceinline__ float atanh_series(float v) {
+    const float v2 = v * v;
+    const float p = fmaf(v2, fmaf(v2, fmaf(v2, fmaf(v2, 1.f / 9.f, 1.f / 7.f), 1.f / 5.f), 1.f / 3.f), 1.f);
+    return v * p;
+}
+
 __device__ __forceinline__ float lam_f32(float d1, float d2, float L) {
     const float v = __fdividef(L, d1 + d2);
-    if (v <= 0.2f) {
-        const float v2 = v * v;
-        const float p = fmaf(v2, fmaf(v2, fmaf(v2, fmaf(v2, 1.f / 9.f, 1.f / 7.f), 1.f / 5.f), 1.f / 3.f), 1.f);
-        return 2.f * v * p;
-    }
+    if (v <= 0.2f) return 2.f * atanh_series(v);
     return log1pf(__fdividef(2.f * v, 1.f - v));
 }
 
-// atan2(y, x); for x > 0 and |y| <= x / 8 (every far pair's solid angle) the
-// Maclaurin series of atan(t), t = y / x, through t^9 (Abramowitz & Stegun
-// 4.4.42; first omitted term below 1e-10 t), else atan2f.
+// atan(t) for |t| <= 1/8: the Maclaurin series through t^9 (Abramowitz &
+// Stegun 4.4.42; first omitted term below 1e-10 t).
+__device__ __forceinline__ float atan_series(float t) {
+    const float t2 = t * t;
+    const float p = fmaf(t2, fmaf(t2, fmaf(t2, fmaf(t2, 1.f / 9.f, -1.f / 7.f), 1.f / 5.f), -1.f / 3.f), 1.f);
+    return t * p;
+}
+
+// atan2(y, x); for x > 0 and |y| <= x / 8 (every far pair's solid angle)
+// atan_series(y / x), else atan2f.
 __device__ __forceinline__ float atan2_far(float y, float x) {
-    if (x > 0.f && fabsf(y) <= 0.125f * x) {
-        const float t = __fdividef(y, x), t2 = t * t;
-        const float p = fmaf(t2, fmaf(t2, fmaf(t2, fmaf(t2, 1.f / 9.f, -1.f / 7.f), 1.f / 5.f), -1.f / 3.f), 1.f);
-        return t * p;
-    }
+    if (x > 0.f && fabsf(y) <= 0.125f * x) return atan_series(__fdividef(y, x));
     return atan2f(y, x);
+}
+
+// True when a far pair lies inside both series' ranges on all four terms:
+// the solid angle's atan2(ny, den) (den > 0, |ny| <= den / 8) and the three
+// edges' atanh (v_i <= 0.2).  Far pairs practically always do, so one test
+// replaces four per-term branches; a pair that fails it takes atan2_far /
+// lam_f32, which select per term, and both routes give the same bits.
+__device__ __forceinline__ bool far_series_ok(float ny, float den, float v0, float v1, float v2) {
+    return den > 0.f && fabsf(ny) <= 0.125f * den && fmaxf(v0, fmaxf(v1, v2)) <= 0.2f;
 }
 
 // FP32 facet record of the far-field forward, staged in shared memory and
@@ -203,7 +218,7 @@ struct __align__(16) FaceF32 {
     float rx0, rx1, rx2, L0;   // local x axis, |ab|
     float ry0, ry1, ry2, cx;   // local y axis, c.x
     float cy, L1, L2, gq;      // c.y, |bc|, |ca|, n_z * gz scale * area
-    float mf, mt0, mt1, mt2;   // TMI facet scales
+    float mf, mt0, mt1, mt2;   // TMI facet scales, doubled
     float q6[12];              // (x, y) of the 6-point rule's points in the local frame
     float q3[8];               // (x, y) of the 3-point rule's points, pad
     double ax, ay, az, zx, zy, zz;
@@ -257,7 +272,10 @@ __device__ __forceinline__ void pair_far_f32(const FaceF32* Fp, double ox, doubl
         acc *= (1.f / 3.f);
     }
     *gz += gq * acc;
-    // TMI: MF * Omega + sum_i MT_i Lambda_i
+    // TMI: MF * Omega + sum_i MT_i Lambda_i with Omega = 2 atan2(ny, den) and
+    // Lambda_i = 2 atanh(v_i); the record holds 2 MF and 2 MT_i, so the terms
+    // below are atan2 and atanh.  Scaling by 2 is exact: the bits equal
+    // MF * (2 atan2) + MT_i * (2 atanh).
     float rbx = L0 - x, rcx = cx - x, rcy = cy - y;
     float la = sqrt_pos(fmaf(x, x, fmaf(y, y, z2)));
     float lb = sqrt_pos(fmaf(rbx, rbx, fmaf(y, y, z2)));
@@ -266,10 +284,20 @@ __device__ __forceinline__ void pair_far_f32(const FaceF32* Fp, double ox, doubl
     float dac = fmaf(-x, rcx, fmaf(-y, rcy, z2));
     float dbc = fmaf(rbx, rcx, fmaf(-y, rcy, z2));
     float den = la * lb * lc + dab * lc + dac * lb + dbc * la;
-    float om = 2.f * atan2_far(-z * (L0 * cy), den);
-    float l0 = lam_f32(la, lb, L0);
-    float l1 = lam_f32(lb, lc, L1);
-    float l2 = lam_f32(lc, la, L2);
+    const float ny = -z * (L0 * cy);
+    const float e0 = __fdividef(L0, la + lb), e1 = __fdividef(L1, lb + lc), e2 = __fdividef(L2, lc + la);
+    float om, l0, l1, l2;
+    if (far_series_ok(ny, den, e0, e1, e2)) {
+        om = atan_series(__fdividef(ny, den));
+        l0 = atanh_series(e0);
+        l1 = atanh_series(e1);
+        l2 = atanh_series(e2);
+    } else {
+        om = atan2_far(ny, den);
+        l0 = 0.5f * lam_f32(la, lb, L0);
+        l1 = 0.5f * lam_f32(lb, lc, L1);
+        l2 = 0.5f * lam_f32(lc, la, L2);
+    }
     *tmi += v3.x * om + v3.y * l0 + v3.z * l1 + v3.w * l2;
 }
 
@@ -351,7 +379,9 @@ __device__ __forceinline__ void forward_mixed_block(double* __restrict__ smd, Fa
             F.L0 = (float)M(MC_L0); F.cx = (float)M(MC_CX); F.cy = (float)M(MC_CY);
             F.L1 = (float)M(MC_L1); F.L2 = (float)M(MC_L2);
             F.gq = (float)(M(MC_SGZ) * 0.5 * M(MC_L0) * M(MC_CY));
-            F.mf = (float)M(MC_MF); F.mt0 = (float)M(MC_MT0); F.mt1 = (float)M(MC_MT1); F.mt2 = (float)M(MC_MT2);
+            // TMI scales doubled: the far pair's series give atan2 and atanh (exact)
+            F.mf = 2.f * (float)M(MC_MF); F.mt0 = 2.f * (float)M(MC_MT0);
+            F.mt1 = 2.f * (float)M(MC_MT1); F.mt2 = 2.f * (float)M(MC_MT2);
 #pragma unroll
             for (int q = 0; q < 6; ++q) {
                 F.q6[2 * q] = kDun6Bb[q] * F.L0 + kDun6Bc[q] * F.cx;
@@ -667,11 +697,22 @@ __global__ void __launch_bounds__(128, 4) k_gradient_warp_far32(int T, const dou
                             const float dac = fmaf(-x, rcx, fmaf(-y, rcy, z2));
                             const float dbc = fmaf(rbx, rcx, fmaf(-y, rcy, z2));
                             const float den = la * lb * lc + dab * lc + dac * lb + dbc * la;
-                            const float om = 2.f * atan2_far(-z * A2, den);
+                            const float ny = -z * A2;
+                            const float e0 = __fdividef(L0, la + lb), e1 = __fdividef(L1, lb + lc),
+                                        e2 = __fdividef(L2, lc + la);
+                            float om, l0, l1, l2;
+                            if (far_series_ok(ny, den, e0, e1, e2)) {
+                                om = 2.f * atan_series(__fdividef(ny, den));
+                                l0 = 2.f * atanh_series(e0);
+                                l1 = 2.f * atanh_series(e1);
+                                l2 = 2.f * atanh_series(e2);
+                            } else {
+                                om = 2.f * atan2_far(ny, den);
+                                l0 = lam_f32(la, lb, L0);
+                                l1 = lam_f32(lb, lc, L1);
+                                l2 = lam_f32(lc, la, L2);
+                            }
                             const float s11 = fmaf(rbx, e1x, -y * e1y), s21 = fmaf(rcx, e2x, rcy * e2y);
-                            const float l0 = lam_f32(la, lb, L0);
-                            const float l1 = lam_f32(lb, lc, L1);
-                            const float l2 = lam_f32(lc, la, L2);
                             const float ia = __fdividef(1.f, la), ib = __fdividef(1.f, lb), ic = __fdividef(1.f, lc);
                             const float kom = Ts * mf;
                             // edge (p1 -> p2): W = L / (d1 d2 + r1.r2), q = r1 - s1 e, Z = e x r1,
