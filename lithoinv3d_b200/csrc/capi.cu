@@ -95,6 +95,7 @@ struct lf_ctx {
     std::vector<GroupConst> gconst;
 
     DevBuf<double> d_pos, d_fc, d_gc, d_mc, d_params, d_grad, d_vgrad, d_out5, d_f, d_refp;
+    DevBuf<FaceF32> d_mf32;  // far-field facet records of the mixed forward [T]
     DevBuf<unsigned long long> d_nearPairs;
     float tau = 3.0f;  // far-field ratio of the mixed path
     DevBuf<int32_t> d_tri, d_dofOff, d_refVertex, d_interpOff, d_interpSrc, d_interpRows, d_syncOff,
@@ -615,6 +616,7 @@ extern "C" lf_status lf_set_model_tables(lf_ctx* c, int G, const double* density
     LF_TRY_CUDA(c, upload(c->d_faceNeeds, fneed.data(), fneed.size(), c->stream));
     LF_TRY_CUDA(c, c->d_fc.reserve((size_t)NFC * nt));
     LF_TRY_CUDA(c, c->d_mc.reserve((size_t)NMC * nt));
+    LF_TRY_CUDA(c, c->d_mf32.reserve((size_t)nt));
     LF_TRY_CUDA(c, c->d_nearPairs.reserve(1));
     LF_TRY_CUDA(c, cudaMemsetAsync(c->d_nearPairs.p, 0, sizeof(unsigned long long), c->stream));
     LF_TRY_CUDA(c, c->d_gc.reserve((size_t)NGC * nt));
@@ -1044,7 +1046,7 @@ static lf_status forward_set_items(lf_ctx* c, const StationSet& s, double* d_gz,
         int slot = prof_begin(c, c->evFwd, c->nFwd);
         if (MIXED)
             k_forward_mixed_items<GZ, TMI, kFwdFacetTile><<<grid, kFwdThreads, 0, c->stream>>>(
-                c->d_items.p, c->nItems, s.d_xyz.p, c->T, c->d_mc.p, c->tau, GZ ? c->d_partG.p : nullptr,
+                c->d_items.p, c->nItems, s.d_xyz.p, c->T, c->d_mc.p, c->d_mf32.p, c->tau, GZ ? c->d_partG.p : nullptr,
                 TMI ? c->d_partM.p : nullptr, c->d_nearPairs.p);
         else
             k_forward_fp64_items<GZ, TMI, kFwdFacetTile><<<grid, kFwdThreads, 0, c->stream>>>(
@@ -1104,7 +1106,8 @@ static lf_status forward_set_mixed(lf_ctx* c, const StationSet& s, double* d_gz,
         dim3 grid(cdiv(S, kFwdThreads), nch);
         int slot = prof_begin(c, c->evFwd, c->nFwd);
         k_forward_mixed<GZ, TMI, kFwdFacetTile><<<grid, kFwdThreads, 0, c->stream>>>(
-            S, s.d_xyz.p, c->T, c->d_mc.p, c->d_chunkBegin.p, c->d_chunkEnd.p, c->tau, GZ ? c->d_partG.p : nullptr,
+            S, s.d_xyz.p, c->T, c->d_mc.p, c->d_mf32.p, c->d_chunkBegin.p, c->d_chunkEnd.p, c->tau,
+            GZ ? c->d_partG.p : nullptr,
             TMI ? c->d_partM.p : nullptr, c->d_nearPairs.p);
         prof_end(c, c->evFwd, slot);
     }
@@ -1121,7 +1124,7 @@ static lf_status forward_set_mixed(lf_ctx* c, const StationSet& s, double* d_gz,
 static lf_status forward_all(lf_ctx* c) {
     if (c->precision == LF_PREC_MIXED) {
         k_face_prep_mixed<<<cdiv(c->T, 128), 128, 0, c->stream>>>(c->T, c->d_tri.p, c->d_pos.p, c->d_faceGroup.p,
-                                                                  c->d_groups.p, c->fdir, c->d_mc.p);
+                                                                  c->d_groups.p, c->fdir, c->d_mc.p, c->d_mf32.p);
         c->counters.launches++;
         LF_CHECK_LAUNCH(c);
         if (c->sameStations) return forward_set_mixed<true, true>(c, c->grav, c->grav.d_pred.p, c->mag.d_pred.p);
@@ -1814,7 +1817,7 @@ extern "C" lf_status lf_unit_response(lf_ctx* c, const double* params, int kind,
         c->groupFilter = group;
         if (c->precision == LF_PREC_MIXED) {
             k_face_prep_mixed<<<cdiv(c->T, 128), 128, 0, c->stream>>>(c->T, c->d_tri.p, c->d_pos.p, c->d_faceGroup.p,
-                                                                      c->d_groups.p, c->fdir, c->d_mc.p);
+                                                                      c->d_groups.p, c->fdir, c->d_mc.p, c->d_mf32.p);
             c->counters.launches++;
             st = kind == LF_UNIT_GRAVITY ? forward_set_mixed<true, false>(c, s, d_g, d_t)
                                          : forward_set_mixed<false, true>(c, s, d_g, d_t);

@@ -92,9 +92,58 @@ __constant__ float kRadon4Bc[28] = {
     0.5298579358948849f, 0.3333333333333333f, 0.1012865073234563f, 0.4493567463382718f, 0.4493567463382718f,
     0.4701420641051151f, 0.2649289679474425f, 0.2649289679474425f};
 
+// FP32 facet record of the far-field forward, written once per evaluation by
+// k_face_prep_mixed (array [T] in HBM), copied 32 facets at a time into
+// shared memory and read there with 128-bit loads (10 per far pair, 9 beyond
+// 4 tau).  The origin and the unit normal stay FP64: the height above the
+// facet plane can be tiny next to |o - a| (a far top facet seen from 1 m
+// above it).  The last row feeds the per-warp near/far test.
+struct __align__(16) FaceF32 {
+    float rx0, rx1, rx2, L0;   // local x axis, |ab|
+    float ry0, ry1, ry2, cx;   // local y axis, c.x
+    float cy, L1, L2, gq;      // c.y, |bc|, |ca|, n_z * gz scale * area
+    float mf, mt0, mt1, mt2;   // TMI facet scales, doubled
+    float q6[12];              // (x, y) of the 6-point rule's points in the local frame
+    float q3[8];               // (x, y) of the 3-point rule's points, pad
+    double ax, ay, az, zx, zy, zz;
+    float cenx, ceny, cenz;    // centroid
+    float size;                // longest edge; -1 for a facet that contributes nothing
+};
+static_assert(sizeof(FaceF32) == 208, "FaceF32 layout");
+constexpr int kFaceF32Vec = sizeof(FaceF32) / 16;  // float4 per record
+
+// The far-field record of one facet from its mixed constants m[NMC].
+__device__ __forceinline__ void make_face_f32(const double* m, FaceF32& F) {
+#define M(k) m[k]
+    F.rx0 = (float)M(MC_XX); F.rx1 = (float)M(MC_XY); F.rx2 = (float)M(MC_XZ);
+    F.ry0 = (float)M(MC_YX); F.ry1 = (float)M(MC_YY); F.ry2 = (float)M(MC_YZ);
+    F.L0 = (float)M(MC_L0); F.cx = (float)M(MC_CX); F.cy = (float)M(MC_CY);
+    F.L1 = (float)M(MC_L1); F.L2 = (float)M(MC_L2);
+    F.gq = (float)(M(MC_SGZ) * 0.5 * M(MC_L0) * M(MC_CY));
+    // TMI scales doubled: the far pair's series give atan2 and atanh (exact)
+    F.mf = 2.f * (float)M(MC_MF); F.mt0 = 2.f * (float)M(MC_MT0);
+    F.mt1 = 2.f * (float)M(MC_MT1); F.mt2 = 2.f * (float)M(MC_MT2);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        F.q6[2 * q] = kDun6Bb[q] * F.L0 + kDun6Bc[q] * F.cx;
+        F.q6[2 * q + 1] = kDun6Bc[q] * F.cy;
+    }
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        F.q3[2 * q] = kTri3Bb[q] * F.L0 + kTri3Bc[q] * F.cx;
+        F.q3[2 * q + 1] = kTri3Bc[q] * F.cy;
+    }
+    F.q3[6] = F.q3[7] = 0.f;
+    F.ax = M(MC_AX); F.ay = M(MC_AY); F.az = M(MC_AZ);
+    F.zx = M(MC_ZX); F.zy = M(MC_ZY); F.zz = M(MC_ZZ);
+    F.cenx = (float)M(MC_CENX); F.ceny = (float)M(MC_CENY); F.cenz = (float)M(MC_CENZ);
+    F.size = M(MC_VALID) != 0.0 ? (float)M(MC_SIZE) : -1.f;
+#undef M
+}
+
 __global__ void k_face_prep_mixed(int T, const int32_t* __restrict__ tri, const double* __restrict__ pos,
                                   const int16_t* __restrict__ face_group, const GroupConst* __restrict__ groups, d3 fdir,
-                                  double* __restrict__ mc) {
+                                  double* __restrict__ mc, FaceF32* __restrict__ mf32) {
     int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= T) return;
     d3 v[3];
@@ -157,6 +206,12 @@ __global__ void k_face_prep_mixed(int T, const int32_t* __restrict__ tri, const 
         out[MC_VALID] = 1.0;
     }
     for (int k = 0; k < NMC; ++k) mc[(size_t)k * T + f] = out[k];
+    FaceF32 F;
+    make_face_f32(out, F);
+    const float4* src = reinterpret_cast<const float4*>(&F);
+    float4* dst = reinterpret_cast<float4*>(mf32 + f);
+#pragma unroll
+    for (int k = 0; k < kFaceF32Vec; ++k) dst[k] = src[k];
 }
 
 // ----------------------------------------------------------- FP32 pieces --
@@ -209,21 +264,6 @@ __device__ __forceinline__ float atan2_far(float y, float x) {
 __device__ __forceinline__ bool far_series_ok(float ny, float den, float v0, float v1, float v2) {
     return den > 0.f && fabsf(ny) <= 0.125f * den && fmaxf(v0, fmaxf(v1, v2)) <= 0.2f;
 }
-
-// FP32 facet record of the far-field forward, staged in shared memory and
-// read with 128-bit loads (10 per far pair, 9 beyond 4 tau).  The origin and the unit normal stay
-// FP64: the height above the facet plane can be tiny next to |o - a| (a far
-// top facet seen from 1 m above it).
-struct __align__(16) FaceF32 {
-    float rx0, rx1, rx2, L0;   // local x axis, |ab|
-    float ry0, ry1, ry2, cx;   // local y axis, c.x
-    float cy, L1, L2, gq;      // c.y, |bc|, |ca|, n_z * gz scale * area
-    float mf, mt0, mt1, mt2;   // TMI facet scales, doubled
-    float q6[12];              // (x, y) of the 6-point rule's points in the local frame
-    float q3[8];               // (x, y) of the 3-point rule's points, pad
-    double ax, ay, az, zx, zy, zz;
-};
-static_assert(sizeof(FaceF32) == 192, "FaceF32 layout");
 
 enum { RULE_TRI3 = 0, RULE_DUN6 = 1, RULE_MID28 = 2 };
 
@@ -336,7 +376,10 @@ __device__ __forceinline__ void pair_near_f64(const double* __restrict__ s, int 
 
 // Station-per-thread forward: CTAs of 128 stations (pre-ordered along a
 // Morton curve, so a warp's 32 stations are spatially compact) x facet
-// chunks, facets staged 32 at a time in shared memory.  The precision class
+// chunks, facets staged 32 at a time in shared memory (their FP32 records,
+// written by k_face_prep_mixed, copied by the whole CTA; the FP64 constants
+// of a near facet fetched into the warp's own slot when it meets one,
+// which is a few per cent of pairs).  The precision class
 // is decided per (warp, facet): lane j tests facet j of the stage against the
 // warp's station bounding box -- centroid at least 4 tau x size away: very
 // far (FP32, 3-point gz); at least tau x size: far (FP32, 6-point gz); at
@@ -345,9 +388,10 @@ __device__ __forceinline__ void pair_near_f64(const double* __restrict__ s, int 
 // One CTA's work: station s (this thread; act = s is a station of the
 // block) against facets [fb, fe); out_gz[s] / out_tmi[s] receive the sums.
 template <bool GZ, bool TMI, int FT>
-__device__ __forceinline__ void forward_mixed_block(double* __restrict__ smd, FaceF32* __restrict__ smf, int s,
+__device__ __forceinline__ void forward_mixed_block(FaceF32* __restrict__ smf, double* __restrict__ smn, int s,
                                                     bool act, const double* __restrict__ sta, int T,
-                                                    const double* __restrict__ mc, int fb, int fe, float tau,
+                                                    const double* __restrict__ mc, const FaceF32* __restrict__ mf32,
+                                                    int fb, int fe, float tau,
                                                     double* __restrict__ out_gz, double* __restrict__ out_tmi,
                                                     unsigned long long* __restrict__ near_pairs) {
     static_assert(FT == 32, "one facet per lane in the near/far test");
@@ -365,50 +409,23 @@ __device__ __forceinline__ void forward_mixed_block(double* __restrict__ smd, Fa
     unsigned long long nearCount = 0;
     for (int f0 = fb; f0 < fe; f0 += FT) {
         const int nf = min(FT, fe - f0);
-        __syncthreads();
-        for (int idx = threadIdx.x; idx < NMC * FT; idx += blockDim.x) {
-            int k = idx / FT, j = idx % FT;
-            smd[idx] = (j < nf) ? mc[(size_t)k * T + f0 + j] : 0.0;
-        }
-        __syncthreads();
-        for (int j = threadIdx.x; j < nf; j += blockDim.x) {
-            FaceF32& F = smf[j];
-#define M(k) smd[(k) * FT + j]
-            F.rx0 = (float)M(MC_XX); F.rx1 = (float)M(MC_XY); F.rx2 = (float)M(MC_XZ);
-            F.ry0 = (float)M(MC_YX); F.ry1 = (float)M(MC_YY); F.ry2 = (float)M(MC_YZ);
-            F.L0 = (float)M(MC_L0); F.cx = (float)M(MC_CX); F.cy = (float)M(MC_CY);
-            F.L1 = (float)M(MC_L1); F.L2 = (float)M(MC_L2);
-            F.gq = (float)(M(MC_SGZ) * 0.5 * M(MC_L0) * M(MC_CY));
-            // TMI scales doubled: the far pair's series give atan2 and atanh (exact)
-            F.mf = 2.f * (float)M(MC_MF); F.mt0 = 2.f * (float)M(MC_MT0);
-            F.mt1 = 2.f * (float)M(MC_MT1); F.mt2 = 2.f * (float)M(MC_MT2);
-#pragma unroll
-            for (int q = 0; q < 6; ++q) {
-                F.q6[2 * q] = kDun6Bb[q] * F.L0 + kDun6Bc[q] * F.cx;
-                F.q6[2 * q + 1] = kDun6Bc[q] * F.cy;
-            }
-#pragma unroll
-            for (int q = 0; q < 3; ++q) {
-                F.q3[2 * q] = kTri3Bb[q] * F.L0 + kTri3Bc[q] * F.cx;
-                F.q3[2 * q + 1] = kTri3Bc[q] * F.cy;
-            }
-            F.q3[6] = F.q3[7] = 0.f;
-            F.ax = M(MC_AX); F.ay = M(MC_AY); F.az = M(MC_AZ);
-            F.zx = M(MC_ZX); F.zy = M(MC_ZY); F.zz = M(MC_ZZ);
-#undef M
+        __syncthreads();  // the previous stage's records are no longer read
+        {
+            const float4* __restrict__ src = reinterpret_cast<const float4*>(mf32 + f0);
+            float4* dst = reinterpret_cast<float4*>(smf);
+            for (int idx = threadIdx.x; idx < nf * kFaceF32Vec; idx += blockDim.x) dst[idx] = __ldg(src + idx);
         }
         __syncthreads();
         // lane j: facet j of the stage against this warp's box
         bool valid = false, vfar = false, far = false, mid = false;
-        if (lane < nf && smd[MC_VALID * FT + lane] != 0.0) {
+        if (lane < nf && !(smf[lane].size < 0.f)) {
             valid = true;
-            const float cxw = (float)smd[MC_CENX * FT + lane], cyw = (float)smd[MC_CENY * FT + lane],
-                        czw = (float)smd[MC_CENZ * FT + lane];
+            const float cxw = smf[lane].cenx, cyw = smf[lane].ceny, czw = smf[lane].cenz;
             const float ddx = fmaxf(0.f, fmaxf(bb[0] - cxw, cxw + bb[3]));
             const float ddy = fmaxf(0.f, fmaxf(bb[1] - cyw, cyw + bb[4]));
             const float ddz = fmaxf(0.f, fmaxf(bb[2] - czw, czw + bb[5]));
             const float d2 = ddx * ddx + ddy * ddy + ddz * ddz;
-            const float lim = tau * (float)smd[MC_SIZE * FT + lane], limMid = 0.5f * lim;
+            const float lim = tau * smf[lane].size, limMid = 0.5f * lim;
             vfar = d2 >= 16.f * (lim * lim);
             far = !vfar && d2 >= lim * lim;
             mid = !vfar && !far && d2 >= limMid * limMid;
@@ -433,14 +450,23 @@ __device__ __forceinline__ void forward_mixed_block(double* __restrict__ smd, Fa
             }
             if (GZ) gz += gacc;
             if (TMI) tmi += tacc;
-            for (unsigned m = nearMask; m; m &= m - 1) {
-                const int j = __ffs(m) - 1;
+            nearCount += __popc(nearMask);
+        }
+        // Near facets (a few per cent of pairs): the warp copies the facet's
+        // FP64 constants from HBM into its own slot of shared memory (lane k
+        // loads constant k), then every lane reads them from there.
+        double* slot = smn + (threadIdx.x >> 5) * NMC;
+        for (unsigned m = nearMask; m; m &= m - 1) {
+            const int j = __ffs(m) - 1;
+            __syncwarp();
+            if (lane < NMC) slot[lane] = __ldg(mc + (size_t)lane * T + f0 + j);
+            __syncwarp();
+            if (act) {
                 double g1 = 0.0, t1 = 0.0;
-                pair_near_f64(smd, j, FT, mk3(ox, oy, oz), &g1, &t1);
+                pair_near_f64(slot, 0, 1, mk3(ox, oy, oz), &g1, &t1);
                 if (GZ) gz += g1;
                 if (TMI) tmi += t1;
             }
-            nearCount += __popc(nearMask);
         }
     }
     if (act) {
@@ -452,15 +478,17 @@ __device__ __forceinline__ void forward_mixed_block(double* __restrict__ smd, Fa
 
 template <bool GZ, bool TMI, int FT>
 __global__ void __launch_bounds__(128) k_forward_mixed(int S, const double* __restrict__ sta, int T,
-                                                       const double* __restrict__ mc, const int32_t* __restrict__ chunk_begin,
+                                                       const double* __restrict__ mc,
+                                                       const FaceF32* __restrict__ mf32,
+                                                       const int32_t* __restrict__ chunk_begin,
                                                        const int32_t* __restrict__ chunk_end, float tau,
                                                        double* __restrict__ part_gz, double* __restrict__ part_tmi,
                                                        unsigned long long* __restrict__ near_pairs) {
-    __shared__ double smd[NMC * FT];
     __shared__ FaceF32 smf[FT];
+    __shared__ double smn[4 * NMC];  // one near-facet slot per warp (128 threads)
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     const int chunk = blockIdx.y;
-    forward_mixed_block<GZ, TMI, FT>(smd, smf, s, s < S, sta, T, mc, chunk_begin[chunk], chunk_end[chunk], tau,
+    forward_mixed_block<GZ, TMI, FT>(smf, smn, s, s < S, sta, T, mc, mf32, chunk_begin[chunk], chunk_end[chunk], tau,
                                      GZ ? part_gz + (size_t)chunk * S : nullptr,
                                      TMI ? part_tmi + (size_t)chunk * S : nullptr, near_pairs);
 }
@@ -469,15 +497,16 @@ __global__ void __launch_bounds__(128) k_forward_mixed(int S, const double* __re
 template <bool GZ, bool TMI, int FT>
 __global__ void __launch_bounds__(128) k_forward_mixed_items(const FwdItem* __restrict__ items, int nitems,
                                                              const double* __restrict__ sta, int T,
-                                                             const double* __restrict__ mc, float tau,
+                                                             const double* __restrict__ mc,
+                                                             const FaceF32* __restrict__ mf32, float tau,
                                                              double* __restrict__ part_gz, double* __restrict__ part_tmi,
                                                              unsigned long long* __restrict__ near_pairs) {
-    __shared__ double smd[NMC * FT];
     __shared__ FaceF32 smf[FT];
+    __shared__ double smn[4 * NMC];  // one near-facet slot per warp (128 threads)
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
         const FwdItem w = items[it];
         const int s = w.s0 + (int)threadIdx.x;
-        forward_mixed_block<GZ, TMI, FT>(smd, smf, s, s < w.s_end, sta, T, mc, w.fb, w.fe, tau,
+        forward_mixed_block<GZ, TMI, FT>(smf, smn, s, s < w.s_end, sta, T, mc, mf32, w.fb, w.fe, tau,
                                          GZ ? part_gz + w.out : nullptr, TMI ? part_tmi + w.out : nullptr,
                                          near_pairs);
     }
