@@ -81,6 +81,11 @@ constexpr double kGSI = 6.67430e-11, kDensityScale = 1000.0, kMs2ToMgal = 1e5;
 struct lf_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
+    // Second stream of the mixed gradient: the FP32 far-field kernel runs
+    // beside the FP64 near-field one (fork and join by events; inside a
+    // captured graph these become two parallel branches).
+    cudaStream_t side = nullptr;
+    cudaEvent_t evFork = nullptr, evJoin = nullptr;
     std::string err;
     int precision = LF_PREC_FP64;
 
@@ -431,6 +436,15 @@ extern "C" lf_status lf_create(lf_ctx** out, int device) {
         delete c;
         return LF_ECUDA;
     }
+    if (cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->evFork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->evJoin, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();  // without them the two gradient kernels run one after the other
+        if (c->evFork) cudaEventDestroy(c->evFork);
+        if (c->side) cudaStreamDestroy(c->side);
+        c->side = nullptr;
+        c->evFork = c->evJoin = nullptr;
+    }
     *out = c;
     return LF_OK;
 }
@@ -453,6 +467,10 @@ extern "C" void lf_destroy(lf_ctx* c) {
     drop_graph(c->gCons);
     clear_events(c->evFwd);
     clear_events(c->evGrad);
+    if (c->side) cudaStreamSynchronize(c->side);
+    if (c->evFork) cudaEventDestroy(c->evFork);
+    if (c->evJoin) cudaEventDestroy(c->evJoin);
+    if (c->side) cudaStreamDestroy(c->side);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -1231,6 +1249,15 @@ static int gradient_set(lf_ctx* c, const StationSet& s, const double* gcoef, con
     const int32_t* grpSta = c->partitioned ? c->d_grpStaOff.p : nullptr;
     const int32_t* grpTile = c->partitioned ? c->d_grpTileOff.p : nullptr;
     const int fblocks = cdiv(c->nGradFacets, kGradWarpsPerBlock);
+    // Mixed precision: the far-field kernel on the side stream, concurrent
+    // with the near-field one (they write disjoint partial slots).  Serial
+    // when the kernels are timed one by one (profiling).
+    bool fork = mixed && c->side && !c->profiling;
+    if (fork && (cudaEventRecord(c->evFork, c->stream) != cudaSuccess ||
+                 cudaStreamWaitEvent(c->side, c->evFork, 0) != cudaSuccess)) {
+        cudaGetLastError();
+        fork = false;
+    }
     int ev = prof_begin(c, c->evGrad, c->nGrad);
     k_gradient_warp_fp64<<<dim3(fblocks, nch), 32 * kGradWarpsPerBlock, 0, c->stream>>>(
         c->T, c->d_gc.p, s.n, s.d_xyz.p, gcoef, mcoef, s.d_tileBox.p, c->d_faceGroup.p, c->d_groups.p, c->fdir, tau,
@@ -1242,11 +1269,15 @@ static int gradient_set(lf_ctx* c, const StationSet& s, const double* gcoef, con
         int nch2 = 1, tpc2 = 1;
         grad_chunks(c, s.n, false, &nch2, &tpc2);
         int ev2 = prof_begin(c, c->evGrad, c->nGrad);
-        k_gradient_warp_far32<<<dim3(fblocks, nch2), 32 * kGradWarpsPerBlock, 0, c->stream>>>(
+        k_gradient_warp_far32<<<dim3(fblocks, nch2), 32 * kGradWarpsPerBlock, 0, fork ? c->side : c->stream>>>(
             c->T, c->d_gc.p, s.n, s.d_xyz.p, gcoef, mcoef, s.d_tileBox.p, c->d_faceGroup.p, c->d_groups.p, c->fdir,
             tau, c->d_gradFacets.p, c->nGradFacets, tpc2, grpSta, grpTile,
             c->d_partGrad.p + (size_t)(slot0 + nch) * 9 * c->T);
         prof_end(c, c->evGrad, ev2);
+        if (fork) {  // join: the main stream waits for the far-field kernel
+            cudaEventRecord(c->evJoin, c->side);
+            cudaStreamWaitEvent(c->stream, c->evJoin, 0);
+        }
         c->counters.launches++;
         used += nch2;
     }
