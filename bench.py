@@ -105,7 +105,7 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-stations", type=int, default=48)
+    ap.add_argument("--cpu-stations", type=int, default=256)
     ap.add_argument("--bodies", type=int, default=256,
                     help="number of bodies of the batch workload (256 is the configuration; fewer for profiling)")
     ap.add_argument("--workload", choices=["contact", "batch", "large", "constraints"], default="contact",

@@ -360,6 +360,23 @@ __global__ void __launch_bounds__(128) k_forward_fp64_items(const FwdItem* __res
     }
 }
 
+// acc + v(c0) + v(c0 + 8) + ... (c < n), added in that order with eight
+// loads in flight: the chunk reductions below are bound by the latency of
+// their partial loads, not by the additions.
+template <class F>
+__device__ __forceinline__ double strided_sum8(int c0, int n, double acc, F v) {
+    int c = c0;
+    for (; c + 56 < n; c += 64) {
+        double x[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) x[u] = v(c + 8 * u);
+#pragma unroll
+        for (int u = 0; u < 8; ++u) acc += x[u];
+    }
+    for (; c < n; c += 8) acc += v(c);
+    return acc;
+}
+
 // Per station of a batch of bodies: sum of its body's chunk partials
 // (grp_part_off[g] + c * n_g + local index, c < grp_nch[g]), times the body's
 // group scales when `groups` is given (FP64 path; the mixed partials carry
@@ -381,10 +398,9 @@ __global__ void __launch_bounds__(256) k_forward_reduce_groups(int S, const int3
         grp = sta_group[s];
         const int n = grp_sta_off[grp + 1] - grp_sta_off[grp], loc = s - grp_sta_off[grp];
         const int64_t base = grp_part_off[grp] + loc;
-        for (int c = ty; c < grp_nch[grp]; c += 8) {
-            if (part_gz) g += part_gz[base + (int64_t)c * n];
-            if (part_tmi) t += part_tmi[base + (int64_t)c * n];
-        }
+        const int nch = grp_nch[grp];
+        if (part_gz) g = strided_sum8(ty, nch, g, [&](int c) { return part_gz[base + (int64_t)c * n]; });
+        if (part_tmi) t = strided_sum8(ty, nch, t, [&](int c) { return part_tmi[base + (int64_t)c * n]; });
     }
     sg[ty][tx] = g;
     st[ty][tx] = t;
@@ -448,12 +464,16 @@ __global__ void __launch_bounds__(256) k_forward_reduce(int S, int nchunks, cons
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const int s = blockIdx.x * 32 + tx;
     double g = 0.0, t = 0.0;
-    if (s < S)
-        for (int c = ty; c < nchunks; c += 8) {
-            const GroupConst& gc = groups[chunk_group[c]];
-            if (part_gz) g += part_gz[(size_t)c * S + s] * gc.gscale_fwd;
-            if (part_tmi) t += -gc.mscale * part_tmi[(size_t)c * S + s];
-        }
+    if (s < S) {
+        if (part_gz)
+            g = strided_sum8(ty, nchunks, g, [&](int c) {
+                return part_gz[(size_t)c * S + s] * groups[chunk_group[c]].gscale_fwd;
+            });
+        if (part_tmi)
+            t = strided_sum8(ty, nchunks, t, [&](int c) {
+                return -groups[chunk_group[c]].mscale * part_tmi[(size_t)c * S + s];
+            });
+    }
     sg[ty][tx] = g;
     st[ty][tx] = t;
     __syncthreads();

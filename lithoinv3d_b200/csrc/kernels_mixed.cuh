@@ -821,11 +821,10 @@ __global__ void __launch_bounds__(256) k_forward_reduce_mixed(int S, int nchunks
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const int s = blockIdx.x * 32 + tx;
     double g = 0.0, t = 0.0;
-    if (s < S)
-        for (int c = ty; c < nchunks; c += 8) {
-            if (part_gz) g += part_gz[(size_t)c * S + s];
-            if (part_tmi) t += part_tmi[(size_t)c * S + s];
-        }
+    if (s < S) {
+        if (part_gz) g = strided_sum8(ty, nchunks, g, [&](int c) { return part_gz[(size_t)c * S + s]; });
+        if (part_tmi) t = strided_sum8(ty, nchunks, t, [&](int c) { return part_tmi[(size_t)c * S + s]; });
+    }
     sg[ty][tx] = g;
     st[ty][tx] = t;
     __syncthreads();
