@@ -61,9 +61,10 @@ SFU_FWD_PAIR = 16   # 3 sqrt + 9 div + 3 log + 1 atan2, one special-function op 
 SFU_GRAD_PAIR = 16
 # DRAM bytes (read + write) of one k_forward_mixed launch on this workload,
 # from an ncu capture (dram__bytes_read.sum + dram__bytes_write.sum; launch
-# shape 148 x 32 CTAs): the facet records are read once per CTA and reused
-# by its 128 stations, so the kernel moves ~5 MB per 78 M pairs.
-FORWARD_DRAM_BYTES_PER_LAUNCH = 4.875e6
+# shape 32 x 151 CTAs): the 208-byte facet records (4 MB) come from DRAM
+# once and from L2 for every further station block, each record reused by
+# the CTA's 128 stations, so the kernel moves ~7 MB per 78 M pairs.
+FORWARD_DRAM_BYTES_PER_LAUNCH = 7.024e6
 # Nominal B200 CUDA-core rates at the 1.965 GHz boost clock (no measured
 # figure for these pipes exists in MEASURED_PEAKS.json): FP32 148 SMs x 128
 # lanes x 2 flop; special-function unit 148 x 16 ops; FP64 148 x 64 x 2 flop.
