@@ -101,7 +101,9 @@ def job_rate(world: int, steps: int, slowest_ms: float) -> float:
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps; default 1000 on the contact model (about a second of device time, so "
+                         "that the clock sampler sees several samples), 20 large, 5 batch, 50 otherwise")
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
@@ -114,7 +116,10 @@ def parse():
                          "large: the 194k-facet single inversion")
     ap.add_argument("--lbfgs-iters", type=int, default=0,
                     help="after timing, run this many L-BFGS-B iterations and report their wall time")
-    return ap.parse_args()
+    args = ap.parse_args()
+    if args.steps is None:
+        args.steps = 50 if args.impl == "reference" else {"contact": 1000, "large": 20, "batch": 5}.get(args.workload, 50)
+    return args
 
 
 def make_problem(workload: str = "contact", bodies: int = 256):
