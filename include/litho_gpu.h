@@ -17,8 +17,12 @@
  *      modules/litho-inversion/src/inversion/lbfgsb_optimizer.cpp:162-263) on the host.
  *
  * Conventions: plain pointers and sizes; every call returns an lf_status.
- * Host arrays are copied in; device buffers belong to the context.  One CUDA
- * stream per context; a context must not be used by two threads at once
+ * Host arrays are copied in; device buffers belong to the context.  Each
+ * context owns one CUDA stream that orders all its work (lf_stream); in
+ * mixed precision the far-field gradient kernel runs on a second, internal
+ * stream that forks from and joins back into it within the same call, so
+ * results are complete in lf_stream order.  A context must not be used by
+ * two threads at once
  * (the reference operators are not re-entrant either).  No CPU fallback:
  * without a usable CUDA device, lf_create returns LF_ECUDA.
  */
@@ -124,12 +128,14 @@ lf_status lf_model_export_tables(lf_model* m, double* pos, int32_t* tri, int32_t
 /* ------------------------------------------------------------------------ */
 typedef struct lf_ctx lf_ctx;
 
-/* Creates a context on CUDA device `device` with its own stream. */
+/* Creates a context on CUDA device `device` with its own stream (and the
+ * internal side stream of the mixed gradient). */
 lf_status lf_create(lf_ctx** out, int device);
 void lf_destroy(lf_ctx* ctx);
 /* Last error message of this context (static storage owned by ctx). */
 const char* lf_last_error(const lf_ctx* ctx);
-/* The cudaStream_t (as void*) every launch of this context goes to. */
+/* The cudaStream_t (as void*) that orders this context's work: every call's
+ * results are complete once this stream reaches the point after it. */
 void* lf_stream(lf_ctx* ctx);
 
 /* Uploads geometry, group properties and DOF tables from a host model. */
@@ -414,8 +420,9 @@ lf_status lf_get_counters(lf_ctx* ctx, lf_counters* c);
 lf_status lf_reset_counters(lf_ctx* ctx);
 
 /* Kernel timing on the context's stream: when enabled, every launch of the
- * forward pair kernel and of the gradient pair kernel is bracketed by CUDA
- * events.  lf_get_kernel_times synchronises the stream and returns the summed
+ * forward pair kernel and of the gradient pair kernels is bracketed by CUDA
+ * events (the two mixed gradient kernels then run one after the other on
+ * the context's stream rather than concurrently).  lf_get_kernel_times synchronises the stream and returns the summed
  * durations (ms) and launch counts since profiling was (re)enabled. */
 lf_status lf_set_profiling(lf_ctx* ctx, int enabled);
 lf_status lf_get_kernel_times(lf_ctx* ctx, double* forward_ms, int* forward_launches,
