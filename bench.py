@@ -49,16 +49,27 @@ WORKLOAD_CONSTRAINTS = ("borehole-constraint gradient on the multi-unit contact 
                         "step (2 x np scatter + ray-cast classification passes per gradient)")
 L2_FLUSH_BYTES = 256 << 20
 
-# Algorithmic work per station-facet pair (frozen; derived from the FP64
-# restatement in oracle/litho_oracle.c with per-facet constants hoisted):
-#   forward gz+TMI pair: 137 floating-point operations (add/sub/mul count 1,
-#   an FMA 2) plus 3 sqrt, 9 div, 3 log, 1 atan2;
-#   gradient pair (both data types): 331 operations plus 3 sqrt, 9 div,
-#   3 log, 1 atan2.
-FLOPS_FWD_PAIR = 137
+# Algorithmic work per station-facet pair (frozen; never tuned).  Forward: one
+# gz + TMI pair sharing the solid angle and the edge line integrals, with the
+# per-facet constants hoisted (unit normal, edge directions and lengths, the
+# in-plane edge normals, the magnetic direction products):
+#   r_a, r_b, r_c = v - o                        9 flops
+#   |r_a|, |r_b|, |r_c|                          15 flops + 3 sqrt
+#   triple product r_a . (r_b x r_c)             14
+#   solid-angle denominator 23, atan2, factor 2  24 + 1 atan2
+#   height h = n . r_a                           5
+#   per edge (x 3): s1, s2 = r . e (10), numerator and denominator (2),
+#     their ratio (1 div + 1), log, d_perp (5), gz/TMI accumulation (4)
+#                                                66 + 3 div + 3 log
+#   final gz / TMI combine                       5
+#   total 138 flops (add/sub/mul 1, FMA 2) + 3 sqrt + 3 div + 3 log + 1 atan2.
+# Gradient pair (both data types, analytic derivatives of the three vertices
+# contracted with the residual adjoints): 331 flops; its special-function ops
+# are the forward's 10 plus the three vertex-distance reciprocals, 13.
+FLOPS_FWD_PAIR = 138
 FLOPS_GRAD_PAIR = 331
-SFU_FWD_PAIR = 16   # 3 sqrt + 9 div + 3 log + 1 atan2, one special-function op each
-SFU_GRAD_PAIR = 16
+SFU_FWD_PAIR = 10   # 3 sqrt + 3 div + 3 log + 1 atan2, one special-function op each
+SFU_GRAD_PAIR = 13
 # DRAM bytes (read + write) of one k_forward_mixed launch on this workload,
 # from an ncu capture (dram__bytes_read.sum + dram__bytes_write.sum; launch
 # shape 32 x 151 CTAs): the 208-byte facet records (4 MB) come from DRAM
@@ -249,29 +260,57 @@ def cpu_baseline(p, x0, gobs, gstd, mobs, mstd, n_sta: int):
                       f"({dt:.1f} s), scaled by station count"}
 
 
-def _ref_worker(args):
+REF_STATIONS_PER_CORE = 8
+
+
+def _ref_process(conn, idx, seed):
+    """One single-threaded reference process (the reference has no threading)
+    over the station sample `idx` of the contact workload.  Set-up, untimed:
+    the seeded geometry from numpy (synth.voxel_contact_model builds meshes
+    only), the reference's LithologyModel / forwards / JointObjective
+    (oracle/_ref), and observations of a seeded true model computed by the
+    reference's own forward.  Each step message then times exactly one
+    objective evaluation and one gradient (objective.cpp:83-105,
+    joint_objective.cpp:42-173) and sends back that duration.  Nothing from
+    the GPU library is loaded here."""
     import numpy as np
 
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_bindings as ob
     from lithoinv3d_b200 import synth
 
-    idx, seed_data = args
-    p, model = make_problem()
-    x0, gobs, gstd, mobs, mstd = seed_data
+    p = synth.voxel_contact_model()
     sub = synth.Problem(p.name, p.densities, p.susceptibilities, p.meshes, p.grav_xyz[idx], p.mag_xyz[idx],
                         inducing=p.inducing, axis_scale=p.axis_scale, cp_stride=p.cp_stride)
-    rm = ob.RefModel(sub, gobs[idx], gstd[idx], mobs[idx], mstd[idx])
-    t0 = time.perf_counter()
-    rm.objective(x0)
-    rm.gradient(x0)
-    return time.perf_counter() - t0
+    truth = ob.RefModel(sub)
+    x0 = truth.assemble()
+    rng = np.random.default_rng(seed)
+    x_true = x0 + rng.normal(0.0, 5.0, len(x0))
+    gz, tmi = truth.forward_gz(x_true), truth.forward_tmi(x_true)
+    del truth
+    gstd = np.full(len(gz), 0.01 * max(float(np.sqrt(np.mean(gz ** 2))), 1e-30))
+    mstd = np.full(len(tmi), 0.01 * max(float(np.sqrt(np.mean(tmi ** 2))), 1e-30))
+    rm = ob.RefModel(sub, gz + gstd * rng.normal(size=len(gz)), gstd, tmi + mstd * rng.normal(size=len(tmi)), mstd)
+    conn.send(("ready", len(p.grav_xyz), p.n_triangles(), int(len(x0))))
+    while True:
+        msg = conn.recv()
+        if msg != "step":
+            break
+        t0 = time.perf_counter()
+        rm.objective(x0)
+        rm.gradient(x0)
+        conn.send(time.perf_counter() - t0)
+    conn.close()
 
 
 def run_reference(args):
-    """--impl reference: the reference's CPU implementation (oracle/_ref, or
-    the C restatement when the reference could not be compiled) on all host
-    cores, one single-threaded process per core over a station sample."""
+    """--impl reference: the reference's CPU implementation of the path (its
+    own sources compiled into oracle/_ref; the C restatement is not used
+    here) on every host core, one persistent single-threaded process per core
+    over a station sample of the contact workload.  A step sends every
+    process one objective + gradient evaluation of its stations; the step
+    time is the slowest process's own timed region, so spawn, set-up and
+    pickling stay outside.  Under torchrun only rank 0 runs."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -281,49 +320,65 @@ def run_reference(args):
 
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_bindings as ob
+    from lithoinv3d_b200 import synth
 
-    p, model = make_problem()
-    ncore = os.cpu_count() or 1
-    per = 4
-    S = len(p.grav_xyz)
-    n_sample = min(S, per * ncore)
-    # observations from the C restatement (the GPU is not used on this arm)
-    om = ob.OracleModel(model.tables(), p.densities, p.susceptibilities, p.inducing)
-    x0 = model.assemble_parameters()
-    rng = np.random.default_rng(1234)
-    x_true = x0 + rng.normal(0.0, 5.0, len(x0))
-    om.scatter(x_true)
+    if not ob.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_litho.so (the reference's own "
+                                                             "sources, built by oracle/Makefile) is not present"}))
+        return
+    try:
+        ncore = len(os.sched_getaffinity(0))
+    except AttributeError:
+        ncore = os.cpu_count() or 1
+    S = len(synth.voxel_contact_model(n_side=64).grav_xyz)
+    n_sample = min(S, REF_STATIONS_PER_CORE * ncore)
     idx_all = np.linspace(0, S - 1, n_sample).astype(int)
-    gz = np.zeros(S)
-    tmi = np.zeros(S)
-    gz[idx_all] = om.forward_gz(p.grav_xyz[idx_all])
-    tmi[idx_all] = om.forward_tmi(p.mag_xyz[idx_all])
-    gstd = np.full(S, 0.01 * np.std(gz[idx_all]))
-    mstd = np.full(S, 0.01 * np.std(tmi[idx_all]))
-    data = (x0, gz + gstd * rng.normal(size=S), gstd, tmi + mstd * rng.normal(size=S), mstd)
     chunks = [idx_all[i::ncore] for i in range(ncore)]
-    kind = "reference" if ob.ref_available() else "port"
     ctx = mp.get_context("spawn")
+    procs, conns = [], []
+    for i, c in enumerate(chunks):
+        a, b = ctx.Pipe()
+        pr = ctx.Process(target=_ref_process, args=(b, c, 1234 + i), daemon=True)
+        pr.start()
+        procs.append(pr)
+        conns.append(a)
+    info = [cn.recv() for cn in conns]
+    _, S, T, np_ = info[0]
     times = []
-    with ctx.Pool(ncore) as pool:
-        for step in range(args.warmup + args.steps):
-            t0 = time.perf_counter()
-            pool.map(_ref_worker, [(c, data) for c in chunks])
-            dt = time.perf_counter() - t0
-            if step >= args.warmup:
-                times.append(dt)
+    for step in range(args.warmup + args.steps):
+        for cn in conns:
+            cn.send("step")
+        dt = max(cn.recv() for cn in conns)  # the slowest process ends the step
+        if step >= args.warmup:
+            times.append(dt)
+    for cn in conns:
+        cn.send("stop")
+    for pr in procs:
+        pr.join(timeout=30)
     t_step = sum(times) / len(times)
-    value = (n_sample / S) / t_step
+    value = (n_sample / S) / t_step  # whole-workload evaluations per second
+    sample = (f"{n_sample} of {S} stations per step ({REF_STATIONS_PER_CORE} per process), one single-threaded "
+              f"reference process per core ({ncore}); each step times one objective + gradient per process, "
+              f"the slowest process's time; evals/s scaled by station count")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": 1,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3 * S / n_sample,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3,
+            "ms_per_full_evaluation": t_step * 1e3 * S / n_sample,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded)", "config": {"workload": WORKLOAD, "stations_sampled": int(n_sample)},
-            "cpu_baseline": {"value": value, "unit": "evals/s", "cores": ncore, "kind": kind,
-                             "sample": f"{n_sample} of {S} stations per step split over {ncore} single-threaded "
-                                       f"processes (the reference has no threading); evals/s scaled by "
-                                       f"station count"},
+            "data": "synthetic (seeded voxel model and observations)",
+            "config": workload_config("contact", T, S, np_),
+            "details": {"stations_per_step": int(n_sample), "processes": ncore},
+            "cpu_baseline": {"value": value, "unit": "evals/s", "cores": ncore, "kind": "reference",
+                             "sample": sample},
             "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def workload_config(workload: str, triangles: int, stations: int, dofs: int, bodies: int = 256) -> dict:
+    """The workload as both arms name it (identical dicts for the same
+    workload); implementation details go elsewhere in the line."""
+    name = {"batch": WORKLOAD_BATCH.replace("256", str(bodies)), "large": WORKLOAD_LARGE}.get(workload, WORKLOAD)
+    return {"workload": name, "triangles": int(triangles), "stations": int(stations), "dofs": int(dofs),
+            "l2": "GPU arm: L2 flushed between steps (256 MiB write); CPU arm: not applicable"}
 
 
 def constraint_intervals(pos, cp_vertices, n_group, rng, n_near=32, n_random=32):
@@ -538,6 +593,7 @@ def main():
     roofline = {"bound": "fp64" if args.precision == "fp64" else "fp32+sfu", "kernel": kname,
                 "achieved": pps * flops / 1e12, "peak": peak_pps * flops / 1e12, "unit": "TFLOP/s",
                 "frac": pps / peak_pps,
+                "fp32_pipe_frac": (pps * flops / FP32_PEAK_FLOPS) if args.precision == "mixed" else None,
                 "traffic": (FORWARD_DRAM_BYTES_PER_LAUNCH if kname == "k_forward_mixed" and args.workload == "contact"
                             else None),
                 "peak_source": ("nominal CUDA-core rates at 1.965 GHz (FP32 74.4 TFLOP/s, SFU 4.65 Tops/s, "
@@ -549,15 +605,12 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
             "data": "synthetic (seeded voxel model and observations)",
-            "config": {"workload": {"batch": WORKLOAD_BATCH.replace("256", str(args.bodies)),
-                                    "large": WORKLOAD_LARGE}.get(args.workload, WORKLOAD),
-                       "triangles": p.n_triangles(), "stations": len(p.grav_xyz),
-                       "dofs": np_, "parallelism": f"replicas x{world}", "l2": "flushed between steps (256 MiB write)",
-                       "precision": args.precision, "fp64_near_pair_fraction": round(near_frac, 4),
-                       "cuda_graph": True,
-                       "tuning": {"fwd_target_blocks": tuned.fwd_target_blocks,
-                                  "grad_target_warps": tuned.grad_target_warps,
-                                  "near_tiles_per_chunk": tuned.near_tiles_per_chunk}},
+            "config": workload_config(args.workload, p.n_triangles(), len(p.grav_xyz), np_, args.bodies),
+            "details": {"parallelism": f"replicas x{world}", "precision": args.precision,
+                        "fp64_near_pair_fraction": round(near_frac, 4), "cuda_graph": True,
+                        "tuning": {"fwd_target_blocks": tuned.fwd_target_blocks,
+                                   "grad_target_warps": tuned.grad_target_warps,
+                                   "near_tiles_per_chunk": tuned.near_tiles_per_chunk}},
             "e2e": {"value": e2e_value, "unit": "evals/s", "h2d_bytes_per_step": 8 * np_,
                     "d2h_bytes_per_step": 8 * (np_ + 1)},
             "gpu_launches": launches, "roofline": roofline}
@@ -572,7 +625,7 @@ def main():
         _, res = ctx.lbfgsb(x0, lo, hi, max_iterations=args.lbfgs_iters)
         wall = time.perf_counter() - t0
         f0 = ctx.objective(x0)
-        line["config"]["lbfgsb"] = {"iterations": res.iterations, "evaluations": res.evaluations,
+        line["details"]["lbfgsb"] = {"iterations": res.iterations, "evaluations": res.evaluations,
                                     "gradients": res.gradients, "wall_s": wall, "objective_start": f0,
                                     "objective_final": res.final_value}
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "contact":

@@ -276,6 +276,15 @@ lf_status lf_mlp_set_engine(lf_mlp* m, int engine);
  * LF_ETIMEOUT if a tensor-core mbarrier wait expired. */
 lf_status lf_gemm_bf16(int engine, int a_trans, int b_trans, int epilogue, int M, int N, int K, const void* A,
                        int lda, const void* B, int ldb, const float* bias, void* C, int ldc, void* stream);
+/* Poll limit of the tensor-core GEMM's main-loop mbarrier waits on the
+ * current device (default 2^24 polls, well under a second; a negative value
+ * restores it).  No counterpart in the reference: failure detection.  A wait
+ * that reaches the limit makes the kernel stop issuing work, wait (with the
+ * full limit) for its own MMAs, free its tensor memory and raise the error
+ * flag that lf_gemm_bf16 / the lf_mlp_* calls report as LF_ETIMEOUT; with 0,
+ * every such wait expires at once, which is how the tests exercise that path.
+ * The device stays usable afterwards. */
+lf_status lf_set_device_wait_limit(long long polls);
 
 /* Stateless parameter scatter (off by default).  The reference's
  * applyParameterVector averages shared vertices from their current positions
@@ -525,11 +534,16 @@ lf_status lf_write_tsurf(const char* path, const char* name, int n_vertices, con
  * Allocates nothing: its scratch is one 8 MiB __device__ array inside the
  * library, so 38*nt + 2*ns must not exceed 1,048,544 (e.g. nt <= 16384 facets
  * with ns <= 212,000 stations); larger sizes return LF_EINVAL.  The first
- * call on a device looks the scratch address up (cudaGetSymbolAddress): make
- * it before any stream capture.  Calls share the scratch, so calls that
- * overlap on the GPU race: serialise them.  Triangle indices outside [0, nv)
- * return LF_EINVAL.  Runs on `stream` (a cudaStream_t, NULL = default stream)
- * and returns after the stream has finished the call. */
+ * call on a device looks the scratch address up (cudaGetSymbolAddress) and
+ * keeps it for the life of the process, so calls after a cudaDeviceReset of
+ * that device are not supported.  Every call reads an error flag back to the
+ * host and waits for its stream, so no call may be made on a stream that is
+ * being captured into a CUDA graph: a capturing stream returns LF_EINVAL.  An
+ * error already pending on the calling thread returns LF_ECUDA (left pending)
+ * before any work is queued.  Calls share the scratch, so calls that overlap
+ * on the GPU race: serialise them.  Triangle indices outside [0, nv) return
+ * LF_EINVAL.  Runs on `stream` (a cudaStream_t, NULL = default stream) and
+ * returns after the stream has finished the call. */
 lf_status lf_forward_noalloc(int nv, const double* d_xyz, int nt, const int32_t* d_tri, int ns,
                              const double* d_sta, double density_gcc, double susceptibility_si,
                              double inc_deg, double dec_deg, double field_nt, double* d_gz,

@@ -120,6 +120,7 @@ SIGNATURES = {
     "lf_mlp_set_engine": (C.c_int, [_vp, C.c_int]),
     "lf_gemm_bf16": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _vp, C.c_int, _vp,
                                C.c_int, _vp, _vp, C.c_int, _vp]),
+    "lf_set_device_wait_limit": (C.c_int, [C.c_longlong]),
     "lf_property_inversion": (C.c_int, [_vp, _dp, C.c_void_p, _dp, _dp]),
     "lf_set_label_grid": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                     C.c_double, C.c_double, _ip]),

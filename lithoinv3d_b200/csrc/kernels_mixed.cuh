@@ -284,9 +284,15 @@ __device__ __forceinline__ void pair_far_f32(const FaceF32* Fp, double ox, doubl
     const float z = (float)(ddx * w1.y + ddy * w2.x + ddz * w2.y);
     const float L0 = v0.w, cx = v1.w, cy = v2.x, L1 = v2.y, L2 = v2.z, gq = v2.w;
     const float z2 = z * z;
-    // gz: n_z * gscale * A * sum_q w_q / r_q
+    // gz: n_z * gscale * A * sum_q w_q / r_q.  A facet with a horizontal unit
+    // normal (n_z == 0 exactly: every vertical face of a voxel-built surface,
+    // which z-only vertex moves keep vertical) has gq == 0 and adds exactly
+    // zero, as in the reference's n_z * (...) product; its quadrature is
+    // skipped.  The facet is the same for every lane, so the branch is
+    // warp-uniform.
     float acc = 0.f;
-    if (RULE == RULE_MID28) {
+    if (gq == 0.f) {
+    } else if (RULE == RULE_MID28) {
 #pragma unroll
         for (int q = 0; q < 28; ++q) {
             float px = fmaf(kRadon4Bb[q], L0, fmaf(kRadon4Bc[q], cx, -x)), py = fmaf(kRadon4Bc[q], cy, -y);
@@ -311,7 +317,7 @@ __device__ __forceinline__ void pair_far_f32(const FaceF32* Fp, double ox, doubl
         }
         acc *= (1.f / 3.f);
     }
-    *gz += gq * acc;
+    if (gq != 0.f) *gz += gq * acc;
     // TMI: MF * Omega + sum_i MT_i Lambda_i with Omega = 2 atan2(ny, den) and
     // Lambda_i = 2 atanh(v_i); the record holds 2 MF and 2 MT_i, so the terms
     // below are atan2 and atanh.  Scaling by 2 is exact: the bits equal

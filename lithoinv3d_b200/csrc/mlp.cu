@@ -407,6 +407,11 @@ extern "C" lf_status lf_mlp_gradients(lf_mlp* m, const float* d_x, const float* 
     return st;
 }
 
+extern "C" lf_status lf_set_device_wait_limit(long long polls) {
+    const long long v = polls < 0 ? kTcWaitLimit : polls;
+    return cudaMemcpyToSymbol(g_tc_stage_wait_limit, &v, sizeof(v)) == cudaSuccess ? LF_OK : LF_ECUDA;
+}
+
 extern "C" lf_status lf_mlp_set_engine(lf_mlp* m, int engine) {
     if (!m || (engine != LF_GEMM_TCGEN05 && engine != LF_GEMM_MMA_SYNC)) return LF_EINVAL;
     m->engine = engine;

@@ -10,11 +10,20 @@
 // What it uses instead of allocations: one file-scope __device__ scratch array
 // of kNoallocScratchBytes (8 MiB).  Every GPU that loads this library holds it
 // until the process exits.  The library looks up its device address once per
-// device with cudaGetSymbolAddress, on the first call made on that device, so
-// make that first call before any stream capture.  All calls share the array
-// and every call overwrites the regions it reads (nothing in it has to start
-// at zero), so calls that overlap on the GPU (two streams, two threads) race
-// on it: serialise them.
+// device with cudaGetSymbolAddress, on the first call made on that device, and
+// keeps it for the life of the process: a cudaDeviceReset of that device
+// invalidates the kept address, so calling this entry point after a device
+// reset is not supported.  All calls share the array and every call
+// overwrites the regions it reads (nothing in it has to start at zero), except
+// the error flag, which each call clears first; calls that overlap on the GPU
+// (two streams, two threads) race on it: serialise them.
+//
+// Every call reads its error flag back into host memory and waits for its
+// stream, neither of which is legal while the stream is being captured into a
+// CUDA graph: the entry point refuses a capturing stream (LF_EINVAL) instead of
+// invalidating the caller's capture.  An error already pending on the calling
+// thread when the call starts (a failed launch of the caller's own) is left in
+// place and reported as LF_ECUDA before any work is queued.
 //
 // The kernels are the library's FP64 forward (facet constants, station-tiled
 // pair kernel, chunk reduction) specialised to one group.
@@ -170,11 +179,17 @@ extern "C" lf_status lf_forward_noalloc(int nv, const double* d_xyz, int nt, con
         cs = (nt + nch - 1) / nch;
         nch = (nt + cs - 1) / cs;
     }
+    // An error left pending by earlier work of the caller is theirs: report it
+    // without clearing it, before queueing anything.
+    if (cudaPeekAtLastError() != cudaSuccess) return LF_ECUDA;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cap) != cudaSuccess) return LF_ECUDA;
+    if (cap != cudaStreamCaptureStatusNone) return LF_EINVAL;  // host read-back and sync cannot be captured
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return LF_ECUDA;
     double* base = nullptr;
     if (scratch_address(dev, &base) != cudaSuccess) return LF_ECUDA;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
     int* err = reinterpret_cast<int*>(base);
     double* fc = base + head;
     double* partG = fc + fcSize;

@@ -41,6 +41,12 @@ constexpr long long kTcWaitLimit = 1ll << 24;   // mbarrier polls before a wait 
 
 // Error flag set by a tensor-core GEMM whose mbarrier wait expired.
 __device__ unsigned int g_tc_gemm_error = 0;
+// Poll limit of the main loop's waits (a stage's MMAs done before the stage
+// is refilled).  Host-settable (lf_set_device_wait_limit) so that the expiry
+// path can be exercised: with 0 every such wait gives up at once.  The final
+// wait for the CTA's own MMAs always uses kTcWaitLimit, so tensor memory is
+// never freed while an MMA of the CTA may still write it.
+__device__ long long g_tc_stage_wait_limit = kTcWaitLimit;
 
 __device__ __forceinline__ uint64_t tc_smem_desc(uint32_t saddr, uint32_t lbo) {
     // start address >> 4 [0,14), leading byte offset >> 4 [16,30) (the K
@@ -60,8 +66,8 @@ __host__ __device__ constexpr uint32_t tc_idesc(int a_mn_major, int b_mn_major, 
 
 // Non-blocking test of the mbarrier phase, polled with a short sleep: the
 // wait gives up after kTcWaitLimit polls (well under a second).
-__device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t parity) {
-    for (long long i = 0; i < kTcWaitLimit; ++i) {
+__device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t parity, long long limit = kTcWaitLimit) {
+    for (long long i = 0; i < limit; ++i) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred P1;\n\t"
@@ -174,7 +180,7 @@ __global__ void __launch_bounds__(kTcThreads) k_gemm_tc(int M, int N, int K, con
         if (nxt < nk) {
             if (kt >= 1) {
                 const int prev = (kt - 1) % kTcStages;
-                if (ok && !tc_wait(bar(prev), ((kt - 1) / kTcStages) & 1)) ok = false;
+                if (ok && !tc_wait(bar(prev), ((kt - 1) / kTcStages) & 1, g_tc_stage_wait_limit)) ok = false;
             }
             if (!__syncthreads_and(ok)) {
                 ok = false;

@@ -460,3 +460,33 @@ def ref_export_ts(directory, base, suffix, xyz, tri):
     t = np.ascontiguousarray(tri, np.int32).reshape(-1, 3)
     ref().ref_export_ts(str(directory).encode(), base.encode(), suffix.encode(), len(x), x.ctypes.data_as(_dp),
                         len(t), t.ctypes.data_as(_ip))
+
+
+def _jacobian_worker(args):
+    tables, densities, susceptibilities, inducing, params, sta, kind = args
+    om = OracleModel(tables, densities, susceptibilities, inducing)
+    om.scatter(params)
+    return om.jacobian(sta, kind)
+
+
+def jacobian_parallel(tables, densities, susceptibilities, inducing, params, sta, kind, procs=None):
+    """OracleModel(...).scatter(params) then .jacobian(sta, kind), split over
+    station chunks in spawned processes (spawned, not forked: the calling
+    process may already hold a CUDA context).  Each process starts from the
+    model's initial positions, like a fresh context evaluated once."""
+    import multiprocessing as mp
+
+    sta = np.ascontiguousarray(sta, np.float64)
+    if procs is None:
+        try:
+            procs = len(os.sched_getaffinity(0))
+        except AttributeError:
+            procs = os.cpu_count() or 1
+    procs = max(1, min(procs, len(sta)))
+    chunks = np.array_split(np.arange(len(sta)), procs)
+    jobs = [(tables, densities, susceptibilities, inducing, params, sta[c], kind) for c in chunks if len(c)]
+    if len(jobs) == 1:
+        return _jacobian_worker(jobs[0])
+    with mp.get_context("spawn").Pool(len(jobs)) as pool:
+        parts = pool.map(_jacobian_worker, jobs)
+    return np.concatenate(parts, axis=0)

@@ -64,3 +64,32 @@ def test_tcgen05_gemm_rejects_bad_shapes():
     st = lib.lf_gemm_bf16(TC, 0, 0, EPI_F32, 128, 128, 96, C.c_void_p(A.data_ptr()), 96, C.c_void_p(B.data_ptr()),
                           128, None, C.c_void_p(Cm.data_ptr()), 128, None)
     assert _native.STATUS[st] == "LF_EINVAL"
+
+
+def test_tcgen05_gemm_wait_expiry_reports_timeout_and_recovers():
+    """Failure detection without a fault: with the main-loop wait limit at 0
+    every stage wait gives up at once, so the kernel abandons the product,
+    drains its own MMAs, frees its tensor memory and raises the error flag;
+    lf_gemm_bf16 returns LF_ETIMEOUT.  With the default limit restored the
+    same call on the same device succeeds and is correct."""
+    lib = _native.load()
+    M, N, K = 256, 512, 576  # 9 K-blocks: more than the stage ring, so refill waits happen
+    g = torch.Generator(device="cuda").manual_seed(5)
+    Am = torch.randn(M, K, generator=g, device="cuda").bfloat16()
+    Bm = torch.randn(K, N, generator=g, device="cuda").bfloat16()
+    bias = torch.zeros(N, device="cuda")
+    Cm = torch.full((M, N), float("nan"), dtype=torch.float32, device="cuda")
+
+    def call():
+        return lib.lf_gemm_bf16(TC, 0, 0, EPI_F32, M, N, K, C.c_void_p(Am.data_ptr()), K, C.c_void_p(Bm.data_ptr()),
+                                N, C.cast(C.c_void_p(bias.data_ptr()), _native._dp), C.c_void_p(Cm.data_ptr()), N,
+                                None)
+
+    try:
+        assert lib.lf_set_device_wait_limit(0) == 0
+        assert call() == 5  # LF_ETIMEOUT
+    finally:
+        assert lib.lf_set_device_wait_limit(-1) == 0
+    assert call() == 0
+    ref = Am.float() @ Bm.float()
+    assert float((Cm - ref).abs().max() / ref.abs().max()) < 2e-5

@@ -88,7 +88,10 @@ def test_writer_matches_reference_exporter(tmp_path):
 
 @needs_ref
 def test_reader_on_real_group_meshes():
-    files = sorted(glob.glob("/root/reference/apps/forrestania/*/baseline/meshes/volume_group_*.ts"))
+    root = os.environ.get("LITHO_REFERENCE")
+    if not root:
+        pytest.skip("LITHO_REFERENCE (the reference tree) is not set")
+    files = sorted(glob.glob(os.path.join(root, "apps/forrestania/*/baseline/meshes/volume_group_*.ts")))
     if not files:
         pytest.skip("reference meshes not present")
     total = 0

@@ -51,6 +51,56 @@ def test_noalloc_forward_matches_allocating_forward():
         assert np.max(np.abs(tmi - tmi_ref)) / np.max(np.abs(tmi_ref)) < TOL, call
 
 
+def test_noalloc_scratch_limited_chunking_and_single_outputs():
+    """A body large enough that the facet constants leave room for fewer
+    facet chunks than the launch would like (27,000 facets x 1,000 stations:
+    room for 11 chunk partials against 74 wanted), so the chunk count is cut
+    to fit the scratch; then each output alone (the other NULL)."""
+    import torch
+
+    lib = _native.load()
+    U, F = synth.latlong_sphere(91, 150)  # 2 * 150 * 90 = 27,000 facets
+    assert len(F) == 27000
+    V = U * 300.0 + np.array([0.0, 0.0, -700.0])
+    st = synth.station_grid(40, 40.0, 1.0, ny=25)  # 1,000 stations
+    p = synth.Problem("sphere27k", [0.25], [0.03], [(V, F, synth.Z_ONLY)], st, st)
+    model = p.build_model()
+    ctx = p.make_context(model)
+    gz_ref, tmi_ref = ctx.forward(model.assemble_parameters())
+    pos = ctx.positions(model.info().n_vertices)
+    tri = model.tables()["tri"]
+    ctx.close()
+    ns, nt = len(st), len(tri)
+    doubles = 1048576 - 32 - 38 * nt
+    room, want = doubles // (2 * ns), (148 * 4 + (ns + 127) // 128 - 1) // ((ns + 127) // 128)
+    assert room < want, (room, want)  # the cut branch runs
+
+    dev = torch.device("cuda", 0)
+    d_xyz = torch.tensor(pos, dtype=torch.float64, device=dev).contiguous()
+    d_tri = torch.tensor(tri, dtype=torch.int32, device=dev).contiguous()
+    d_sta = torch.tensor(st, dtype=torch.float64, device=dev).contiguous()
+    inc, dec, Fld = p.inducing
+
+    def run(want_gz, want_tmi):
+        d_gz = torch.full((ns,), float("nan"), dtype=torch.float64, device=dev)
+        d_tmi = torch.full((ns,), float("nan"), dtype=torch.float64, device=dev)
+        torch.cuda.synchronize()
+        status = lib.lf_forward_noalloc(len(pos), d_xyz.data_ptr(), nt, d_tri.data_ptr(), ns, d_sta.data_ptr(),
+                                        p.densities[0], p.susceptibilities[0], inc, dec, Fld,
+                                        d_gz.data_ptr() if want_gz else None,
+                                        d_tmi.data_ptr() if want_tmi else None, None)
+        assert status == 0, status
+        return d_gz.cpu().numpy(), d_tmi.cpu().numpy()
+
+    gz, tmi = run(True, True)
+    assert np.max(np.abs(gz - gz_ref)) / np.max(np.abs(gz_ref)) < TOL
+    assert np.max(np.abs(tmi - tmi_ref)) / np.max(np.abs(tmi_ref)) < TOL
+    gz_only, untouched = run(True, False)
+    assert np.array_equal(gz_only, gz) and np.all(np.isnan(untouched))
+    untouched, tmi_only = run(False, True)
+    assert np.array_equal(tmi_only, tmi) and np.all(np.isnan(untouched))
+
+
 def test_noalloc_rejects_oversize_and_bad_indices():
     import torch
 
