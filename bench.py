@@ -610,7 +610,8 @@ def main():
                         "fp64_near_pair_fraction": round(near_frac, 4), "cuda_graph": True,
                         "tuning": {"fwd_target_blocks": tuned.fwd_target_blocks,
                                    "grad_target_warps": tuned.grad_target_warps,
-                                   "near_tiles_per_chunk": tuned.near_tiles_per_chunk}},
+                                   "near_tiles_per_chunk": tuned.near_tiles_per_chunk,
+                                   "patch_threads": tuned.patch_threads, "far_ratio": tuned.far_ratio}},
             "e2e": {"value": e2e_value, "unit": "evals/s", "h2d_bytes_per_step": 8 * np_,
                     "d2h_bytes_per_step": 8 * (np_ + 1)},
             "gpu_launches": launches, "roofline": roofline}

@@ -118,6 +118,16 @@ lf_status lf_model_apply_parameters(lf_model* m, const double* params);
 lf_status lf_model_get_positions(lf_model* m, double* xyz);
 
 /* Flat tables (sizes from lf_model_get_info).  Any pointer may be NULL. */
+/* Facet patches of the mixed-precision forward (no reference counterpart;
+ * host only, no device needed): groups of at most 32 facets of one group with
+ * at most 32 distinct corner vertices, over which the forward evaluates each
+ * vertex distance and each edge line integral once per station.  Fills
+ * *n_patches and, for arrays that are not NULL, the patch of every facet
+ * (patch_of_facet[nt]) and each patch's distinct vertex and edge counts
+ * (patch_verts / patch_edges, at least nt entries each). */
+lf_status lf_facet_patches(int nv, const double* xyz, int nt, const int32_t* tri, int n_groups,
+                           const int32_t* grp_tri_off, int* n_patches, int32_t* patch_of_facet,
+                           int32_t* patch_verts, int32_t* patch_edges);
 lf_status lf_model_export_tables(lf_model* m, double* pos, int32_t* tri, int32_t* grp_tri_off,
                                  int32_t* dof_off, int32_t* ref_vertex, uint8_t* ref_axis,
                                  double* ref_scale, int32_t* interp_off, int32_t* interp_src,
@@ -200,21 +210,36 @@ lf_status lf_get_near_pairs(lf_ctx* ctx, unsigned long long* n);
 lf_status lf_forward(lf_ctx* ctx, const double* params, double* gz, double* tmi);
 
 /* Launch shapes of the hot kernels (no reference counterpart).
- *  fwd_target_blocks     forward CTAs per launch: stations/128 x facet chunks;
- *                        more chunks = more CTAs, each over fewer facets
+ *  fwd_target_blocks     forward CTAs per launch (in 128-station units):
+ *                        station blocks x facet (patch) chunks; more chunks =
+ *                        more CTAs, each over fewer facets
  *                        (candidates 148 x {4, 8, 16, 32, 64, 128})
  *  grad_target_warps     gradient warps per launch: DOF facets x station chunks
  *                        (148 x {16, 32, 64, 128, 256})
  *  near_tiles_per_chunk  mixed near-field gradient: 64-station tiles per warp
  *                        (0: the grad_target_warps split; candidates 0, 1, 2, 4, 8)
+ *  patch_threads         stations per CTA of the mixed forward (128 or 256;
+ *                        each CTA walks 32-facet patches, so this is the
+ *                        station x facet tile of one shared-memory stage)
+ *  far_ratio             mixed precision: facet-distance / facet-size ratio tau
+ *                        beyond which a pair is FP32 far field (FP32 28-point
+ *                        mid field from tau/2, FP64 nearer); the same value as
+ *                        lf_set_far_field_ratio.  lf_autotune tries
+ *                        {2, 2.5, 3, 4} and accepts a ratio only if the mixed
+ *                        gz and TMI stay within 0.3e-6 (norm-wise relative) of
+ *                        the FP64 path at params and the gradient within
+ *                        max(0.3e-5, 1.5 x the error at the current ratio)
  * lf_autotune measures candidates on the context's own model, stations and
  * precision, at params, and keeps the fastest; lf_set_tuning / lf_get_tuning
- * set and read them directly.  Results do not depend on the shapes beyond
- * the summation order of partial sums. */
+ * set and read them directly.  Results do not depend on the launch shapes
+ * beyond the summation order of partial sums (far_ratio changes which pairs
+ * run in FP32, within the tolerances above). */
 typedef struct {
     int fwd_target_blocks;
     int grad_target_warps;
     int near_tiles_per_chunk;
+    int patch_threads;
+    double far_ratio;
 } lf_tuning;
 lf_status lf_set_tuning(lf_ctx* ctx, const lf_tuning* t);
 lf_status lf_get_tuning(lf_ctx* ctx, lf_tuning* t);

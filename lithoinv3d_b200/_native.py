@@ -29,7 +29,8 @@ class LbfgsbResult(C.Structure):
 
 
 class Tuning(C.Structure):
-    _fields_ = [("fwd_target_blocks", C.c_int), ("grad_target_warps", C.c_int), ("near_tiles_per_chunk", C.c_int)]
+    _fields_ = [("fwd_target_blocks", C.c_int), ("grad_target_warps", C.c_int), ("near_tiles_per_chunk", C.c_int),
+                ("patch_threads", C.c_int), ("far_ratio", C.c_double)]
 
 
 class PropertyOptions(C.Structure):
@@ -121,6 +122,7 @@ SIGNATURES = {
     "lf_gemm_bf16": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _vp, C.c_int, _vp,
                                C.c_int, _vp, _vp, C.c_int, _vp]),
     "lf_set_device_wait_limit": (C.c_int, [C.c_longlong]),
+    "lf_facet_patches": (C.c_int, [C.c_int, _dp, C.c_int, _ip, C.c_int, _ip, C.POINTER(C.c_int), _ip, _ip, _ip]),
     "lf_property_inversion": (C.c_int, [_vp, _dp, C.c_void_p, _dp, _dp]),
     "lf_set_label_grid": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                     C.c_double, C.c_double, _ip]),

@@ -260,8 +260,13 @@ class Context:
         self._check(self.lib.lf_get_tuning(self.h, C.byref(t)), "get_tuning")
         return t
 
-    def set_tuning(self, fwd_target_blocks: int, grad_target_warps: int, near_tiles_per_chunk: int = 0):
-        t = Tuning(fwd_target_blocks, grad_target_warps, near_tiles_per_chunk)
+    def set_tuning(self, fwd_target_blocks: int, grad_target_warps: int, near_tiles_per_chunk: int = 0,
+                   patch_threads: Optional[int] = None, far_ratio: Optional[float] = None):
+        """lf_set_tuning; patch_threads / far_ratio default to their current values."""
+        cur = self.tuning()
+        t = Tuning(fwd_target_blocks, grad_target_warps, near_tiles_per_chunk,
+                   cur.patch_threads if patch_threads is None else patch_threads,
+                   cur.far_ratio if far_ratio is None else far_ratio)
         self._check(self.lib.lf_set_tuning(self.h, C.byref(t)), "set_tuning")
 
     def autotune(self, params, repeats: int = 3):

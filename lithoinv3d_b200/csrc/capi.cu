@@ -3,8 +3,10 @@
 #include "../../include/litho_gpu.h"
 #include "kernels_classify.cuh"
 #include "kernels_mixed.cuh"
+#include "kernels_patch.cuh"
 #include "lbfgsb.hpp"
 #include "model_builder.hpp"
+#include "patches.hpp"
 
 #include <cuda_runtime.h>
 
@@ -103,6 +105,26 @@ struct lf_ctx {
     DevBuf<FaceF32> d_mf32;  // far-field facet records of the mixed forward [T]
     DevBuf<unsigned long long> d_nearPairs;
     float tau = 3.0f;  // far-field ratio of the mixed path
+
+    // patch forward of the mixed path (kernels_patch.cuh): topology built
+    // once per model, record blobs rewritten every evaluation
+    PatchTopology ptopo;
+    DevBuf<int32_t> d_pFacetOff, d_pFacets, d_pVertOff, d_pVerts, d_pEdgeOff, d_pBlobOff, d_pChunkBegin, d_pChunkEnd;
+    DevBuf<uint32_t> d_pCorners, d_pEdgeInfo;
+    DevBuf<uint8_t> d_pEdgeSlot, d_blobs;
+    DevBuf<unsigned int> d_patchErr;
+    std::vector<int32_t> pchunkBegin, pchunkEnd;
+    int pchunkS = 0, pchunkFilter = -2, pchunkThreads = 0;
+    int64_t pchunkFacets = 0;
+    bool pchunksDirty = true;
+    int patchThreads = 128;  // stations per CTA of the patch forward (lf_tuning.patch_threads)
+    DevBuf<FwdItem> d_pItems;
+    DevBuf<int64_t> d_pGrpPartOff;
+    DevBuf<int32_t> d_pGrpNch;
+    int npItems = 0;
+    int64_t pPartTotal = 0, pItemPairs = 0;
+    uint64_t pItemsEpoch = ~0ull;
+    int pItemsThreads = 0;
     DevBuf<int32_t> d_tri, d_dofOff, d_refVertex, d_interpOff, d_interpSrc, d_interpRows, d_syncOff,
         d_syncVertex, d_vfOff, d_vf, d_gradVerts, d_gradFacets, d_chunkBegin, d_chunkEnd, d_chunkGroup;
     DevBuf<uint8_t> d_refAxis, d_faceNeeds;
@@ -181,7 +203,7 @@ struct lf_ctx {
 
     // launch shapes chosen by lf_autotune (defaults: measured on the
     // 19k-facet, 4096-station contact model)
-    lf_tuning tune{148 * 4, 148 * 64, 0};
+    lf_tuning tune{148 * 4, 148 * 64, 0, 128, 3.0};
 
     // Batched bodies (lf_set_station_groups): each group is one body and
     // sees only its own station range [grpStaOff[g], grpStaOff[g+1]) of both
@@ -419,6 +441,28 @@ extern "C" lf_status lf_model_export_tables(lf_model* m, double* pos, int32_t* t
     return LF_OK;
 }
 
+// Facet patches of the mixed forward for a triangle set (host only; the
+// context builds the same patches in lf_set_model_tables).
+extern "C" lf_status lf_facet_patches(int nv, const double* xyz, int nt, const int32_t* tri, int G,
+                                      const int32_t* grpTriOff, int* nPatches, int32_t* patchOfFacet,
+                                      int32_t* patchVerts, int32_t* patchEdges) {
+    if (nv <= 0 || nt <= 0 || G <= 0 || !xyz || !tri || !grpTriOff || !nPatches) return LF_EINVAL;
+    if (grpTriOff[0] != 0 || grpTriOff[G] != nt) return LF_EINVAL;
+    for (int g = 0; g < G; ++g)
+        if (grpTriOff[g + 1] < grpTriOff[g]) return LF_EINVAL;
+    for (int k = 0; k < 3 * nt; ++k)
+        if (tri[k] < 0 || tri[k] >= nv) return LF_EINVAL;
+    const PatchTopology pt = build_patches(nv, xyz, nt, tri, G, grpTriOff);
+    *nPatches = pt.P;
+    for (int p = 0; p < pt.P; ++p) {
+        if (patchOfFacet)
+            for (int k = pt.facetOff[p]; k < pt.facetOff[p + 1]; ++k) patchOfFacet[pt.facets[k]] = p;
+        if (patchVerts) patchVerts[p] = pt.vertOff[p + 1] - pt.vertOff[p];
+        if (patchEdges) patchEdges[p] = pt.edgeOff[p + 1] - pt.edgeOff[p];
+    }
+    return LF_OK;
+}
+
 // ---------------------------------------------------------------- context --
 extern "C" lf_status lf_create(lf_ctx** out, int device) {
     if (!out) return LF_EINVAL;
@@ -635,6 +679,24 @@ extern "C" lf_status lf_set_model_tables(lf_ctx* c, int G, const double* density
     LF_TRY_CUDA(c, c->d_fc.reserve((size_t)NFC * nt));
     LF_TRY_CUDA(c, c->d_mc.reserve((size_t)NMC * nt));
     LF_TRY_CUDA(c, c->d_mf32.reserve((size_t)nt));
+    {  // facet patches of the mixed forward
+        c->ptopo = build_patches(nv, xyz, nt, tri, G, grpTriOff);
+        const PatchTopology& pt = c->ptopo;
+        LF_TRY_CUDA(c, upload(c->d_pFacetOff, pt.facetOff.data(), pt.facetOff.size(), c->stream));
+        LF_TRY_CUDA(c, upload(c->d_pFacets, pt.facets.data(), pt.facets.size(), c->stream));
+        LF_TRY_CUDA(c, upload(c->d_pCorners, pt.facetCorners.data(), pt.facetCorners.size(), c->stream));
+        LF_TRY_CUDA(c, upload(c->d_pVertOff, pt.vertOff.data(), pt.vertOff.size(), c->stream));
+        LF_TRY_CUDA(c, upload(c->d_pVerts, pt.verts.data(), pt.verts.size(), c->stream));
+        LF_TRY_CUDA(c, upload(c->d_pEdgeOff, pt.edgeOff.data(), pt.edgeOff.size(), c->stream));
+        LF_TRY_CUDA(c, upload(c->d_pEdgeInfo, pt.edgeInfo.data(), pt.edgeInfo.size(), c->stream));
+        LF_TRY_CUDA(c, upload(c->d_pEdgeSlot, pt.edgeSlot.data(), pt.edgeSlot.size(), c->stream));
+        LF_TRY_CUDA(c, upload(c->d_pBlobOff, pt.blobOff.data(), pt.blobOff.size(), c->stream));
+        LF_TRY_CUDA(c, c->d_blobs.reserve((size_t)std::max(pt.blobOff.back(), 16)));
+        LF_TRY_CUDA(c, c->d_patchErr.reserve(1));
+        LF_TRY_CUDA(c, cudaMemsetAsync(c->d_patchErr.p, 0, sizeof(unsigned int), c->stream));
+        c->pchunkS = 0;
+        c->pItemsEpoch = ~0ull;
+    }
     LF_TRY_CUDA(c, c->d_nearPairs.reserve(1));
     LF_TRY_CUDA(c, cudaMemsetAsync(c->d_nearPairs.p, 0, sizeof(unsigned long long), c->stream));
     LF_TRY_CUDA(c, c->d_gc.reserve((size_t)NGC * nt));
@@ -878,6 +940,7 @@ extern "C" lf_status lf_set_far_field_ratio(lf_ctx* c, double tau) {
     if (!c || !std::isfinite(tau)) return LF_EINVAL;
     c->epoch++;
     c->tau = tau <= 0.0 ? 3.0e38f : static_cast<float>(tau);
+    c->tune.far_ratio = tau;
     return LF_OK;
 }
 
@@ -1062,12 +1125,7 @@ static lf_status forward_set_items(lf_ctx* c, const StationSet& s, double* d_gz,
     if (c->nItems > 0) {
         const int grid = std::min(c->nItems, c->tune.fwd_target_blocks);
         int slot = prof_begin(c, c->evFwd, c->nFwd);
-        if (MIXED)
-            k_forward_mixed_items<GZ, TMI, kFwdFacetTile><<<grid, kFwdThreads, 0, c->stream>>>(
-                c->d_items.p, c->nItems, s.d_xyz.p, c->T, c->d_mc.p, c->d_mf32.p, c->tau, GZ ? c->d_partG.p : nullptr,
-                TMI ? c->d_partM.p : nullptr, c->d_nearPairs.p);
-        else
-            k_forward_fp64_items<GZ, TMI, kFwdFacetTile><<<grid, kFwdThreads, 0, c->stream>>>(
+        k_forward_fp64_items<GZ, TMI, kFwdFacetTile><<<grid, kFwdThreads, 0, c->stream>>>(
                 c->d_items.p, c->nItems, s.d_xyz.p, c->T, c->d_fc.p, GZ ? c->d_partG.p : nullptr,
                 TMI ? c->d_partM.p : nullptr);
         prof_end(c, c->evFwd, slot);
@@ -1109,31 +1167,187 @@ static lf_status forward_set(lf_ctx* c, const StationSet& s, double* d_gz, doubl
     return LF_OK;
 }
 
+// Patch chunks of the mixed forward: contiguous patch ranges inside one
+// group (patches never cross groups), sized so that station blocks x chunks
+// fill the GPU.  Honours c->groupFilter like plan_chunks.
+static void plan_patch_chunks(lf_ctx* c, int S) {
+    const int NT = c->patchThreads;
+    if (c->pchunkS == S && c->pchunkFilter == c->groupFilter && c->pchunkThreads == NT && !c->pchunkBegin.empty())
+        return;
+    const PatchTopology& pt = c->ptopo;
+    const int g0 = c->groupFilter >= 0 ? c->groupFilter : 0, g1 = c->groupFilter >= 0 ? c->groupFilter + 1 : c->G;
+    const int np = pt.grpPatchOff[g1] - pt.grpPatchOff[g0];
+    const int sBlocks = std::max(1, cdiv(S, NT));
+    const int want = std::max(1, cdiv((long long)c->tune.fwd_target_blocks * 128 / NT, sBlocks));
+    const int per = std::max(1, cdiv(std::max(np, 1), want));
+    c->pchunkBegin.clear();
+    c->pchunkEnd.clear();
+    for (int g = g0; g < g1; ++g)
+        for (int q = pt.grpPatchOff[g]; q < pt.grpPatchOff[g + 1]; q += per) {
+            c->pchunkBegin.push_back(q);
+            c->pchunkEnd.push_back(std::min(q + per, pt.grpPatchOff[g + 1]));
+        }
+    c->pchunkS = S;
+    c->pchunkFilter = c->groupFilter;
+    c->pchunkThreads = NT;
+    c->pchunkFacets = c->grpTriOff[g1] - c->grpTriOff[g0];
+    c->pchunksDirty = true;
+    c->epoch++;
+}
+
+template <bool GZ, bool TMI, int NT>
+static cudaError_t patch_kernel_attrs() {
+    static const cudaError_t e = [] {
+        cudaError_t a = cudaFuncSetAttribute(k_forward_patch<GZ, TMI, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)sizeof(PatchSmem<NT>));
+        cudaError_t b = cudaFuncSetAttribute(k_forward_patch_items<GZ, TMI, NT>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(PatchSmem<NT>));
+        return a != cudaSuccess ? a : b;
+    }();
+    return e;
+}
+
+// Per-evaluation records of the mixed forward: the per-facet FP64 / FP32
+// records (near and mid facets) and the patch blobs (far facets).
+static lf_status mixed_prep(lf_ctx* c) {
+    k_face_prep_mixed<<<cdiv(c->T, 128), 128, 0, c->stream>>>(c->T, c->d_tri.p, c->d_pos.p, c->d_faceGroup.p,
+                                                              c->d_groups.p, c->fdir, c->d_mc.p, c->d_mf32.p);
+    const PatchTopology& pt = c->ptopo;
+    if (pt.P > 0)
+        k_patch_prep<<<pt.P, 32, 0, c->stream>>>(pt.P, c->d_tri.p, c->d_pos.p, c->d_faceGroup.p, c->d_groups.p,
+                                                  c->fdir, c->d_pFacetOff.p, c->d_pFacets.p, c->d_pCorners.p,
+                                                  c->d_pVertOff.p, c->d_pVerts.p, c->d_pEdgeOff.p, c->d_pEdgeInfo.p,
+                                                  c->d_pEdgeSlot.p, c->d_pBlobOff.p, c->d_blobs.p);
+    c->counters.launches += pt.P > 0 ? 2 : 1;
+    LF_CHECK_LAUNCH(c);
+    return LF_OK;
+}
+
+// Item list of the batched patch forward: (group, station block of NT,
+// patch range) with about 32 items per persistent CTA, largest first.
+static lf_status plan_patch_items(lf_ctx* c) {
+    const int NT = c->patchThreads;
+    if (c->pItemsEpoch == c->planEpoch && c->pItemsThreads == NT) return LF_OK;
+    const int G = c->G;
+    const PatchTopology& pt = c->ptopo;
+    int64_t pairs = 0;
+    for (int g = 0; g < G; ++g)
+        pairs += (int64_t)(c->grpStaOff[g + 1] - c->grpStaOff[g]) * (c->grpTriOff[g + 1] - c->grpTriOff[g]);
+    const int64_t targetItems = 32 * (int64_t)c->tune.fwd_target_blocks * 128 / NT;
+    const double facetsPerPatch = pt.P > 0 ? (double)c->T / pt.P : 1.0;
+    const int per = (int)std::max<int64_t>(1, (int64_t)((double)pairs / ((double)NT * targetItems * facetsPerPatch)));
+    std::vector<FwdItem> items;
+    std::vector<int64_t> partOff(G + 1, 0);
+    std::vector<int32_t> nch(G, 0);
+    int64_t off = 0;
+    for (int g = 0; g < G; ++g) {
+        const int sb = c->grpStaOff[g], se = c->grpStaOff[g + 1], Sg = se - sb;
+        const int pb = pt.grpPatchOff[g], Pg = pt.grpPatchOff[g + 1] - pb;
+        partOff[g] = off;
+        if (Sg == 0 || Pg == 0) continue;
+        nch[g] = cdiv(Pg, per);
+        for (int k = 0; k < nch[g]; ++k)
+            for (int s0 = sb; s0 < se; s0 += NT)
+                items.push_back({s0, std::min(se, s0 + NT), pb + k * per, std::min(pb + Pg, pb + (k + 1) * per),
+                                 off + (int64_t)k * Sg - sb});
+        off += (int64_t)nch[g] * Sg;
+    }
+    partOff[G] = off;
+    std::vector<int64_t> cost(items.size());
+    std::vector<size_t> order(items.size());
+    for (size_t i = 0; i < items.size(); ++i) {
+        const FwdItem& w = items[i];
+        cost[i] = (int64_t)(w.s_end - w.s0) * (pt.facetOff[w.fe] - pt.facetOff[w.fb]);
+        order[i] = i;
+    }
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return cost[a] > cost[b]; });
+    std::vector<FwdItem> sorted(items.size());
+    for (size_t i = 0; i < items.size(); ++i) sorted[i] = items[order[i]];
+    if (!sorted.empty()) LF_TRY_CUDA(c, upload(c->d_pItems, sorted.data(), sorted.size(), c->stream));
+    LF_TRY_CUDA(c, upload(c->d_pGrpPartOff, partOff.data(), partOff.size(), c->stream));
+    LF_TRY_CUDA(c, upload(c->d_pGrpNch, nch.data(), nch.size(), c->stream));
+    c->npItems = static_cast<int>(sorted.size());
+    c->pPartTotal = std::max<int64_t>(off, 1);
+    c->pItemPairs = pairs;
+    c->pItemsEpoch = c->planEpoch;
+    c->pItemsThreads = NT;
+    c->epoch++;
+    return LF_OK;
+}
+
+template <bool GZ, bool TMI, int NT>
+static lf_status launch_patch_items(lf_ctx* c, const StationSet& s, int grid) {
+    LF_TRY_CUDA(c, (patch_kernel_attrs<GZ, TMI, NT>()));
+    k_forward_patch_items<GZ, TMI, NT><<<grid, NT, sizeof(PatchSmem<NT>), c->stream>>>(
+        c->d_pItems.p, c->npItems, s.d_xyz.p, c->d_blobs.p, c->d_pBlobOff.p, c->d_mc.p, c->d_mf32.p, c->T, c->tau,
+        GZ ? c->d_partG.p : nullptr, TMI ? c->d_partM.p : nullptr, c->d_nearPairs.p, c->d_patchErr.p);
+    return LF_OK;
+}
+
+template <bool GZ, bool TMI>
+static lf_status forward_set_patch_items(lf_ctx* c, const StationSet& s, double* d_gz, double* d_tmi) {
+    const int S = s.n;
+    if (S == 0) return LF_OK;
+    LF_RET_IF(plan_patch_items(c));
+    if (GZ) LF_TRY_CUDA(c, c->d_partG.reserve((size_t)c->pPartTotal));
+    if (TMI) LF_TRY_CUDA(c, c->d_partM.reserve((size_t)c->pPartTotal));
+    if (c->npItems > 0) {
+        const int grid = std::min(c->npItems, c->tune.fwd_target_blocks * 128 / c->patchThreads);
+        int slot = prof_begin(c, c->evFwd, c->nFwd);
+        if (c->patchThreads == 256)
+            LF_RET_IF((launch_patch_items<GZ, TMI, 256>(c, s, grid)));
+        else
+            LF_RET_IF((launch_patch_items<GZ, TMI, 128>(c, s, grid)));
+        prof_end(c, c->evFwd, slot);
+    }
+    k_forward_reduce_groups<<<cdiv(S, 32), 256, 0, c->stream>>>(
+        S, c->d_staGroup.p, c->d_grpStaOff.p, c->d_pGrpPartOff.p, c->d_pGrpNch.p, nullptr,
+        GZ ? c->d_partG.p : nullptr, TMI ? c->d_partM.p : nullptr, GZ ? d_gz : nullptr, TMI ? d_tmi : nullptr);
+    c->counters.launches += 2;
+    c->counters.forward_pairs += (uint64_t)c->pItemPairs;
+    LF_CHECK_LAUNCH(c);
+    return LF_OK;
+}
+
+template <bool GZ, bool TMI, int NT>
+static lf_status launch_patch(lf_ctx* c, const StationSet& s, int nch) {
+    LF_TRY_CUDA(c, (patch_kernel_attrs<GZ, TMI, NT>()));
+    dim3 grid(cdiv(s.n, NT), nch);
+    k_forward_patch<GZ, TMI, NT><<<grid, NT, sizeof(PatchSmem<NT>), c->stream>>>(
+        s.n, s.d_xyz.p, c->d_blobs.p, c->d_pBlobOff.p, c->d_pChunkBegin.p, c->d_pChunkEnd.p, c->d_mc.p, c->d_mf32.p,
+        c->T, c->tau, GZ ? c->d_partG.p : nullptr, TMI ? c->d_partM.p : nullptr, c->d_nearPairs.p, c->d_patchErr.p);
+    return LF_OK;
+}
+
 template <bool GZ, bool TMI>
 static lf_status forward_set_mixed(lf_ctx* c, const StationSet& s, double* d_gz, double* d_tmi) {
-    if (c->partitioned) return forward_set_items<GZ, TMI, true>(c, s, d_gz, d_tmi);
+    if (c->partitioned) return forward_set_patch_items<GZ, TMI>(c, s, d_gz, d_tmi);
     int S = s.n;
     if (S == 0) return LF_OK;
-    plan_chunks(c, S);
-    lf_status st = upload_chunks(c);
-    if (st != LF_OK) return st;
-    int nch = static_cast<int>(c->chunkBegin.size());
+    plan_patch_chunks(c, S);
+    if (c->pchunksDirty) {
+        if (!c->pchunkBegin.empty()) {
+            LF_TRY_CUDA(c, upload(c->d_pChunkBegin, c->pchunkBegin.data(), c->pchunkBegin.size(), c->stream));
+            LF_TRY_CUDA(c, upload(c->d_pChunkEnd, c->pchunkEnd.data(), c->pchunkEnd.size(), c->stream));
+        }
+        c->pchunksDirty = false;
+    }
+    int nch = static_cast<int>(c->pchunkBegin.size());
     if (GZ) LF_TRY_CUDA(c, c->d_partG.reserve((size_t)nch * S));
     if (TMI) LF_TRY_CUDA(c, c->d_partM.reserve((size_t)nch * S));
     if (nch > 0) {
-        dim3 grid(cdiv(S, kFwdThreads), nch);
         int slot = prof_begin(c, c->evFwd, c->nFwd);
-        k_forward_mixed<GZ, TMI, kFwdFacetTile><<<grid, kFwdThreads, 0, c->stream>>>(
-            S, s.d_xyz.p, c->T, c->d_mc.p, c->d_mf32.p, c->d_chunkBegin.p, c->d_chunkEnd.p, c->tau,
-            GZ ? c->d_partG.p : nullptr,
-            TMI ? c->d_partM.p : nullptr, c->d_nearPairs.p);
+        if (c->patchThreads == 256)
+            LF_RET_IF((launch_patch<GZ, TMI, 256>(c, s, nch)));
+        else
+            LF_RET_IF((launch_patch<GZ, TMI, 128>(c, s, nch)));
         prof_end(c, c->evFwd, slot);
     }
     k_forward_reduce_mixed<<<cdiv(S, 32), 256, 0, c->stream>>>(S, nch, GZ ? c->d_partG.p : nullptr,
                                                                 TMI ? c->d_partM.p : nullptr, GZ ? d_gz : nullptr,
                                                                 TMI ? d_tmi : nullptr);
     c->counters.launches += 2;
-    c->counters.forward_pairs += (uint64_t)S * (uint64_t)c->chunkFacets;
+    c->counters.forward_pairs += (uint64_t)S * (uint64_t)c->pchunkFacets;
     LF_CHECK_LAUNCH(c);
     return LF_OK;
 }
@@ -1141,10 +1355,7 @@ static lf_status forward_set_mixed(lf_ctx* c, const StationSet& s, double* d_gz,
 // Positions must be current.  Writes grav.d_pred / mag.d_pred.
 static lf_status forward_all(lf_ctx* c) {
     if (c->precision == LF_PREC_MIXED) {
-        k_face_prep_mixed<<<cdiv(c->T, 128), 128, 0, c->stream>>>(c->T, c->d_tri.p, c->d_pos.p, c->d_faceGroup.p,
-                                                                  c->d_groups.p, c->fdir, c->d_mc.p, c->d_mf32.p);
-        c->counters.launches++;
-        LF_CHECK_LAUNCH(c);
+        LF_RET_IF(mixed_prep(c));
         if (c->sameStations) return forward_set_mixed<true, true>(c, c->grav, c->grav.d_pred.p, c->mag.d_pred.p);
         lf_status st = forward_set_mixed<true, false>(c, c->grav, c->grav.d_pred.p, nullptr);
         if (st != LF_OK) return st;
@@ -1468,11 +1679,15 @@ static lf_status run_cached(lf_ctx* c, lf_ctx::GraphSet& set, const double* p, d
 }
 
 extern "C" lf_status lf_set_tuning(lf_ctx* c, const lf_tuning* t) {
-    if (!c || !t || t->fwd_target_blocks < 1 || t->grad_target_warps < 1 || t->near_tiles_per_chunk < 0)
+    if (!c || !t || t->fwd_target_blocks < 1 || t->grad_target_warps < 1 || t->near_tiles_per_chunk < 0 ||
+        (t->patch_threads != 128 && t->patch_threads != 256) || !std::isfinite(t->far_ratio))
         return LF_EINVAL;
     c->epoch++;
     c->tune = *t;
+    c->patchThreads = t->patch_threads;
+    c->tau = t->far_ratio <= 0.0 ? 3.0e38f : static_cast<float>(t->far_ratio);
     c->chunkCapacityS = 0;  // re-plan the forward chunks
+    c->pchunkS = 0;
     c->planEpoch++;
     return LF_OK;
 }
@@ -1483,9 +1698,21 @@ extern "C" lf_status lf_get_tuning(lf_ctx* c, lf_tuning* t) {
     return LF_OK;
 }
 
+// Max-norm relative difference of two host vectors.
+static double rel_diff(const std::vector<double>& a, const std::vector<double>& b) {
+    double num = 0.0, den = 0.0;
+    for (size_t i = 0; i < a.size() && i < b.size(); ++i) {
+        num = std::max(num, std::fabs(a[i] - b[i]));
+        den = std::max(den, std::fabs(b[i]));
+    }
+    return den > 0.0 ? num / den : num;
+}
+
 // Coordinate search over the launch shapes, each candidate timed with device
 // events over `repeats` direct (not replayed) objective+gradient evaluations
-// after one untimed evaluation that sizes buffers and uploads its plan.
+// after one untimed evaluation that sizes buffers and uploads its plan.  In
+// mixed precision the far-field ratio is searched last, each candidate
+// accepted only within its accuracy gate against one FP64 evaluation.
 extern "C" lf_status lf_autotune(lf_ctx* c, const double* params, int repeats, lf_tuning* chosen, double* best_ms) {
     LF_RET_IF(check_ready(c));
     if (repeats <= 0) repeats = 3;
@@ -1510,21 +1737,75 @@ extern "C" lf_status lf_autotune(lf_ctx* c, const double* params, int repeats, l
         *ms = t_ms / repeats;
         return LF_OK;
     };
+    // predictions (both data sets, device order) and gradient of one evaluation
+    auto evaluate = [&](std::vector<double>& pg, std::vector<double>& pm, std::vector<double>& gr) -> lf_status {
+        LF_RET_IF(lf_objective_grad_device(c, c->d_params.p, c->d_f.p, c->d_grad.p));
+        pg.resize(c->grav.n);
+        pm.resize(c->mag.n);
+        gr.resize(c->np);
+        if (c->grav.n)
+            LF_TRY_CUDA(c, cudaMemcpyAsync(pg.data(), c->grav.d_pred.p, sizeof(double) * c->grav.n,
+                                           cudaMemcpyDeviceToHost, c->stream));
+        if (c->mag.n)
+            LF_TRY_CUDA(c, cudaMemcpyAsync(pm.data(), c->mag.d_pred.p, sizeof(double) * c->mag.n,
+                                           cudaMemcpyDeviceToHost, c->stream));
+        if (c->np)
+            LF_TRY_CUDA(c, cudaMemcpyAsync(gr.data(), c->d_grad.p, sizeof(double) * c->np, cudaMemcpyDeviceToHost,
+                                           c->stream));
+        LF_TRY_CUDA(c, cudaStreamSynchronize(c->stream));
+        return LF_OK;
+    };
     lf_tuning best = c->tune;
     double bestMs = 0.0;
     lf_status st = timeit(best, &bestMs);
+    const bool mixed = c->precision == LF_PREC_MIXED;
     const int fwdC[] = {148 * 4, 148 * 8, 148 * 16, 148 * 32, 148 * 64, 148 * 128};
     const int gradC[] = {148 * 16, 148 * 32, 148 * 64, 148 * 128, 148 * 256};
     const int nearC[] = {0, 1, 2, 4, 8};
-    for (int dim = 0; dim < 3 && st == LF_OK; ++dim) {
-        const int* cand = dim == 0 ? fwdC : (dim == 1 ? gradC : nearC);
-        const int nc = dim == 0 ? 6 : 5;
-        if (dim == 2 && c->precision != LF_PREC_MIXED) break;
+    const int threadsC[] = {128, 256};
+    for (int dim = 0; dim < 4 && st == LF_OK; ++dim) {
+        const int* cand = dim == 0 ? fwdC : (dim == 1 ? gradC : (dim == 2 ? nearC : threadsC));
+        const int nc = dim == 0 ? 6 : (dim == 3 ? 2 : 5);
+        if (dim >= 2 && !mixed) break;
         for (int k = 0; k < nc && st == LF_OK; ++k) {
             lf_tuning t = best;
-            int& field = dim == 0 ? t.fwd_target_blocks : (dim == 1 ? t.grad_target_warps : t.near_tiles_per_chunk);
+            int& field = dim == 0 ? t.fwd_target_blocks
+                                  : (dim == 1 ? t.grad_target_warps
+                                              : (dim == 2 ? t.near_tiles_per_chunk : t.patch_threads));
             if (field == cand[k]) continue;
             field = cand[k];
+            double ms = 0.0;
+            st = timeit(t, &ms);
+            if (st == LF_OK && ms < bestMs) {
+                bestMs = ms;
+                best = t;
+            }
+        }
+    }
+    // far-field ratio: accepted only within the accuracy gate against FP64
+    if (st == LF_OK && mixed) {
+        std::vector<double> rg, rm, rgr, g0, m0, gr0, pg, pm, gr;
+        st = lf_set_tuning(c, &best);
+        if (st == LF_OK) {
+            c->precision = LF_PREC_FP64;
+            c->epoch++;
+            st = evaluate(rg, rm, rgr);
+            c->precision = LF_PREC_MIXED;
+            c->epoch++;
+        }
+        if (st == LF_OK) st = evaluate(g0, m0, gr0);  // the current ratio
+        const double gradBase = st == LF_OK ? rel_diff(gr0, rgr) : 0.0;
+        const double ratios[] = {2.0, 2.5, 3.0, 4.0};
+        for (double tau : ratios) {
+            if (st != LF_OK || tau == best.far_ratio) continue;
+            lf_tuning t = best;
+            t.far_ratio = tau;
+            st = lf_set_tuning(c, &t);
+            if (st == LF_OK) st = evaluate(pg, pm, gr);
+            if (st != LF_OK) break;
+            const bool okFwd = rel_diff(pg, rg) <= 0.3e-6 && rel_diff(pm, rm) <= 0.3e-6;
+            const bool okGrad = rel_diff(gr, rgr) <= std::max(0.3e-5, 1.5 * gradBase);
+            if (!okFwd || !okGrad) continue;
             double ms = 0.0;
             st = timeit(t, &ms);
             if (st == LF_OK && ms < bestMs) {
@@ -1847,10 +2128,9 @@ extern "C" lf_status lf_unit_response(lf_ctx* c, const double* params, int kind,
     if (st == LF_OK) {
         c->groupFilter = group;
         if (c->precision == LF_PREC_MIXED) {
-            k_face_prep_mixed<<<cdiv(c->T, 128), 128, 0, c->stream>>>(c->T, c->d_tri.p, c->d_pos.p, c->d_faceGroup.p,
-                                                                      c->d_groups.p, c->fdir, c->d_mc.p, c->d_mf32.p);
-            c->counters.launches++;
-            st = kind == LF_UNIT_GRAVITY ? forward_set_mixed<true, false>(c, s, d_g, d_t)
+            st = mixed_prep(c);
+            if (st == LF_OK)
+                st = kind == LF_UNIT_GRAVITY ? forward_set_mixed<true, false>(c, s, d_g, d_t)
                                          : forward_set_mixed<false, true>(c, s, d_g, d_t);
         } else {
             k_face_prep_fwd<<<cdiv(c->T, 128), 128, 0, c->stream>>>(c->T, c->d_tri.p, c->d_pos.p, c->d_faceGroup.p,

@@ -1,0 +1,499 @@
+// Patch forward of the mixed-precision path: the far field evaluated once per
+// (station, vertex) and once per (station, edge) instead of three times per
+// (station, facet).
+//
+// For a station o and a facet f of a patch (patches.hpp), the reference's
+// facet terms (faceNagyContribution gravity_forward.cpp:13-42, magneticFacet
+// magnetic_forward.cpp:312-347) use
+//   * d_v = |v - o| for the three corners,
+//   * Lambda_e = log((d1 + d2 + L) / (d1 + d2 - L)) = 2 atanh(L / (d1 + d2))
+//     for the three edges (the symmetric form of lineIntegralTerm
+//     geometry.cpp:32-52, equal to the oriented one because d2^2 - d1^2 =
+//     s2^2 - s1^2 along the edge's line),
+//   * Omega_f = 2 atan2(r_a . N, d_a d_b d_c + (r_a.r_b) d_c + (r_a.r_c) d_b
+//     + (r_b.r_c) d_a) (solidAngle geometry.cpp:10-30) with N = (b-a)x(c-a)
+//     and r_a.r_b = (d_a^2 + d_b^2 - |ab|^2) / 2.
+// TMI of the far facets is then sum_e MT_e Lambda_e + sum_f MF_f Omega_f,
+// where MT_e sums the TMI edge coefficients (m.t_i)(f.t_i) (times the group
+// scale) of the patch facets that use edge e: an exact regrouping of the
+// reference's per-facet sum.  gz of a far facet is n_z * G rho * the
+// integral of 1/r over the facet, by Dunavant's 6-point rule (3-point beyond
+// 4 tau x size), skipped when n_z == 0 exactly (a vertical facet: its gz
+// term is zero).  All of this runs in FP32 in a frame centred on the patch's
+// first vertex (the station is moved into it once per patch in FP64).
+// Mid-field facets (tau/2 <= distance / size < tau) keep the per-facet FP32
+// record path and near ones the FP64 path of kernels_mixed.cuh; their edge
+// shares are masked out of MT_e for the warps that see them that close.
+#pragma once
+#include "kernels_mixed.cuh"
+#include "patches.hpp"
+
+namespace litho_b200 {
+
+struct __align__(16) PatchHead {
+    int nv, ne, nf, nbytes;
+    double ox, oy, oz, pad;  // frame origin: the patch's first vertex
+};
+struct __align__(16) PatchVert {
+    float x, y, z, pad;  // position - origin
+};
+struct __align__(16) PatchEdgeA {
+    int lv1, lv2;  // local vertex indices
+    float L;       // edge length
+    float mt;      // doubled TMI edge coefficient, summed over the users
+};
+struct __align__(16) PatchEdgeB {
+    int users;       // lf1 | lf2 << 8 (kNoFacet: none)
+    float mt1, mt2;  // each user's share of mt
+    int pad;
+};
+struct __align__(16) PatchFacet {
+    uint32_t corners;              // local vertex indices a | b << 8 | c << 16
+    float nx, ny, nz;              // N = (b - a) x (c - a) (twice the area times the unit normal)
+    float cf;                      // (a - origin) . N
+    float mf2;                     // doubled TMI solid-angle coefficient (the series gives atan, not 2 atan)
+    float gq;                      // n_z * G rho 1e8 * area (0: no gz term)
+    float size;                    // longest edge; -1: contributes nothing
+    float l2ab, l2bc, l2ca;        // squared edge lengths
+    int gfacet;                    // global facet index (mid / near fallbacks)
+    float cenx, ceny, cenz, pad0;  // centroid (absolute): the near/far test
+    float q3[9];                   // the 3-point rule's points - origin
+    float q6[18];                  // the 6-point rule's points - origin
+    float pad1;
+};
+static_assert(sizeof(PatchHead) == kPatchHeadBytes, "PatchHead");
+static_assert(sizeof(PatchVert) == kPatchVertBytes, "PatchVert");
+static_assert(sizeof(PatchEdgeA) + sizeof(PatchEdgeB) == kPatchEdgeBytes, "PatchEdge");
+static_assert(sizeof(PatchFacet) == kPatchFacetBytes, "PatchFacet");
+static_assert(kPatchMaxBytes % 16 == 0, "bulk copies move multiples of 16 bytes");
+
+// Per-evaluation records: one warp per patch.  Facet constants in the
+// reference's FP64 operation order (as k_face_prep_mixed), then rounded.
+__global__ void __launch_bounds__(32) k_patch_prep(int P, const int32_t* __restrict__ tri,
+                                                   const double* __restrict__ pos,
+                                                   const int16_t* __restrict__ face_group,
+                                                   const GroupConst* __restrict__ groups, d3 fdir,
+                                                   const int32_t* __restrict__ facetOff,
+                                                   const int32_t* __restrict__ facets,
+                                                   const uint32_t* __restrict__ corners,
+                                                   const int32_t* __restrict__ vertOff,
+                                                   const int32_t* __restrict__ verts,
+                                                   const int32_t* __restrict__ edgeOff,
+                                                   const uint32_t* __restrict__ edgeInfo,
+                                                   const uint8_t* __restrict__ edgeSlot,
+                                                   const int32_t* __restrict__ blobOff,
+                                                   unsigned char* __restrict__ blobs) {
+    __shared__ float share[kPatchFacets][3];
+    const int p = blockIdx.x, lane = threadIdx.x;
+    if (p >= P) return;
+    const int f0 = facetOff[p], nf = facetOff[p + 1] - f0;
+    const int v0 = vertOff[p], nv = vertOff[p + 1] - v0;
+    const int e0 = edgeOff[p], ne = edgeOff[p + 1] - e0;
+    unsigned char* B = blobs + blobOff[p];
+    PatchHead* H = reinterpret_cast<PatchHead*>(B);
+    PatchVert* PV = reinterpret_cast<PatchVert*>(B + kPatchHeadBytes);
+    PatchEdgeA* EA = reinterpret_cast<PatchEdgeA*>(B + kPatchHeadBytes + nv * kPatchVertBytes);
+    PatchEdgeB* EB = reinterpret_cast<PatchEdgeB*>(EA + ne);
+    PatchFacet* PF = reinterpret_cast<PatchFacet*>(B + kPatchHeadBytes + nv * kPatchVertBytes + ne * kPatchEdgeBytes);
+    const double* o = pos + 3 * (size_t)verts[v0];
+    const d3 org = mk3(o[0], o[1], o[2]);
+    if (lane == 0) {
+        PatchHead h;
+        h.nv = nv; h.ne = ne; h.nf = nf; h.nbytes = blobOff[p + 1] - blobOff[p];
+        h.ox = org.x; h.oy = org.y; h.oz = org.z; h.pad = 0.0;
+        *H = h;
+    }
+    if (lane < nv) {
+        const double* q = pos + 3 * (size_t)verts[v0 + lane];
+        PatchVert pv;
+        pv.x = (float)(q[0] - org.x); pv.y = (float)(q[1] - org.y); pv.z = (float)(q[2] - org.z); pv.pad = 0.f;
+        PV[lane] = pv;
+    }
+    if (lane < nf) {
+        const int f = facets[f0 + lane];
+        d3 v[3];
+        for (int k = 0; k < 3; ++k) {
+            const double* q = pos + 3 * (size_t)tri[3 * f + k];
+            v[k] = mk3(q[0], q[1], q[2]);
+        }
+        PatchFacet F;
+        F.corners = corners[f0 + lane];
+        F.gfacet = f;
+        F.pad0 = 0.f;
+        F.pad1 = 0.f;
+        const d3 n = cross_rn(sub_rn(v[1], v[0]), sub_rn(v[2], v[0]));
+        const double area2 = norm_rn(n);
+        const bool valid = !(area2 < kEps);
+        double mt[3] = {0.0, 0.0, 0.0}, L[3] = {0.0, 0.0, 0.0}, mfv = 0.0, sgz = 0.0;
+        const GroupConst& g = groups[face_group[f]];
+        for (int i = 0; i < 3; ++i) L[i] = norm_rn(sub_rn(v[(i + 1) % 3], v[i]));
+        if (valid) {
+            const d3 un = div_rn(n, area2);
+            const d3 m = mk3(g.mdir[0], g.mdir[1], g.mdir[2]);
+            mfv = -g.mscale * __dmul_rn(dot_rn(m, un), dot_rn(fdir, un));
+            for (int i = 0; i < 3; ++i) {
+                const d3 e = sub_rn(v[(i + 1) % 3], v[i]);
+                const d3 eh = (L[i] < kEps) ? mk3(0, 0, 0) : div_rn(e, L[i]);
+                const d3 perp = cross_rn(un, eh);
+                mt[i] = -g.mscale * __dmul_rn(dot_rn(m, perp), dot_rn(fdir, perp));
+            }
+            sgz = un.z * g.gscale_fwd;
+        }
+        F.nx = (float)n.x; F.ny = (float)n.y; F.nz = (float)n.z;
+        F.cf = (float)dot3(v[0] - org, n);
+        F.mf2 = (float)(2.0 * mfv);
+        F.gq = (float)(sgz * 0.5 * area2);
+        F.size = valid ? (float)fmax(L[0], fmax(L[1], L[2])) : -1.f;
+        F.l2ab = (float)(L[0] * L[0]); F.l2bc = (float)(L[1] * L[1]); F.l2ca = (float)(L[2] * L[2]);
+        F.cenx = (float)((v[0].x + v[1].x + v[2].x) / 3.0);
+        F.ceny = (float)((v[0].y + v[1].y + v[2].y) / 3.0);
+        F.cenz = (float)((v[0].z + v[1].z + v[2].z) / 3.0);
+        const d3 eb = v[1] - v[0], ec = v[2] - v[0], a0 = v[0] - org;
+        for (int q = 0; q < 3; ++q) {
+            const d3 pq = a0 + eb * (double)kTri3Bb[q] + ec * (double)kTri3Bc[q];
+            F.q3[3 * q] = (float)pq.x; F.q3[3 * q + 1] = (float)pq.y; F.q3[3 * q + 2] = (float)pq.z;
+        }
+        for (int q = 0; q < 6; ++q) {
+            const d3 pq = a0 + eb * (double)kDun6Bb[q] + ec * (double)kDun6Bc[q];
+            F.q6[3 * q] = (float)pq.x; F.q6[3 * q + 1] = (float)pq.y; F.q6[3 * q + 2] = (float)pq.z;
+        }
+        const float4* src = reinterpret_cast<const float4*>(&F);
+        float4* dst = reinterpret_cast<float4*>(PF + lane);
+#pragma unroll
+        for (int k = 0; k < kPatchFacetBytes / 16; ++k) dst[k] = src[k];
+        for (int i = 0; i < 3; ++i) share[lane][i] = (float)(2.0 * mt[i]);
+    }
+    __syncwarp();
+    for (int e = lane; e < ne; e += 32) {
+        const uint32_t info = edgeInfo[e0 + e], slot = edgeSlot[e0 + e];
+        const int lv1 = info & 0xff, lv2 = (info >> 8) & 0xff, lf1 = (info >> 16) & 0xff, lf2 = info >> 24;
+        const float m1 = share[lf1][slot & 3];
+        const float m2 = lf2 != kNoFacet ? share[lf2][(slot >> 2) & 3] : 0.f;
+        const double* qa = pos + 3 * (size_t)verts[v0 + lv1];
+        const double* qb = pos + 3 * (size_t)verts[v0 + lv2];
+        PatchEdgeA a;
+        a.lv1 = lv1; a.lv2 = lv2;
+        a.L = (float)norm3(mk3(qb[0] - qa[0], qb[1] - qa[1], qb[2] - qa[2]));
+        a.mt = m1 + m2;
+        PatchEdgeB b;
+        b.users = lf1 | lf2 << 8; b.mt1 = m1; b.mt2 = m2; b.pad = 0;
+        EA[e] = a;
+        EB[e] = b;
+    }
+}
+
+// ------------------------------------------------------- FP32 primitives --
+// atanh(L / dsum) (half of Lambda).  For v = L / dsum <= 1/4 the Maclaurin
+// series through v^13 (Abramowitz & Stegun 4.1.28), whose first omitted term
+// is below 4e-10 v there; larger arguments take 0.5 log1p(2 v / (1 - v)).
+__device__ __forceinline__ float atanh_half_lambda(float L, float dsum) {
+    const float v = __fdividef(L, dsum);
+    if (v <= 0.25f) {
+        const float v2 = v * v;
+        const float p = fmaf(v2, fmaf(v2, fmaf(v2, fmaf(v2, fmaf(v2, fmaf(v2, 1.f / 13.f, 1.f / 11.f), 1.f / 9.f),
+                                                     1.f / 7.f), 1.f / 5.f), 1.f / 3.f), 1.f);
+        return v * p;
+    }
+    return 0.5f * log1pf(__fdividef(2.f * v, 1.f - v));
+}
+
+// atan(y / x) (half the solid angle): series when x > 0 and |y| <= x / 8,
+// else atan2f.
+__device__ __forceinline__ float atan_half_omega(float y, float x) {
+    if (x > 0.f && fabsf(y) <= 0.125f * x) return atan_series(__fdividef(y, x));
+    return atan2f(y, x);
+}
+
+constexpr long long kPatchWaitLimit = 1ll << 22;  // mbarrier polls for one patch copy (well under a second)
+
+__device__ __forceinline__ uint32_t patch_smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ bool patch_wait(uint32_t mbar, uint32_t parity) {
+    for (long long i = 0; i < kPatchWaitLimit; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred P1;\n\t"
+            "mbarrier.test_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, P1;\n\t}"
+            : "=r"(done)
+            : "r"(mbar), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (i > 16) __nanosleep(64);
+    }
+    return false;
+}
+
+// One patch blob into shared memory by the bulk-copy engine (no multicast:
+// the source is this GPU's own memory).  Called by one thread.
+__device__ __forceinline__ void patch_issue(void* dst, const unsigned char* src, int bytes, uint32_t mbar) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // earlier generic reads of the buffer come first
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     patch_smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(mbar)
+                 : "memory");
+}
+
+template <int NT>
+struct PatchSmem {
+    unsigned char buf[2][kPatchMaxBytes];
+    float dv[kPatchVerts][NT];      // per-station vertex distances of the current patch
+    double nearSlot[NT / 32][NMC];  // one near facet's FP64 constants per warp
+    FaceF32 midSlot[NT / 32];       // one mid facet's FP32 record per warp
+    unsigned long long mbar[2];
+};
+
+// Station block (this thread: station s, live when act) against patches
+// [pb, pe); out_gz[s] / out_tmi[s] receive the sums.  Returns false when a
+// patch copy did not land within the wait limit (block-uniform): the error
+// flag is raised and the block's stations get NaN.
+template <bool GZ, bool TMI, int NT>
+__device__ __forceinline__ bool forward_patch_block(PatchSmem<NT>& sm, int s, bool act,
+                                                    const double* __restrict__ sta,
+                                                    const unsigned char* __restrict__ blobs,
+                                                    const int32_t* __restrict__ blobOff, int pb, int pe,
+                                                    const double* __restrict__ mc, const FaceF32* __restrict__ mf32,
+                                                    int T, float tau, double* __restrict__ out_gz,
+                                                    double* __restrict__ out_tmi,
+                                                    unsigned long long* __restrict__ near_pairs,
+                                                    unsigned int* __restrict__ err, uint32_t& phases) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, tid = threadIdx.x;
+    // inactive lanes evaluate the warp's first live station (results dropped)
+    const unsigned live = __ballot_sync(0xffffffffu, act);
+    const int src = live ? (s - lane + __ffs(live) - 1) : s;
+    double ox = 0.0, oy = 0.0, oz = 0.0;
+    if (act) {
+        ox = sta[3 * s]; oy = sta[3 * s + 1]; oz = sta[3 * s + 2];
+    } else if (live) {
+        ox = sta[3 * src]; oy = sta[3 * src + 1]; oz = sta[3 * src + 2];
+    }
+    float bb[6] = {act ? (float)ox : 3e38f, act ? (float)oy : 3e38f, act ? (float)oz : 3e38f,
+                   act ? -(float)ox : 3e38f, act ? -(float)oy : 3e38f, act ? -(float)oz : 3e38f};
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) bb[k] = fminf(bb[k], __shfl_xor_sync(0xffffffffu, bb[k], off));
+    float* dvp = &sm.dv[0][tid];
+    double gz = 0.0, tmi = 0.0;
+    unsigned long long nearCount = 0;
+    const int nP = pe - pb;
+    const uint32_t mb0 = patch_smem_addr(&sm.mbar[0]), mb1 = patch_smem_addr(&sm.mbar[1]);
+    if (tid == 0 && nP > 0) {
+        const int o0 = __ldg(blobOff + pb);
+        patch_issue(sm.buf[0], blobs + o0, __ldg(blobOff + pb + 1) - o0, mb0);
+    }
+    for (int i = 0; i < nP; ++i) {
+        const int b = i & 1;
+        const bool ok = patch_wait(b ? mb1 : mb0, (phases >> b) & 1u);
+        if (!__syncthreads_and(ok)) {  // every thread is past the previous patch here
+            if (tid == 0) {
+                atomicOr(err, 1u);
+                patch_wait(b ? mb1 : mb0, (phases >> b) & 1u);  // drain the copy in flight before leaving
+            }
+            if (act) {  // the station's sums are incomplete: make that visible
+                if (GZ) out_gz[s] = __longlong_as_double(0x7ff8000000000000ll);
+                if (TMI) out_tmi[s] = __longlong_as_double(0x7ff8000000000000ll);
+            }
+            return false;
+        }
+        phases ^= 1u << b;
+        if (tid == 0 && i + 1 < nP) {  // the other buffer held patch i - 1, which every warp has finished
+            const int o1 = __ldg(blobOff + pb + i + 1);
+            patch_issue(sm.buf[b ^ 1], blobs + o1, __ldg(blobOff + pb + i + 2) - o1, b ? mb0 : mb1);
+        }
+        const unsigned char* B = sm.buf[b];
+        const PatchHead& H = *reinterpret_cast<const PatchHead*>(B);
+        const int nv = H.nv, ne = H.ne, nf = H.nf;
+        const PatchVert* PV = reinterpret_cast<const PatchVert*>(B + kPatchHeadBytes);
+        const PatchEdgeA* EA = reinterpret_cast<const PatchEdgeA*>(B + kPatchHeadBytes + nv * kPatchVertBytes);
+        const PatchEdgeB* EB = reinterpret_cast<const PatchEdgeB*>(EA + ne);
+        const PatchFacet* PF =
+            reinterpret_cast<const PatchFacet*>(B + kPatchHeadBytes + nv * kPatchVertBytes + ne * kPatchEdgeBytes);
+        // lane j: facet j against this warp's station box
+        bool valid = false, vfar = false, far = false, mid = false;
+        if (lane < nf && !(PF[lane].size < 0.f)) {
+            valid = true;
+            const float cxw = PF[lane].cenx, cyw = PF[lane].ceny, czw = PF[lane].cenz;
+            const float ddx = fmaxf(0.f, fmaxf(bb[0] - cxw, cxw + bb[3]));
+            const float ddy = fmaxf(0.f, fmaxf(bb[1] - cyw, cyw + bb[4]));
+            const float ddz = fmaxf(0.f, fmaxf(bb[2] - czw, czw + bb[5]));
+            const float d2 = ddx * ddx + ddy * ddy + ddz * ddz;
+            const float lim = tau * PF[lane].size, limMid = 0.5f * lim;
+            vfar = d2 >= 16.f * (lim * lim);
+            far = !vfar && d2 >= lim * lim;
+            mid = !vfar && !far && d2 >= limMid * limMid;
+        }
+        const unsigned vfarMask = __ballot_sync(0xffffffffu, valid && vfar);
+        const unsigned fastMask = __ballot_sync(0xffffffffu, valid && (vfar || far));
+        const unsigned midMask = __ballot_sync(0xffffffffu, valid && mid);
+        const unsigned nearMask = __ballot_sync(0xffffffffu, valid && !vfar && !far && !mid);
+        if (fastMask) {
+            const float xo = (float)(ox - H.ox), yo = (float)(oy - H.oy), zo = (float)(oz - H.oz);
+            if (TMI) {
+#pragma unroll 4
+                for (int v = 0; v < nv; ++v) {
+                    const float4 q = *reinterpret_cast<const float4*>(PV + v);
+                    const float rx = q.x - xo, ry = q.y - yo, rz = q.z - zo;
+                    const float d2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+                    dvp[v * NT] = d2 * rsqrtf(d2);
+                }
+                float tacc = 0.f;
+                const unsigned excl = midMask | nearMask;
+                if (!excl) {
+#pragma unroll 4
+                    for (int e = 0; e < ne; ++e) {
+                        const PatchEdgeA ea = EA[e];
+                        tacc = fmaf(ea.mt, atanh_half_lambda(ea.L, dvp[ea.lv1 * NT] + dvp[ea.lv2 * NT]), tacc);
+                    }
+                } else {
+                    for (int e = 0; e < ne; ++e) {
+                        const PatchEdgeA ea = EA[e];
+                        const PatchEdgeB eb = EB[e];
+                        const int lf1 = eb.users & 0xff, lf2 = eb.users >> 8;
+                        const float m = ((excl >> lf1) & 1u ? 0.f : eb.mt1) +
+                                        (lf2 != kNoFacet && !((excl >> lf2) & 1u) ? eb.mt2 : 0.f);
+                        if (m != 0.f)
+                            tacc = fmaf(m, atanh_half_lambda(ea.L, dvp[ea.lv1 * NT] + dvp[ea.lv2 * NT]), tacc);
+                    }
+                }
+                for (unsigned m = fastMask; m; m &= m - 1) {
+                    const PatchFacet& F = PF[__ffs(m) - 1];
+                    const uint32_t c = F.corners;
+                    const float da = dvp[(c & 0xff) * NT], db = dvp[((c >> 8) & 0xff) * NT],
+                                dc = dvp[(c >> 16) * NT];
+                    const float da2 = da * da, db2 = db * db, dc2 = dc * dc;
+                    // 2 x the dot products r_a.r_b, r_b.r_c, r_c.r_a from the distances and edge lengths
+                    const float sab = da2 + db2 - F.l2ab, sbc = db2 + dc2 - F.l2bc, sca = dc2 + da2 - F.l2ca;
+                    const float den = fmaf(0.5f, fmaf(sab, dc, fmaf(sbc, da, sca * db)), da * db * dc);
+                    const float num = F.cf - fmaf(xo, F.nx, fmaf(yo, F.ny, zo * F.nz));
+                    tacc = fmaf(F.mf2, atan_half_omega(num, den), tacc);
+                }
+                tmi += tacc;
+            }
+            if (GZ) {
+                float gacc = 0.f;
+                for (unsigned m = fastMask; m; m &= m - 1) {
+                    const int j = __ffs(m) - 1;
+                    const PatchFacet& F = PF[j];
+                    const float gq = F.gq;
+                    if (gq == 0.f) continue;  // horizontal normal: the gz term is zero (warp-uniform)
+                    float acc = 0.f;
+                    if ((vfarMask >> j) & 1u) {
+#pragma unroll
+                        for (int q = 0; q < 3; ++q) {
+                            const float px = F.q3[3 * q] - xo, py = F.q3[3 * q + 1] - yo, pz = F.q3[3 * q + 2] - zo;
+                            acc += rsqrtf(fmaf(px, px, fmaf(py, py, pz * pz)));
+                        }
+                        acc *= (1.f / 3.f);
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < 6; ++q) {
+                            const float px = F.q6[3 * q] - xo, py = F.q6[3 * q + 1] - yo, pz = F.q6[3 * q + 2] - zo;
+                            acc = fmaf(kDun6W[q], rsqrtf(fmaf(px, px, fmaf(py, py, pz * pz))), acc);
+                        }
+                    }
+                    gacc = fmaf(gq, acc, gacc);
+                }
+                gz += gacc;
+            }
+        }
+        // mid facets: the per-facet FP32 record (local frame, 28-point gz,
+        // analytic TMI), fetched into the warp's slot
+        for (unsigned m = midMask; m; m &= m - 1) {
+            const int f = PF[__ffs(m) - 1].gfacet;
+            __syncwarp();
+            if (lane < kFaceF32Vec)
+                reinterpret_cast<float4*>(&sm.midSlot[warp])[lane] =
+                    __ldg(reinterpret_cast<const float4*>(mf32 + f) + lane);
+            __syncwarp();
+            float g1 = 0.f, t1 = 0.f;
+            pair_far_f32<RULE_MID28>(&sm.midSlot[warp], ox, oy, oz, &g1, &t1);
+            if (GZ) gz += g1;
+            if (TMI) tmi += t1;
+        }
+        // near facets: FP64 analytic in the facet's local frame
+        double* slot = sm.nearSlot[warp];
+        for (unsigned m = nearMask; m; m &= m - 1) {
+            const int f = PF[__ffs(m) - 1].gfacet;
+            __syncwarp();
+            if (lane < NMC) slot[lane] = __ldg(mc + (size_t)lane * T + f);
+            __syncwarp();
+            double g1 = 0.0, t1 = 0.0;
+            pair_near_f64(slot, 0, 1, mk3(ox, oy, oz), &g1, &t1);
+            if (GZ) gz += g1;
+            if (TMI) tmi += t1;
+        }
+        nearCount += __popc(nearMask);
+    }
+    if (act) {
+        if (GZ) out_gz[s] = gz;
+        if (TMI) out_tmi[s] = tmi;
+        if (near_pairs && nearCount) atomicAdd(near_pairs, nearCount);
+    }
+    return true;
+}
+
+template <int NT>
+__device__ __forceinline__ PatchSmem<NT>& patch_smem_init() {
+    extern __shared__ __align__(128) unsigned char patch_dyn_smem[];
+    PatchSmem<NT>& sm = *reinterpret_cast<PatchSmem<NT>*>(patch_dyn_smem);
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(patch_smem_addr(&sm.mbar[0])));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(patch_smem_addr(&sm.mbar[1])));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    return sm;
+}
+
+// Station blocks of NT stations (blockIdx.x) x patch chunks (blockIdx.y).
+template <bool GZ, bool TMI, int NT>
+__global__ void __launch_bounds__(NT) k_forward_patch(int S, const double* __restrict__ sta,
+                                                      const unsigned char* __restrict__ blobs,
+                                                      const int32_t* __restrict__ blobOff,
+                                                      const int32_t* __restrict__ chunk_begin,
+                                                      const int32_t* __restrict__ chunk_end,
+                                                      const double* __restrict__ mc,
+                                                      const FaceF32* __restrict__ mf32, int T, float tau,
+                                                      double* __restrict__ part_gz, double* __restrict__ part_tmi,
+                                                      unsigned long long* __restrict__ near_pairs,
+                                                      unsigned int* __restrict__ err) {
+    PatchSmem<NT>& sm = patch_smem_init<NT>();
+    uint32_t phases = 0;
+    const int s = blockIdx.x * NT + threadIdx.x;
+    const int chunk = blockIdx.y;
+    forward_patch_block<GZ, TMI, NT>(sm, s, s < S, sta, blobs, blobOff, chunk_begin[chunk], chunk_end[chunk], mc,
+                                     mf32, T, tau, GZ ? part_gz + (size_t)chunk * S : nullptr,
+                                     TMI ? part_tmi + (size_t)chunk * S : nullptr, near_pairs, err, phases);
+}
+
+// Batched bodies: a persistent grid over (body, station block, patch range)
+// items; FwdItem's facet range holds the patch range.
+template <bool GZ, bool TMI, int NT>
+__global__ void __launch_bounds__(NT) k_forward_patch_items(const FwdItem* __restrict__ items, int nitems,
+                                                            const double* __restrict__ sta,
+                                                            const unsigned char* __restrict__ blobs,
+                                                            const int32_t* __restrict__ blobOff,
+                                                            const double* __restrict__ mc,
+                                                            const FaceF32* __restrict__ mf32, int T, float tau,
+                                                            double* __restrict__ part_gz,
+                                                            double* __restrict__ part_tmi,
+                                                            unsigned long long* __restrict__ near_pairs,
+                                                            unsigned int* __restrict__ err) {
+    PatchSmem<NT>& sm = patch_smem_init<NT>();
+    uint32_t phases = 0;
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const FwdItem w = items[it];
+        const int s = w.s0 + (int)threadIdx.x;
+        if (!forward_patch_block<GZ, TMI, NT>(sm, s, s < w.s_end, sta, blobs, blobOff, w.fb, w.fe, mc, mf32, T,
+                                              tau, GZ ? part_gz + w.out : nullptr, TMI ? part_tmi + w.out : nullptr,
+                                              near_pairs, err, phases))
+            return;  // a copy did not land (block-uniform): leave the remaining items untouched
+        __syncthreads();  // the next item's first copy reuses buffer 0
+    }
+}
+
+}  // namespace litho_b200
