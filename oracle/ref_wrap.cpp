@@ -21,6 +21,8 @@
 #include <litho_invert/regularization/smoothness.h>
 #include <litho_invert/core/geometry.h>
 
+#include "gpu_dropin.hpp"
+
 #include <array>
 #include <cstdint>
 #include <cstring>
@@ -49,12 +51,23 @@ struct RefCtx {
     VectorXd refParams;
     std::shared_ptr<ConstraintHandler> cons;
     bool built = false;
+    // the operators the objective runs on: the reference's own forwards, or
+    // the GPU drop-ins after ref_use_gpu
+    std::shared_ptr<litho_dropin::GpuSession> gpu;
+    std::shared_ptr<ForwardModel> gfwd;
+    std::shared_ptr<MagneticForward> mfwd;
 
     void build() {
         gf = std::make_shared<GravityForward>(model, grav);
         mf = std::make_shared<MagneticForward>(model, mag, inc, dec, field);
         mf->setRemanenceMode(static_cast<RemanentMagnetizationMode>(remMode));
-        gobj = std::make_shared<ObjectiveFunction>(gf, grav);
+        gfwd = gf;
+        mfwd = mf;
+        if (gpu) {
+            gfwd = std::make_shared<litho_dropin::GpuGravityForward>(gpu);
+            mfwd = std::make_shared<litho_dropin::GpuMagneticForward>(gpu, model, mag, inc, dec, field);
+        }
+        gobj = std::make_shared<ObjectiveFunction>(gfwd, grav);
         // the runner registers the smoothness first, then the reference model
         // (runner.cpp:164-179)
         smooth = std::make_shared<SurfaceSmoothness>(model);
@@ -66,7 +79,7 @@ struct RefCtx {
             refReg->captureReference(refParams);
             gobj->addRegularization(refReg);
         }
-        jobj = std::make_shared<JointObjective>(gobj, mag.empty() ? nullptr : mf, mag, alphaMag);
+        jobj = std::make_shared<JointObjective>(gobj, mag.empty() ? nullptr : mfwd, mag, alphaMag);
         built = true;
     }
     void ensure() { if (!built) build(); }
@@ -317,13 +330,13 @@ void ref_group_magnetization(void* h, int g, double* amp, double* dir3) {
 void ref_forward_gz(void* h, const double* params, double* out) {
     auto* c = static_cast<RefCtx*>(h);
     c->ensure();
-    fromVec(c->gf->compute(toVec(static_cast<int>(c->gf->parameterCount()), params)), out);
+    fromVec(c->gfwd->compute(toVec(static_cast<int>(c->gfwd->parameterCount()), params)), out);
 }
 
 void ref_forward_tmi(void* h, const double* params, double* out) {
     auto* c = static_cast<RefCtx*>(h);
     c->ensure();
-    fromVec(c->mf->compute(toVec(static_cast<int>(c->mf->parameterCount()), params)), out);
+    fromVec(c->mfwd->compute(toVec(static_cast<int>(c->mfwd->parameterCount()), params)), out);
 }
 
 // Unit responses at params (kind 0 gravity, 1 induced, 2 direction, 3 remanence).
@@ -558,13 +571,93 @@ void ref_property_inversion(void* h, const double* params, const double* opt, in
 void ref_jacobian_gz(void* h, const double* params, double* J) {
     auto* c = static_cast<RefCtx*>(h);
     c->ensure();
-    fromMat(c->gf->computeJacobian(toVec(static_cast<int>(c->gf->parameterCount()), params)), J);
+    fromMat(c->gfwd->computeJacobian(toVec(static_cast<int>(c->gfwd->parameterCount()), params)), J);
 }
 
 void ref_jacobian_tmi(void* h, const double* params, double* J) {
     auto* c = static_cast<RefCtx*>(h);
     c->ensure();
-    fromMat(c->mf->computeJacobian(toVec(static_cast<int>(c->mf->parameterCount()), params)), J);
+    fromMat(c->mfwd->computeJacobian(toVec(static_cast<int>(c->mfwd->parameterCount()), params)), J);
+}
+
+// Switches this model's objective to the GPU drop-in operators
+// (gpu_dropin.hpp): opens liblitho_gpu.so at `lib_path`, creates a context on
+// `device` and uploads the reference model's groups, meshes and DOF tables
+// (built here from the reference's own dofMappings / globalDofIndex, as
+// ref_dof_tables does), the inducing field and both station sets.  The
+// control-point interpolation rows and shared-vertex groups are private in
+// the reference; a model that has them passes them in (interp_* / sync_*,
+// NULL otherwise).  Call after the model and the data are set.  Returns 0 on
+// success, -1 if the library cannot be opened, else the lf_status.
+int ref_use_gpu(void* h, const char* lib_path, int device, int precision, const int32_t* interp_off,
+                const int32_t* interp_src, const double* interp_w, int n_sync, const int32_t* sync_off,
+                const int32_t* sync_vertex) {
+    auto* c = static_cast<RefCtx*>(h);
+    auto s = std::make_shared<litho_dropin::GpuSession>();
+    if (!s->api.open(lib_path)) return -1;
+    lf_status st = s->api.create(&s->ctx, device);
+    if (st != LF_OK) return st;
+    auto& M = *c->model;
+    const int G = M.groupCount();
+    std::vector<double> rho(G), chi(G), rm(G), ri(G), rd(G), rv(3 * G);
+    for (int g = 0; g < G; ++g) {
+        const LithoGroup& gr = M.group(g);
+        rho[g] = gr.density; chi[g] = gr.susceptibility; rm[g] = gr.remanence_magnitude;
+        ri[g] = gr.remanence_inclination; rd[g] = gr.remanence_declination;
+        rv[3 * g] = gr.magnetization.x(); rv[3 * g + 1] = gr.magnetization.y(); rv[3 * g + 2] = gr.magnetization.z();
+    }
+    std::vector<double> xyz;
+    std::vector<int32_t> tri, grpTriOff(1, 0);
+    int vbase = 0;
+    for (int g = 0; g < G; ++g) {
+        const SurfaceMesh* mesh = g < M.groupMeshCount() ? M.groupMesh(g) : nullptr;
+        if (mesh) {
+            for (uint32_t v = 0; v < mesh->vertexCount(); ++v) {
+                const auto& p = mesh->vertex(v).position;
+                xyz.push_back(p.x()); xyz.push_back(p.y()); xyz.push_back(p.z());
+            }
+            for (uint32_t t = 0; t < mesh->triangleCount(); ++t) {
+                const auto& tr = mesh->triangle(t);
+                tri.push_back(vbase + static_cast<int32_t>(tr.v0));
+                tri.push_back(vbase + static_cast<int32_t>(tr.v1));
+                tri.push_back(vbase + static_cast<int32_t>(tr.v2));
+            }
+            vbase += static_cast<int>(mesh->vertexCount());
+        }
+        grpTriOff.push_back(static_cast<int32_t>(tri.size() / 3));
+    }
+    const int np = static_cast<int>(M.totalDofCount());
+    std::vector<int32_t> dofOff(np + 1), refVertex(3 * (size_t)vbase + 8);
+    std::vector<uint8_t> refAxis(3 * (size_t)vbase + 8);
+    std::vector<double> refScale(3 * (size_t)vbase + 8);
+    ref_dof_tables(h, dofOff.data(), refVertex.data(), refAxis.data(), refScale.data());
+    st = s->api.set_model_tables(s->ctx, G, rho.data(), chi.data(), rm.data(), ri.data(), rd.data(), rv.data(), vbase,
+                                 xyz.data(), static_cast<int>(tri.size() / 3), tri.data(), grpTriOff.data(), np,
+                                 dofOff.data(), refVertex.data(), refAxis.data(), refScale.data(), interp_off,
+                                 interp_src, interp_w, n_sync, sync_off, sync_vertex);
+    if (st == LF_OK) st = s->api.set_field(s->ctx, c->inc, c->dec, c->field, c->remMode);
+    auto upload = [&](auto& data, auto fn, auto value, auto sigma) {
+        std::vector<double> p, o, sd;
+        for (const auto& d : data) {
+            p.push_back(d.position.x()); p.push_back(d.position.y()); p.push_back(d.position.z());
+            o.push_back(value(d)); sd.push_back(sigma(d));
+        }
+        return fn(s->ctx, static_cast<int>(data.size()), p.data(), o.data(), sd.data());
+    };
+    if (st == LF_OK)
+        st = upload(c->grav, s->api.set_gravity_data, [](const GravityPoint& d) { return d.g_obs; },
+                    [](const GravityPoint& d) { return d.g_std; });
+    if (st == LF_OK)
+        st = upload(c->mag, s->api.set_magnetic_data, [](const MagneticPoint& d) { return d.t_obs; },
+                    [](const MagneticPoint& d) { return d.t_std; });
+    if (st == LF_OK) st = s->api.set_precision(s->ctx, precision);
+    if (st != LF_OK) return st;
+    s->ng = static_cast<int>(c->grav.size());
+    s->nm = static_cast<int>(c->mag.size());
+    s->np = np;
+    c->gpu = s;
+    c->built = false;
+    return 0;
 }
 
 // JointObjective::evaluateComponents (joint_objective.cpp:113-173):

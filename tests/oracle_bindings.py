@@ -129,6 +129,7 @@ def ref() -> C.CDLL:
             "ref_set_constraints": (None, [V, C.c_int, _dp, _dp, _dp, _ip, C.c_double]),
             "ref_constraint_value": (C.c_double, [V, _dp]),
             "ref_constraint_gradient": (None, [V, _dp, _dp]),
+            "ref_use_gpu": (C.c_int, [V, C.c_char_p, C.c_int, C.c_int, _ip, _ip, _dp, C.c_int, _ip, _ip]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -319,6 +320,25 @@ class RefModel:
         d = np.zeros(3)
         self.lib.ref_group_magnetization(self.h, g, amp.ctypes.data_as(_dp), d.ctypes.data_as(_dp))
         return float(amp[0]), d
+
+    def use_gpu(self, lib_path, device=0, precision=0, tables=None):
+        """Runs this model's objective on the GPU drop-in operators
+        (oracle/gpu_dropin.hpp) over liblitho_gpu.so at lib_path.  `tables`
+        (the library builder's tables) supplies the control-point and
+        shared-vertex rows the reference keeps private; None for models
+        without them.  Call after the data are set."""
+        io = isrc = iw = so = sv = None
+        ns = 0
+        if tables is not None:
+            self._keep = [np.ascontiguousarray(tables[k]) for k in
+                          ("interp_off", "interp_src", "interp_w", "sync_off", "sync_vertex")]
+            io, isrc, iw, so, sv = self._keep
+            ns = len(so) - 1
+            io, isrc, so, sv = (a.ctypes.data_as(_ip) for a in (io, isrc, so, sv))
+            iw = iw.ctypes.data_as(_dp)
+        st = self.lib.ref_use_gpu(self.h, str(lib_path).encode(), device, precision, io, isrc, iw, ns, so, sv)
+        if st != 0:
+            raise RuntimeError(f"ref_use_gpu failed: {st}")
 
     def lbfgsb(self, x0, lo, hi, max_iter=30, ftol=1e-6, history=10):
         x = np.zeros(self.np)
