@@ -102,7 +102,6 @@ struct lf_ctx {
     std::vector<GroupConst> gconst;
 
     DevBuf<double> d_pos, d_fc, d_gc, d_mc, d_params, d_grad, d_vgrad, d_out5, d_f, d_refp;
-    DevBuf<FaceF32> d_mf32;  // far-field facet records of the mixed forward [T]
     DevBuf<unsigned long long> d_nearPairs;
     float tau = 3.0f;  // far-field ratio of the mixed path
 
@@ -678,7 +677,6 @@ extern "C" lf_status lf_set_model_tables(lf_ctx* c, int G, const double* density
     LF_TRY_CUDA(c, upload(c->d_faceNeeds, fneed.data(), fneed.size(), c->stream));
     LF_TRY_CUDA(c, c->d_fc.reserve((size_t)NFC * nt));
     LF_TRY_CUDA(c, c->d_mc.reserve((size_t)NMC * nt));
-    LF_TRY_CUDA(c, c->d_mf32.reserve((size_t)nt));
     {  // facet patches of the mixed forward
         c->ptopo = build_patches(nv, xyz, nt, tri, G, grpTriOff);
         const PatchTopology& pt = c->ptopo;
@@ -1211,7 +1209,7 @@ static cudaError_t patch_kernel_attrs() {
 // records (near and mid facets) and the patch blobs (far facets).
 static lf_status mixed_prep(lf_ctx* c) {
     k_face_prep_mixed<<<cdiv(c->T, 128), 128, 0, c->stream>>>(c->T, c->d_tri.p, c->d_pos.p, c->d_faceGroup.p,
-                                                              c->d_groups.p, c->fdir, c->d_mc.p, c->d_mf32.p);
+                                                              c->d_groups.p, c->fdir, c->d_mc.p);
     const PatchTopology& pt = c->ptopo;
     if (pt.P > 0)
         k_patch_prep<<<pt.P, 32, 0, c->stream>>>(pt.P, c->d_tri.p, c->d_pos.p, c->d_faceGroup.p, c->d_groups.p,
@@ -1279,7 +1277,7 @@ template <bool GZ, bool TMI, int NT>
 static lf_status launch_patch_items(lf_ctx* c, const StationSet& s, int grid) {
     LF_TRY_CUDA(c, (patch_kernel_attrs<GZ, TMI, NT>()));
     k_forward_patch_items<GZ, TMI, NT><<<grid, NT, sizeof(PatchSmem<NT>), c->stream>>>(
-        c->d_pItems.p, c->npItems, s.d_xyz.p, c->d_blobs.p, c->d_pBlobOff.p, c->d_mc.p, c->d_mf32.p, c->T, c->tau,
+        c->d_pItems.p, c->npItems, s.d_xyz.p, c->d_blobs.p, c->d_pBlobOff.p, c->d_mc.p, c->T, c->tau,
         GZ ? c->d_partG.p : nullptr, TMI ? c->d_partM.p : nullptr, c->d_nearPairs.p, c->d_patchErr.p);
     return LF_OK;
 }
@@ -1314,8 +1312,7 @@ static lf_status launch_patch(lf_ctx* c, const StationSet& s, int nch) {
     LF_TRY_CUDA(c, (patch_kernel_attrs<GZ, TMI, NT>()));
     dim3 grid(cdiv(s.n, NT), nch);
     k_forward_patch<GZ, TMI, NT><<<grid, NT, sizeof(PatchSmem<NT>), c->stream>>>(
-        s.n, s.d_xyz.p, c->d_blobs.p, c->d_pBlobOff.p, c->d_pChunkBegin.p, c->d_pChunkEnd.p, c->d_mc.p, c->d_mf32.p,
-        c->T, c->tau, GZ ? c->d_partG.p : nullptr, TMI ? c->d_partM.p : nullptr, c->d_nearPairs.p, c->d_patchErr.p);
+        s.n, s.d_xyz.p, c->d_blobs.p, c->d_pBlobOff.p, c->d_pChunkBegin.p, c->d_pChunkEnd.p, c->d_mc.p, c->T, c->tau, GZ ? c->d_partG.p : nullptr, TMI ? c->d_partM.p : nullptr, c->d_nearPairs.p, c->d_patchErr.p);
     return LF_OK;
 }
 

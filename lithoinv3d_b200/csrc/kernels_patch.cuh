@@ -242,7 +242,6 @@ struct PatchSmem {
     unsigned char buf[2][kPatchMaxBytes];
     float dv[kPatchVerts][NT];      // per-station vertex distances of the current patch
     double nearSlot[NT / 32][NMC];  // one near facet's FP64 constants per warp
-    FaceF32 midSlot[NT / 32];       // one mid facet's FP32 record per warp
     unsigned long long mbar[2];
 };
 
@@ -255,8 +254,7 @@ __device__ __forceinline__ bool forward_patch_block(PatchSmem<NT>& sm, int s, bo
                                                     const double* __restrict__ sta,
                                                     const unsigned char* __restrict__ blobs,
                                                     const int32_t* __restrict__ blobOff, int pb, int pe,
-                                                    const double* __restrict__ mc, const FaceF32* __restrict__ mf32,
-                                                    int T, float tau, double* __restrict__ out_gz,
+                                                    const double* __restrict__ mc, int T, float tau, double* __restrict__ out_gz,
                                                     double* __restrict__ out_tmi,
                                                     unsigned long long* __restrict__ near_pairs,
                                                     unsigned int* __restrict__ err, uint32_t& phases) {
@@ -327,8 +325,8 @@ __device__ __forceinline__ bool forward_patch_block(PatchSmem<NT>& sm, int s, bo
             mid = !vfar && !far && d2 >= limMid * limMid;
         }
         const unsigned vfarMask = __ballot_sync(0xffffffffu, valid && vfar);
-        const unsigned fastMask = __ballot_sync(0xffffffffu, valid && (vfar || far));
         const unsigned midMask = __ballot_sync(0xffffffffu, valid && mid);
+        const unsigned fastMask = __ballot_sync(0xffffffffu, valid && (vfar || far || mid));
         const unsigned nearMask = __ballot_sync(0xffffffffu, valid && !vfar && !far && !mid);
         if (fastMask) {
             const float xo = (float)(ox - H.ox), yo = (float)(oy - H.oy), zo = (float)(oz - H.oz);
@@ -341,7 +339,7 @@ __device__ __forceinline__ bool forward_patch_block(PatchSmem<NT>& sm, int s, bo
                     dvp[v * NT] = d2 * rsqrtf(d2);
                 }
                 float tacc = 0.f;
-                const unsigned excl = midMask | nearMask;
+                const unsigned excl = nearMask;
                 if (!excl) {
 #pragma unroll 4
                     for (int e = 0; e < ne; ++e) {
@@ -360,16 +358,17 @@ __device__ __forceinline__ bool forward_patch_block(PatchSmem<NT>& sm, int s, bo
                     }
                 }
                 for (unsigned m = fastMask; m; m &= m - 1) {
-                    const PatchFacet& F = PF[__ffs(m) - 1];
-                    const uint32_t c = F.corners;
+                    const float4* F4 = reinterpret_cast<const float4*>(PF + (__ffs(m) - 1));
+                    const float4 w0 = F4[0], w1 = F4[1], w2 = F4[2];  // corners, N | cf, mf2 | squared edges
+                    const uint32_t c = __float_as_uint(w0.x);
                     const float da = dvp[(c & 0xff) * NT], db = dvp[((c >> 8) & 0xff) * NT],
                                 dc = dvp[(c >> 16) * NT];
                     const float da2 = da * da, db2 = db * db, dc2 = dc * dc;
                     // 2 x the dot products r_a.r_b, r_b.r_c, r_c.r_a from the distances and edge lengths
-                    const float sab = da2 + db2 - F.l2ab, sbc = db2 + dc2 - F.l2bc, sca = dc2 + da2 - F.l2ca;
+                    const float sab = da2 + db2 - w2.x, sbc = db2 + dc2 - w2.y, sca = dc2 + da2 - w2.z;
                     const float den = fmaf(0.5f, fmaf(sab, dc, fmaf(sbc, da, sca * db)), da * db * dc);
-                    const float num = F.cf - fmaf(xo, F.nx, fmaf(yo, F.ny, zo * F.nz));
-                    tacc = fmaf(F.mf2, atan_half_omega(num, den), tacc);
+                    const float num = w1.x - fmaf(xo, w0.y, fmaf(yo, w0.z, zo * w0.w));
+                    tacc = fmaf(w1.y, atan_half_omega(num, den), tacc);
                 }
                 tmi += tacc;
             }
@@ -377,42 +376,53 @@ __device__ __forceinline__ bool forward_patch_block(PatchSmem<NT>& sm, int s, bo
                 float gacc = 0.f;
                 for (unsigned m = fastMask; m; m &= m - 1) {
                     const int j = __ffs(m) - 1;
-                    const PatchFacet& F = PF[j];
-                    const float gq = F.gq;
+                    const float4* F4 = reinterpret_cast<const float4*>(PF + j);
+                    const float gq = F4[1].z;
                     if (gq == 0.f) continue;  // horizontal normal: the gz term is zero (warp-uniform)
-                    float acc = 0.f;
-                    if ((vfarMask >> j) & 1u) {
+                    // floats 16..42 of the record: q3[9] then q6[18]
+                    float q[28];
 #pragma unroll
-                        for (int q = 0; q < 3; ++q) {
-                            const float px = F.q3[3 * q] - xo, py = F.q3[3 * q + 1] - yo, pz = F.q3[3 * q + 2] - zo;
+                    for (int k = 0; k < 7; ++k) {
+                        const float4 w = F4[4 + k];
+                        q[4 * k] = w.x; q[4 * k + 1] = w.y; q[4 * k + 2] = w.z; q[4 * k + 3] = w.w;
+                    }
+                    float acc = 0.f;
+                    if ((midMask >> j) & 1u) {
+                        // Radon's 7-point rule on the four midpoint sub-triangles
+                        // (28 points), built from the patch-frame corners
+                        const uint32_t c = __float_as_uint(F4[0].x);
+                        const float4 pa = *reinterpret_cast<const float4*>(PV + (c & 0xff));
+                        const float4 pb = *reinterpret_cast<const float4*>(PV + ((c >> 8) & 0xff));
+                        const float4 pc = *reinterpret_cast<const float4*>(PV + (c >> 16));
+                        const float ax = pa.x - xo, ay = pa.y - yo, az = pa.z - zo;
+                        const float bx = pb.x - pa.x, by = pb.y - pa.y, bz = pb.z - pa.z;
+                        const float cx = pc.x - pa.x, cy = pc.y - pa.y, cz = pc.z - pa.z;
+#pragma unroll 7
+                        for (int k = 0; k < 28; ++k) {
+                            const float u = kRadon4Bb[k], w = kRadon4Bc[k];
+                            const float px = fmaf(u, bx, fmaf(w, cx, ax)), py = fmaf(u, by, fmaf(w, cy, ay)),
+                                        pz = fmaf(u, bz, fmaf(w, cz, az));
+                            acc = fmaf(kRadonW[k % 7], rsqrtf(fmaf(px, px, fmaf(py, py, pz * pz))), acc);
+                        }
+                        acc *= 0.25f;
+                    } else if ((vfarMask >> j) & 1u) {
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) {
+                            const float px = q[3 * k] - xo, py = q[3 * k + 1] - yo, pz = q[3 * k + 2] - zo;
                             acc += rsqrtf(fmaf(px, px, fmaf(py, py, pz * pz)));
                         }
                         acc *= (1.f / 3.f);
                     } else {
 #pragma unroll
-                        for (int q = 0; q < 6; ++q) {
-                            const float px = F.q6[3 * q] - xo, py = F.q6[3 * q + 1] - yo, pz = F.q6[3 * q + 2] - zo;
-                            acc = fmaf(kDun6W[q], rsqrtf(fmaf(px, px, fmaf(py, py, pz * pz))), acc);
+                        for (int k = 0; k < 6; ++k) {
+                            const float px = q[9 + 3 * k] - xo, py = q[10 + 3 * k] - yo, pz = q[11 + 3 * k] - zo;
+                            acc = fmaf(kDun6W[k], rsqrtf(fmaf(px, px, fmaf(py, py, pz * pz))), acc);
                         }
                     }
                     gacc = fmaf(gq, acc, gacc);
                 }
                 gz += gacc;
             }
-        }
-        // mid facets: the per-facet FP32 record (local frame, 28-point gz,
-        // analytic TMI), fetched into the warp's slot
-        for (unsigned m = midMask; m; m &= m - 1) {
-            const int f = PF[__ffs(m) - 1].gfacet;
-            __syncwarp();
-            if (lane < kFaceF32Vec)
-                reinterpret_cast<float4*>(&sm.midSlot[warp])[lane] =
-                    __ldg(reinterpret_cast<const float4*>(mf32 + f) + lane);
-            __syncwarp();
-            float g1 = 0.f, t1 = 0.f;
-            pair_far_f32<RULE_MID28>(&sm.midSlot[warp], ox, oy, oz, &g1, &t1);
-            if (GZ) gz += g1;
-            if (TMI) tmi += t1;
         }
         // near facets: FP64 analytic in the facet's local frame
         double* slot = sm.nearSlot[warp];
@@ -456,8 +466,7 @@ __global__ void __launch_bounds__(NT) k_forward_patch(int S, const double* __res
                                                       const int32_t* __restrict__ blobOff,
                                                       const int32_t* __restrict__ chunk_begin,
                                                       const int32_t* __restrict__ chunk_end,
-                                                      const double* __restrict__ mc,
-                                                      const FaceF32* __restrict__ mf32, int T, float tau,
+                                                      const double* __restrict__ mc, int T, float tau,
                                                       double* __restrict__ part_gz, double* __restrict__ part_tmi,
                                                       unsigned long long* __restrict__ near_pairs,
                                                       unsigned int* __restrict__ err) {
@@ -466,7 +475,7 @@ __global__ void __launch_bounds__(NT) k_forward_patch(int S, const double* __res
     const int s = blockIdx.x * NT + threadIdx.x;
     const int chunk = blockIdx.y;
     forward_patch_block<GZ, TMI, NT>(sm, s, s < S, sta, blobs, blobOff, chunk_begin[chunk], chunk_end[chunk], mc,
-                                     mf32, T, tau, GZ ? part_gz + (size_t)chunk * S : nullptr,
+                                     T, tau, GZ ? part_gz + (size_t)chunk * S : nullptr,
                                      TMI ? part_tmi + (size_t)chunk * S : nullptr, near_pairs, err, phases);
 }
 
@@ -477,8 +486,7 @@ __global__ void __launch_bounds__(NT) k_forward_patch_items(const FwdItem* __res
                                                             const double* __restrict__ sta,
                                                             const unsigned char* __restrict__ blobs,
                                                             const int32_t* __restrict__ blobOff,
-                                                            const double* __restrict__ mc,
-                                                            const FaceF32* __restrict__ mf32, int T, float tau,
+                                                            const double* __restrict__ mc, int T, float tau,
                                                             double* __restrict__ part_gz,
                                                             double* __restrict__ part_tmi,
                                                             unsigned long long* __restrict__ near_pairs,
@@ -488,7 +496,7 @@ __global__ void __launch_bounds__(NT) k_forward_patch_items(const FwdItem* __res
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
         const FwdItem w = items[it];
         const int s = w.s0 + (int)threadIdx.x;
-        if (!forward_patch_block<GZ, TMI, NT>(sm, s, s < w.s_end, sta, blobs, blobOff, w.fb, w.fe, mc, mf32, T,
+        if (!forward_patch_block<GZ, TMI, NT>(sm, s, s < w.s_end, sta, blobs, blobOff, w.fb, w.fe, mc, T,
                                               tau, GZ ? part_gz + w.out : nullptr, TMI ? part_tmi + w.out : nullptr,
                                               near_pairs, err, phases))
             return;  // a copy did not land (block-uniform): leave the remaining items untouched

@@ -310,10 +310,19 @@ def main():
     ap.add_argument("--heldout", type=int, default=64)
     ap.add_argument("--epochs", type=int, default=60)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--out", default=None, help="also write the summary and the per-model runs to this JSON file")
     a = ap.parse_args()
-    p = synth.voxel_contact_model(shape=(16, 16, 8), cell=150.0, n_side=64, cp_stride=0)
+    # the config-2 family: 4 groups on 24 x 24 x 12 voxels of 100 m, control-point
+    # stride 4, 64 x 64 stations (2 x 64 x 64 residual inputs)
+    p = synth.voxel_contact_model()
     out = experiment(p, a.pairs, a.heldout, a.epochs, a.seed)
-    out.pop("runs")
+    out["model"] = dict(triangles=p.n_triangles(), stations=len(p.grav_xyz), width=512, depth=4)
+    runs = out.pop("runs")
+    out["per_model_wall_ratio"] = [r["plain"]["wall_s"] / r["learned"]["wall_s"] for r in runs]
+    out["fallbacks"] = int(sum(not r["learned"]["proposal_used"] for r in runs))
+    if a.out:
+        with open(a.out, "w") as fh:
+            json.dump(dict(summary=out, runs=runs), fh, indent=1)
     print(json.dumps(out), flush=True)
 
 

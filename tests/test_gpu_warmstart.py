@@ -23,3 +23,15 @@ def test_warm_start_gains_over_plain():
     for r in out["runs"]:
         if r["plain"]["reached"]:
             assert r["learned"]["reached"]
+
+
+def test_warm_start_on_config2_family_beats_plain_wall_time():
+    """The config-2 family itself (4 groups on 24 x 24 x 12 voxels of 100 m,
+    control-point stride 4, 64 x 64 stations, network 4 x 512) at reduced
+    training size: the learned start must reach chi^2 = N in less mean wall
+    time than plain L-BFGS-B over the held-out models."""
+    p = synth.voxel_contact_model()
+    out = experiment(p, n_pairs=6144, n_heldout=8, epochs=30, seed=0, width=512, depth=4, batch=256)
+    assert out["loss_last"] < 0.5 * out["loss_first"]
+    assert out["learned"]["reached"] >= out["plain"]["reached"]
+    assert out["learned"]["mean_wall_s"] < out["plain"]["mean_wall_s"], (out["learned"], out["plain"])
