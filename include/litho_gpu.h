@@ -213,7 +213,10 @@ lf_status lf_forward(lf_ctx* ctx, const double* params, double* gz, double* tmi)
  *  fwd_target_blocks     forward CTAs per launch (in 128-station units):
  *                        station blocks x facet (patch) chunks; more chunks =
  *                        more CTAs, each over fewer facets
- *                        (candidates 148 x {4, 8, 16, 32, 64, 128})
+ *                        (candidates 148 x {4, 8, 16, 32, 64, 128}); 0 (mixed
+ *                        precision only) = a persistent grid of one CTA per
+ *                        resident slot, each over a balanced contiguous range
+ *                        of (station block, patch) units
  *  grad_target_warps     gradient warps per launch: DOF facets x station chunks
  *                        (148 x {16, 32, 64, 128, 256})
  *  near_tiles_per_chunk  mixed near-field gradient: 64-station tiles per warp

@@ -124,6 +124,10 @@ struct lf_ctx {
     int64_t pPartTotal = 0, pItemPairs = 0;
     uint64_t pItemsEpoch = ~0ull;
     int pItemsThreads = 0;
+    // persistent schedule (tune.fwd_target_blocks == 0): per-block slot counts
+    DevBuf<int32_t> d_pBlockNch;
+    long long pPersistKey = -1;
+    int pPersistSlots = 0, pPersistGrid = 0;
     DevBuf<int32_t> d_tri, d_dofOff, d_refVertex, d_interpOff, d_interpSrc, d_interpRows, d_syncOff,
         d_syncVertex, d_vfOff, d_vf, d_gradVerts, d_gradFacets, d_chunkBegin, d_chunkEnd, d_chunkGroup;
     DevBuf<uint8_t> d_refAxis, d_faceNeeds;
@@ -964,6 +968,10 @@ static constexpr int kFwdFacetTile = 32;
 static constexpr int kGradThreads = 32;             // Jacobian rows: one warp of facets per CTA
 static constexpr int kGradWarpsPerBlock = 4;        // objective gradient: one warp per facet
 
+// Forward CTAs per launch of the chunked and item schedules; 0 (the mixed
+// path's persistent schedule) counts as 148 x 8 there.
+static int fwd_blocks(const lf_ctx* c) { return c->tune.fwd_target_blocks > 0 ? c->tune.fwd_target_blocks : 148 * 8; }
+
 // Facet chunks for the forward: contiguous ranges inside one group, sized so
 // that station tiles x chunks fill the GPU.
 // With c->groupFilter >= 0 only that group's facets are planned (unit
@@ -974,7 +982,7 @@ static void plan_chunks(lf_ctx* c, int S) {
     const int g0 = c->groupFilter >= 0 ? c->groupFilter : 0, g1 = c->groupFilter >= 0 ? c->groupFilter + 1 : c->G;
     const int nf = c->grpTriOff[g1] - c->grpTriOff[g0];
     int sBlocks = std::max(1, cdiv(S, kFwdThreads));
-    int want = std::max(1, cdiv(c->tune.fwd_target_blocks, sBlocks));
+    int want = std::max(1, cdiv(fwd_blocks(c), sBlocks));
     int chunkSize = std::max(64, cdiv(std::max(nf, 1), want));
     c->chunkBegin.clear(); c->chunkEnd.clear(); c->chunkGroup.clear();
     for (int g = g0; g < g1; ++g)
@@ -1079,7 +1087,7 @@ static lf_status plan_items(lf_ctx* c) {
     int64_t pairs = 0;
     for (int g = 0; g < G; ++g)
         pairs += (int64_t)(c->grpStaOff[g + 1] - c->grpStaOff[g]) * (c->grpTriOff[g + 1] - c->grpTriOff[g]);
-    const int64_t targetItems = 32 * (int64_t)c->tune.fwd_target_blocks;
+    const int64_t targetItems = 32 * (int64_t)fwd_blocks(c);
     const int64_t F64 = std::max<int64_t>(kFwdFacetTile, (pairs / (128 * targetItems) + 31) / 32 * 32);
     const int F = static_cast<int>(std::min<int64_t>(F64, 1 << 30));
     std::vector<FwdItem> items;
@@ -1121,7 +1129,7 @@ static lf_status forward_set_items(lf_ctx* c, const StationSet& s, double* d_gz,
     if (GZ) LF_TRY_CUDA(c, c->d_partG.reserve((size_t)c->partTotal));
     if (TMI) LF_TRY_CUDA(c, c->d_partM.reserve((size_t)c->partTotal));
     if (c->nItems > 0) {
-        const int grid = std::min(c->nItems, c->tune.fwd_target_blocks);
+        const int grid = std::min(c->nItems, fwd_blocks(c));
         int slot = prof_begin(c, c->evFwd, c->nFwd);
         k_forward_fp64_items<GZ, TMI, kFwdFacetTile><<<grid, kFwdThreads, 0, c->stream>>>(
                 c->d_items.p, c->nItems, s.d_xyz.p, c->T, c->d_fc.p, GZ ? c->d_partG.p : nullptr,
@@ -1176,7 +1184,7 @@ static void plan_patch_chunks(lf_ctx* c, int S) {
     const int g0 = c->groupFilter >= 0 ? c->groupFilter : 0, g1 = c->groupFilter >= 0 ? c->groupFilter + 1 : c->G;
     const int np = pt.grpPatchOff[g1] - pt.grpPatchOff[g0];
     const int sBlocks = std::max(1, cdiv(S, NT));
-    const int want = std::max(1, cdiv((long long)c->tune.fwd_target_blocks * 128 / NT, sBlocks));
+    const int want = std::max(1, cdiv((long long)fwd_blocks(c) * 128 / NT, sBlocks));
     const int per = std::max(1, cdiv(std::max(np, 1), want));
     c->pchunkBegin.clear();
     c->pchunkEnd.clear();
@@ -1200,7 +1208,9 @@ static cudaError_t patch_kernel_attrs() {
                                              (int)sizeof(PatchSmem<NT>));
         cudaError_t b = cudaFuncSetAttribute(k_forward_patch_items<GZ, TMI, NT>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(PatchSmem<NT>));
-        return a != cudaSuccess ? a : b;
+        cudaError_t d = cudaFuncSetAttribute(k_forward_patch_persistent<GZ, TMI, NT>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(PatchSmem<NT>));
+        return a != cudaSuccess ? a : (b != cudaSuccess ? b : d);
     }();
     return e;
 }
@@ -1231,7 +1241,7 @@ static lf_status plan_patch_items(lf_ctx* c) {
     int64_t pairs = 0;
     for (int g = 0; g < G; ++g)
         pairs += (int64_t)(c->grpStaOff[g + 1] - c->grpStaOff[g]) * (c->grpTriOff[g + 1] - c->grpTriOff[g]);
-    const int64_t targetItems = 32 * (int64_t)c->tune.fwd_target_blocks * 128 / NT;
+    const int64_t targetItems = 32 * (int64_t)fwd_blocks(c) * 128 / NT;
     const double facetsPerPatch = pt.P > 0 ? (double)c->T / pt.P : 1.0;
     const int per = (int)std::max<int64_t>(1, (int64_t)((double)pairs / ((double)NT * targetItems * facetsPerPatch)));
     std::vector<FwdItem> items;
@@ -1290,7 +1300,7 @@ static lf_status forward_set_patch_items(lf_ctx* c, const StationSet& s, double*
     if (GZ) LF_TRY_CUDA(c, c->d_partG.reserve((size_t)c->pPartTotal));
     if (TMI) LF_TRY_CUDA(c, c->d_partM.reserve((size_t)c->pPartTotal));
     if (c->npItems > 0) {
-        const int grid = std::min(c->npItems, c->tune.fwd_target_blocks * 128 / c->patchThreads);
+        const int grid = std::min(c->npItems, fwd_blocks(c) * 128 / c->patchThreads);
         int slot = prof_begin(c, c->evFwd, c->nFwd);
         if (c->patchThreads == 256)
             LF_RET_IF((launch_patch_items<GZ, TMI, 256>(c, s, grid)));
@@ -1316,11 +1326,65 @@ static lf_status launch_patch(lf_ctx* c, const StationSet& s, int nch) {
     return LF_OK;
 }
 
+// Persistent schedule: one CTA per resident slot on the device, each over a
+// balanced contiguous range of (station block, patch) units.
+template <bool GZ, bool TMI, int NT>
+static lf_status forward_patch_persistent(lf_ctx* c, const StationSet& s, double* d_gz, double* d_tmi) {
+    LF_TRY_CUDA(c, (patch_kernel_attrs<GZ, TMI, NT>()));
+    static int occupancy = 0, sms = 0;
+    if (!occupancy) {
+        LF_TRY_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occupancy, k_forward_patch_persistent<GZ, TMI, NT>,
+                                                                     NT, sizeof(PatchSmem<NT>)));
+        LF_TRY_CUDA(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+        occupancy = std::max(occupancy, 1);
+    }
+    const int S = s.n;
+    const PatchTopology& pt = c->ptopo;
+    const int g0 = c->groupFilter >= 0 ? c->groupFilter : 0, g1 = c->groupFilter >= 0 ? c->groupFilter + 1 : c->G;
+    const int pbase = pt.grpPatchOff[g0], P = pt.grpPatchOff[g1] - pbase;
+    const int NB = cdiv(S, NT);
+    const long long nunits = (long long)NB * P;
+    if (nunits == 0) return LF_OK;
+    const int G = (int)std::min<long long>((long long)occupancy * sms, nunits);
+    const long long key = ((((long long)S * 1000003 + P) * 131 + pbase) * 4099 + G) * 3 + (NT == 256);
+    if (key != c->pPersistKey) {
+        std::vector<int32_t> nch(NB);
+        int mx = 1;
+        auto owner = [&](long long u) { return static_cast<int>(((u + 1) * G - 1) / nunits); };
+        for (int b = 0; b < NB; ++b) {
+            nch[b] = owner((long long)b * P + P - 1) - owner((long long)b * P) + 1;
+            mx = std::max(mx, nch[b]);
+        }
+        LF_TRY_CUDA(c, upload(c->d_pBlockNch, nch.data(), nch.size(), c->stream));
+        c->pPersistKey = key;
+        c->pPersistSlots = mx;
+        c->pPersistGrid = G;
+        c->epoch++;
+    }
+    if (GZ) LF_TRY_CUDA(c, c->d_partG.reserve((size_t)c->pPersistSlots * S));
+    if (TMI) LF_TRY_CUDA(c, c->d_partM.reserve((size_t)c->pPersistSlots * S));
+    int slot = prof_begin(c, c->evFwd, c->nFwd);
+    k_forward_patch_persistent<GZ, TMI, NT><<<G, NT, sizeof(PatchSmem<NT>), c->stream>>>(
+        S, s.d_xyz.p, c->d_blobs.p, c->d_pBlobOff.p, pbase, P, nunits, c->d_mc.p, c->T, c->tau,
+        GZ ? c->d_partG.p : nullptr, TMI ? c->d_partM.p : nullptr, c->d_nearPairs.p, c->d_patchErr.p);
+    prof_end(c, c->evFwd, slot);
+    k_forward_reduce_mixed<<<cdiv(S, 32), 256, 0, c->stream>>>(S, c->pPersistSlots, GZ ? c->d_partG.p : nullptr,
+                                                                TMI ? c->d_partM.p : nullptr, GZ ? d_gz : nullptr,
+                                                                TMI ? d_tmi : nullptr, c->d_pBlockNch.p, NT);
+    c->counters.launches += 2;
+    c->counters.forward_pairs += (uint64_t)S * (uint64_t)(c->grpTriOff[g1] - c->grpTriOff[g0]);
+    LF_CHECK_LAUNCH(c);
+    return LF_OK;
+}
+
 template <bool GZ, bool TMI>
 static lf_status forward_set_mixed(lf_ctx* c, const StationSet& s, double* d_gz, double* d_tmi) {
     if (c->partitioned) return forward_set_patch_items<GZ, TMI>(c, s, d_gz, d_tmi);
     int S = s.n;
     if (S == 0) return LF_OK;
+    if (c->tune.fwd_target_blocks == 0)
+        return c->patchThreads == 256 ? forward_patch_persistent<GZ, TMI, 256>(c, s, d_gz, d_tmi)
+                                      : forward_patch_persistent<GZ, TMI, 128>(c, s, d_gz, d_tmi);
     plan_patch_chunks(c, S);
     if (c->pchunksDirty) {
         if (!c->pchunkBegin.empty()) {
@@ -1676,7 +1740,7 @@ static lf_status run_cached(lf_ctx* c, lf_ctx::GraphSet& set, const double* p, d
 }
 
 extern "C" lf_status lf_set_tuning(lf_ctx* c, const lf_tuning* t) {
-    if (!c || !t || t->fwd_target_blocks < 1 || t->grad_target_warps < 1 || t->near_tiles_per_chunk < 0 ||
+    if (!c || !t || t->fwd_target_blocks < 0 || t->grad_target_warps < 1 || t->near_tiles_per_chunk < 0 ||
         (t->patch_threads != 128 && t->patch_threads != 256) || !std::isfinite(t->far_ratio))
         return LF_EINVAL;
     c->epoch++;
@@ -1756,20 +1820,20 @@ extern "C" lf_status lf_autotune(lf_ctx* c, const double* params, int repeats, l
     double bestMs = 0.0;
     lf_status st = timeit(best, &bestMs);
     const bool mixed = c->precision == LF_PREC_MIXED;
-    const int fwdC[] = {148 * 4, 148 * 8, 148 * 16, 148 * 32, 148 * 64, 148 * 128};
+    const int fwdC[] = {0, 148 * 4, 148 * 8, 148 * 16, 148 * 32, 148 * 64, 148 * 128};
     const int gradC[] = {148 * 16, 148 * 32, 148 * 64, 148 * 128, 148 * 256};
     const int nearC[] = {0, 1, 2, 4, 8};
     const int threadsC[] = {128, 256};
     for (int dim = 0; dim < 4 && st == LF_OK; ++dim) {
         const int* cand = dim == 0 ? fwdC : (dim == 1 ? gradC : (dim == 2 ? nearC : threadsC));
-        const int nc = dim == 0 ? 6 : (dim == 3 ? 2 : 5);
+        const int nc = dim == 0 ? 7 : (dim == 3 ? 2 : 5);
         if (dim >= 2 && !mixed) break;
         for (int k = 0; k < nc && st == LF_OK; ++k) {
             lf_tuning t = best;
             int& field = dim == 0 ? t.fwd_target_blocks
                                   : (dim == 1 ? t.grad_target_warps
                                               : (dim == 2 ? t.near_tiles_per_chunk : t.patch_threads));
-            if (field == cand[k]) continue;
+            if (field == cand[k] || (dim == 0 && cand[k] == 0 && !mixed)) continue;
             field = cand[k];
             double ms = 0.0;
             st = timeit(t, &ms);

@@ -547,13 +547,18 @@ __global__ void __launch_bounds__(128, 4) k_gradient_warp_far32(int T, const dou
 // Per station: sum of chunk partials (facet scales are already applied).
 // Blocks of 32 stations x 8 chunk lanes: lane y sums chunks y, y+8, ...
 // (coalesced over stations), then the 8 lane sums are added in lane order.
+// With block_nch, station s sums block_nch[s / block] chunks (the persistent
+// patch forward), else nchunks.
 __global__ void __launch_bounds__(256) k_forward_reduce_mixed(int S, int nchunks, const double* __restrict__ part_gz,
                                                               const double* __restrict__ part_tmi,
-                                                              double* __restrict__ gz, double* __restrict__ tmi) {
+                                                              double* __restrict__ gz, double* __restrict__ tmi,
+                                                              const int32_t* __restrict__ block_nch = nullptr,
+                                                              int block = 1) {
     __shared__ double sg[8][33], st[8][33];
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const int s = blockIdx.x * 32 + tx;
     double g = 0.0, t = 0.0;
+    if (block_nch && s < S) nchunks = block_nch[s / block];
     if (s < S) {
         if (part_gz) g = strided_sum8(ty, nchunks, g, [&](int c) { return part_gz[(size_t)c * S + s]; });
         if (part_tmi) t = strided_sum8(ty, nchunks, t, [&](int c) { return part_tmi[(size_t)c * S + s]; });

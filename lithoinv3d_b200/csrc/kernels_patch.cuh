@@ -479,6 +479,44 @@ __global__ void __launch_bounds__(NT) k_forward_patch(int S, const double* __res
                                      TMI ? part_tmi + (size_t)chunk * S : nullptr, near_pairs, err, phases);
 }
 
+// Persistent grid (one CTA per resident slot): the (station block, patch)
+// units b * P + p, block-major over `nunits` = blocks x P, are split into
+// gridDim.x balanced contiguous ranges; a CTA walks its range block by block,
+// so each of its blocks is one pipelined patch run.  Block b's partial of CTA
+// c goes to slot c - (the CTA holding unit b * P); k_forward_reduce_mixed
+// sums block_nch[b] slots for the stations of block b.
+__device__ __forceinline__ int patch_unit_owner(long long u, long long nunits, int G) {
+    return static_cast<int>(((u + 1) * G - 1) / nunits);
+}
+
+template <bool GZ, bool TMI, int NT>
+__global__ void __launch_bounds__(NT) k_forward_patch_persistent(int S, const double* __restrict__ sta,
+                                                                 const unsigned char* __restrict__ blobs,
+                                                                 const int32_t* __restrict__ blobOff, int pbase, int P,
+                                                                 long long nunits, const double* __restrict__ mc,
+                                                                 int T, float tau, double* __restrict__ part_gz,
+                                                                 double* __restrict__ part_tmi,
+                                                                 unsigned long long* __restrict__ near_pairs,
+                                                                 unsigned int* __restrict__ err) {
+    PatchSmem<NT>& sm = patch_smem_init<NT>();
+    uint32_t phases = 0;
+    const int G = gridDim.x, c = blockIdx.x;
+    const long long u0 = (long long)c * nunits / G, u1 = (long long)(c + 1) * nunits / G;
+    if (u0 >= u1) return;
+    const int b0 = static_cast<int>(u0 / P), b1 = static_cast<int>((u1 - 1) / P);
+    for (int b = b0; b <= b1; ++b) {
+        const int pb = b == b0 ? static_cast<int>(u0 % P) : 0;
+        const int pe = b == b1 ? static_cast<int>((u1 - 1) % P) + 1 : P;
+        const int slot = c - patch_unit_owner((long long)b * P, nunits, G);
+        const int s = b * NT + (int)threadIdx.x;
+        if (!forward_patch_block<GZ, TMI, NT>(sm, s, s < S, sta, blobs, blobOff, pbase + pb, pbase + pe, mc, T, tau,
+                                              GZ ? part_gz + (size_t)slot * S : nullptr,
+                                              TMI ? part_tmi + (size_t)slot * S : nullptr, near_pairs, err, phases))
+            return;
+        __syncthreads();  // the next block's first copy reuses buffer 0
+    }
+}
+
 // Batched bodies: a persistent grid over (body, station block, patch range)
 // items; FwdItem's facet range holds the patch range.
 template <bool GZ, bool TMI, int NT>
