@@ -197,6 +197,17 @@ __device__ __forceinline__ float atanh_half_lambda(float L, float dsum) {
     return 0.5f * log1pf(__fdividef(2.f * v, 1.f - v));
 }
 
+// atanh(v) / v = 1 + v^2/3 + ... + v^12/13 and atan(t) / t = 1 - t^2/3 + ...
+// + t^8/9 (Abramowitz & Stegun 4.1.28, 4.4.42) as polynomials in the square:
+// below 8e-8 relative for v <= 3/8, below 1e-10 for |t| <= 1/8.
+__device__ __forceinline__ float atanh_poly(float v2) {
+    return fmaf(v2, fmaf(v2, fmaf(v2, fmaf(v2, fmaf(v2, fmaf(v2, 1.f / 13.f, 1.f / 11.f), 1.f / 9.f), 1.f / 7.f),
+                              1.f / 5.f), 1.f / 3.f), 1.f);
+}
+__device__ __forceinline__ float atan_poly(float t2) {
+    return fmaf(t2, fmaf(t2, fmaf(t2, fmaf(t2, 1.f / 9.f, -1.f / 7.f), 1.f / 5.f), -1.f / 3.f), 1.f);
+}
+
 // atan(y / x) (half the solid angle): series when x > 0 and |y| <= x / 8,
 // else atan2f.
 __device__ __forceinline__ float atan_half_omega(float y, float x) {
@@ -311,9 +322,10 @@ __device__ __forceinline__ bool forward_patch_block(PatchSmem<NT>& sm, int s, bo
         const PatchFacet* PF =
             reinterpret_cast<const PatchFacet*>(B + kPatchHeadBytes + nv * kPatchVertBytes + ne * kPatchEdgeBytes);
         // lane j: facet j against this warp's station box
-        bool valid = false, vfar = false, far = false, mid = false;
+        bool valid = false, vfar = false, far = false, mid = false, hasGz = false;
         if (lane < nf && !(PF[lane].size < 0.f)) {
             valid = true;
+            hasGz = PF[lane].gq != 0.f;  // n_z == 0: no gz term
             const float cxw = PF[lane].cenx, cyw = PF[lane].ceny, czw = PF[lane].cenz;
             const float ddx = fmaxf(0.f, fmaxf(bb[0] - cxw, cxw + bb[3]));
             const float ddy = fmaxf(0.f, fmaxf(bb[1] - cyw, cyw + bb[4]));
@@ -328,6 +340,7 @@ __device__ __forceinline__ bool forward_patch_block(PatchSmem<NT>& sm, int s, bo
         const unsigned midMask = __ballot_sync(0xffffffffu, valid && mid);
         const unsigned fastMask = __ballot_sync(0xffffffffu, valid && (vfar || far || mid));
         const unsigned nearMask = __ballot_sync(0xffffffffu, valid && !vfar && !far && !mid);
+        const unsigned gzMask = __ballot_sync(0xffffffffu, hasGz);
         if (fastMask) {
             const float xo = (float)(ox - H.ox), yo = (float)(oy - H.oy), zo = (float)(oz - H.oz);
             if (TMI) {
@@ -339,14 +352,45 @@ __device__ __forceinline__ bool forward_patch_block(PatchSmem<NT>& sm, int s, bo
                     dvp[v * NT] = d2 * rsqrtf(d2);
                 }
                 float tacc = 0.f;
-                const unsigned excl = nearMask;
-                if (!excl) {
+                // Far facets only (no mid or near facet in this warp's view of the
+                // patch): every edge's v = L / (d1 + d2) is below 3/8 and every
+                // solid-angle ratio below 1/8 for tau >= 2, so both series run
+                // without branches (independent chains the compiler can
+                // interleave).  A warp that meets an argument outside those
+                // ranges redoes the patch's TMI with the per-term fallbacks.
+                bool exact = (midMask | nearMask) != 0u;
+                if (!exact) {
+                    bool bad = false;
+                    float tsum = 0.f;
 #pragma unroll 4
                     for (int e = 0; e < ne; ++e) {
                         const PatchEdgeA ea = EA[e];
-                        tacc = fmaf(ea.mt, atanh_half_lambda(ea.L, dvp[ea.lv1 * NT] + dvp[ea.lv2 * NT]), tacc);
+                        const float v = __fdividef(ea.L, dvp[ea.lv1 * NT] + dvp[ea.lv2 * NT]);
+                        bad |= !(v <= 0.375f);
+                        tsum = fmaf(ea.mt, v * atanh_poly(v * v), tsum);
                     }
-                } else {
+#pragma unroll 2
+                    for (unsigned m = fastMask; m; m &= m - 1) {
+                        const float4* F4 = reinterpret_cast<const float4*>(PF + (__ffs(m) - 1));
+                        const float4 w0 = F4[0], w1 = F4[1], w2 = F4[2];  // corners, N | cf, mf2 | squared edges
+                        const uint32_t c = __float_as_uint(w0.x);
+                        const float da = dvp[(c & 0xff) * NT], db = dvp[((c >> 8) & 0xff) * NT],
+                                    dc = dvp[(c >> 16) * NT];
+                        const float da2 = da * da, db2 = db * db, dc2 = dc * dc;
+                        const float sab = da2 + db2 - w2.x, sbc = db2 + dc2 - w2.y, sca = dc2 + da2 - w2.z;
+                        const float den = fmaf(0.5f, fmaf(sab, dc, fmaf(sbc, da, sca * db)), da * db * dc);
+                        const float num = w1.x - fmaf(xo, w0.y, fmaf(yo, w0.z, zo * w0.w));
+                        const float t = __fdividef(num, den);
+                        bad |= !(den > 0.f && fabsf(t) <= 0.125f);
+                        tsum = fmaf(w1.y, t * atan_poly(t * t), tsum);
+                    }
+                    if (__any_sync(0xffffffffu, bad))
+                        exact = true;
+                    else
+                        tacc = tsum;
+                }
+                if (exact) {
+                    const unsigned excl = nearMask;
                     for (int e = 0; e < ne; ++e) {
                         const PatchEdgeA ea = EA[e];
                         const PatchEdgeB eb = EB[e];
@@ -356,70 +400,76 @@ __device__ __forceinline__ bool forward_patch_block(PatchSmem<NT>& sm, int s, bo
                         if (m != 0.f)
                             tacc = fmaf(m, atanh_half_lambda(ea.L, dvp[ea.lv1 * NT] + dvp[ea.lv2 * NT]), tacc);
                     }
-                }
-                for (unsigned m = fastMask; m; m &= m - 1) {
-                    const float4* F4 = reinterpret_cast<const float4*>(PF + (__ffs(m) - 1));
-                    const float4 w0 = F4[0], w1 = F4[1], w2 = F4[2];  // corners, N | cf, mf2 | squared edges
-                    const uint32_t c = __float_as_uint(w0.x);
-                    const float da = dvp[(c & 0xff) * NT], db = dvp[((c >> 8) & 0xff) * NT],
-                                dc = dvp[(c >> 16) * NT];
-                    const float da2 = da * da, db2 = db * db, dc2 = dc * dc;
-                    // 2 x the dot products r_a.r_b, r_b.r_c, r_c.r_a from the distances and edge lengths
-                    const float sab = da2 + db2 - w2.x, sbc = db2 + dc2 - w2.y, sca = dc2 + da2 - w2.z;
-                    const float den = fmaf(0.5f, fmaf(sab, dc, fmaf(sbc, da, sca * db)), da * db * dc);
-                    const float num = w1.x - fmaf(xo, w0.y, fmaf(yo, w0.z, zo * w0.w));
-                    tacc = fmaf(w1.y, atan_half_omega(num, den), tacc);
+                    for (unsigned m = fastMask; m; m &= m - 1) {
+                        const float4* F4 = reinterpret_cast<const float4*>(PF + (__ffs(m) - 1));
+                        const float4 w0 = F4[0], w1 = F4[1], w2 = F4[2];
+                        const uint32_t c = __float_as_uint(w0.x);
+                        const float da = dvp[(c & 0xff) * NT], db = dvp[((c >> 8) & 0xff) * NT],
+                                    dc = dvp[(c >> 16) * NT];
+                        const float da2 = da * da, db2 = db * db, dc2 = dc * dc;
+                        // 2 x the dot products r_a.r_b, r_b.r_c, r_c.r_a from the distances and edge lengths
+                        const float sab = da2 + db2 - w2.x, sbc = db2 + dc2 - w2.y, sca = dc2 + da2 - w2.z;
+                        const float den = fmaf(0.5f, fmaf(sab, dc, fmaf(sbc, da, sca * db)), da * db * dc);
+                        const float num = w1.x - fmaf(xo, w0.y, fmaf(yo, w0.z, zo * w0.w));
+                        tacc = fmaf(w1.y, atan_half_omega(num, den), tacc);
+                    }
                 }
                 tmi += tacc;
             }
             if (GZ) {
                 float gacc = 0.f;
-                for (unsigned m = fastMask; m; m &= m - 1) {
-                    const int j = __ffs(m) - 1;
-                    const float4* F4 = reinterpret_cast<const float4*>(PF + j);
-                    const float gq = F4[1].z;
-                    if (gq == 0.f) continue;  // horizontal normal: the gz term is zero (warp-uniform)
-                    // floats 16..42 of the record: q3[9] then q6[18]
-                    float q[28];
+                // facets with a gz term (n_z != 0), by rule: 3-point beyond 4 tau,
+                // 6-point beyond tau, 28-point in the mid field
+#pragma unroll 2
+                for (unsigned m = fastMask & gzMask & vfarMask; m; m &= m - 1) {
+                    const float4* F4 = reinterpret_cast<const float4*>(PF + (__ffs(m) - 1));
+                    const float4 w4 = F4[4], w5 = F4[5], w6 = F4[6];  // q3[0..8]
+                    const float q[9] = {w4.x, w4.y, w4.z, w4.w, w5.x, w5.y, w5.z, w5.w, w6.x};
+                    float acc = 0.f;
 #pragma unroll
-                    for (int k = 0; k < 7; ++k) {
-                        const float4 w = F4[4 + k];
+                    for (int k = 0; k < 3; ++k) {
+                        const float px = q[3 * k] - xo, py = q[3 * k + 1] - yo, pz = q[3 * k + 2] - zo;
+                        acc += rsqrtf(fmaf(px, px, fmaf(py, py, pz * pz)));
+                    }
+                    gacc = fmaf(F4[1].z * (1.f / 3.f), acc, gacc);
+                }
+#pragma unroll 2
+                for (unsigned m = fastMask & gzMask & ~vfarMask & ~midMask; m; m &= m - 1) {
+                    const float4* F4 = reinterpret_cast<const float4*>(PF + (__ffs(m) - 1));
+                    float q[20];  // floats 24..43 of the record: q3[8], then q6[0..17], pad
+#pragma unroll
+                    for (int k = 0; k < 5; ++k) {
+                        const float4 w = F4[6 + k];
                         q[4 * k] = w.x; q[4 * k + 1] = w.y; q[4 * k + 2] = w.z; q[4 * k + 3] = w.w;
                     }
                     float acc = 0.f;
-                    if ((midMask >> j) & 1u) {
-                        // Radon's 7-point rule on the four midpoint sub-triangles
-                        // (28 points), built from the patch-frame corners
-                        const uint32_t c = __float_as_uint(F4[0].x);
-                        const float4 pa = *reinterpret_cast<const float4*>(PV + (c & 0xff));
-                        const float4 pb = *reinterpret_cast<const float4*>(PV + ((c >> 8) & 0xff));
-                        const float4 pc = *reinterpret_cast<const float4*>(PV + (c >> 16));
-                        const float ax = pa.x - xo, ay = pa.y - yo, az = pa.z - zo;
-                        const float bx = pb.x - pa.x, by = pb.y - pa.y, bz = pb.z - pa.z;
-                        const float cx = pc.x - pa.x, cy = pc.y - pa.y, cz = pc.z - pa.z;
-#pragma unroll 7
-                        for (int k = 0; k < 28; ++k) {
-                            const float u = kRadon4Bb[k], w = kRadon4Bc[k];
-                            const float px = fmaf(u, bx, fmaf(w, cx, ax)), py = fmaf(u, by, fmaf(w, cy, ay)),
-                                        pz = fmaf(u, bz, fmaf(w, cz, az));
-                            acc = fmaf(kRadonW[k % 7], rsqrtf(fmaf(px, px, fmaf(py, py, pz * pz))), acc);
-                        }
-                        acc *= 0.25f;
-                    } else if ((vfarMask >> j) & 1u) {
 #pragma unroll
-                        for (int k = 0; k < 3; ++k) {
-                            const float px = q[3 * k] - xo, py = q[3 * k + 1] - yo, pz = q[3 * k + 2] - zo;
-                            acc += rsqrtf(fmaf(px, px, fmaf(py, py, pz * pz)));
-                        }
-                        acc *= (1.f / 3.f);
-                    } else {
-#pragma unroll
-                        for (int k = 0; k < 6; ++k) {
-                            const float px = q[9 + 3 * k] - xo, py = q[10 + 3 * k] - yo, pz = q[11 + 3 * k] - zo;
-                            acc = fmaf(kDun6W[k], rsqrtf(fmaf(px, px, fmaf(py, py, pz * pz))), acc);
-                        }
+                    for (int k = 0; k < 6; ++k) {
+                        const float px = q[1 + 3 * k] - xo, py = q[2 + 3 * k] - yo, pz = q[3 + 3 * k] - zo;
+                        acc = fmaf(kDun6W[k], rsqrtf(fmaf(px, px, fmaf(py, py, pz * pz))), acc);
                     }
-                    gacc = fmaf(gq, acc, gacc);
+                    gacc = fmaf(F4[1].z, acc, gacc);
+                }
+                for (unsigned m = gzMask & midMask; m; m &= m - 1) {
+                    // Radon's 7-point rule on the four midpoint sub-triangles
+                    // (28 points), built from the patch-frame corners
+                    const float4* F4 = reinterpret_cast<const float4*>(PF + (__ffs(m) - 1));
+                    const uint32_t c = __float_as_uint(F4[0].x);
+                    const float4 pa = *reinterpret_cast<const float4*>(PV + (c & 0xff));
+                    const float4 pb = *reinterpret_cast<const float4*>(PV + ((c >> 8) & 0xff));
+                    const float4 pc = *reinterpret_cast<const float4*>(PV + (c >> 16));
+                    const float ax = pa.x - xo, ay = pa.y - yo, az = pa.z - zo;
+                    const float bx = pb.x - pa.x, by = pb.y - pa.y, bz = pb.z - pa.z;
+                    const float cx = pc.x - pa.x, cy = pc.y - pa.y, cz = pc.z - pa.z;
+                    float acc = 0.f;
+#pragma unroll 7
+                    for (int k = 0; k < 28; ++k) {
+                        const float u = kRadon4Bb[k], w = kRadon4Bc[k];
+                        const float px = fmaf(u, bx, fmaf(w, cx, ax)), py = fmaf(u, by, fmaf(w, cy, ay)),
+                                    pz = fmaf(u, bz, fmaf(w, cz, az));
+                        acc = fmaf(kRadonW[k % 7], rsqrtf(fmaf(px, px, fmaf(py, py, pz * pz))), acc);
+                    }
+                    gacc = fmaf(F4[1].z * 0.25f, acc, gacc);
                 }
                 gz += gacc;
             }
