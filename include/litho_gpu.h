@@ -292,7 +292,7 @@ lf_status lf_mlp_gradients(lf_mlp* m, const float* d_x, const float* d_y, float*
  * descriptors, accumulator in tensor memory, 128 x 256 or 128 x 128 tiles).
  * Both give the same results to FP32 summation order; at the network's
  * shapes the mma.sync kernel is the faster of the two. */
-enum { LF_GEMM_TCGEN05 = 0, LF_GEMM_MMA_SYNC = 1 };
+enum { LF_GEMM_TCGEN05 = 0, LF_GEMM_MMA_SYNC = 1, LF_GEMM_TCGEN05_TMA = 2 };
 lf_status lf_mlp_set_engine(lf_mlp* m, int engine);
 /* The network's BF16 GEMM on device buffers: C[M x N] = A[M x K] . B[K x N]
  * with A stored [M][K] (a_trans = 0) or [K][M] (a_trans = 1), B stored

@@ -10,6 +10,9 @@
 #include "../../include/litho_gpu.h"
 #include "mlp_kernels.cuh"
 #include "tc_gemm.cuh"
+#include "tc_gemm_tma.cuh"
+
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cmath>
@@ -110,9 +113,63 @@ static cudaError_t gemm_tc(cudaStream_t stream, int M, int N, int K, const __nv_
     return cudaPeekAtLastError();  // left for the caller's launch check
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the
+// library does not link the driver library itself).
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// 2-D tensor map of a row-major bf16 array [rows][cols] with row length ld
+// (elements): boxes of 64 columns x box_rows rows, 128-byte swizzle.
+static bool bf16_map(CUtensorMap* map, const void* base, int rows, int cols, int ld, int box_rows) {
+    const auto encode = tensor_map_encoder();
+    if (!encode) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+    const cuuint32_t box[2] = {64u, (cuuint32_t)box_rows};
+    const cuuint32_t elem[2] = {1u, 1u};
+    return encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, elem,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// One GEMM on the TMA-fed, warp-specialised tcgen05 kernel (tc_gemm_tma.cuh).
+template <bool A_T, bool B_T, int EPI, int BN>
+static cudaError_t gemm_tma(cudaStream_t stream, int M, int N, int K, const __nv_bfloat16* A, int lda,
+                            const __nv_bfloat16* B, int ldb, const float* bias, float* Cf, __nv_bfloat16* Cb, int ldc) {
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(k_gemm_tma<A_T, B_T, EPI, BN>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, TmaShape<BN>::kSmem);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    CUtensorMap mapA, mapB;
+    const bool okA = A_T ? bf16_map(&mapA, A, K, M, lda, 64) : bf16_map(&mapA, A, M, K, lda, kBM);
+    const bool okB = B_T ? bf16_map(&mapB, B, N, K, ldb, BN) : bf16_map(&mapB, B, K, N, ldb, 64);
+    if (!okA || !okB) return cudaErrorInvalidValue;
+    dim3 grid(N / BN, M / kBM);
+    k_gemm_tma<A_T, B_T, EPI, BN><<<grid, kTmaThreads, TmaShape<BN>::kSmem, stream>>>(M, N, K, mapA, mapB, bias, Cf,
+                                                                                     Cb, ldc);
+    return cudaPeekAtLastError();
+}
+
 template <bool A_T, bool B_T, int EPI>
 static cudaError_t gemm_on(int engine, cudaStream_t stream, int M, int N, int K, const __nv_bfloat16* A, int lda,
                            const __nv_bfloat16* B, int ldb, const float* bias, float* Cf, __nv_bfloat16* Cb, int ldc) {
+    if (engine == LF_GEMM_TCGEN05_TMA) {
+        if (N % 256 == 0)
+            return gemm_tma<A_T, B_T, EPI, 256>(stream, M, N, K, A, lda, B, ldb, bias, Cf, Cb, ldc);
+        return gemm_tma<A_T, B_T, EPI, 128>(stream, M, N, K, A, lda, B, ldb, bias, Cf, Cb, ldc);
+    }
     if (engine == LF_GEMM_TCGEN05) {
         if (N % 256 == 0)
             return gemm_tc<A_T, B_T, EPI, 256>(stream, M, N, K, A, lda, B, ldb, bias, Cf, Cb, ldc);
@@ -308,7 +365,7 @@ extern "C" lf_status lf_mlp_train_step(lf_mlp* m, const float* d_x, const float*
                                                            nullptr);
     }
     st = mlp_check_launch(m);
-    if (st == LF_OK && m->engine == LF_GEMM_TCGEN05) st = tc_check(m);
+    if (st == LF_OK && m->engine != LF_GEMM_MMA_SYNC) st = tc_check(m);
     return st;
 }
 
@@ -402,7 +459,7 @@ extern "C" lf_status lf_mlp_gradients(lf_mlp* m, const float* d_x, const float* 
     lf_status st = load_input(m, d_x, m->batch);
     if (st == LF_OK) st = forward(m);
     if (st == LF_OK) st = backward(m, d_y, loss);
-    if (st == LF_OK && m->engine == LF_GEMM_TCGEN05) st = tc_check(m);
+    if (st == LF_OK && m->engine != LF_GEMM_MMA_SYNC) st = tc_check(m);
     if (st == LF_OK && host_grads) st = copy_params(m, 1, host_grads);
     return st;
 }
@@ -413,7 +470,8 @@ extern "C" lf_status lf_set_device_wait_limit(long long polls) {
 }
 
 extern "C" lf_status lf_mlp_set_engine(lf_mlp* m, int engine) {
-    if (!m || (engine != LF_GEMM_TCGEN05 && engine != LF_GEMM_MMA_SYNC)) return LF_EINVAL;
+    if (!m || (engine != LF_GEMM_TCGEN05 && engine != LF_GEMM_MMA_SYNC && engine != LF_GEMM_TCGEN05_TMA))
+        return LF_EINVAL;
     m->engine = engine;
     return LF_OK;
 }
@@ -421,8 +479,9 @@ extern "C" lf_status lf_mlp_set_engine(lf_mlp* m, int engine) {
 extern "C" lf_status lf_gemm_bf16(int engine, int a_trans, int b_trans, int epilogue, int M, int N, int K,
                                   const void* A, int lda, const void* B, int ldb, const float* bias, void* C, int ldc,
                                   void* stream) {
-    if ((engine != LF_GEMM_TCGEN05 && engine != LF_GEMM_MMA_SYNC) || M <= 0 || N <= 0 || K <= 0 || M % kBM ||
-        N % kBN || K % (engine == LF_GEMM_TCGEN05 ? kTcBK : kBK) || !A || !B || !C ||
+    const bool tc = engine == LF_GEMM_TCGEN05 || engine == LF_GEMM_TCGEN05_TMA;
+    if ((!tc && engine != LF_GEMM_MMA_SYNC) || M <= 0 || N <= 0 || K <= 0 || M % kBM ||
+        N % kBN || K % (tc ? kTcBK : kBK) || !A || !B || !C ||
         (epilogue != EPI_F32 && epilogue != EPI_BF16 && epilogue != EPI_BIAS_RELU && epilogue != EPI_BIAS_F32) ||
         ((epilogue == EPI_BIAS_RELU || epilogue == EPI_BIAS_F32) && !bias) || lda % 8 || ldb % 8 || ldc % 2 ||
         (reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B)) % 16)
@@ -453,7 +512,7 @@ extern "C" lf_status lf_gemm_bf16(int engine, int a_trans, int b_trans, int epil
 #undef LF_GEMM_CASE
     if (e != cudaSuccess) return LF_ECUDA;
     if (cudaStreamSynchronize(st) != cudaSuccess) return LF_ECUDA;
-    if (engine == LF_GEMM_TCGEN05) {
+    if (tc) {
         unsigned int flag = 0;
         if (cudaMemcpyFromSymbol(&flag, g_tc_gemm_error, sizeof(flag)) != cudaSuccess) return LF_ECUDA;
         if (flag) {

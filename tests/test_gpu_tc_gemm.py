@@ -16,7 +16,7 @@ pytestmark = pytest.mark.gpu
 
 torch = pytest.importorskip("torch")
 
-TC, SYNC = 0, 1
+TC, SYNC, TMA = 0, 1, 2
 EPI_F32, EPI_BIAS_RELU, EPI_BIAS_F32, EPI_BF16 = 0, 1, 2, 3
 
 
@@ -30,9 +30,10 @@ def run(lib, engine, a_t, b_t, epi, A, B, bias, M, N, K):
     return Cm.float()
 
 
+@pytest.mark.parametrize("engine", [TC, TMA])
 @pytest.mark.parametrize("a_t,b_t", [(0, 1), (1, 0), (0, 0), (1, 1)])
 @pytest.mark.parametrize("epi", [EPI_F32, EPI_BIAS_RELU, EPI_BIAS_F32, EPI_BF16])
-def test_tcgen05_gemm_matches_fp32_product(a_t, b_t, epi):
+def test_tcgen05_gemm_matches_fp32_product(a_t, b_t, epi, engine):
     lib = _native.load()
     # N = 512 runs the 128 x 256 tiles, N = 384 the 128 x 128 ones
     M, N, K = 256, (512 if epi in (EPI_F32, EPI_BIAS_RELU) else 384), 576
@@ -47,7 +48,7 @@ def test_tcgen05_gemm_matches_fp32_product(a_t, b_t, epi):
         want = want + bias
     if epi == EPI_BIAS_RELU:
         want = torch.relu(want)
-    got = run(lib, TC, a_t, b_t, epi, A, B, bias, M, N, K)
+    got = run(lib, engine, a_t, b_t, epi, A, B, bias, M, N, K)
     legacy = run(lib, SYNC, a_t, b_t, epi, A, B, bias, M, N, K)
     scale = float(want.abs().max())
     tol = 2e-5 if epi in (EPI_F32, EPI_BIAS_F32) else 1e-2
@@ -66,7 +67,8 @@ def test_tcgen05_gemm_rejects_bad_shapes():
     assert _native.STATUS[st] == "LF_EINVAL"
 
 
-def test_tcgen05_gemm_wait_expiry_reports_timeout_and_recovers():
+@pytest.mark.parametrize("engine", [TC, TMA])
+def test_tcgen05_gemm_wait_expiry_reports_timeout_and_recovers(engine):
     """Failure detection without a fault: with the main-loop wait limit at 0
     every stage wait gives up at once, so the kernel abandons the product,
     drains its own MMAs, frees its tensor memory and raises the error flag;
@@ -81,7 +83,7 @@ def test_tcgen05_gemm_wait_expiry_reports_timeout_and_recovers():
     Cm = torch.full((M, N), float("nan"), dtype=torch.float32, device="cuda")
 
     def call():
-        return lib.lf_gemm_bf16(TC, 0, 0, EPI_F32, M, N, K, C.c_void_p(Am.data_ptr()), K, C.c_void_p(Bm.data_ptr()),
+        return lib.lf_gemm_bf16(engine, 0, 0, EPI_F32, M, N, K, C.c_void_p(Am.data_ptr()), K, C.c_void_p(Bm.data_ptr()),
                                 N, C.cast(C.c_void_p(bias.data_ptr()), _native._dp), C.c_void_p(Cm.data_ptr()), N,
                                 None)
 
