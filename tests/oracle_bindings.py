@@ -483,13 +483,23 @@ def ref_export_ts(directory, base, suffix, xyz, tri):
 
 
 def _jacobian_worker(args):
-    tables, densities, susceptibilities, inducing, params, sta, kind = args
+    tables, densities, susceptibilities, inducing, params, sta, kind, true_h = args
     om = OracleModel(tables, densities, susceptibilities, inducing)
     om.scatter(params)
-    return om.jacobian(sta, kind)
+    return om.jacobian(sta, kind, true_h=true_h)
 
 
-def jacobian_parallel(tables, densities, susceptibilities, inducing, params, sta, kind, procs=None):
+# Step of the Richardson "true" derivative for models whose DOF vertices lie
+# far (>= ~100 m) from every station: the reference's oriented line-integral
+# form loses digits for edges nearly collinear with a station, and a central
+# difference amplifies that rounding by 1/h (on the icosphere the truth moves
+# by 2e-6 between h = 1e-2 and 0.3, and by 4e-8 between 0.3 and 1), while
+# the O(h^4) truncation at 100 m stays below 1e-9.
+FAR_TRUE_H = 0.3
+
+
+def jacobian_parallel(tables, densities, susceptibilities, inducing, params, sta, kind, procs=None,
+                      true_h=FAR_TRUE_H):
     """OracleModel(...).scatter(params) then .jacobian(sta, kind), split over
     station chunks in spawned processes (spawned, not forked: the calling
     process may already hold a CUDA context).  Each process starts from the
@@ -504,7 +514,7 @@ def jacobian_parallel(tables, densities, susceptibilities, inducing, params, sta
             procs = os.cpu_count() or 1
     procs = max(1, min(procs, len(sta)))
     chunks = np.array_split(np.arange(len(sta)), procs)
-    jobs = [(tables, densities, susceptibilities, inducing, params, sta[c], kind) for c in chunks if len(c)]
+    jobs = [(tables, densities, susceptibilities, inducing, params, sta[c], kind, true_h) for c in chunks if len(c)]
     if len(jobs) == 1:
         return _jacobian_worker(jobs[0])
     with mp.get_context("spawn").Pool(len(jobs)) as pool:

@@ -59,4 +59,4 @@ def test_autotune_keeps_results(mixed):
         f2, g2 = ctx.objective_and_gradient(x0)
         assert abs(f2 - f0) <= tol * abs(f0) and rel(g2, g0) < tol
     with pytest.raises(LithoError):
-        ctx.set_tuning(0, 1, 0)
+        ctx.set_tuning(-1, 1, 0)
