@@ -108,7 +108,9 @@ struct lf_ctx {
     // patch forward of the mixed path (kernels_patch.cuh): topology built
     // once per model, record blobs rewritten every evaluation
     PatchTopology ptopo;
-    DevBuf<int32_t> d_pFacetOff, d_pFacets, d_pVertOff, d_pVerts, d_pEdgeOff, d_pBlobOff, d_pChunkBegin, d_pChunkEnd;
+    DevBuf<int32_t> d_pFacetOff, d_pFacets, d_pVertOff, d_pVerts, d_pEdgeOff, d_pBlobOff, d_pChunkBegin, d_pChunkEnd,
+        d_pFacetPatch, d_pFacetSlot;
+    DevBuf<float> d_mt2;  // doubled TMI edge coefficients of every facet [3][T]
     DevBuf<uint32_t> d_pCorners, d_pEdgeInfo;
     DevBuf<uint8_t> d_pEdgeSlot, d_blobs;
     DevBuf<unsigned int> d_patchErr;
@@ -693,6 +695,15 @@ extern "C" lf_status lf_set_model_tables(lf_ctx* c, int G, const double* density
         LF_TRY_CUDA(c, upload(c->d_pEdgeInfo, pt.edgeInfo.data(), pt.edgeInfo.size(), c->stream));
         LF_TRY_CUDA(c, upload(c->d_pEdgeSlot, pt.edgeSlot.data(), pt.edgeSlot.size(), c->stream));
         LF_TRY_CUDA(c, upload(c->d_pBlobOff, pt.blobOff.data(), pt.blobOff.size(), c->stream));
+        std::vector<int32_t> fpatch(nt, 0), fslot(nt, 0);
+        for (int q = 0; q < pt.P; ++q)
+            for (int k = pt.facetOff[q]; k < pt.facetOff[q + 1]; ++k) {
+                fpatch[pt.facets[k]] = q;
+                fslot[pt.facets[k]] = k - pt.facetOff[q];
+            }
+        LF_TRY_CUDA(c, upload(c->d_pFacetPatch, fpatch.data(), fpatch.size(), c->stream));
+        LF_TRY_CUDA(c, upload(c->d_pFacetSlot, fslot.data(), fslot.size(), c->stream));
+        LF_TRY_CUDA(c, c->d_mt2.reserve((size_t)3 * nt));
         LF_TRY_CUDA(c, c->d_blobs.reserve((size_t)std::max(pt.blobOff.back(), 16)));
         LF_TRY_CUDA(c, c->d_patchErr.reserve(1));
         LF_TRY_CUDA(c, cudaMemsetAsync(c->d_patchErr.p, 0, sizeof(unsigned int), c->stream));
@@ -1218,14 +1229,15 @@ static cudaError_t patch_kernel_attrs() {
 // Per-evaluation records of the mixed forward: the per-facet FP64 / FP32
 // records (near and mid facets) and the patch blobs (far facets).
 static lf_status mixed_prep(lf_ctx* c) {
-    k_face_prep_mixed<<<cdiv(c->T, 128), 128, 0, c->stream>>>(c->T, c->d_tri.p, c->d_pos.p, c->d_faceGroup.p,
-                                                              c->d_groups.p, c->fdir, c->d_mc.p);
     const PatchTopology& pt = c->ptopo;
+    k_face_prep_patch<<<cdiv(c->T, 128), 128, 0, c->stream>>>(
+        c->T, c->d_tri.p, c->d_pos.p, c->d_faceGroup.p, c->d_groups.p, c->fdir, c->d_pFacetPatch.p, c->d_pFacetSlot.p,
+        c->d_pFacetOff.p, c->d_pCorners.p, c->d_pVertOff.p, c->d_pVerts.p, c->d_pEdgeOff.p, c->d_pBlobOff.p,
+        c->d_mc.p, c->d_mt2.p, c->d_blobs.p);
     if (pt.P > 0)
-        k_patch_prep<<<pt.P, 32, 0, c->stream>>>(pt.P, c->d_tri.p, c->d_pos.p, c->d_faceGroup.p, c->d_groups.p,
-                                                  c->fdir, c->d_pFacetOff.p, c->d_pFacets.p, c->d_pCorners.p,
-                                                  c->d_pVertOff.p, c->d_pVerts.p, c->d_pEdgeOff.p, c->d_pEdgeInfo.p,
-                                                  c->d_pEdgeSlot.p, c->d_pBlobOff.p, c->d_blobs.p);
+        k_patch_prep<<<pt.P, 32, 0, c->stream>>>(pt.P, c->d_pos.p, c->d_pFacetOff.p, c->d_pFacets.p, c->d_pVertOff.p,
+                                                  c->d_pVerts.p, c->d_pEdgeOff.p, c->d_pEdgeInfo.p, c->d_pEdgeSlot.p,
+                                                  c->d_pBlobOff.p, c->T, c->d_mt2.p, c->d_blobs.p);
     c->counters.launches += pt.P > 0 ? 2 : 1;
     LF_CHECK_LAUNCH(c);
     return LF_OK;

@@ -92,75 +92,6 @@ __constant__ float kRadon4Bc[28] = {
     0.5298579358948849f, 0.3333333333333333f, 0.1012865073234563f, 0.4493567463382718f, 0.4493567463382718f,
     0.4701420641051151f, 0.2649289679474425f, 0.2649289679474425f};
 
-// Per-facet FP64 constants of the mixed path (near facets of the forward read
-// them; the patch records of kernels_patch.cuh cover the rest).
-__global__ void k_face_prep_mixed(int T, const int32_t* __restrict__ tri, const double* __restrict__ pos,
-                                  const int16_t* __restrict__ face_group, const GroupConst* __restrict__ groups, d3 fdir,
-                                  double* __restrict__ mc) {
-    int f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= T) return;
-    d3 v[3];
-    for (int k = 0; k < 3; ++k) {
-        const double* p = pos + 3 * tri[3 * f + k];
-        v[k] = mk3(p[0], p[1], p[2]);
-    }
-    // reference-order normal and magnetic products (bit-identical to the
-    // reference, which matters for facets collapsed to a line)
-    d3 n = cross_rn(sub_rn(v[1], v[0]), sub_rn(v[2], v[0]));
-    double area2 = norm_rn(n);
-    double out[NMC];
-    for (int k = 0; k < NMC; ++k) out[k] = 0.0;
-    if (!(area2 < kEps)) {
-        d3 un = div_rn(n, area2);
-        const GroupConst& g = groups[face_group[f]];
-        d3 m = mk3(g.mdir[0], g.mdir[1], g.mdir[2]);
-        double mf = __dmul_rn(dot_rn(m, un), dot_rn(fdir, un));
-        double mt[3], L[3];
-        for (int i = 0; i < 3; ++i) {
-            d3 e = sub_rn(v[(i + 1) % 3], v[i]);
-            L[i] = norm_rn(e);
-            d3 eh = (L[i] < kEps) ? mk3(0, 0, 0) : div_rn(e, L[i]);
-            d3 perp = cross_rn(un, eh);
-            mt[i] = __dmul_rn(dot_rn(m, perp), dot_rn(fdir, perp));
-        }
-        int k = 0;  // rotate so that edge 0 is the longest
-        if (L[1] > L[k]) k = 1;
-        if (L[2] > L[k]) k = 2;
-        d3 a = v[k], b = v[(k + 1) % 3], c = v[(k + 2) % 3];
-        double L0 = L[k];
-        d3 xh = (b - a) * (1.0 / L0);
-        // On a facet collapsed onto a line the reference's unit normal is
-        // rounding noise and not perpendicular to the edges; the frame must
-        // stay orthonormal for the local coordinates (and so Lambda, which the
-        // reference takes from positions alone) to be right.
-        d3 zh = un - xh * dot3(un, xh);
-        zh = zh * (1.0 / norm3(zh));
-        d3 yh = cross3(zh, xh);
-        d3 ca = c - a;
-        double cx = dot3(ca, xh), cy = dot3(ca, yh);
-        double L1 = L[(k + 1) % 3], L2 = L[(k + 2) % 3];
-        out[MC_AX] = a.x; out[MC_AY] = a.y; out[MC_AZ] = a.z;
-        out[MC_XX] = xh.x; out[MC_XY] = xh.y; out[MC_XZ] = xh.z;
-        out[MC_YX] = yh.x; out[MC_YY] = yh.y; out[MC_YZ] = yh.z;
-        out[MC_ZX] = zh.x; out[MC_ZY] = zh.y; out[MC_ZZ] = zh.z;
-        out[MC_L0] = L0; out[MC_CX] = cx; out[MC_CY] = cy;
-        out[MC_L1] = L1; out[MC_L2] = L2;
-        if (!(L1 < kEps)) { out[MC_E1X] = (cx - L0) / L1; out[MC_E1Y] = cy / L1; }
-        if (!(L2 < kEps)) { out[MC_E2X] = -cx / L2; out[MC_E2Y] = -cy / L2; }
-        out[MC_SGZ] = un.z * g.gscale_fwd;
-        out[MC_MF] = -g.mscale * mf;
-        out[MC_MT0] = -g.mscale * mt[k];
-        out[MC_MT1] = -g.mscale * mt[(k + 1) % 3];
-        out[MC_MT2] = -g.mscale * mt[(k + 2) % 3];
-        out[MC_CENX] = (v[0].x + v[1].x + v[2].x) / 3.0;
-        out[MC_CENY] = (v[0].y + v[1].y + v[2].y) / 3.0;
-        out[MC_CENZ] = (v[0].z + v[1].z + v[2].z) / 3.0;
-        out[MC_SIZE] = L0;
-        out[MC_VALID] = 1.0;
-    }
-    for (int k = 0; k < NMC; ++k) mc[(size_t)k * T + f] = out[k];
-}
-
 // ----------------------------------------------------------- FP32 pieces --
 // sqrt for arguments known to be positive and normal (far-field distances):
 // r2 * rsqrt(r2), within 2 ulp.

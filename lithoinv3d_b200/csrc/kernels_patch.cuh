@@ -67,41 +67,156 @@ static_assert(sizeof(PatchEdgeA) + sizeof(PatchEdgeB) == kPatchEdgeBytes, "Patch
 static_assert(sizeof(PatchFacet) == kPatchFacetBytes, "PatchFacet");
 static_assert(kPatchMaxBytes % 16 == 0, "bulk copies move multiples of 16 bytes");
 
-// Per-evaluation records: one warp per patch.  Facet constants in the
-// reference's FP64 operation order (as k_face_prep_mixed), then rounded.
-__global__ void __launch_bounds__(32) k_patch_prep(int P, const int32_t* __restrict__ tri,
-                                                   const double* __restrict__ pos,
-                                                   const int16_t* __restrict__ face_group,
-                                                   const GroupConst* __restrict__ groups, d3 fdir,
+// Per-evaluation records, part 1: one thread per facet.  The facet's FP64
+// constants in the reference's operation order (the SoA mc[NMC][T] that near
+// pairs read, kernels_mixed.cuh's MixedConst layout), its patch facet record
+// (in its patch's frame) and its doubled, group-scaled TMI edge coefficients
+// mt2[3][T] in the facet's own edge order (edge i: v_i -> v_{i+1}).
+__global__ void __launch_bounds__(128) k_face_prep_patch(int T, const int32_t* __restrict__ tri,
+                                                         const double* __restrict__ pos,
+                                                         const int16_t* __restrict__ face_group,
+                                                         const GroupConst* __restrict__ groups, d3 fdir,
+                                                         const int32_t* __restrict__ facetPatch,
+                                                         const int32_t* __restrict__ facetSlot,
+                                                         const int32_t* __restrict__ facetOff,
+                                                         const uint32_t* __restrict__ corners,
+                                                         const int32_t* __restrict__ vertOff,
+                                                         const int32_t* __restrict__ verts,
+                                                         const int32_t* __restrict__ edgeOff,
+                                                         const int32_t* __restrict__ blobOff,
+                                                         double* __restrict__ mc, float* __restrict__ mt2,
+                                                         unsigned char* __restrict__ blobs) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= T) return;
+    d3 v[3];
+    for (int k = 0; k < 3; ++k) {
+        const double* q = pos + 3 * (size_t)tri[3 * f + k];
+        v[k] = mk3(q[0], q[1], q[2]);
+    }
+    // reference-order normal and magnetic products (bit-identical to the
+    // reference, which matters for facets collapsed to a line)
+    const d3 n = cross_rn(sub_rn(v[1], v[0]), sub_rn(v[2], v[0]));
+    const double area2 = norm_rn(n);
+    const bool valid = !(area2 < kEps);
+    double out[NMC];
+    for (int k = 0; k < NMC; ++k) out[k] = 0.0;
+    double mt[3] = {0.0, 0.0, 0.0}, L[3], mfv = 0.0, sgz = 0.0;
+    for (int i = 0; i < 3; ++i) L[i] = norm_rn(sub_rn(v[(i + 1) % 3], v[i]));
+    if (valid) {
+        const d3 un = div_rn(n, area2);
+        const GroupConst& g = groups[face_group[f]];
+        const d3 m = mk3(g.mdir[0], g.mdir[1], g.mdir[2]);
+        const double mf = __dmul_rn(dot_rn(m, un), dot_rn(fdir, un));
+        for (int i = 0; i < 3; ++i) {
+            const d3 e = sub_rn(v[(i + 1) % 3], v[i]);
+            const d3 eh = (L[i] < kEps) ? mk3(0, 0, 0) : div_rn(e, L[i]);
+            const d3 perp = cross_rn(un, eh);
+            mt[i] = -g.mscale * __dmul_rn(dot_rn(m, perp), dot_rn(fdir, perp));
+        }
+        mfv = -g.mscale * mf;
+        sgz = un.z * g.gscale_fwd;
+        int k = 0;  // local frame: rotated so that edge 0 is the longest
+        if (L[1] > L[k]) k = 1;
+        if (L[2] > L[k]) k = 2;
+        const d3 a = v[k], b = v[(k + 1) % 3], c = v[(k + 2) % 3];
+        const double L0 = L[k];
+        const d3 xh = (b - a) * (1.0 / L0);
+        // On a facet collapsed onto a line the reference's unit normal is
+        // rounding noise and not perpendicular to the edges; the frame must
+        // stay orthonormal for the local coordinates (and so Lambda, which the
+        // reference takes from positions alone) to be right.
+        d3 zh = un - xh * dot3(un, xh);
+        zh = zh * (1.0 / norm3(zh));
+        const d3 yh = cross3(zh, xh);
+        const d3 ca = c - a;
+        const double cx = dot3(ca, xh), cy = dot3(ca, yh);
+        const double L1 = L[(k + 1) % 3], L2 = L[(k + 2) % 3];
+        out[MC_AX] = a.x; out[MC_AY] = a.y; out[MC_AZ] = a.z;
+        out[MC_XX] = xh.x; out[MC_XY] = xh.y; out[MC_XZ] = xh.z;
+        out[MC_YX] = yh.x; out[MC_YY] = yh.y; out[MC_YZ] = yh.z;
+        out[MC_ZX] = zh.x; out[MC_ZY] = zh.y; out[MC_ZZ] = zh.z;
+        out[MC_L0] = L0; out[MC_CX] = cx; out[MC_CY] = cy;
+        out[MC_L1] = L1; out[MC_L2] = L2;
+        if (!(L1 < kEps)) { out[MC_E1X] = (cx - L0) / L1; out[MC_E1Y] = cy / L1; }
+        if (!(L2 < kEps)) { out[MC_E2X] = -cx / L2; out[MC_E2Y] = -cy / L2; }
+        out[MC_SGZ] = sgz;
+        out[MC_MF] = mfv;
+        out[MC_MT0] = mt[k];
+        out[MC_MT1] = mt[(k + 1) % 3];
+        out[MC_MT2] = mt[(k + 2) % 3];
+        out[MC_CENX] = (v[0].x + v[1].x + v[2].x) / 3.0;
+        out[MC_CENY] = (v[0].y + v[1].y + v[2].y) / 3.0;
+        out[MC_CENZ] = (v[0].z + v[1].z + v[2].z) / 3.0;
+        out[MC_SIZE] = L0;
+        out[MC_VALID] = 1.0;
+    }
+    for (int k = 0; k < NMC; ++k) mc[(size_t)k * T + f] = out[k];
+    for (int i = 0; i < 3; ++i) mt2[(size_t)i * T + f] = (float)(2.0 * mt[i]);
+    // the patch facet record, in the patch's frame
+    const int p = facetPatch[f], slot = facetSlot[f];
+    const int nv = vertOff[p + 1] - vertOff[p], ne = edgeOff[p + 1] - edgeOff[p];
+    const double* o = pos + 3 * (size_t)verts[vertOff[p]];
+    const d3 org = mk3(o[0], o[1], o[2]);
+    PatchFacet F;
+    F.corners = corners[facetOff[p] + slot];
+    F.pad0 = 0.f;
+    F.pad1 = 0.f;
+    F.gfacet = f;
+    F.nx = (float)n.x; F.ny = (float)n.y; F.nz = (float)n.z;
+    F.cf = (float)dot3(v[0] - org, n);
+    F.mf2 = (float)(2.0 * mfv);
+    F.gq = (float)(sgz * 0.5 * area2);
+    F.size = valid ? (float)fmax(L[0], fmax(L[1], L[2])) : -1.f;
+    F.l2ab = (float)(L[0] * L[0]); F.l2bc = (float)(L[1] * L[1]); F.l2ca = (float)(L[2] * L[2]);
+    F.cenx = (float)((v[0].x + v[1].x + v[2].x) / 3.0);
+    F.ceny = (float)((v[0].y + v[1].y + v[2].y) / 3.0);
+    F.cenz = (float)((v[0].z + v[1].z + v[2].z) / 3.0);
+    const d3 eb = v[1] - v[0], ec = v[2] - v[0], a0 = v[0] - org;
+    for (int q = 0; q < 3; ++q) {
+        const d3 pq = a0 + eb * (double)kTri3Bb[q] + ec * (double)kTri3Bc[q];
+        F.q3[3 * q] = (float)pq.x; F.q3[3 * q + 1] = (float)pq.y; F.q3[3 * q + 2] = (float)pq.z;
+    }
+    for (int q = 0; q < 6; ++q) {
+        const d3 pq = a0 + eb * (double)kDun6Bb[q] + ec * (double)kDun6Bc[q];
+        F.q6[3 * q] = (float)pq.x; F.q6[3 * q + 1] = (float)pq.y; F.q6[3 * q + 2] = (float)pq.z;
+    }
+    unsigned char* B = blobs + blobOff[p];
+    float4* dst = reinterpret_cast<float4*>(B + kPatchHeadBytes + nv * kPatchVertBytes + ne * kPatchEdgeBytes +
+                                            slot * kPatchFacetBytes);
+    const float4* src = reinterpret_cast<const float4*>(&F);
+#pragma unroll
+    for (int k = 0; k < kPatchFacetBytes / 16; ++k) dst[k] = src[k];
+}
+
+// Per-evaluation records, part 2: one warp per patch writes the header, the
+// patch-frame vertices and the edges (length, summed coefficient and the two
+// users' shares of it, from the facets' mt2 written by k_face_prep_patch).
+__global__ void __launch_bounds__(32) k_patch_prep(int P, const double* __restrict__ pos,
                                                    const int32_t* __restrict__ facetOff,
                                                    const int32_t* __restrict__ facets,
-                                                   const uint32_t* __restrict__ corners,
                                                    const int32_t* __restrict__ vertOff,
                                                    const int32_t* __restrict__ verts,
                                                    const int32_t* __restrict__ edgeOff,
                                                    const uint32_t* __restrict__ edgeInfo,
                                                    const uint8_t* __restrict__ edgeSlot,
-                                                   const int32_t* __restrict__ blobOff,
-                                                   unsigned char* __restrict__ blobs) {
-    __shared__ float share[kPatchFacets][3];
+                                                   const int32_t* __restrict__ blobOff, int T,
+                                                   const float* __restrict__ mt2, unsigned char* __restrict__ blobs) {
     const int p = blockIdx.x, lane = threadIdx.x;
     if (p >= P) return;
     const int f0 = facetOff[p], nf = facetOff[p + 1] - f0;
     const int v0 = vertOff[p], nv = vertOff[p + 1] - v0;
     const int e0 = edgeOff[p], ne = edgeOff[p + 1] - e0;
     unsigned char* B = blobs + blobOff[p];
-    PatchHead* H = reinterpret_cast<PatchHead*>(B);
     PatchVert* PV = reinterpret_cast<PatchVert*>(B + kPatchHeadBytes);
     PatchEdgeA* EA = reinterpret_cast<PatchEdgeA*>(B + kPatchHeadBytes + nv * kPatchVertBytes);
     PatchEdgeB* EB = reinterpret_cast<PatchEdgeB*>(EA + ne);
-    PatchFacet* PF = reinterpret_cast<PatchFacet*>(B + kPatchHeadBytes + nv * kPatchVertBytes + ne * kPatchEdgeBytes);
     const double* o = pos + 3 * (size_t)verts[v0];
     const d3 org = mk3(o[0], o[1], o[2]);
     if (lane == 0) {
         PatchHead h;
         h.nv = nv; h.ne = ne; h.nf = nf; h.nbytes = blobOff[p + 1] - blobOff[p];
         h.ox = org.x; h.oy = org.y; h.oz = org.z; h.pad = 0.0;
-        *H = h;
+        *reinterpret_cast<PatchHead*>(B) = h;
     }
     if (lane < nv) {
         const double* q = pos + 3 * (size_t)verts[v0 + lane];
@@ -109,66 +224,11 @@ __global__ void __launch_bounds__(32) k_patch_prep(int P, const int32_t* __restr
         pv.x = (float)(q[0] - org.x); pv.y = (float)(q[1] - org.y); pv.z = (float)(q[2] - org.z); pv.pad = 0.f;
         PV[lane] = pv;
     }
-    if (lane < nf) {
-        const int f = facets[f0 + lane];
-        d3 v[3];
-        for (int k = 0; k < 3; ++k) {
-            const double* q = pos + 3 * (size_t)tri[3 * f + k];
-            v[k] = mk3(q[0], q[1], q[2]);
-        }
-        PatchFacet F;
-        F.corners = corners[f0 + lane];
-        F.gfacet = f;
-        F.pad0 = 0.f;
-        F.pad1 = 0.f;
-        const d3 n = cross_rn(sub_rn(v[1], v[0]), sub_rn(v[2], v[0]));
-        const double area2 = norm_rn(n);
-        const bool valid = !(area2 < kEps);
-        double mt[3] = {0.0, 0.0, 0.0}, L[3] = {0.0, 0.0, 0.0}, mfv = 0.0, sgz = 0.0;
-        const GroupConst& g = groups[face_group[f]];
-        for (int i = 0; i < 3; ++i) L[i] = norm_rn(sub_rn(v[(i + 1) % 3], v[i]));
-        if (valid) {
-            const d3 un = div_rn(n, area2);
-            const d3 m = mk3(g.mdir[0], g.mdir[1], g.mdir[2]);
-            mfv = -g.mscale * __dmul_rn(dot_rn(m, un), dot_rn(fdir, un));
-            for (int i = 0; i < 3; ++i) {
-                const d3 e = sub_rn(v[(i + 1) % 3], v[i]);
-                const d3 eh = (L[i] < kEps) ? mk3(0, 0, 0) : div_rn(e, L[i]);
-                const d3 perp = cross_rn(un, eh);
-                mt[i] = -g.mscale * __dmul_rn(dot_rn(m, perp), dot_rn(fdir, perp));
-            }
-            sgz = un.z * g.gscale_fwd;
-        }
-        F.nx = (float)n.x; F.ny = (float)n.y; F.nz = (float)n.z;
-        F.cf = (float)dot3(v[0] - org, n);
-        F.mf2 = (float)(2.0 * mfv);
-        F.gq = (float)(sgz * 0.5 * area2);
-        F.size = valid ? (float)fmax(L[0], fmax(L[1], L[2])) : -1.f;
-        F.l2ab = (float)(L[0] * L[0]); F.l2bc = (float)(L[1] * L[1]); F.l2ca = (float)(L[2] * L[2]);
-        F.cenx = (float)((v[0].x + v[1].x + v[2].x) / 3.0);
-        F.ceny = (float)((v[0].y + v[1].y + v[2].y) / 3.0);
-        F.cenz = (float)((v[0].z + v[1].z + v[2].z) / 3.0);
-        const d3 eb = v[1] - v[0], ec = v[2] - v[0], a0 = v[0] - org;
-        for (int q = 0; q < 3; ++q) {
-            const d3 pq = a0 + eb * (double)kTri3Bb[q] + ec * (double)kTri3Bc[q];
-            F.q3[3 * q] = (float)pq.x; F.q3[3 * q + 1] = (float)pq.y; F.q3[3 * q + 2] = (float)pq.z;
-        }
-        for (int q = 0; q < 6; ++q) {
-            const d3 pq = a0 + eb * (double)kDun6Bb[q] + ec * (double)kDun6Bc[q];
-            F.q6[3 * q] = (float)pq.x; F.q6[3 * q + 1] = (float)pq.y; F.q6[3 * q + 2] = (float)pq.z;
-        }
-        const float4* src = reinterpret_cast<const float4*>(&F);
-        float4* dst = reinterpret_cast<float4*>(PF + lane);
-#pragma unroll
-        for (int k = 0; k < kPatchFacetBytes / 16; ++k) dst[k] = src[k];
-        for (int i = 0; i < 3; ++i) share[lane][i] = (float)(2.0 * mt[i]);
-    }
-    __syncwarp();
     for (int e = lane; e < ne; e += 32) {
-        const uint32_t info = edgeInfo[e0 + e], slot = edgeSlot[e0 + e];
+        const uint32_t info = edgeInfo[e0 + e], sl = edgeSlot[e0 + e];
         const int lv1 = info & 0xff, lv2 = (info >> 8) & 0xff, lf1 = (info >> 16) & 0xff, lf2 = info >> 24;
-        const float m1 = share[lf1][slot & 3];
-        const float m2 = lf2 != kNoFacet ? share[lf2][(slot >> 2) & 3] : 0.f;
+        const float m1 = mt2[(size_t)(sl & 3) * T + facets[f0 + lf1]];
+        const float m2 = lf2 != kNoFacet ? mt2[(size_t)((sl >> 2) & 3) * T + facets[f0 + lf2]] : 0.f;
         const double* qa = pos + 3 * (size_t)verts[v0 + lv1];
         const double* qb = pos + 3 * (size_t)verts[v0 + lv2];
         PatchEdgeA a;
