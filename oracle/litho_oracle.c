@@ -179,6 +179,34 @@ static double face_central(const facefn *f, v3 obs, v3 a, v3 b, v3 c, int which,
     return (fp - fm) / (2.0 * h);
 }
 
+/* Distance from o to the triangle abc (closest point by the Voronoi regions
+ * of the vertices, edges and face: Ericson, Real-Time Collision Detection,
+ * sec. 5.1.5).  Sizes the adaptive step of the true derivative. */
+static double point_triangle_distance(v3 o, v3 a, v3 b, v3 c) {
+    v3 ab = sub(b, a), ac = sub(c, a), ap = sub(o, a);
+    double d1 = dot(ab, ap), d2 = dot(ac, ap);
+    if (d1 <= 0.0 && d2 <= 0.0) return norm(ap);
+    v3 bp = sub(o, b);
+    double d3 = dot(ab, bp), d4 = dot(ac, bp);
+    if (d3 >= 0.0 && d4 <= d3) return norm(bp);
+    double vc = d1 * d4 - d3 * d2;
+    if (vc <= 0.0 && d1 >= 0.0 && d3 <= 0.0) return norm(sub(ap, scl(ab, d1 / (d1 - d3))));
+    v3 cp = sub(o, c);
+    double d5 = dot(ab, cp), d6 = dot(ac, cp);
+    if (d6 >= 0.0 && d5 <= d6) return norm(cp);
+    double vb = d5 * d2 - d1 * d6;
+    if (vb <= 0.0 && d2 >= 0.0 && d6 <= 0.0) return norm(sub(ap, scl(ac, d2 / (d2 - d6))));
+    double va = d3 * d6 - d5 * d4;
+    if (va <= 0.0 && (d4 - d3) >= 0.0 && (d5 - d6) >= 0.0) {
+        double w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+        return norm(sub(bp, scl(sub(c, b), w)));
+    }
+    double den = va + vb + vc;
+    if (!(fabs(den) > 0.0)) return norm(ap); /* degenerate triangle */
+    double v = vb / den, w = vc / den;
+    return norm(sub(ap, add(scl(ab, v), scl(ac, w))));
+}
+
 static void face_true_gradient(const facefn *f, v3 obs, v3 a, v3 b, v3 c, double h,
                                v3 *ga, v3 *gb, v3 *gc) {
     v3 *out[3] = {ga, gb, gc};
@@ -364,7 +392,8 @@ void lo_forward_tmi(int S, const double *sta, int G, const int32_t *grp_tri_off,
 /* computeGravityAnalyticJacobian gravity_forward.cpp:184-292 and           */
 /* computeMagneticAnalyticJacobian magnetic_forward.cpp:196-306.            */
 /*  - per (station, face): forward-FD gradient, h = 1e-4 (kind < 2) or the  */
-/*    Richardson central "true" derivative (kind >= 2, test truth only);    */
+/*    Richardson central "true" derivative (kind >= 2, test truth only;     */
+/*    step true_h, or -true_h x the station-triangle distance if < 0);     */
 /*  - vertex gradients accumulated per mesh with faceScale;                 */
 /*  - gather: J(i, dof) += vg[vertex][axis] * axisScale for each ref,       */
 /*    skipping |vg| < 1e-30 (reference semantics, kind < 2 only).           */
@@ -399,9 +428,20 @@ void lo_jacobian(int kind, int S, const double *sta, int G, const int32_t *grp_t
                 int ia = tri[3 * t], ib = tri[3 * t + 1], ic = tri[3 * t + 2];
                 v3 ga, gb, gc; double val;
                 if (truth && collapsed(mk(pos + 3 * ia), mk(pos + 3 * ib), mk(pos + 3 * ic))) continue;
-                if (truth)
-                    face_true_gradient(&f, o, mk(pos + 3 * ia), mk(pos + 3 * ib), mk(pos + 3 * ic),
-                                       true_h, &ga, &gb, &gc);
+                if (truth) {
+                    /* true_h > 0: that step; true_h < 0: |true_h| x the
+                     * station-triangle distance (floor 1e-6 m), which keeps the
+                     * O(h^4) truncation and the 1/h rounding both small for
+                     * near and far facets alike */
+                    double h = true_h;
+                    if (h < 0.0) {
+                        h = -true_h * point_triangle_distance(o, mk(pos + 3 * ia), mk(pos + 3 * ib),
+                                                              mk(pos + 3 * ic));
+                        if (h < 1e-6) h = 1e-6;
+                    }
+                    face_true_gradient(&f, o, mk(pos + 3 * ia), mk(pos + 3 * ib), mk(pos + 3 * ic), h, &ga,
+                                       &gb, &gc);
+                }
                 else
                     face_with_fd_gradient(&f, o, mk(pos + 3 * ia), mk(pos + 3 * ib),
                                           mk(pos + 3 * ic), &val, &ga, &gb, &gc);

@@ -489,17 +489,20 @@ def _jacobian_worker(args):
     return om.jacobian(sta, kind, true_h=true_h)
 
 
-# Step of the Richardson "true" derivative for models whose DOF vertices lie
-# far (>= ~100 m) from every station: the reference's oriented line-integral
-# form loses digits for edges nearly collinear with a station, and a central
-# difference amplifies that rounding by 1/h (on the icosphere the truth moves
-# by 2e-6 between h = 1e-2 and 0.3, and by 4e-8 between 0.3 and 1), while
-# the O(h^4) truncation at 100 m stays below 1e-9.
-FAR_TRUE_H = 0.3
+# Step of the Richardson "true" derivative used by the full-size tests: a
+# negative value makes the oracle take |TRUE_H| x the station-triangle
+# distance per (station, facet).  A fixed step cannot serve every facet: the
+# reference's oriented line-integral form loses digits for edges nearly
+# collinear with a station, which a central difference amplifies by 1/h (on
+# the icosphere the fixed 1e-2 m truth is 2.3e-6 off), while facets of deep
+# DOF vertices can reach within 1 m of a station, where a large fixed step
+# has O((h / d)^4) truncation.  The adaptive step converges on both (5e-8 on
+# the icosphere, 1e-10 on the voxel model, between factors 1e-3 and 1e-2).
+TRUE_H = -3e-3
 
 
 def jacobian_parallel(tables, densities, susceptibilities, inducing, params, sta, kind, procs=None,
-                      true_h=FAR_TRUE_H):
+                      true_h=TRUE_H):
     """OracleModel(...).scatter(params) then .jacobian(sta, kind), split over
     station chunks in spawned processes (spawned, not forked: the calling
     process may already hold a CUDA context).  Each process starts from the

@@ -17,7 +17,7 @@ joint_objective.cpp, lbfgsb_optimizer.cpp in oracle/_ref).
 import numpy as np
 import pytest
 
-from oracle_bindings import FAR_TRUE_H, OracleModel, RefModel, ref_available
+from oracle_bindings import TRUE_H, OracleModel, RefModel, ref_available
 from lithoinv3d_b200 import library_path
 from test_gpu_inversion import BOUND, c1_data, c1_problem
 
@@ -43,7 +43,7 @@ def test_reference_objective_and_optimizer_on_gpu_operators():
     truth.scatter(x)
     for kind, gpu_j, cpu_j in ((2, gpu.jacobian_gz(x), cpu.jacobian_gz(x)), (3, gpu.jacobian_tmi(x),
                                                                               cpu.jacobian_tmi(x))):
-        true_j = truth.jacobian(p.grav_xyz, kind, true_h=FAR_TRUE_H)
+        true_j = truth.jacobian(p.grav_xyz, kind, true_h=TRUE_H)
         assert rel(gpu_j, true_j) < 1e-6
         assert rel(cpu_j, true_j) < 1e-3 and rel(gpu_j, cpu_j) < 1e-3
     o_cpu, o_gpu = cpu.objective(x), gpu.objective(x)
