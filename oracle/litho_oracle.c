@@ -167,16 +167,84 @@ static void face_with_fd_gradient(const facefn *f, v3 obs, v3 a, v3 b, v3 c,
     }
 }
 
-/* Central-difference derivative of one face term with one Richardson step
- * (error O(h^4)).  NOT part of the reference: this is the "true derivative"
- * the analytic device gradient is checked against. */
-static double face_central(const facefn *f, v3 obs, v3 a, v3 b, v3 c, int which, int k, double h) {
-    v3 vp[3] = {a, b, c}, vm[3] = {a, b, c};
-    setc(&vp[which], k, comp(vp[which], k) + h);
-    setc(&vm[which], k, comp(vm[which], k) - h);
-    double fp = face_eval(f, obs, vp[0], vp[1], vp[2]);
-    double fm = face_eval(f, obs, vm[0], vm[1], vm[2]);
-    return (fp - fm) / (2.0 * h);
+/* ------------------------------------------------------------------------ */
+/* The "true derivative" (NOT part of the reference; the analytic device   */
+/* gradient is checked against it): a central difference with one           */
+/* Richardson step (error O(h^4)) of the same facet formulas evaluated in   */
+/* x87 extended precision (64-bit significand).  The reference's oriented   */
+/* line-integral form loses digits for edges nearly collinear with the      */
+/* station, and a central difference divides that rounding by h; with 11    */
+/* more bits the step can follow the facet's own scale (see lo_jacobian)    */
+/* instead of being held large to keep the rounding down.                   */
+/* ------------------------------------------------------------------------ */
+typedef long double ld;
+typedef struct { ld x, y, z; } l3;
+
+static inline l3 lmk(v3 a) { l3 r = {a.x, a.y, a.z}; return r; }
+static inline l3 lsub(l3 a, l3 b) { l3 r = {a.x - b.x, a.y - b.y, a.z - b.z}; return r; }
+static inline l3 ldvs(l3 a, ld s) { l3 r = {a.x / s, a.y / s, a.z / s}; return r; }
+static inline ld ldot(l3 a, l3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline l3 lcross(l3 a, l3 b) {
+    l3 r = {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+    return r;
+}
+static inline ld lnorm(l3 a) { return sqrtl(ldot(a, a)); }
+
+static ld l_solid_angle(l3 a, l3 b, l3 c, l3 o) {
+    l3 ra = lsub(a, o), rb = lsub(b, o), rc = lsub(c, o);
+    ld la = lnorm(ra), lb = lnorm(rb), lc = lnorm(rc);
+    if (la < LO_EPS || lb < LO_EPS || lc < LO_EPS) return 0.0L;
+    ld num = ldot(ra, lcross(rb, rc));
+    ld den = la * lb * lc + ldot(ra, rb) * lc + ldot(ra, rc) * lb + ldot(rb, rc) * la;
+    return 2.0L * atan2l(num, den);
+}
+
+static ld l_line_integral_term(l3 a, l3 b, l3 o) {
+    l3 ra = lsub(a, o), rb = lsub(b, o), e = lsub(b, a);
+    ld L = lnorm(e);
+    if (L < LO_EPS) return 0.0L;
+    ld s1 = ldot(ra, e) / L, s2 = ldot(rb, e) / L;
+    ld d1 = lnorm(ra), d2 = lnorm(rb);
+    ld num = s2 + d2, den = s1 + d1;
+    if (fabsl(den) < LO_EPS) return 0.0L;
+    if (num <= 0.0L || den <= 0.0L) return 0.0L;
+    return logl(num / den);
+}
+
+/* face_nagy / magnetic_facet above, term for term. */
+static ld l_face_eval(const facefn *f, l3 obs, l3 a, l3 b, l3 c) {
+    l3 n = lcross(lsub(b, a), lsub(c, a));
+    ld area_x2 = lnorm(n);
+    if (area_x2 < LO_EPS) return 0.0L;
+    l3 un = ldvs(n, area_x2);
+    ld omega = l_solid_angle(a, b, c, obs);
+    l3 md = lmk(f->mdir), fd = lmk(f->fdir);
+    ld acc = f->kind == 0 ? -ldot(lsub(a, obs), un) * omega : ldot(md, un) * ldot(fd, un) * omega;
+    l3 vs[3] = {a, b, c};
+    for (int i = 0; i < 3; ++i) {
+        l3 p1 = vs[i], p2 = vs[(i + 1) % 3];
+        l3 e = lsub(p2, p1);
+        ld L = lnorm(e);
+        if (L < LO_EPS) continue;
+        l3 perp = lcross(un, ldvs(e, L));
+        ld lam = l_line_integral_term(p1, p2, obs);
+        acc += (f->kind == 0 ? ldot(lsub(obs, p1), perp) : ldot(md, perp) * ldot(fd, perp)) * lam;
+    }
+    return f->kind == 0 ? un.z * acc : acc;
+}
+
+static ld lcomp(l3 a, int k) { return k == 0 ? a.x : (k == 1 ? a.y : a.z); }
+static void lsetc(l3 *a, int k, ld v) {
+    if (k == 0) a->x = v; else if (k == 1) a->y = v; else a->z = v;
+}
+
+static ld face_central(const facefn *f, l3 obs, l3 a, l3 b, l3 c, int which, int k, ld h) {
+    l3 vp[3] = {a, b, c}, vm[3] = {a, b, c};
+    lsetc(&vp[which], k, lcomp(vp[which], k) + h);
+    lsetc(&vm[which], k, lcomp(vm[which], k) - h);
+    ld fp = l_face_eval(f, obs, vp[0], vp[1], vp[2]);
+    ld fm = l_face_eval(f, obs, vm[0], vm[1], vm[2]);
+    return (fp - fm) / (2.0L * h);
 }
 
 /* Distance from o to the triangle abc (closest point by the Voronoi regions
@@ -210,12 +278,20 @@ static double point_triangle_distance(v3 o, v3 a, v3 b, v3 c) {
 static void face_true_gradient(const facefn *f, v3 obs, v3 a, v3 b, v3 c, double h,
                                v3 *ga, v3 *gb, v3 *gc) {
     v3 *out[3] = {ga, gb, gc};
+    l3 lo = lmk(obs), la = lmk(a), lb = lmk(b), lc = lmk(c);
     for (int w = 0; w < 3; ++w)
         for (int k = 0; k < 3; ++k) {
-            double d1 = face_central(f, obs, a, b, c, w, k, h);
-            double d2 = face_central(f, obs, a, b, c, w, k, 0.5 * h);
-            setc(out[w], k, (4.0 * d2 - d1) / 3.0);
+            ld d1 = face_central(f, lo, la, lb, lc, w, k, h);
+            ld d2 = face_central(f, lo, la, lb, lc, w, k, 0.5L * h);
+            setc(out[w], k, (double)((4.0L * d2 - d1) / 3.0L));
         }
+}
+
+/* Smallest altitude of the triangle abc (twice-area / longest edge): the
+ * scale on which its unit normal, and with it the facet term, turns. */
+static double min_altitude(v3 a, v3 b, v3 c) {
+    double lm = fmax(norm(sub(b, a)), fmax(norm(sub(c, b)), norm(sub(a, c))));
+    return lm > 0.0 ? norm(cross(sub(b, a), sub(c, a))) / lm : 0.0;
 }
 
 /* A facet collapsed onto a line (twice-area < 1e-10 * longest edge^2): its
@@ -342,6 +418,54 @@ void lo_scatter(int np, const double *params, const int32_t *dof_off, const int3
     }
 }
 
+/* Adjoint of lo_scatter (no reference counterpart: the reference gathers   */
+/* vertex derivatives at the DOF vertices only, gravity_forward.cpp:270-289 */
+/* and magnetic_forward.cpp's copy of it).  Maps a gradient with respect to */
+/* the scattered positions, vg[3V], to the parameters: the three steps of   */
+/* lo_scatter transposed in reverse order.  vg is overwritten (scratch).    */
+/*  3'. averaging: every member of a group of >= 2 receives the mean of the  */
+/*      group's gradients (the averaging matrix is symmetric);              */
+/*  2'. interpolation: a row's gradient moves to its sources with the row's  */
+/*      weights, and the row keeps none (its position is overwritten);      */
+/*  1'. DOF writes: grad[d] = sum over d's slots of scale x vg[slot].        */
+/* ------------------------------------------------------------------------ */
+void lo_chain_gather(int V, double *vg, int np, const int32_t *dof_off, const int32_t *ref_vertex,
+                     const uint8_t *ref_axis, const double *ref_scale, const int32_t *interp_off,
+                     const int32_t *interp_src, const double *interp_w, int ns, const int32_t *sync_off,
+                     const int32_t *sync_vertex, double *grad) {
+    for (int s = 0; s < ns; ++s) {
+        int b = sync_off[s], e = sync_off[s + 1];
+        if (e - b < 2) continue;
+        v3 sum = {0.0, 0.0, 0.0};
+        for (int k = b; k < e; ++k) sum = add(sum, mk(vg + 3 * sync_vertex[k]));
+        sum = dvs(sum, (double)(e - b));
+        for (int k = b; k < e; ++k) {
+            vg[3 * sync_vertex[k]] = sum.x;
+            vg[3 * sync_vertex[k] + 1] = sum.y;
+            vg[3 * sync_vertex[k] + 2] = sum.z;
+        }
+    }
+    if (interp_off) {
+        for (int v = 0; v < V; ++v) {
+            int b = interp_off[v], e = interp_off[v + 1];
+            if (b == e) continue;
+            v3 g = mk(vg + 3 * v);
+            for (int k = b; k < e; ++k) {
+                double *q = vg + 3 * interp_src[k];
+                q[0] += interp_w[k] * g.x;
+                q[1] += interp_w[k] * g.y;
+                q[2] += interp_w[k] * g.z;
+            }
+            vg[3 * v] = vg[3 * v + 1] = vg[3 * v + 2] = 0.0;
+        }
+    }
+    for (int d = 0; d < np; ++d) {
+        double acc = 0.0;
+        for (int r = dof_off[d]; r < dof_off[d + 1]; ++r) acc += ref_scale[r] * vg[3 * ref_vertex[r] + ref_axis[r]];
+        grad[d] = acc;
+    }
+}
+
 /* ------------------------------------------------------------------------ */
 /* Forward: GravityForward::compute gravity_forward.cpp:105-118 ->          */
 /* computeUnitGravity :124-130 -> gravityClosedMesh :162-178.                */
@@ -393,7 +517,8 @@ void lo_forward_tmi(int S, const double *sta, int G, const int32_t *grp_tri_off,
 /* computeMagneticAnalyticJacobian magnetic_forward.cpp:196-306.            */
 /*  - per (station, face): forward-FD gradient, h = 1e-4 (kind < 2) or the  */
 /*    Richardson central "true" derivative (kind >= 2, test truth only;     */
-/*    step true_h, or -true_h x the station-triangle distance if < 0);     */
+/*    step true_h, or -true_h x min(station-triangle distance, smallest    */
+/*    altitude) if < 0; extended precision);                               */
 /*  - vertex gradients accumulated per mesh with faceScale;                 */
 /*  - gather: J(i, dof) += vg[vertex][axis] * axisScale for each ref,       */
 /*    skipping |vg| < 1e-30 (reference semantics, kind < 2 only).           */
@@ -430,14 +555,17 @@ void lo_jacobian(int kind, int S, const double *sta, int G, const int32_t *grp_t
                 if (truth && collapsed(mk(pos + 3 * ia), mk(pos + 3 * ib), mk(pos + 3 * ic))) continue;
                 if (truth) {
                     /* true_h > 0: that step; true_h < 0: |true_h| x the
-                     * station-triangle distance (floor 1e-6 m), which keeps the
-                     * O(h^4) truncation and the 1/h rounding both small for
-                     * near and far facets alike */
+                     * smaller of the station-triangle distance and the
+                     * triangle's smallest altitude (floor 1e-9 m), the two
+                     * scales of the facet term, so that the O(h^4)
+                     * truncation stays small for near, far and thin facets
+                     * alike; the extended-precision evaluation keeps the
+                     * 1/h rounding below it */
                     double h = true_h;
                     if (h < 0.0) {
-                        h = -true_h * point_triangle_distance(o, mk(pos + 3 * ia), mk(pos + 3 * ib),
-                                                              mk(pos + 3 * ic));
-                        if (h < 1e-6) h = 1e-6;
+                        v3 pa = mk(pos + 3 * ia), pb = mk(pos + 3 * ib), pc = mk(pos + 3 * ic);
+                        h = -true_h * fmin(point_triangle_distance(o, pa, pb, pc), min_altitude(pa, pb, pc));
+                        if (h < 1e-9) h = 1e-9;
                     }
                     face_true_gradient(&f, o, mk(pos + 3 * ia), mk(pos + 3 * ib), mk(pos + 3 * ic), h, &ga,
                                        &gb, &gc);

@@ -69,6 +69,9 @@ def oracle() -> C.CDLL:
         lib.lo_jacobian.restype = None
         lib.lo_jacobian.argtypes = [C.c_int, C.c_int, _dp, C.c_int, _ip, _ip, C.c_int, _dp, _dp, _dp, _dp, _dp,
                                     C.c_int, _ip, _ip, _u8p, _dp, C.c_double, _dp]
+        lib.lo_chain_gather.restype = None
+        lib.lo_chain_gather.argtypes = [C.c_int, _dp, C.c_int, _ip, _ip, _u8p, _dp, _ip, _ip, _dp, C.c_int, _ip, _ip,
+                                        _dp]
         lib.lo_misfit.restype = C.c_double
         lib.lo_misfit.argtypes = [C.c_int, _dp, _dp, _dp]
         lib.lo_misfit_gradient.restype = None
@@ -449,6 +452,46 @@ class OracleModel:
                            t["ref_axis"].ctypes.data_as(_u8p), t["ref_scale"].ctypes.data_as(_dp), true_h,
                            J.ctypes.data_as(_dp))
         return J
+
+    def vertex_jacobian(self, sta, kind, true_h=-3e-3):
+        """Jacobian with respect to every vertex coordinate, columns 3 v + axis
+        (kind 2 gravity / 3 magnetic true derivative, 0 / 1 the reference's
+        per-facet forward differences)."""
+        sta = np.ascontiguousarray(sta, np.float64)
+        V = self.pos.size // 3
+        dof_off = np.arange(3 * V + 1, dtype=np.int32)
+        ref_vertex = np.repeat(np.arange(V, dtype=np.int32), 3)
+        ref_axis = np.tile(np.arange(3, dtype=np.uint8), V)
+        ref_scale = np.ones(3 * V)
+        J = np.zeros((len(sta), 3 * V))
+        t = self.t
+        self.o.lo_jacobian(kind, len(sta), sta.ctypes.data_as(_dp), self.G, self._ip("grp_tri_off"),
+                           self._ip("tri"), V, self.pos.ctypes.data_as(_dp), self.rho.ctypes.data_as(_dp),
+                           self.amp.ctypes.data_as(_dp), self.mdir.ctypes.data_as(_dp),
+                           self.fdir.ctypes.data_as(_dp), 3 * V, dof_off.ctypes.data_as(_ip),
+                           ref_vertex.ctypes.data_as(_ip), ref_axis.ctypes.data_as(_u8p), _d(ref_scale), true_h,
+                           J.ctypes.data_as(_dp))
+        return J
+
+    def chain_gather(self, vg):
+        """Gradient with respect to the parameters from one with respect to the
+        scattered positions (vg[3V]): lo_chain_gather, the adjoint of scatter."""
+        t = self.t
+        vg = np.array(vg, np.float64).ravel().copy()
+        out = np.zeros(self.np)
+        self.o.lo_chain_gather(len(self.pos), vg.ctypes.data_as(_dp), self.np, self._ip("dof_off"),
+                               self._ip("ref_vertex"), t["ref_axis"].ctypes.data_as(_u8p),
+                               t["ref_scale"].ctypes.data_as(_dp), self._ip("interp_off"), self._ip("interp_src"),
+                               t["interp_w"].ctypes.data_as(_dp), len(t["sync_off"]) - 1, self._ip("sync_off"),
+                               self._ip("sync_vertex"), out.ctypes.data_as(_dp))
+        return out
+
+    def chain_jacobian(self, sta, kind, true_h=-3e-3):
+        """Derivative of the forward at the scattered positions with respect to
+        the parameters through the whole scatter (DOF writes, control-point
+        interpolation, shared-vertex averaging)."""
+        Jv = self.vertex_jacobian(sta, kind, true_h)
+        return np.stack([self.chain_gather(row) for row in Jv]) if len(Jv) else np.zeros((0, self.np))
 
 
 def misfit(pred, obs, std):
