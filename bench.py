@@ -127,6 +127,13 @@ def parse():
                          "large: the 194k-facet single inversion")
     ap.add_argument("--lbfgs-iters", type=int, default=0,
                     help="after timing, run this many L-BFGS-B iterations and report their wall time")
+    ap.add_argument("--gather", choices=["reference", "chain"], default="reference",
+                    help="objective-gradient gather: the reference's DOF-vertex gather, or the exact derivative "
+                         "through the control-point interpolation and shared-vertex averaging")
+    ap.add_argument("--xy-derivative", choices=["analytic", "fd"], default="analytic",
+                    help="x/y vertex derivatives of the gradient: closed form, or per-facet forward differences "
+                         "with --xy-step (the large-inversion configuration's h = 0.5 m)")
+    ap.add_argument("--xy-step", type=float, default=0.5)
     args = ap.parse_args()
     if args.steps is None:
         args.steps = 50 if args.impl == "reference" else {"contact": 1000, "large": 20, "batch": 5}.get(args.workload, 50)
@@ -489,6 +496,14 @@ def main():
     if args.workload == "large":  # reference-model regularisation around the start (reference_model.cpp:16-25)
         ctx.set_objective(alpha_mag=1.0, ref_weight=1e-3, ref_params=x0)
         ctx.set_scatter_stateless(True)
+    if args.gather == "chain":
+        from lithoinv3d_b200 import GATHER_CHAIN
+
+        ctx.set_gradient_gather(GATHER_CHAIN)
+    if args.xy_derivative == "fd":
+        from lithoinv3d_b200 import XY_FORWARD_DIFFERENCE
+
+        ctx.set_xy_derivative(XY_FORWARD_DIFFERENCE, args.xy_step)
     ctx.set_graph_mode(True)
     tuned, _ = ctx.autotune(x0, repeats=3)
     np_ = model.n_dofs
@@ -608,6 +623,9 @@ def main():
             "config": workload_config(args.workload, p.n_triangles(), len(p.grav_xyz), np_, args.bodies),
             "details": {"parallelism": f"replicas x{world}", "precision": args.precision,
                         "fp64_near_pair_fraction": round(near_frac, 4), "cuda_graph": True,
+                        "gradient_gather": args.gather,
+                        "xy_derivative": (f"forward difference, h = {args.xy_step} m" if args.xy_derivative == "fd"
+                                          else "analytic"),
                         "tuning": {"fwd_target_blocks": tuned.fwd_target_blocks,
                                    "grad_target_warps": tuned.grad_target_warps,
                                    "near_tiles_per_chunk": tuned.near_tiles_per_chunk,
@@ -628,7 +646,8 @@ def main():
         f0 = ctx.objective(x0)
         line["details"]["lbfgsb"] = {"iterations": res.iterations, "evaluations": res.evaluations,
                                     "gradients": res.gradients, "wall_s": wall, "objective_start": f0,
-                                    "objective_final": res.final_value}
+                                    "objective_final": res.final_value, "message": res.message.decode(),
+                                    "gather": args.gather}
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "contact":
         try:
             line["cpu_baseline"] = cpu_baseline(p, x0, gobs, gstd, mobs, mstd, args.cpu_stations)

@@ -325,6 +325,40 @@ lf_status lf_set_device_wait_limit(long long polls);
  * given to lf_set_model, so the evaluation at p depends on p alone. */
 lf_status lf_set_scatter_stateless(lf_ctx* ctx, int enabled);
 
+/* Gradient gather of the objective gradient (lf_objective_grad,
+ * lf_objective_grad_device, graph mode).  No reference counterpart.
+ *  LF_GATHER_REFERENCE (default): the reference's gather -- the vertex
+ *    gradient read at each DOF's own (vertex, axis) slots times the axis scale
+ *    (gravity_forward.cpp:270-289, magnetic_forward.cpp's copy).  With
+ *    control-point interpolation or shared-vertex averaging this is not the
+ *    derivative of the objective: vertices that follow the control points
+ *    contribute nothing, and a line search along it can fail to descend.
+ *  LF_GATHER_CHAIN: the exact derivative of the objective with respect to
+ *    the parameters through the whole scatter -- the vertex gradient (misfit
+ *    plus weighted smoothness) mapped back through the averaging and the
+ *    interpolation, then gathered as above.  The gradient is computed at
+ *    every vertex whose position depends on the parameters, so the gradient
+ *    kernels cover more facets.  With lf_set_scatter_stateless it is the
+ *    gradient of a function of p alone.
+ * lf_jacobian and the calibration products keep the reference's gather. */
+enum { LF_GATHER_REFERENCE = 0, LF_GATHER_CHAIN = 1 };
+lf_status lf_set_gradient_gather(lf_ctx* ctx, int mode);
+
+/* x / y vertex derivatives of the objective gradient.
+ *  LF_XY_ANALYTIC (default): closed-form derivatives on every axis.
+ *  LF_XY_FORWARD_DIFFERENCE: x and y by per-facet forward differences of the
+ *    reference's facet formula with the given step (metres; the
+ *    large-inversion configuration uses 0.5), z analytic -- the reference's
+ *    per-facet differencing (faceNagyWithGradient gravity_forward.cpp:48-85,
+ *    magneticFacetWithGradient magnetic_forward.cpp:14-50, there with
+ *    h = 1e-4 on every axis) restricted to x and y.  Evaluated in FP64 in
+ *    both precision modes (six moved copies of each gradient facet per
+ *    station).  Facets collapsed onto a line contribute zero, as in the
+ *    analytic path.  lf_jacobian keeps its analytic derivatives.
+ * step is ignored for LF_XY_ANALYTIC; otherwise it must be positive. */
+enum { LF_XY_ANALYTIC = 0, LF_XY_FORWARD_DIFFERENCE = 1 };
+lf_status lf_set_xy_derivative(lf_ctx* ctx, int mode, double step);
+
 /* Graph mode (no reference counterpart: the reference evaluates on one CPU
  * thread).  When enabled, lf_objective, lf_objective_grad and
  * lf_objective_grad_device replay a CUDA graph of the whole evaluation

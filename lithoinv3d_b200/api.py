@@ -19,6 +19,8 @@ from ._native import Counters, LbfgsbOptions, LbfgsbResult, ModelInfo, Tuning
 FIXED, Z_ONLY, X_ONLY, Y_ONLY, ALONG_VECTOR, XY_FREE, XZ_FREE, YZ_FREE, XYZ_FREE = range(9)
 GRAVITY, MAGNETIC = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
+GATHER_REFERENCE, GATHER_CHAIN = 0, 1
+XY_ANALYTIC, XY_FORWARD_DIFFERENCE = 0, 1
 UNIT_GRAVITY, UNIT_INDUCED, UNIT_DIRECTION, UNIT_REMANENCE = range(4)
 
 
@@ -375,6 +377,18 @@ class Context:
     def set_scatter_stateless(self, enabled: bool = True):
         """Every scatter from the model's given positions (lf_set_scatter_stateless)."""
         self._check(self.lib.lf_set_scatter_stateless(self.h, int(bool(enabled))), "set_scatter_stateless")
+
+    def set_gradient_gather(self, mode: int):
+        """GATHER_REFERENCE (the reference's DOF-vertex gather) or GATHER_CHAIN
+        (the objective's exact derivative through the control-point
+        interpolation and shared-vertex averaging); lf_set_gradient_gather."""
+        self._check(self.lib.lf_set_gradient_gather(self.h, int(mode)), "set_gradient_gather")
+
+    def set_xy_derivative(self, mode: int, step: float = 0.5):
+        """XY_ANALYTIC, or XY_FORWARD_DIFFERENCE: x / y vertex derivatives of the
+        objective gradient by per-facet forward differences with `step` metres
+        (FP64), z analytic; lf_set_xy_derivative."""
+        self._check(self.lib.lf_set_xy_derivative(self.h, int(mode), float(step)), "set_xy_derivative")
 
     def set_graph_mode(self, enabled: bool = True):
         """Replay evaluations as a captured CUDA graph (lf_set_graph_mode)."""

@@ -142,6 +142,20 @@ struct lf_ctx {
     DevBuf<double> d_pos0;          // the model's positions as given
     DevBuf<double> d_vel, d_posSave, d_tmpP, d_tmpS;  // matrix-free products (calibration)
     std::vector<int32_t> hGradFacets;
+    // Gradient gather (lf_set_gradient_gather): LF_GATHER_REFERENCE reads the
+    // vertex gradient at the DOF vertices only; LF_GATHER_CHAIN first maps it
+    // back through the shared-vertex averaging and the control-point
+    // interpolation.  The vertex / facet sets each mode needs, per model.
+    int gatherMode = 0;
+    std::vector<int32_t> hGvertsRef, hGvertsChain, hGfacetsRef, hGfacetsChain;
+    std::vector<uint8_t> hFneedRef, hFneedChain;
+    DevBuf<int32_t> d_adjOff, d_adjRow;  // interpolation transposed: source -> (row, weight)
+    DevBuf<double> d_adjW, d_vgrad2;
+    // lf_set_xy_derivative: x and y vertex derivatives of the objective
+    // gradient by per-facet forward differences with step xyStep (FP64)
+    int xyMode = 0;
+    double xyStep = 0.5;
+    DevBuf<double> d_fcfd;  // [7][NFC][nGradFacets] moved-facet constants
 
     // forward chunking (plan cached per station count and group filter;
     // uploaded only when it changes)
@@ -565,6 +579,22 @@ static lf_status upload_groups(lf_ctx* c) {
     return LF_OK;
 }
 
+// Vertex / facet sets of the current gather mode onto the device.
+static lf_status apply_gather_sets(lf_ctx* c) {
+    const bool chain = c->gatherMode == LF_GATHER_CHAIN;
+    const std::vector<int32_t>& gv = chain ? c->hGvertsChain : c->hGvertsRef;
+    const std::vector<int32_t>& gf = chain ? c->hGfacetsChain : c->hGfacetsRef;
+    const std::vector<uint8_t>& fn = chain ? c->hFneedChain : c->hFneedRef;
+    c->nGradVerts = static_cast<int>(gv.size());
+    c->nGradFacets = static_cast<int>(gf.size());
+    c->hGradFacets = gf;
+    if (!gf.empty()) LF_TRY_CUDA(c, upload(c->d_gradFacets, gf.data(), gf.size(), c->stream));
+    LF_TRY_CUDA(c, upload(c->d_gradVerts, gv.data(), gv.size(), c->stream));
+    LF_TRY_CUDA(c, upload(c->d_faceNeeds, fn.data(), fn.size(), c->stream));
+    c->epoch++;
+    return LF_OK;
+}
+
 extern "C" lf_status lf_set_model_tables(lf_ctx* c, int G, const double* density, const double* chi,
                                          const double* remMag, const double* remInc, const double* remDec,
                                          const double* remVec, int nv, const double* xyz, int nt, const int32_t* tri,
@@ -665,22 +695,61 @@ extern "C" lf_status lf_set_model_tables(lf_ctx* c, int G, const double* density
     }
     LF_TRY_CUDA(c, upload(c->d_vfOff, vfOff.data(), vfOff.size(), c->stream));
     LF_TRY_CUDA(c, upload(c->d_vf, vf.data(), vf.size(), c->stream));
-    std::vector<uint8_t> vneed(nv, 0), fneed(nt, 0);
-    for (int r = 0; r < nref; ++r) vneed[refVertex[r]] = 1;
-    std::vector<int32_t> gverts;
-    for (int v = 0; v < nv; ++v)
-        if (vneed[v]) gverts.push_back(v);
-    for (int f = 0; f < nt; ++f)
-        fneed[f] = vneed[tri[3 * f]] | vneed[tri[3 * f + 1]] | vneed[tri[3 * f + 2]];
-    c->nGradVerts = static_cast<int>(gverts.size());
-    std::vector<int32_t> gfacets;
-    for (int f = 0; f < nt; ++f)
-        if (fneed[f]) gfacets.push_back(f);
-    c->nGradFacets = static_cast<int>(gfacets.size());
-    c->hGradFacets = gfacets;
-    if (!gfacets.empty()) LF_TRY_CUDA(c, upload(c->d_gradFacets, gfacets.data(), gfacets.size(), c->stream));
-    LF_TRY_CUDA(c, upload(c->d_gradVerts, gverts.data(), gverts.size(), c->stream));
-    LF_TRY_CUDA(c, upload(c->d_faceNeeds, fneed.data(), fneed.size(), c->stream));
+    {
+        // Reference gather: the DOF vertices.  Chain gather: every vertex whose
+        // scattered position depends on the parameters -- the DOF vertices,
+        // interpolation rows with such a source (a row's own DOF write is
+        // overwritten), then whole averaging groups with such a member.
+        std::vector<uint8_t> vref(nv, 0), vdep(nv, 0);
+        for (int r = 0; r < nref; ++r) vref[refVertex[r]] = vdep[refVertex[r]] = 1;
+        if (interpOff)
+            for (int v = 0; v < nv; ++v) {
+                if (interpOff[v + 1] == interpOff[v]) continue;
+                uint8_t d = 0;
+                for (int k = interpOff[v]; k < interpOff[v + 1]; ++k) d |= vref[interpSrc[k]];
+                vdep[v] = d;
+            }
+        for (int q = 0; q < c->nSync; ++q) {
+            uint8_t d = 0;
+            for (int k = syncOff[q]; k < syncOff[q + 1]; ++k) d |= vdep[syncVertex[k]];
+            if (d)
+                for (int k = syncOff[q]; k < syncOff[q + 1]; ++k) vdep[syncVertex[k]] = 1;
+        }
+        auto sets = [&](const std::vector<uint8_t>& vn, std::vector<int32_t>& gv, std::vector<int32_t>& gf,
+                        std::vector<uint8_t>& fn) {
+            gv.clear();
+            gf.clear();
+            fn.assign(nt, 0);
+            for (int v = 0; v < nv; ++v)
+                if (vn[v]) gv.push_back(v);
+            for (int f = 0; f < nt; ++f) {
+                fn[f] = vn[tri[3 * f]] | vn[tri[3 * f + 1]] | vn[tri[3 * f + 2]];
+                if (fn[f]) gf.push_back(f);
+            }
+        };
+        sets(vref, c->hGvertsRef, c->hGfacetsRef, c->hFneedRef);
+        sets(vdep, c->hGvertsChain, c->hGfacetsChain, c->hFneedChain);
+        // interpolation transposed (CSR over sources, rows in increasing order)
+        std::vector<int32_t> adjOff(nv + 1, 0), adjRow;
+        std::vector<double> adjW;
+        if (interpOff) {
+            for (int k = 0; k < nInterp; ++k) adjOff[interpSrc[k] + 1]++;
+            for (int v = 0; v < nv; ++v) adjOff[v + 1] += adjOff[v];
+            adjRow.resize(nInterp);
+            adjW.resize(nInterp);
+            std::vector<int32_t> fill(adjOff.begin(), adjOff.end() - 1);
+            for (int v = 0; v < nv; ++v)
+                for (int k = interpOff[v]; k < interpOff[v + 1]; ++k) {
+                    adjRow[fill[interpSrc[k]]] = v;
+                    adjW[fill[interpSrc[k]]++] = interpW[k];
+                }
+        }
+        LF_TRY_CUDA(c, upload(c->d_adjOff, adjOff.data(), adjOff.size(), c->stream));
+        LF_TRY_CUDA(c, upload(c->d_adjRow, adjRow.data(), adjRow.size(), c->stream));
+        LF_TRY_CUDA(c, upload(c->d_adjW, adjW.data(), adjW.size(), c->stream));
+        LF_TRY_CUDA(c, c->d_vgrad2.reserve((size_t)nv * 3));
+    }
+    LF_RET_IF(apply_gather_sets(c));
     LF_TRY_CUDA(c, c->d_fc.reserve((size_t)NFC * nt));
     LF_TRY_CUDA(c, c->d_mc.reserve((size_t)NMC * nt));
     {  // facet patches of the mixed forward
@@ -1577,6 +1646,20 @@ static int gradient_set(lf_ctx* c, const StationSet& s, const double* gcoef, con
     return used;
 }
 
+// Finite-difference-XY partials of one station set into slots
+// [slot0, slot0 + returned count): the FP64 chunking of the analytic kernels.
+static int gradient_fdxy_set(lf_ctx* c, const StationSet& s, const double* gcoef, const double* mcoef, int slot0) {
+    if (s.n == 0 || c->nGradFacets == 0) return 0;
+    int nch = 1, tpc = 1;
+    grad_chunks(c, s.n, false, &nch, &tpc);
+    const int32_t* grpSta = c->partitioned ? c->d_grpStaOff.p : nullptr;
+    k_gradient_fdxy<<<dim3(cdiv(c->nGradFacets, 4), nch), 128, 0, c->stream>>>(
+        c->T, c->nGradFacets, c->d_gradFacets.p, c->d_fcfd.p, c->d_gc.p, s.n, s.d_xyz.p, gcoef, mcoef,
+        c->d_faceGroup.p, 1.0 / c->xyStep, tpc, grpSta, c->d_partGrad.p + (size_t)slot0 * 9 * c->T);
+    c->counters.launches++;
+    return nch;
+}
+
 static lf_status gradient_all(lf_ctx* c, const double* d_params, double* d_grad) {
     bool gOn = c->grav.n > 0, mOn = c->mag.n > 0 && c->alphaMag > 0.0;
     k_face_prep_grad<<<cdiv(c->T, 128), 128, 0, c->stream>>>(c->T, c->d_tri.p, c->d_pos.p, c->d_faceGroup.p,
@@ -1592,6 +1675,17 @@ static lf_status gradient_all(lf_ctx* c, const double* d_params, double* d_grad)
         if (mOn) slots += grad_slots(c, c->mag.n);
     }
     if (c->nGradFacets == 0) slots = 0;
+    const bool fdxy = c->xyMode == LF_XY_FORWARD_DIFFERENCE && slots > 0;
+    if (fdxy) {  // one FP64 finite-difference slot per station chunk
+        int n = 1, t = 1;
+        if (c->sameStations && gOn) {
+            grad_chunks(c, c->grav.n, false, &n, &t);
+            slots += n;
+        } else {
+            if (gOn) { grad_chunks(c, c->grav.n, false, &n, &t); slots += n; }
+            if (mOn) { grad_chunks(c, c->mag.n, false, &n, &t); slots += n; }
+        }
+    }
     if (slots == 0) {
         LF_TRY_CUDA(c, cudaMemsetAsync(c->d_vgrad.p, 0, sizeof(double) * 3 * c->V, c->stream));
     } else {
@@ -1603,11 +1697,27 @@ static lf_status gradient_all(lf_ctx* c, const double* d_params, double* d_grad)
             if (gOn) used += gradient_set(c, c->grav, c->grav.d_coef.p, nullptr, used);
             if (mOn) used += gradient_set(c, c->mag, nullptr, c->mag.d_coef.p, used);
         }
+        const int fdFrom = used;
+        if (fdxy) {
+            const int nf = c->nGradFacets;
+            LF_TRY_CUDA(c, c->d_fcfd.reserve((size_t)7 * NFC * nf));
+            k_face_prep_fdxy<<<dim3(cdiv(nf, 128), 7), 128, 0, c->stream>>>(nf, c->d_gradFacets.p, c->d_tri.p,
+                                                                           c->d_pos.p, c->d_faceGroup.p,
+                                                                           c->d_groups.p, c->fdir, c->xyStep,
+                                                                           c->d_fcfd.p);
+            c->counters.launches++;
+            if (c->sameStations && gOn) {
+                used += gradient_fdxy_set(c, c->grav, c->grav.d_coef.p, mOn ? c->mag.d_coef.p : nullptr, used);
+            } else {
+                if (gOn) used += gradient_fdxy_set(c, c->grav, c->grav.d_coef.p, nullptr, used);
+                if (mOn) used += gradient_fdxy_set(c, c->mag, nullptr, c->mag.d_coef.p, used);
+            }
+        }
         LF_CHECK_LAUNCH(c);
         if (c->nGradVerts > 0) {
             k_vertex_reduce<<<cdiv(c->nGradVerts, 4), 128, 0, c->stream>>>(c->nGradVerts, c->d_gradVerts.p,
                                                                               c->d_vfOff.p, c->d_vf.p, c->T, used,
-                                                                              c->d_partGrad.p, c->d_vgrad.p);
+                                                                              fdFrom, c->d_partGrad.p, c->d_vgrad.p);
             c->counters.launches++;
         }
     }
@@ -1616,11 +1726,33 @@ static lf_status gradient_all(lf_ctx* c, const double* d_params, double* d_grad)
                                                                c->d_smDiff.p, c->d_smVgrad.p);
         c->counters.launches++;
     }
+    const double* vg = c->d_vgrad.p;
+    bool smoothInGather = c->smoothOn;
+    if (c->gatherMode == LF_GATHER_CHAIN && c->np > 0) {
+        if (c->smoothOn) {
+            k_axpy<<<cdiv(3LL * c->V, 256), 256, 0, c->stream>>>((size_t)3 * c->V, c->smoothWeight, c->d_smVgrad.p,
+                                                                 c->d_vgrad.p);
+            c->counters.launches++;
+            smoothInGather = false;
+        }
+        if (c->nSync > 0) {
+            k_sync_shared<<<cdiv(c->nSync, 256), 256, 0, c->stream>>>(c->nSync, c->d_syncOff.p, c->d_syncVertex.p,
+                                                                       c->d_vgrad.p);
+            c->counters.launches++;
+        }
+        if (c->nInterpRows > 0) {
+            k_interp_adjoint<<<cdiv(c->V, 256), 256, 0, c->stream>>>(c->V, c->d_interpOff.p, c->d_adjOff.p,
+                                                                     c->d_adjRow.p, c->d_adjW.p, c->d_vgrad.p,
+                                                                     c->d_vgrad2.p);
+            c->counters.launches++;
+            vg = c->d_vgrad2.p;
+        }
+    }
     if (c->np > 0) {
         k_dof_gather<<<cdiv(c->np, 256), 256, 0, c->stream>>>(c->np, c->d_dofOff.p, c->d_refVertex.p, c->d_refAxis.p,
-                                                              c->d_refScale.p, c->d_vgrad.p, d_params,
+                                                              c->d_refScale.p, vg, d_params,
                                                               c->hasRef ? c->d_refp.p : nullptr, c->refWeight,
-                                                              c->smoothOn ? c->d_smVgrad.p : nullptr,
+                                                              smoothInGather ? c->d_smVgrad.p : nullptr,
                                                               c->smoothWeight, d_grad);
         c->counters.launches++;
     }
@@ -1898,6 +2030,28 @@ extern "C" lf_status lf_autotune(lf_ctx* c, const double* params, int repeats, l
     return LF_OK;
 }
 
+extern "C" lf_status lf_set_xy_derivative(lf_ctx* c, int mode, double step) {
+    if (!c) return LF_EINVAL;
+    if (mode != LF_XY_ANALYTIC && mode != LF_XY_FORWARD_DIFFERENCE)
+        return fail(c, LF_EINVAL, "xy derivative mode must be LF_XY_ANALYTIC or LF_XY_FORWARD_DIFFERENCE");
+    if (mode == LF_XY_FORWARD_DIFFERENCE && !(step > 0.0 && std::isfinite(step)))
+        return fail(c, LF_EINVAL, "finite-difference step must be positive and finite");
+    c->xyMode = mode;
+    if (mode == LF_XY_FORWARD_DIFFERENCE) c->xyStep = step;
+    c->epoch++;
+    return LF_OK;
+}
+
+extern "C" lf_status lf_set_gradient_gather(lf_ctx* c, int mode) {
+    if (!c) return LF_EINVAL;
+    if (mode != LF_GATHER_REFERENCE && mode != LF_GATHER_CHAIN)
+        return fail(c, LF_EINVAL, "gather mode must be LF_GATHER_REFERENCE or LF_GATHER_CHAIN");
+    c->gatherMode = mode;
+    if (!c->hasModel) return LF_OK;
+    cudaSetDevice(c->device);
+    return apply_gather_sets(c);
+}
+
 extern "C" lf_status lf_set_scatter_stateless(lf_ctx* c, int enabled) {
     if (!c) return LF_EINVAL;
     c->epoch++;
@@ -2028,7 +2182,7 @@ static lf_status jtw_product(lf_ctx* c, StationSet& s, bool grav, const std::vec
     const int used = gradient_set(c, s, grav ? c->d_tmpS.p : nullptr, grav ? nullptr : c->d_tmpS.p, 0);
     if (used > 0 && c->nGradVerts > 0)
         k_vertex_reduce<<<cdiv(c->nGradVerts, 4), 128, 0, c->stream>>>(c->nGradVerts, c->d_gradVerts.p, c->d_vfOff.p,
-                                                                        c->d_vf.p, c->T, used, c->d_partGrad.p,
+                                                                        c->d_vf.p, c->T, used, used, c->d_partGrad.p,
                                                                         c->d_vgrad.p);
     else
         LF_TRY_CUDA(c, cudaMemsetAsync(c->d_vgrad.p, 0, sizeof(double) * 3 * c->V, c->stream));

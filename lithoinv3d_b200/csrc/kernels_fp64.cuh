@@ -161,23 +161,15 @@ __device__ __forceinline__ d3 cross_rn(d3 a, d3 b) {
 __device__ __forceinline__ double norm_rn(d3 a) { return __dsqrt_rn(dot_rn(a, a)); }
 __device__ __forceinline__ d3 div_rn(d3 a, double s) { return {__ddiv_rn(a.x, s), __ddiv_rn(a.y, s), __ddiv_rn(a.z, s)}; }
 
-__global__ void k_face_prep_fwd(int T, const int32_t* __restrict__ tri, const double* __restrict__ pos,
-                                const int16_t* __restrict__ face_group, const GroupConst* __restrict__ groups,
-                                d3 fdir, double* __restrict__ fc) {
-    int f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= T) return;
-    const double* pa = pos + 3 * tri[3 * f];
-    const double* pb = pos + 3 * tri[3 * f + 1];
-    const double* pc = pos + 3 * tri[3 * f + 2];
-    d3 v[3] = {mk3(pa[0], pa[1], pa[2]), mk3(pb[0], pb[1], pb[2]), mk3(pc[0], pc[1], pc[2])};
+// Forward constants of one facet (vertices v) in the reference's operation
+// order; out[NFC].
+__device__ __forceinline__ void face_consts_fwd(const d3 (&v)[3], const GroupConst& g, d3 fdir, double (&out)[NFC]) {
     // faceNagyContribution / magneticFacet: n = (b-a) x (c-a), unit_n = n / |n|
     d3 n = cross_rn(sub_rn(v[1], v[0]), sub_rn(v[2], v[0]));
     double area2 = norm_rn(n);
     bool valid = !(area2 < kEps);
     d3 un = valid ? div_rn(n, area2) : mk3(0, 0, 0);
-    const GroupConst& g = groups[face_group[f]];
     d3 m = mk3(g.mdir[0], g.mdir[1], g.mdir[2]);
-    double out[NFC];
     out[FC_AX] = v[0].x; out[FC_AY] = v[0].y; out[FC_AZ] = v[0].z;
     out[FC_BX] = v[1].x; out[FC_BY] = v[1].y; out[FC_BZ] = v[1].z;
     out[FC_CX] = v[2].x; out[FC_CY] = v[2].y; out[FC_CZ] = v[2].z;
@@ -194,7 +186,48 @@ __global__ void k_face_prep_fwd(int T, const int32_t* __restrict__ tri, const do
         out[FC_MT0 + i] = __dmul_rn(dot_rn(m, perp), dot_rn(fdir, perp));  // mt * ft
     }
     out[FC_VALID] = valid ? 1.0 : 0.0;
+}
+
+__global__ void k_face_prep_fwd(int T, const int32_t* __restrict__ tri, const double* __restrict__ pos,
+                                const int16_t* __restrict__ face_group, const GroupConst* __restrict__ groups,
+                                d3 fdir, double* __restrict__ fc) {
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= T) return;
+    const double* pa = pos + 3 * tri[3 * f];
+    const double* pb = pos + 3 * tri[3 * f + 1];
+    const double* pc = pos + 3 * tri[3 * f + 2];
+    d3 v[3] = {mk3(pa[0], pa[1], pa[2]), mk3(pb[0], pb[1], pb[2]), mk3(pc[0], pc[1], pc[2])};
+    double out[NFC];
+    face_consts_fwd(v, groups[face_group[f]], fdir, out);
     for (int k = 0; k < NFC; ++k) fc[(size_t)k * T + f] = out[k];
+}
+
+// Finite-difference-XY gradient mode (no reference counterpart; the
+// reference differentiates every axis by per-facet forward differences with
+// h = 1e-4 m, faceNagyWithGradient gravity_forward.cpp:48-85): forward
+// constants of each listed facet and of its six copies with one vertex moved
+// by +h in x or y, variant k = 1 + 2 * corner + axis.  Layout
+// [7][NFC][nf] over the list index.
+__global__ void k_face_prep_fdxy(int nf, const int32_t* __restrict__ facets, const int32_t* __restrict__ tri,
+                                 const double* __restrict__ pos, const int16_t* __restrict__ face_group,
+                                 const GroupConst* __restrict__ groups, d3 fdir, double h, double* __restrict__ fcfd) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.y;  // variant
+    if (i >= nf) return;
+    const int f = facets[i];
+    d3 v[3];
+    for (int c = 0; c < 3; ++c) {
+        const double* p = pos + 3 * tri[3 * f + c];
+        v[c] = mk3(p[0], p[1], p[2]);
+    }
+    if (k > 0) {
+        const int c = (k - 1) >> 1;
+        if ((k - 1) & 1) v[c].y = __dadd_rn(v[c].y, h);
+        else v[c].x = __dadd_rn(v[c].x, h);
+    }
+    double out[NFC];
+    face_consts_fwd(v, groups[face_group[f]], fdir, out);
+    for (int q = 0; q < NFC; ++q) fcfd[((size_t)k * NFC + q) * nf + i] = out[q];
 }
 
 __global__ void k_face_prep_grad(int T, const int32_t* __restrict__ tri, const double* __restrict__ pos,
@@ -830,12 +863,76 @@ __global__ void __launch_bounds__(128, 3) k_gradient_warp_fp64(int T, const doub
         for (int k = 0; k < 9; ++k) part[(size_t)k * T + f] = outv[k];
 }
 
+// Finite-difference-XY partials (see k_face_prep_fdxy): one warp per listed
+// facet x station chunk (tiles_per_chunk tiles of kStationTile stations),
+// lanes over the chunk's stations.  Per station, the facet term of the base
+// record and of the six moved copies (pair_forward_fp64, the reference's
+// operation order), contracted with the station adjoints and the group
+// scales of the analytic kernels (zero for collapsed facets):
+//   sum_s (G_s (F_k - F_0) + T_s (M_k - M_0)) / h.
+// Writes the x and y partials of the three corners, and zero z, into this
+// chunk's slot of part ([chunk][9][T]).
+__global__ void __launch_bounds__(128) k_gradient_fdxy(int T, int nf, const int32_t* __restrict__ facets,
+                                                       const double* __restrict__ fcfd, const double* __restrict__ gc,
+                                                       int S, const double* __restrict__ sta,
+                                                       const double* __restrict__ gcoef,
+                                                       const double* __restrict__ mcoef,
+                                                       const int16_t* __restrict__ face_group, double inv_h,
+                                                       int tiles_per_chunk, const int32_t* __restrict__ grp_sta_off,
+                                                       double* __restrict__ part) {
+    const int lane = threadIdx.x & 31;
+    const int w = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+    if (w >= nf) return;  // warp-uniform
+    const int f = facets[w];
+    if (grp_sta_off) {  // batched bodies: only the facet's own body's stations
+        const int g = face_group[f], sb = grp_sta_off[g];
+        S = grp_sta_off[g + 1] - sb;
+        sta += 3 * (size_t)sb;
+        if (gcoef) gcoef += sb;
+        if (mcoef) mcoef += sb;
+    }
+    const int s0 = blockIdx.y * tiles_per_chunk * kStationTile;
+    const int s1 = min(S, s0 + tiles_per_chunk * kStationTile);
+    part += (size_t)blockIdx.y * 9 * T;
+    __shared__ double R[4][7 * NFC];
+    double* rec = R[threadIdx.x >> 5];
+    for (int q = lane; q < 7 * NFC; q += 32) rec[q] = fcfd[(size_t)q * nf + w];
+    __syncwarp();
+    const double gs = gc[(size_t)GC_GS * T + f], ms = gc[(size_t)GC_MS * T + f];
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    if (gs != 0.0 || ms != 0.0) {
+        for (int j = s0 + lane; j < s1; j += 32) {
+            const double G = gcoef ? gcoef[j] * gs : 0.0, M = mcoef ? mcoef[j] * ms : 0.0;
+            if (G == 0.0 && M == 0.0) continue;
+            const d3 o = mk3(sta[3 * (size_t)j], sta[3 * (size_t)j + 1], sta[3 * (size_t)j + 2]);
+            double g0 = 0.0, m0 = 0.0;
+            pair_forward_fp64<true, true>(rec, 0, 1, o, &g0, &m0);
+#pragma unroll 1
+            for (int k = 0; k < 6; ++k) {
+                double gk = 0.0, mk = 0.0;
+                pair_forward_fp64<true, true>(rec + (k + 1) * NFC, 0, 1, o, &gk, &mk);
+                acc[k] += G * (gk - g0) + M * (mk - m0);
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 6; ++k) acc[k] = warp_sum(acc[k]);
+    if (lane == 0)
+        for (int c = 0; c < 3; ++c) {
+            part[(size_t)(3 * c) * T + f] = acc[2 * c] * inv_h;
+            part[(size_t)(3 * c + 1) * T + f] = acc[2 * c + 1] * inv_h;
+            part[(size_t)(3 * c + 2) * T + f] = 0.0;
+        }
+}
+
 // Sums facet partials into vertex gradients: one warp per listed vertex,
 // lanes over its (chunk, incident facet corner) items, then a fixed warp
-// reduction (deterministic).
+// reduction (deterministic).  Slots from fd_from on hold
+// finite-difference-XY partials: when fd_from < nchunks, x and y come from
+// those slots only and z from the slots before them.
 __global__ void k_vertex_reduce(int nverts, const int32_t* __restrict__ verts, const int32_t* __restrict__ vf_off,
-                                const int32_t* __restrict__ vf, int T, int nchunks, const double* __restrict__ part,
-                                double* __restrict__ vgrad) {
+                                const int32_t* __restrict__ vf, int T, int nchunks, int fd_from,
+                                const double* __restrict__ part, double* __restrict__ vgrad) {
     const int i = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
     if (i >= nverts) return;  // warp-uniform
@@ -847,9 +944,12 @@ __global__ void k_vertex_reduce(int nverts, const int32_t* __restrict__ verts, c
         const int c = it / ninc, k = b + it % ninc;
         const int f = vf[k] / 3, corner = vf[k] % 3;
         const double* p = part + ((size_t)c * 9 + 3 * corner) * T + f;
-        gx += p[0];
-        gy += p[(size_t)T];
-        gz += p[(size_t)2 * T];
+        const bool xy = fd_from >= nchunks || c >= fd_from;
+        if (xy) {
+            gx += p[0];
+            gy += p[(size_t)T];
+        }
+        if (c < fd_from) gz += p[(size_t)2 * T];
     }
     gx = warp_sum(gx);
     gy = warp_sum(gy);
@@ -881,6 +981,42 @@ __global__ void k_dof_gather(int np, const int32_t* __restrict__ dof_off, const 
     }
     if (ref_params) acc += ref_weight * (params[d] - ref_params[d]);
     grad[d] = acc;
+}
+
+// Chain gather (no reference counterpart; the reference reads the vertex
+// gradient at the DOF vertices only, gravity_forward.cpp:270-289).  The
+// scatter is DOF writes -> interpolation -> averaging; its adjoint runs the
+// transposes in reverse.  The averaging's transpose is the averaging itself
+// (k_sync_shared on the gradient: its matrix is symmetric).  The
+// interpolation's transpose, out of place: a source receives w x the
+// gradient of each row it feeds, a row keeps nothing (its position was
+// overwritten), every other vertex keeps its own.  Fixed summation order,
+// no atomics.
+__global__ void k_interp_adjoint(int V, const int32_t* __restrict__ interp_off, const int32_t* __restrict__ adj_off,
+                                 const int32_t* __restrict__ adj_row, const double* __restrict__ adj_w,
+                                 const double* __restrict__ vg, double* __restrict__ out) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= V) return;
+    const bool row = interp_off[v + 1] > interp_off[v];
+    double g0 = row ? 0.0 : vg[3 * (size_t)v], g1 = row ? 0.0 : vg[3 * (size_t)v + 1],
+           g2 = row ? 0.0 : vg[3 * (size_t)v + 2];
+    for (int k = adj_off[v]; k < adj_off[v + 1]; ++k) {
+        const double w = adj_w[k];
+        const double* q = vg + 3 * (size_t)adj_row[k];
+        g0 += w * q[0];
+        g1 += w * q[1];
+        g2 += w * q[2];
+    }
+    out[3 * (size_t)v] = g0;
+    out[3 * (size_t)v + 1] = g1;
+    out[3 * (size_t)v + 2] = g2;
+}
+
+// y += a x over n doubles (the smoothness vertex gradient into the misfit's
+// before the chain gather).
+__global__ void k_axpy(size_t n, double a, const double* __restrict__ x, double* __restrict__ y) {
+    const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i < n) y[i] += a * x[i];
 }
 
 // Dense Jacobian rows from per-station facet partials (one chunk per

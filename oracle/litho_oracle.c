@@ -167,6 +167,24 @@ static void face_with_fd_gradient(const facefn *f, v3 obs, v3 a, v3 b, v3 c,
     }
 }
 
+/* The x and y derivatives of the finite-difference-XY gradient mode (no
+ * reference counterpart; its step is a parameter, h = 0.5 m in the
+ * large-inversion configuration): forward differences of the reference's
+ * facet formula as in face_with_fd_gradient, written into the x and y slots
+ * of ga, gb, gc. */
+static void face_xy_forward_difference(const facefn *f, v3 obs, v3 a, v3 b, v3 c, double h, v3 *ga, v3 *gb,
+                                       v3 *gc) {
+    double v = face_eval(f, obs, a, b, c);
+    for (int k = 0; k < 2; ++k) {
+        v3 p = a; setc(&p, k, comp(a, k) + h);
+        setc(ga, k, (face_eval(f, obs, p, b, c) - v) / h);
+        p = b; setc(&p, k, comp(b, k) + h);
+        setc(gb, k, (face_eval(f, obs, a, p, c) - v) / h);
+        p = c; setc(&p, k, comp(c, k) + h);
+        setc(gc, k, (face_eval(f, obs, a, b, p) - v) / h);
+    }
+}
+
 /* ------------------------------------------------------------------------ */
 /* The "true derivative" (NOT part of the reference; the analytic device   */
 /* gradient is checked against it): a central difference with one           */
@@ -518,7 +536,9 @@ void lo_forward_tmi(int S, const double *sta, int G, const int32_t *grp_tri_off,
 /*  - per (station, face): forward-FD gradient, h = 1e-4 (kind < 2) or the  */
 /*    Richardson central "true" derivative (kind >= 2, test truth only;     */
 /*    step true_h, or -true_h x min(station-triangle distance, smallest    */
-/*    altitude) if < 0; extended precision);                               */
+/*    altitude) if < 0; extended precision); kind 4 / 5: z the truth with  */
+/*    step -3e-3, x and y forward differences with step true_h (the        */
+/*    finite-difference-XY mode of the device gradient);                   */
 /*  - vertex gradients accumulated per mesh with faceScale;                 */
 /*  - gather: J(i, dof) += vg[vertex][axis] * axisScale for each ref,       */
 /*    skipping |vg| < 1e-30 (reference semantics, kind < 2 only).           */
@@ -530,7 +550,7 @@ void lo_jacobian(int kind, int S, const double *sta, int G, const int32_t *grp_t
                  const double *mag_amp, const double *mag_dir, const double *fdir, int np,
                  const int32_t *dof_off, const int32_t *ref_vertex, const uint8_t *ref_axis,
                  const double *ref_scale, double true_h, double *J) {
-    int mag = kind & 1, truth = kind >= 2;
+    int mag = kind & 1, truth = kind >= 2, fdxy = kind >= 4;
     double *vg = (double *)calloc((size_t)V * 3, sizeof(double));
     const double gscale = LO_G_SI * LO_DENSITY_SCALE * LO_M_S2_TO_MGAL;
     const double kInv4Pi = 1.0 / (4.0 * LO_PI);
@@ -551,7 +571,8 @@ void lo_jacobian(int kind, int S, const double *sta, int G, const int32_t *grp_t
             }
             for (int t = grp_tri_off[g]; t < grp_tri_off[g + 1]; ++t) {
                 int ia = tri[3 * t], ib = tri[3 * t + 1], ic = tri[3 * t + 2];
-                v3 ga, gb, gc; double val;
+                v3 ga = {0, 0, 0}, gb = {0, 0, 0}, gc = {0, 0, 0};
+                double val;
                 if (truth && collapsed(mk(pos + 3 * ia), mk(pos + 3 * ib), mk(pos + 3 * ic))) continue;
                 if (truth) {
                     /* true_h > 0: that step; true_h < 0: |true_h| x the
@@ -561,18 +582,21 @@ void lo_jacobian(int kind, int S, const double *sta, int G, const int32_t *grp_t
                      * truncation stays small for near, far and thin facets
                      * alike; the extended-precision evaluation keeps the
                      * 1/h rounding below it */
-                    double h = true_h;
+                    double h = fdxy ? -3e-3 : true_h;
                     if (h < 0.0) {
                         v3 pa = mk(pos + 3 * ia), pb = mk(pos + 3 * ib), pc = mk(pos + 3 * ic);
-                        h = -true_h * fmin(point_triangle_distance(o, pa, pb, pc), min_altitude(pa, pb, pc));
+                        h = -h * fmin(point_triangle_distance(o, pa, pb, pc), min_altitude(pa, pb, pc));
                         if (h < 1e-9) h = 1e-9;
                     }
                     face_true_gradient(&f, o, mk(pos + 3 * ia), mk(pos + 3 * ib), mk(pos + 3 * ic), h, &ga,
                                        &gb, &gc);
                 }
-                else
+                else if (!truth)
                     face_with_fd_gradient(&f, o, mk(pos + 3 * ia), mk(pos + 3 * ib),
                                           mk(pos + 3 * ic), &val, &ga, &gb, &gc);
+                if (fdxy) /* x and y of each vertex: forward difference with step true_h */
+                    face_xy_forward_difference(&f, o, mk(pos + 3 * ia), mk(pos + 3 * ib), mk(pos + 3 * ic),
+                                               true_h, &ga, &gb, &gc);
                 int ids[3] = {ia, ib, ic};
                 v3 gs[3] = {ga, gb, gc};
                 for (int w = 0; w < 3; ++w) {

@@ -93,3 +93,36 @@ def test_reference_gather_is_not_the_derivative_with_interpolation():
     g_ref = om.jacobian(p.grav_xyz, 2, true_h=-3e-3).T @ w
     g_chain = om.chain_gather(om.vertex_jacobian(p.grav_xyz, 2).T @ w)
     assert np.abs(g_ref - g_chain).max() > 0.1 * np.abs(g_chain).max()
+
+
+def test_fdxy_kinds_are_forward_differences_of_the_forward():
+    """Oracle kinds 4 / 5 (finite-difference-XY mode): the x / y columns of
+    the vertex Jacobian are forward differences of the whole forward with
+    one vertex moved (the per-facet differences sum to it), the z columns are
+    the true derivative (kinds 2 / 3)."""
+    p, model, t = _problem(synth.XYZ_FREE)
+    x = model.assemble_parameters() + np.random.default_rng(3).normal(0.0, 5.0, model.n_dofs)
+    om = OracleModel(t, p.densities, p.susceptibilities, p.inducing)
+    om.scatter(x)
+    P, T = om.pos.reshape(-1, 3), t["tri"].reshape(-1, 3)
+    a, b, c = P[T[:, 0]], P[T[:, 1]], P[T[:, 2]]
+    area2 = np.linalg.norm(np.cross(b - a, c - a), axis=1)
+    longest = np.max([np.sum((b - a) ** 2, 1), np.sum((c - b) ** 2, 1), np.sum((a - c) ** 2, 1)], axis=0)
+    bad = np.zeros(len(P), bool)
+    bad[T[area2 < 1e-10 * longest].ravel()] = True
+    h = 0.5
+    sta = p.grav_xyz[::4]
+    for kind, fwd in ((4, "forward_gz"), (5, "forward_tmi")):
+        Jfd = om.vertex_jacobian(sta, kind, h)
+        Jt = om.vertex_jacobian(sta, kind - 2, -3e-3)
+        np.testing.assert_allclose(Jfd[:, 2::3], Jt[:, 2::3], rtol=0, atol=1e-12 * np.abs(Jt).max())
+        base = getattr(om, fwd)(sta)
+        rng = np.random.default_rng(kind)
+        moved = [v for v in rng.permutation(len(P)) if not bad[v] and np.abs(Jt[:, 3 * v:3 * v + 3]).max() > 0]
+        for v in moved[:6]:
+            for ax in (0, 1):
+                o2 = OracleModel(t, p.densities, p.susceptibilities, p.inducing)
+                o2.pos[:] = om.pos
+                o2.pos.reshape(-1, 3)[v, ax] += h
+                fd = (getattr(o2, fwd)(sta) - base) / h
+                np.testing.assert_allclose(Jfd[:, 3 * v + ax], fd, rtol=0, atol=1e-9 * np.abs(Jt).max())
