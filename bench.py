@@ -70,12 +70,12 @@ FLOPS_FWD_PAIR = 138
 FLOPS_GRAD_PAIR = 331
 SFU_FWD_PAIR = 10   # 3 sqrt + 3 div + 3 log + 1 atan2, one special-function op each
 SFU_GRAD_PAIR = 13
-# DRAM bytes (read + write) of one mixed-precision forward launch
-# (k_forward_patch) on this workload, from an ncu capture
-# (dram__bytes_read.sum + dram__bytes_write.sum, profiles/): the patch record
-# blobs (~5 MB) and the stations come from DRAM once and from L2 for every
-# further station block; the partial sums stay in L2.
-FORWARD_DRAM_BYTES_PER_LAUNCH = 9.605e6
+# DRAM bytes (read + write) of one mixed-precision forward launch on this
+# workload, per engine, from ncu captures (dram__bytes_read.sum +
+# dram__bytes_write.sum): the facet records (208 bytes each, ~4 MB) or the
+# patch blobs (~5 MB) and the stations come from DRAM once and from L2 for
+# every further station block; the partial sums stay in L2.
+FORWARD_DRAM_BYTES_PER_LAUNCH = {"k_forward_mixed": 7.024e6, "k_forward_patch": 9.605e6}
 # Nominal B200 CUDA-core rates at the 1.965 GHz boost clock (no measured
 # figure for these pipes exists in MEASURED_PEAKS.json): FP32 148 SMs x 128
 # lanes x 2 flop; special-function unit 148 x 16 ops; FP64 148 x 64 x 2 flop.
@@ -602,15 +602,15 @@ def main():
         kname = "k_gradient_warp_fp64 + k_gradient_warp_far32" if args.precision == "mixed" else "k_gradient_warp_fp64"
         kms, pps, flops, sfu = grad_per_launch_ms, pps_grad, FLOPS_GRAD_PAIR, SFU_GRAD_PAIR
     else:
-        kname = "k_forward_patch" if args.precision == "mixed" else "k_forward_fp64"
+        kname = (("k_forward_mixed" if tuned.fwd_engine == 0 else "k_forward_patch") if args.precision == "mixed"
+                 else "k_forward_fp64")
         kms, pps, flops, sfu = fwd_per_launch_ms, pps_fwd, FLOPS_FWD_PAIR, SFU_FWD_PAIR
     peak_pps = pair_roofline(flops, sfu, args.precision)
     roofline = {"bound": "fp64" if args.precision == "fp64" else "fp32+sfu", "kernel": kname,
                 "achieved": pps * flops / 1e12, "peak": peak_pps * flops / 1e12, "unit": "TFLOP/s",
                 "frac": pps / peak_pps,
                 "fp32_pipe_frac": (pps * flops / FP32_PEAK_FLOPS) if args.precision == "mixed" else None,
-                "traffic": (FORWARD_DRAM_BYTES_PER_LAUNCH if kname == "k_forward_patch" and args.workload == "contact"
-                            else None),
+                "traffic": (FORWARD_DRAM_BYTES_PER_LAUNCH.get(kname) if args.workload == "contact" else None),
                 "peak_source": ("nominal CUDA-core rates at 1.965 GHz (FP32 74.4 TFLOP/s, SFU 4.65 Tops/s, "
                                 "FP64 37.2 TFLOP/s); MEASURED_PEAKS.json holds only HBM and bf16 GEMM figures"),
                 "flops_per_pair": flops, "sfu_ops_per_pair": sfu, "kernel_ms_per_launch": kms,
@@ -629,7 +629,8 @@ def main():
                         "tuning": {"fwd_target_blocks": tuned.fwd_target_blocks,
                                    "grad_target_warps": tuned.grad_target_warps,
                                    "near_tiles_per_chunk": tuned.near_tiles_per_chunk,
-                                   "patch_threads": tuned.patch_threads, "far_ratio": tuned.far_ratio}},
+                                   "patch_threads": tuned.patch_threads, "far_ratio": tuned.far_ratio,
+                                   "fwd_engine": "facet" if tuned.fwd_engine == 0 else "patch"}},
             "e2e": {"value": e2e_value, "unit": "evals/s", "h2d_bytes_per_step": 8 * np_,
                     "d2h_bytes_per_step": 8 * (np_ + 1)},
             "gpu_launches": launches, "roofline": roofline}

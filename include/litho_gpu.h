@@ -213,17 +213,23 @@ lf_status lf_forward(lf_ctx* ctx, const double* params, double* gz, double* tmi)
  *  fwd_target_blocks     forward CTAs per launch (in 128-station units):
  *                        station blocks x facet (patch) chunks; more chunks =
  *                        more CTAs, each over fewer facets
- *                        (candidates 148 x {4, 8, 16, 32, 64, 128}); 0 (mixed
- *                        precision only) = a persistent grid of one CTA per
+ *                        (candidates 148 x {4, 8, 16, 32, 64, 128}); 0 (patch
+ *                        engine only) = a persistent grid of one CTA per
  *                        resident slot, each over a balanced contiguous range
  *                        of (station block, patch) units
  *  grad_target_warps     gradient warps per launch: DOF facets x station chunks
  *                        (148 x {16, 32, 64, 128, 256})
  *  near_tiles_per_chunk  mixed near-field gradient: 64-station tiles per warp
  *                        (0: the grad_target_warps split; candidates 0, 1, 2, 4, 8)
- *  patch_threads         stations per CTA of the mixed forward (128 or 256;
+ *  patch_threads         stations per CTA of the patch engine (128 or 256;
  *                        each CTA walks 32-facet patches, so this is the
  *                        station x facet tile of one shared-memory stage)
+ *  fwd_engine            mixed-precision forward: LF_FWD_FACET (one FP32 record
+ *                        per facet; every pair evaluates its own three vertex
+ *                        distances, edge integrals and solid angle) or
+ *                        LF_FWD_PATCH (32-facet patches: vertex distances and
+ *                        edge integrals once per station and patch, shared by
+ *                        the patch's facets); lf_autotune times both
  *  far_ratio             mixed precision: facet-distance / facet-size ratio tau
  *                        beyond which a pair is FP32 far field (FP32 28-point
  *                        mid field from tau/2, FP64 nearer); the same value as
@@ -237,12 +243,14 @@ lf_status lf_forward(lf_ctx* ctx, const double* params, double* gz, double* tmi)
  * set and read them directly.  Results do not depend on the launch shapes
  * beyond the summation order of partial sums (far_ratio changes which pairs
  * run in FP32, within the tolerances above). */
+enum { LF_FWD_FACET = 0, LF_FWD_PATCH = 1 };
 typedef struct {
     int fwd_target_blocks;
     int grad_target_warps;
     int near_tiles_per_chunk;
     int patch_threads;
     double far_ratio;
+    int fwd_engine;
 } lf_tuning;
 lf_status lf_set_tuning(lf_ctx* ctx, const lf_tuning* t);
 lf_status lf_get_tuning(lf_ctx* ctx, lf_tuning* t);

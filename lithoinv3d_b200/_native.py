@@ -30,7 +30,7 @@ class LbfgsbResult(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("fwd_target_blocks", C.c_int), ("grad_target_warps", C.c_int), ("near_tiles_per_chunk", C.c_int),
-                ("patch_threads", C.c_int), ("far_ratio", C.c_double)]
+                ("patch_threads", C.c_int), ("far_ratio", C.c_double), ("fwd_engine", C.c_int)]
 
 
 class PropertyOptions(C.Structure):

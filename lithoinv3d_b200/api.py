@@ -21,6 +21,7 @@ GRAVITY, MAGNETIC = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
 GATHER_REFERENCE, GATHER_CHAIN = 0, 1
 XY_ANALYTIC, XY_FORWARD_DIFFERENCE = 0, 1
+FWD_FACET, FWD_PATCH = 0, 1
 UNIT_GRAVITY, UNIT_INDUCED, UNIT_DIRECTION, UNIT_REMANENCE = range(4)
 
 
@@ -263,12 +264,15 @@ class Context:
         return t
 
     def set_tuning(self, fwd_target_blocks: int, grad_target_warps: int, near_tiles_per_chunk: int = 0,
-                   patch_threads: Optional[int] = None, far_ratio: Optional[float] = None):
-        """lf_set_tuning; patch_threads / far_ratio default to their current values."""
+                   patch_threads: Optional[int] = None, far_ratio: Optional[float] = None,
+                   fwd_engine: Optional[int] = None):
+        """lf_set_tuning; patch_threads / far_ratio / fwd_engine default to their
+        current values."""
         cur = self.tuning()
         t = Tuning(fwd_target_blocks, grad_target_warps, near_tiles_per_chunk,
                    cur.patch_threads if patch_threads is None else patch_threads,
-                   cur.far_ratio if far_ratio is None else far_ratio)
+                   cur.far_ratio if far_ratio is None else far_ratio,
+                   cur.fwd_engine if fwd_engine is None else fwd_engine)
         self._check(self.lib.lf_set_tuning(self.h, C.byref(t)), "set_tuning")
 
     def autotune(self, params, repeats: int = 3):

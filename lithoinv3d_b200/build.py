@@ -17,7 +17,9 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "_lib")
 LIBNAME = "liblitho_gpu.so"
 SOURCES = ["capi.cu", "noalloc.cu", "mlp.cu", "model_builder.cpp", "lbfgsb.cpp", "surface_io.cpp", "patches.cpp"]
-HEADERS = ["kernels_fp64.cuh", "kernels_mixed.cuh", "kernels_patch.cuh", "patches.hpp", "kernels_classify.cuh", "mlp_kernels.cuh", "tc_gemm.cuh", "model_builder.hpp", "lbfgsb.hpp"]
+HEADERS = ["kernels_fp64.cuh", "kernels_mixed.cuh", "kernels_facet.cuh", "kernels_patch.cuh", "patches.hpp",
+           "kernels_classify.cuh", "mlp_kernels.cuh", "tc_gemm.cuh", "tc_gemm_tma.cuh", "model_builder.hpp",
+           "lbfgsb.hpp"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

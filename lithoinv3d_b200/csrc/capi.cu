@@ -3,6 +3,7 @@
 #include "../../include/litho_gpu.h"
 #include "kernels_classify.cuh"
 #include "kernels_mixed.cuh"
+#include "kernels_facet.cuh"
 #include "kernels_patch.cuh"
 #include "lbfgsb.hpp"
 #include "model_builder.hpp"
@@ -102,6 +103,7 @@ struct lf_ctx {
     std::vector<GroupConst> gconst;
 
     DevBuf<double> d_pos, d_fc, d_gc, d_mc, d_params, d_grad, d_vgrad, d_out5, d_f, d_refp;
+    DevBuf<FaceF32> d_mf32;  // per-facet FP32 records of the facet engine [T]
     DevBuf<unsigned long long> d_nearPairs;
     float tau = 3.0f;  // far-field ratio of the mixed path
 
@@ -222,7 +224,7 @@ struct lf_ctx {
 
     // launch shapes chosen by lf_autotune (defaults: measured on the
     // 19k-facet, 4096-station contact model)
-    lf_tuning tune{148 * 4, 148 * 64, 0, 128, 3.0};
+    lf_tuning tune{148 * 4, 148 * 64, 0, 128, 3.0, LF_FWD_FACET};
 
     // Batched bodies (lf_set_station_groups): each group is one body and
     // sees only its own station range [grpStaOff[g], grpStaOff[g+1]) of both
@@ -1211,7 +1213,12 @@ static lf_status forward_set_items(lf_ctx* c, const StationSet& s, double* d_gz,
     if (c->nItems > 0) {
         const int grid = std::min(c->nItems, fwd_blocks(c));
         int slot = prof_begin(c, c->evFwd, c->nFwd);
-        k_forward_fp64_items<GZ, TMI, kFwdFacetTile><<<grid, kFwdThreads, 0, c->stream>>>(
+        if (MIXED)
+            k_forward_mixed_items<GZ, TMI, kFwdFacetTile><<<grid, kFwdThreads, 0, c->stream>>>(
+                c->d_items.p, c->nItems, s.d_xyz.p, c->T, c->d_mc.p, c->d_mf32.p, c->tau, GZ ? c->d_partG.p : nullptr,
+                TMI ? c->d_partM.p : nullptr, c->d_nearPairs.p);
+        else
+            k_forward_fp64_items<GZ, TMI, kFwdFacetTile><<<grid, kFwdThreads, 0, c->stream>>>(
                 c->d_items.p, c->nItems, s.d_xyz.p, c->T, c->d_fc.p, GZ ? c->d_partG.p : nullptr,
                 TMI ? c->d_partM.p : nullptr);
         prof_end(c, c->evFwd, slot);
@@ -1298,6 +1305,14 @@ static cudaError_t patch_kernel_attrs() {
 // Per-evaluation records of the mixed forward: the per-facet FP64 / FP32
 // records (near and mid facets) and the patch blobs (far facets).
 static lf_status mixed_prep(lf_ctx* c) {
+    if (c->tune.fwd_engine == LF_FWD_FACET) {
+        LF_TRY_CUDA(c, c->d_mf32.reserve((size_t)std::max(c->T, 1)));
+        k_face_prep_mixed<<<cdiv(c->T, 128), 128, 0, c->stream>>>(c->T, c->d_tri.p, c->d_pos.p, c->d_faceGroup.p,
+                                                                  c->d_groups.p, c->fdir, c->d_mc.p, c->d_mf32.p);
+        c->counters.launches++;
+        LF_CHECK_LAUNCH(c);
+        return LF_OK;
+    }
     const PatchTopology& pt = c->ptopo;
     k_face_prep_patch<<<cdiv(c->T, 128), 128, 0, c->stream>>>(
         c->T, c->d_tri.p, c->d_pos.p, c->d_faceGroup.p, c->d_groups.p, c->fdir, c->d_pFacetPatch.p, c->d_pFacetSlot.p,
@@ -1459,7 +1474,35 @@ static lf_status forward_patch_persistent(lf_ctx* c, const StationSet& s, double
 }
 
 template <bool GZ, bool TMI>
+static lf_status forward_set_facet(lf_ctx* c, const StationSet& s, double* d_gz, double* d_tmi) {
+    if (c->partitioned) return forward_set_items<GZ, TMI, true>(c, s, d_gz, d_tmi);
+    int S = s.n;
+    if (S == 0) return LF_OK;
+    plan_chunks(c, S);
+    LF_RET_IF(upload_chunks(c));
+    int nch = static_cast<int>(c->chunkBegin.size());
+    if (GZ) LF_TRY_CUDA(c, c->d_partG.reserve((size_t)nch * S));
+    if (TMI) LF_TRY_CUDA(c, c->d_partM.reserve((size_t)nch * S));
+    if (nch > 0) {
+        dim3 grid(cdiv(S, kFwdThreads), nch);
+        int slot = prof_begin(c, c->evFwd, c->nFwd);
+        k_forward_mixed<GZ, TMI, kFwdFacetTile><<<grid, kFwdThreads, 0, c->stream>>>(
+            S, s.d_xyz.p, c->T, c->d_mc.p, c->d_mf32.p, c->d_chunkBegin.p, c->d_chunkEnd.p, c->tau,
+            GZ ? c->d_partG.p : nullptr, TMI ? c->d_partM.p : nullptr, c->d_nearPairs.p);
+        prof_end(c, c->evFwd, slot);
+    }
+    k_forward_reduce_mixed<<<cdiv(S, 32), 256, 0, c->stream>>>(S, nch, GZ ? c->d_partG.p : nullptr,
+                                                                TMI ? c->d_partM.p : nullptr, GZ ? d_gz : nullptr,
+                                                                TMI ? d_tmi : nullptr);
+    c->counters.launches += 2;
+    c->counters.forward_pairs += (uint64_t)S * (uint64_t)c->chunkFacets;
+    LF_CHECK_LAUNCH(c);
+    return LF_OK;
+}
+
+template <bool GZ, bool TMI>
 static lf_status forward_set_mixed(lf_ctx* c, const StationSet& s, double* d_gz, double* d_tmi) {
+    if (c->tune.fwd_engine == LF_FWD_FACET) return forward_set_facet<GZ, TMI>(c, s, d_gz, d_tmi);
     if (c->partitioned) return forward_set_patch_items<GZ, TMI>(c, s, d_gz, d_tmi);
     int S = s.n;
     if (S == 0) return LF_OK;
@@ -1885,7 +1928,8 @@ static lf_status run_cached(lf_ctx* c, lf_ctx::GraphSet& set, const double* p, d
 
 extern "C" lf_status lf_set_tuning(lf_ctx* c, const lf_tuning* t) {
     if (!c || !t || t->fwd_target_blocks < 0 || t->grad_target_warps < 1 || t->near_tiles_per_chunk < 0 ||
-        (t->patch_threads != 128 && t->patch_threads != 256) || !std::isfinite(t->far_ratio))
+        (t->patch_threads != 128 && t->patch_threads != 256) || !std::isfinite(t->far_ratio) ||
+        (t->fwd_engine != LF_FWD_FACET && t->fwd_engine != LF_FWD_PATCH))
         return LF_EINVAL;
     c->epoch++;
     c->tune = *t;
@@ -1964,21 +2008,31 @@ extern "C" lf_status lf_autotune(lf_ctx* c, const double* params, int repeats, l
     double bestMs = 0.0;
     lf_status st = timeit(best, &bestMs);
     const bool mixed = c->precision == LF_PREC_MIXED;
+    const int engineC[] = {LF_FWD_FACET, LF_FWD_PATCH};
     const int fwdC[] = {0, 148 * 4, 148 * 8, 148 * 16, 148 * 32, 148 * 64, 148 * 128};
     const int gradC[] = {148 * 16, 148 * 32, 148 * 64, 148 * 128, 148 * 256};
     const int nearC[] = {0, 1, 2, 4, 8};
     const int threadsC[] = {128, 256};
-    for (int dim = 0; dim < 4 && st == LF_OK; ++dim) {
-        const int* cand = dim == 0 ? fwdC : (dim == 1 ? gradC : (dim == 2 ? nearC : threadsC));
-        const int nc = dim == 0 ? 7 : (dim == 3 ? 2 : 5);
-        if (dim >= 2 && !mixed) break;
+    // dimensions in turn: forward engine (mixed only), forward CTAs, gradient
+    // warps, near tiles (mixed), patch threads (patch engine)
+    for (int dim = 0; dim < 5 && st == LF_OK; ++dim) {
+        if ((dim == 0 || dim == 3) && !mixed) continue;
+        if (dim == 4 && (!mixed || best.fwd_engine != LF_FWD_PATCH)) continue;
+        const int* cand = dim == 0 ? engineC : dim == 1 ? fwdC : dim == 2 ? gradC : dim == 3 ? nearC : threadsC;
+        const int nc = dim == 0 ? 2 : dim == 1 ? 7 : dim == 4 ? 2 : 5;
         for (int k = 0; k < nc && st == LF_OK; ++k) {
             lf_tuning t = best;
-            int& field = dim == 0 ? t.fwd_target_blocks
-                                  : (dim == 1 ? t.grad_target_warps
-                                              : (dim == 2 ? t.near_tiles_per_chunk : t.patch_threads));
-            if (field == cand[k] || (dim == 0 && cand[k] == 0 && !mixed)) continue;
+            int& field = dim == 0 ? t.fwd_engine
+                                  : dim == 1 ? t.fwd_target_blocks
+                                             : dim == 2 ? t.grad_target_warps
+                                                        : dim == 3 ? t.near_tiles_per_chunk : t.patch_threads;
+            if (field == cand[k]) continue;
             field = cand[k];
+            // the persistent schedule (0 forward CTAs) exists for the patch engine only
+            if (t.fwd_target_blocks == 0 && !(mixed && t.fwd_engine == LF_FWD_PATCH)) {
+                if (dim == 1) continue;
+                t.fwd_target_blocks = 148 * 8;
+            }
             double ms = 0.0;
             st = timeit(t, &ms);
             if (st == LF_OK && ms < bestMs) {

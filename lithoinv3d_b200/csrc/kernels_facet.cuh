@@ -1,0 +1,358 @@
+// Per-facet mixed-precision forward (engine LF_FWD_FACET of lf_tuning): one
+// FP32 record per facet, written once per evaluation by k_face_prep_mixed,
+// streamed through shared memory 32 facets at a time; each (station, facet)
+// pair evaluates its three vertex distances, three edge integrals and the
+// solid angle on its own.  The patch engine (kernels_patch.cuh) shares the
+// vertex distances and edge integrals across the facets of a patch instead;
+// lf_autotune picks the faster engine per model.
+#pragma once
+#include "kernels_mixed.cuh"
+
+namespace litho_b200 {
+
+// FP32 facet record of the far-field forward, written once per evaluation by
+// k_face_prep_mixed (array [T] in HBM), copied 32 facets at a time into
+// shared memory and read there with 128-bit loads (10 per far pair, 9 beyond
+// 4 tau).  The origin and the unit normal stay FP64: the height above the
+// facet plane can be tiny next to |o - a| (a far top facet seen from 1 m
+// above it).  The last row feeds the per-warp near/far test.
+struct __align__(16) FaceF32 {
+    float rx0, rx1, rx2, L0;   // local x axis, |ab|
+    float ry0, ry1, ry2, cx;   // local y axis, c.x
+    float cy, L1, L2, gq;      // c.y, |bc|, |ca|, n_z * gz scale * area
+    float mf, mt0, mt1, mt2;   // TMI facet scales, doubled
+    float q6[12];              // (x, y) of the 6-point rule's points in the local frame
+    float q3[8];               // (x, y) of the 3-point rule's points, pad
+    double ax, ay, az, zx, zy, zz;
+    float cenx, ceny, cenz;    // centroid
+    float size;                // longest edge; -1 for a facet that contributes nothing
+};
+static_assert(sizeof(FaceF32) == 208, "FaceF32 layout");
+constexpr int kFaceF32Vec = sizeof(FaceF32) / 16;  // float4 per record
+
+// The far-field record of one facet from its mixed constants m[NMC].
+__device__ __forceinline__ void make_face_f32(const double* m, FaceF32& F) {
+#define M(k) m[k]
+    F.rx0 = (float)M(MC_XX); F.rx1 = (float)M(MC_XY); F.rx2 = (float)M(MC_XZ);
+    F.ry0 = (float)M(MC_YX); F.ry1 = (float)M(MC_YY); F.ry2 = (float)M(MC_YZ);
+    F.L0 = (float)M(MC_L0); F.cx = (float)M(MC_CX); F.cy = (float)M(MC_CY);
+    F.L1 = (float)M(MC_L1); F.L2 = (float)M(MC_L2);
+    F.gq = (float)(M(MC_SGZ) * 0.5 * M(MC_L0) * M(MC_CY));
+    // TMI scales doubled: the far pair's series give atan2 and atanh (exact)
+    F.mf = 2.f * (float)M(MC_MF); F.mt0 = 2.f * (float)M(MC_MT0);
+    F.mt1 = 2.f * (float)M(MC_MT1); F.mt2 = 2.f * (float)M(MC_MT2);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        F.q6[2 * q] = kDun6Bb[q] * F.L0 + kDun6Bc[q] * F.cx;
+        F.q6[2 * q + 1] = kDun6Bc[q] * F.cy;
+    }
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        F.q3[2 * q] = kTri3Bb[q] * F.L0 + kTri3Bc[q] * F.cx;
+        F.q3[2 * q + 1] = kTri3Bc[q] * F.cy;
+    }
+    F.q3[6] = F.q3[7] = 0.f;
+    F.ax = M(MC_AX); F.ay = M(MC_AY); F.az = M(MC_AZ);
+    F.zx = M(MC_ZX); F.zy = M(MC_ZY); F.zz = M(MC_ZZ);
+    F.cenx = (float)M(MC_CENX); F.ceny = (float)M(MC_CENY); F.cenz = (float)M(MC_CENZ);
+    F.size = M(MC_VALID) != 0.0 ? (float)M(MC_SIZE) : -1.f;
+#undef M
+}
+
+__global__ void k_face_prep_mixed(int T, const int32_t* __restrict__ tri, const double* __restrict__ pos,
+                                  const int16_t* __restrict__ face_group, const GroupConst* __restrict__ groups, d3 fdir,
+                                  double* __restrict__ mc, FaceF32* __restrict__ mf32) {
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= T) return;
+    d3 v[3];
+    for (int k = 0; k < 3; ++k) {
+        const double* p = pos + 3 * tri[3 * f + k];
+        v[k] = mk3(p[0], p[1], p[2]);
+    }
+    // reference-order normal and magnetic products (bit-identical to the
+    // reference, which matters for facets collapsed to a line)
+    d3 n = cross_rn(sub_rn(v[1], v[0]), sub_rn(v[2], v[0]));
+    double area2 = norm_rn(n);
+    double out[NMC];
+    for (int k = 0; k < NMC; ++k) out[k] = 0.0;
+    if (!(area2 < kEps)) {
+        d3 un = div_rn(n, area2);
+        const GroupConst& g = groups[face_group[f]];
+        d3 m = mk3(g.mdir[0], g.mdir[1], g.mdir[2]);
+        double mf = __dmul_rn(dot_rn(m, un), dot_rn(fdir, un));
+        double mt[3], L[3];
+        for (int i = 0; i < 3; ++i) {
+            d3 e = sub_rn(v[(i + 1) % 3], v[i]);
+            L[i] = norm_rn(e);
+            d3 eh = (L[i] < kEps) ? mk3(0, 0, 0) : div_rn(e, L[i]);
+            d3 perp = cross_rn(un, eh);
+            mt[i] = __dmul_rn(dot_rn(m, perp), dot_rn(fdir, perp));
+        }
+        int k = 0;  // rotate so that edge 0 is the longest
+        if (L[1] > L[k]) k = 1;
+        if (L[2] > L[k]) k = 2;
+        d3 a = v[k], b = v[(k + 1) % 3], c = v[(k + 2) % 3];
+        double L0 = L[k];
+        d3 xh = (b - a) * (1.0 / L0);
+        // On a facet collapsed onto a line the reference's unit normal is
+        // rounding noise and not perpendicular to the edges; the frame must
+        // stay orthonormal for the local coordinates (and so Lambda, which the
+        // reference takes from positions alone) to be right.
+        d3 zh = un - xh * dot3(un, xh);
+        zh = zh * (1.0 / norm3(zh));
+        d3 yh = cross3(zh, xh);
+        d3 ca = c - a;
+        double cx = dot3(ca, xh), cy = dot3(ca, yh);
+        double L1 = L[(k + 1) % 3], L2 = L[(k + 2) % 3];
+        out[MC_AX] = a.x; out[MC_AY] = a.y; out[MC_AZ] = a.z;
+        out[MC_XX] = xh.x; out[MC_XY] = xh.y; out[MC_XZ] = xh.z;
+        out[MC_YX] = yh.x; out[MC_YY] = yh.y; out[MC_YZ] = yh.z;
+        out[MC_ZX] = zh.x; out[MC_ZY] = zh.y; out[MC_ZZ] = zh.z;
+        out[MC_L0] = L0; out[MC_CX] = cx; out[MC_CY] = cy;
+        out[MC_L1] = L1; out[MC_L2] = L2;
+        if (!(L1 < kEps)) { out[MC_E1X] = (cx - L0) / L1; out[MC_E1Y] = cy / L1; }
+        if (!(L2 < kEps)) { out[MC_E2X] = -cx / L2; out[MC_E2Y] = -cy / L2; }
+        out[MC_SGZ] = un.z * g.gscale_fwd;
+        out[MC_MF] = -g.mscale * mf;
+        out[MC_MT0] = -g.mscale * mt[k];
+        out[MC_MT1] = -g.mscale * mt[(k + 1) % 3];
+        out[MC_MT2] = -g.mscale * mt[(k + 2) % 3];
+        out[MC_CENX] = (v[0].x + v[1].x + v[2].x) / 3.0;
+        out[MC_CENY] = (v[0].y + v[1].y + v[2].y) / 3.0;
+        out[MC_CENZ] = (v[0].z + v[1].z + v[2].z) / 3.0;
+        out[MC_SIZE] = L0;
+        out[MC_VALID] = 1.0;
+    }
+    for (int k = 0; k < NMC; ++k) mc[(size_t)k * T + f] = out[k];
+    FaceF32 F;
+    make_face_f32(out, F);
+    const float4* src = reinterpret_cast<const float4*>(&F);
+    float4* dst = reinterpret_cast<float4*>(mf32 + f);
+#pragma unroll
+    for (int k = 0; k < kFaceF32Vec; ++k) dst[k] = src[k];
+}
+
+
+enum { RULE_TRI3 = 0, RULE_DUN6 = 1, RULE_MID28 = 2 };
+
+// Far pair: gz by quadrature (RULE_TRI3 beyond 4 tau, RULE_DUN6 beyond tau,
+// RULE_MID28: Radon's rule on the midpoint subdivision beyond tau/2), TMI
+// analytic, both FP32; o = station (FP64).
+template <int RULE>
+__device__ __forceinline__ void pair_far_f32(const FaceF32* Fp, double ox, double oy, double oz, float* gz,
+                                             float* tmi) {
+    const float4* v = reinterpret_cast<const float4*>(Fp);
+    const double2* w = reinterpret_cast<const double2*>(Fp);
+    const float4 v0 = v[0], v1 = v[1], v2 = v[2], v3 = v[3];
+    const double2 w0 = w[9], w1 = w[10], w2 = w[11];
+    const double ddx = ox - w0.x, ddy = oy - w0.y, ddz = oz - w1.x;
+    const float dx = (float)ddx, dy = (float)ddy, dz = (float)ddz;
+    const float x = fmaf(dx, v0.x, fmaf(dy, v0.y, dz * v0.z));
+    const float y = fmaf(dx, v1.x, fmaf(dy, v1.y, dz * v1.z));
+    const float z = (float)(ddx * w1.y + ddy * w2.x + ddz * w2.y);
+    const float L0 = v0.w, cx = v1.w, cy = v2.x, L1 = v2.y, L2 = v2.z, gq = v2.w;
+    const float z2 = z * z;
+    // gz: n_z * gscale * A * sum_q w_q / r_q.  A facet with a horizontal unit
+    // normal (n_z == 0 exactly: every vertical face of a voxel-built surface,
+    // which z-only vertex moves keep vertical) has gq == 0 and adds exactly
+    // zero, as in the reference's n_z * (...) product; its quadrature is
+    // skipped.  The facet is the same for every lane, so the branch is
+    // warp-uniform.
+    float acc = 0.f;
+    if (gq == 0.f) {
+    } else if (RULE == RULE_MID28) {
+#pragma unroll
+        for (int q = 0; q < 28; ++q) {
+            float px = fmaf(kRadon4Bb[q], L0, fmaf(kRadon4Bc[q], cx, -x)), py = fmaf(kRadon4Bc[q], cy, -y);
+            acc = fmaf(kRadonW[q % 7], rsqrtf(fmaf(px, px, fmaf(py, py, z2))), acc);
+        }
+        acc *= 0.25f;
+    } else if (RULE == RULE_DUN6) {
+        const float4 qa = v[4], qb = v[5], qc = v[6];
+        const float q[12] = {qa.x, qa.y, qa.z, qa.w, qb.x, qb.y, qb.z, qb.w, qc.x, qc.y, qc.z, qc.w};
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            float px = q[2 * k] - x, py = q[2 * k + 1] - y;
+            acc = fmaf(kDun6W[k], rsqrtf(fmaf(px, px, fmaf(py, py, z2))), acc);
+        }
+    } else {
+        const float4 qa = v[7], qb = v[8];
+        const float q[6] = {qa.x, qa.y, qa.z, qa.w, qb.x, qb.y};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            float px = q[2 * k] - x, py = q[2 * k + 1] - y;
+            acc += rsqrtf(fmaf(px, px, fmaf(py, py, z2)));
+        }
+        acc *= (1.f / 3.f);
+    }
+    if (gq != 0.f) *gz += gq * acc;
+    // TMI: MF * Omega + sum_i MT_i Lambda_i with Omega = 2 atan2(ny, den) and
+    // Lambda_i = 2 atanh(v_i); the record holds 2 MF and 2 MT_i, so the terms
+    // below are atan2 and atanh.  Scaling by 2 is exact: the bits equal
+    // MF * (2 atan2) + MT_i * (2 atanh).
+    float rbx = L0 - x, rcx = cx - x, rcy = cy - y;
+    float la = sqrt_pos(fmaf(x, x, fmaf(y, y, z2)));
+    float lb = sqrt_pos(fmaf(rbx, rbx, fmaf(y, y, z2)));
+    float lc = sqrt_pos(fmaf(rcx, rcx, fmaf(rcy, rcy, z2)));
+    float dab = fmaf(-x, rbx, fmaf(y, y, z2));
+    float dac = fmaf(-x, rcx, fmaf(-y, rcy, z2));
+    float dbc = fmaf(rbx, rcx, fmaf(-y, rcy, z2));
+    float den = la * lb * lc + dab * lc + dac * lb + dbc * la;
+    const float ny = -z * (L0 * cy);
+    const float e0 = __fdividef(L0, la + lb), e1 = __fdividef(L1, lb + lc), e2 = __fdividef(L2, lc + la);
+    float om, l0, l1, l2;
+    if (far_series_ok(ny, den, e0, e1, e2)) {
+        om = atan_series(__fdividef(ny, den));
+        l0 = atanh_series(e0);
+        l1 = atanh_series(e1);
+        l2 = atanh_series(e2);
+    } else {
+        om = atan2_far(ny, den);
+        l0 = 0.5f * lam_f32(la, lb, L0);
+        l1 = 0.5f * lam_f32(lb, lc, L1);
+        l2 = 0.5f * lam_f32(lc, la, L2);
+    }
+    *tmi += v3.x * om + v3.y * l0 + v3.z * l1 + v3.w * l2;
+}
+
+
+// Station-per-thread forward: CTAs of 128 stations (pre-ordered along a
+// Morton curve, so a warp's 32 stations are spatially compact) x facet
+// chunks, facets staged 32 at a time in shared memory (their FP32 records,
+// written by k_face_prep_mixed, copied by the whole CTA; the FP64 constants
+// of a near facet fetched into the warp's own slot when it meets one,
+// which is a few per cent of pairs).  The precision class
+// is decided per (warp, facet): lane j tests facet j of the stage against the
+// warp's station bounding box -- centroid at least 4 tau x size away: very
+// far (FP32, 3-point gz); at least tau x size: far (FP32, 6-point gz); at
+// least tau/2 x size: mid (FP32, 28-point gz); else near (FP64 analytic) --
+// and the warp walks each class warp-uniformly.
+// One CTA's work: station s (this thread; act = s is a station of the
+// block) against facets [fb, fe); out_gz[s] / out_tmi[s] receive the sums.
+template <bool GZ, bool TMI, int FT>
+__device__ __forceinline__ void forward_mixed_block(FaceF32* __restrict__ smf, double* __restrict__ smn, int s,
+                                                    bool act, const double* __restrict__ sta, int T,
+                                                    const double* __restrict__ mc, const FaceF32* __restrict__ mf32,
+                                                    int fb, int fe, float tau,
+                                                    double* __restrict__ out_gz, double* __restrict__ out_tmi,
+                                                    unsigned long long* __restrict__ near_pairs) {
+    static_assert(FT == 32, "one facet per lane in the near/far test");
+    const int lane = threadIdx.x & 31;
+    double ox = 0.0, oy = 0.0, oz = 0.0;
+    if (act) { ox = sta[3 * s]; oy = sta[3 * s + 1]; oz = sta[3 * s + 2]; }
+    // the warp's station bounding box: lo = min, hi = -min(-x)
+    float bb[6] = {act ? (float)ox : 3e38f, act ? (float)oy : 3e38f, act ? (float)oz : 3e38f,
+                   act ? -(float)ox : 3e38f, act ? -(float)oy : 3e38f, act ? -(float)oz : 3e38f};
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) bb[k] = fminf(bb[k], __shfl_xor_sync(0xffffffffu, bb[k], off));
+    double gz = 0.0, tmi = 0.0;
+    unsigned long long nearCount = 0;
+    for (int f0 = fb; f0 < fe; f0 += FT) {
+        const int nf = min(FT, fe - f0);
+        __syncthreads();  // the previous stage's records are no longer read
+        {
+            const float4* __restrict__ src = reinterpret_cast<const float4*>(mf32 + f0);
+            float4* dst = reinterpret_cast<float4*>(smf);
+            for (int idx = threadIdx.x; idx < nf * kFaceF32Vec; idx += blockDim.x) dst[idx] = __ldg(src + idx);
+        }
+        __syncthreads();
+        // lane j: facet j of the stage against this warp's box
+        bool valid = false, vfar = false, far = false, mid = false;
+        if (lane < nf && !(smf[lane].size < 0.f)) {
+            valid = true;
+            const float cxw = smf[lane].cenx, cyw = smf[lane].ceny, czw = smf[lane].cenz;
+            const float ddx = fmaxf(0.f, fmaxf(bb[0] - cxw, cxw + bb[3]));
+            const float ddy = fmaxf(0.f, fmaxf(bb[1] - cyw, cyw + bb[4]));
+            const float ddz = fmaxf(0.f, fmaxf(bb[2] - czw, czw + bb[5]));
+            const float d2 = ddx * ddx + ddy * ddy + ddz * ddz;
+            const float lim = tau * smf[lane].size, limMid = 0.5f * lim;
+            vfar = d2 >= 16.f * (lim * lim);
+            far = !vfar && d2 >= lim * lim;
+            mid = !vfar && !far && d2 >= limMid * limMid;
+        }
+        const unsigned vfarMask = __ballot_sync(0xffffffffu, valid && vfar);
+        const unsigned farMask = __ballot_sync(0xffffffffu, valid && far);
+        const unsigned midMask = __ballot_sync(0xffffffffu, valid && mid);
+        const unsigned nearMask = __ballot_sync(0xffffffffu, valid && !vfar && !far && !mid);
+        if (act) {
+            float gacc = 0.f, tacc = 0.f;
+            for (unsigned m = vfarMask; m; m &= m - 1) {
+                const int j = __ffs(m) - 1;
+                pair_far_f32<RULE_TRI3>(&smf[j], ox, oy, oz, &gacc, &tacc);
+            }
+            for (unsigned m = farMask; m; m &= m - 1) {
+                const int j = __ffs(m) - 1;
+                pair_far_f32<RULE_DUN6>(&smf[j], ox, oy, oz, &gacc, &tacc);
+            }
+            for (unsigned m = midMask; m; m &= m - 1) {
+                const int j = __ffs(m) - 1;
+                pair_far_f32<RULE_MID28>(&smf[j], ox, oy, oz, &gacc, &tacc);
+            }
+            if (GZ) gz += gacc;
+            if (TMI) tmi += tacc;
+            nearCount += __popc(nearMask);
+        }
+        // Near facets (a few per cent of pairs): the warp copies the facet's
+        // FP64 constants from HBM into its own slot of shared memory (lane k
+        // loads constant k), then every lane reads them from there.
+        double* slot = smn + (threadIdx.x >> 5) * NMC;
+        for (unsigned m = nearMask; m; m &= m - 1) {
+            const int j = __ffs(m) - 1;
+            __syncwarp();
+            if (lane < NMC) slot[lane] = __ldg(mc + (size_t)lane * T + f0 + j);
+            __syncwarp();
+            if (act) {
+                double g1 = 0.0, t1 = 0.0;
+                pair_near_f64(slot, 0, 1, mk3(ox, oy, oz), &g1, &t1);
+                if (GZ) gz += g1;
+                if (TMI) tmi += t1;
+            }
+        }
+    }
+    if (act) {
+        if (GZ) out_gz[s] = gz;
+        if (TMI) out_tmi[s] = tmi;
+        if (near_pairs && nearCount) atomicAdd(near_pairs, nearCount);
+    }
+}
+
+template <bool GZ, bool TMI, int FT>
+__global__ void __launch_bounds__(128) k_forward_mixed(int S, const double* __restrict__ sta, int T,
+                                                       const double* __restrict__ mc,
+                                                       const FaceF32* __restrict__ mf32,
+                                                       const int32_t* __restrict__ chunk_begin,
+                                                       const int32_t* __restrict__ chunk_end, float tau,
+                                                       double* __restrict__ part_gz, double* __restrict__ part_tmi,
+                                                       unsigned long long* __restrict__ near_pairs) {
+    __shared__ FaceF32 smf[FT];
+    __shared__ double smn[4 * NMC];  // one near-facet slot per warp (128 threads)
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const int chunk = blockIdx.y;
+    forward_mixed_block<GZ, TMI, FT>(smf, smn, s, s < S, sta, T, mc, mf32, chunk_begin[chunk], chunk_end[chunk], tau,
+                                     GZ ? part_gz + (size_t)chunk * S : nullptr,
+                                     TMI ? part_tmi + (size_t)chunk * S : nullptr, near_pairs);
+}
+
+// Batched bodies (item list as for k_forward_fp64_items).
+template <bool GZ, bool TMI, int FT>
+__global__ void __launch_bounds__(128) k_forward_mixed_items(const FwdItem* __restrict__ items, int nitems,
+                                                             const double* __restrict__ sta, int T,
+                                                             const double* __restrict__ mc,
+                                                             const FaceF32* __restrict__ mf32, float tau,
+                                                             double* __restrict__ part_gz, double* __restrict__ part_tmi,
+                                                             unsigned long long* __restrict__ near_pairs) {
+    __shared__ FaceF32 smf[FT];
+    __shared__ double smn[4 * NMC];  // one near-facet slot per warp (128 threads)
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const FwdItem w = items[it];
+        const int s = w.s0 + (int)threadIdx.x;
+        forward_mixed_block<GZ, TMI, FT>(smf, smn, s, s < w.s_end, sta, T, mc, mf32, w.fb, w.fe, tau,
+                                         GZ ? part_gz + w.out : nullptr, TMI ? part_tmi + w.out : nullptr,
+                                         near_pairs);
+    }
+}
+
+
+}  // namespace litho_b200

@@ -3,13 +3,15 @@ sets, and the objective and gradient under any shape agree with the default
 shapes up to the summation order of partial sums: 1e-12 relative in FP64;
 1e-6 in mixed precision, where chunk boundaries regroup the FP32 far-field
 partial sums (the mixed gradient's own tolerance is 1e-5).  In mixed
-precision the tuner also picks the station-block size of the patch forward
-(128 or 256) and the far-field ratio tau from {2, 2.5, 3, 4}, the latter only
-within its accuracy gate against the FP64 path, which the test re-checks."""
+precision the tuner also picks the forward engine (per-facet records or
+facet patches), the station-block size of the patch forward (128 or 256)
+and the far-field ratio tau from {2, 2.5, 3, 4}, the latter only within its
+accuracy gate against the FP64 path, which the test re-checks."""
 import numpy as np
 import pytest
 
 from lithoinv3d_b200 import PREC_MIXED, LithoError, synth
+from lithoinv3d_b200.api import FWD_FACET, FWD_PATCH
 
 pytestmark = pytest.mark.gpu
 
@@ -38,10 +40,13 @@ def test_autotune_keeps_results(mixed):
     assert t.near_tiles_per_chunk in (0, 1, 2, 4, 8)
     assert t.patch_threads in (128, 256)
     assert t.far_ratio in (2.0, 2.5, 3.0, 4.0)
+    assert t.fwd_engine in (FWD_FACET, FWD_PATCH)
+    if t.fwd_target_blocks == 0:
+        assert t.fwd_engine == FWD_PATCH
     got = ctx.tuning()
     assert (got.fwd_target_blocks, got.grad_target_warps, got.near_tiles_per_chunk, got.patch_threads,
-            got.far_ratio) == (t.fwd_target_blocks, t.grad_target_warps, t.near_tiles_per_chunk, t.patch_threads,
-                               t.far_ratio)
+            got.far_ratio, got.fwd_engine) == (t.fwd_target_blocks, t.grad_target_warps, t.near_tiles_per_chunk,
+                                               t.patch_threads, t.far_ratio, t.fwd_engine)
     f1, g1 = ctx.objective_and_gradient(x0)
     if mixed:  # tau may have moved: hold the tuned result to the FP64 path
         ref = p.make_context(m, grav_obs=gobs, mag_obs=mobs)
@@ -58,5 +63,12 @@ def test_autotune_keeps_results(mixed):
         ctx.set_tuning(*shape)
         f2, g2 = ctx.objective_and_gradient(x0)
         assert abs(f2 - f0) <= tol * abs(f0) and rel(g2, g0) < tol
+    if mixed:  # the two forward engines agree within the mixed path's tolerances
+        for engine in (FWD_FACET, FWD_PATCH):
+            ctx.set_tuning(148 * 8, 148 * 64, 0, 128, 3.0, engine)
+            fe, ge = ctx.objective_and_gradient(x0)
+            assert abs(fe - f0) <= 1e-6 * abs(f0) and rel(ge, g0) < 1e-5
     with pytest.raises(LithoError):
         ctx.set_tuning(-1, 1, 0)
+    with pytest.raises(LithoError):
+        ctx.set_tuning(148 * 8, 148 * 64, 0, 128, 3.0, 7)
