@@ -134,6 +134,9 @@ def parse():
                     help="x/y vertex derivatives of the gradient: closed form, or per-facet forward differences "
                          "with --xy-step (the large-inversion configuration's h = 0.5 m)")
     ap.add_argument("--xy-step", type=float, default=0.5)
+    ap.add_argument("--drop-collapsed", action="store_true",
+                    help="facets collapsed onto a line contribute nothing to the forward either (their reference "
+                         "TMI term is rounding noise and discontinuous)")
     args = ap.parse_args()
     if args.steps is None:
         args.steps = 50 if args.impl == "reference" else {"contact": 1000, "large": 20, "batch": 5}.get(args.workload, 50)
@@ -500,6 +503,10 @@ def main():
         from lithoinv3d_b200 import GATHER_CHAIN
 
         ctx.set_gradient_gather(GATHER_CHAIN)
+    if args.drop_collapsed:
+        from lithoinv3d_b200.api import COLLAPSED_DROP
+
+        ctx.set_collapsed_facets(COLLAPSED_DROP)
     if args.xy_derivative == "fd":
         from lithoinv3d_b200 import XY_FORWARD_DIFFERENCE
 
@@ -624,6 +631,7 @@ def main():
             "details": {"parallelism": f"replicas x{world}", "precision": args.precision,
                         "fp64_near_pair_fraction": round(near_frac, 4), "cuda_graph": True,
                         "gradient_gather": args.gather,
+                        "collapsed_facets": "dropped" if args.drop_collapsed else "reference",
                         "xy_derivative": (f"forward difference, h = {args.xy_step} m" if args.xy_derivative == "fd"
                                           else "analytic"),
                         "tuning": {"fwd_target_blocks": tuned.fwd_target_blocks,

@@ -367,6 +367,23 @@ lf_status lf_set_gradient_gather(lf_ctx* ctx, int mode);
 enum { LF_XY_ANALYTIC = 0, LF_XY_FORWARD_DIFFERENCE = 1 };
 lf_status lf_set_xy_derivative(lf_ctx* ctx, int mode, double step);
 
+/* Facets collapsed onto a line (twice-area below 1e-10 x the longest edge
+ * squared; the control-point interpolation produces them).  No reference
+ * counterpart.
+ *  LF_COLLAPSED_KEEP (default): the forward evaluates them as the reference
+ *    does.  Their unit normal is rounding noise and the reference's TMI facet
+ *    term (magnetic_forward.cpp:312-347) does not vanish with the area, so
+ *    their TMI contribution is reproduced bit for bit but is a discontinuous
+ *    function of the positions: central differences of the objective jump
+ *    by orders of magnitude between steps of 1e-1 and 1e-3 m.
+ *  LF_COLLAPSED_DROP: they contribute nothing to the forward either (the
+ *    gradient kernels always take them as zero), so that the objective is
+ *    the function its gradient differentiates.
+ * Applies to every forward of the context (both precisions and engines,
+ * unit responses included). */
+enum { LF_COLLAPSED_KEEP = 0, LF_COLLAPSED_DROP = 1 };
+lf_status lf_set_collapsed_facets(lf_ctx* ctx, int mode);
+
 /* Graph mode (no reference counterpart: the reference evaluates on one CPU
  * thread).  When enabled, lf_objective, lf_objective_grad and
  * lf_objective_grad_device replay a CUDA graph of the whole evaluation

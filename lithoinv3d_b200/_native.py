@@ -87,6 +87,7 @@ SIGNATURES = {
     "lf_set_scatter_stateless": (C.c_int, [_vp, C.c_int]),
     "lf_set_gradient_gather": (C.c_int, [_vp, C.c_int]),
     "lf_set_xy_derivative": (C.c_int, [_vp, C.c_int, C.c_double]),
+    "lf_set_collapsed_facets": (C.c_int, [_vp, C.c_int]),
     "lf_calibrate_data_weights": (C.c_int, [_vp, _dp, C.c_uint, _dp, _dp, _dp]),
     "lf_mlp_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint, C.POINTER(_vp)]),
     "lf_mlp_destroy": (None, [_vp]),

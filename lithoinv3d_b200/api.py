@@ -22,6 +22,7 @@ PREC_FP64, PREC_MIXED = 0, 1
 GATHER_REFERENCE, GATHER_CHAIN = 0, 1
 XY_ANALYTIC, XY_FORWARD_DIFFERENCE = 0, 1
 FWD_FACET, FWD_PATCH = 0, 1
+COLLAPSED_KEEP, COLLAPSED_DROP = 0, 1
 UNIT_GRAVITY, UNIT_INDUCED, UNIT_DIRECTION, UNIT_REMANENCE = range(4)
 
 
@@ -393,6 +394,11 @@ class Context:
         objective gradient by per-facet forward differences with `step` metres
         (FP64), z analytic; lf_set_xy_derivative."""
         self._check(self.lib.lf_set_xy_derivative(self.h, int(mode), float(step)), "set_xy_derivative")
+
+    def set_collapsed_facets(self, mode: int):
+        """COLLAPSED_KEEP (the reference's forward) or COLLAPSED_DROP (facets
+        collapsed onto a line contribute nothing); lf_set_collapsed_facets."""
+        self._check(self.lib.lf_set_collapsed_facets(self.h, int(mode)), "set_collapsed_facets")
 
     def set_graph_mode(self, enabled: bool = True):
         """Replay evaluations as a captured CUDA graph (lf_set_graph_mode)."""

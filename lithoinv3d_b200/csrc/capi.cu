@@ -155,6 +155,7 @@ struct lf_ctx {
     DevBuf<double> d_adjW, d_vgrad2;
     // lf_set_xy_derivative: x and y vertex derivatives of the objective
     // gradient by per-facet forward differences with step xyStep (FP64)
+    int dropCollapsed = 0;  // lf_set_collapsed_facets
     int xyMode = 0;
     double xyStep = 0.5;
     DevBuf<double> d_fcfd;  // [7][NFC][nGradFacets] moved-facet constants
@@ -1308,7 +1309,8 @@ static lf_status mixed_prep(lf_ctx* c) {
     if (c->tune.fwd_engine == LF_FWD_FACET) {
         LF_TRY_CUDA(c, c->d_mf32.reserve((size_t)std::max(c->T, 1)));
         k_face_prep_mixed<<<cdiv(c->T, 128), 128, 0, c->stream>>>(c->T, c->d_tri.p, c->d_pos.p, c->d_faceGroup.p,
-                                                                  c->d_groups.p, c->fdir, c->d_mc.p, c->d_mf32.p);
+                                                                  c->d_groups.p, c->fdir, c->d_mc.p, c->d_mf32.p,
+                                                                  c->dropCollapsed);
         c->counters.launches++;
         LF_CHECK_LAUNCH(c);
         return LF_OK;
@@ -1317,7 +1319,7 @@ static lf_status mixed_prep(lf_ctx* c) {
     k_face_prep_patch<<<cdiv(c->T, 128), 128, 0, c->stream>>>(
         c->T, c->d_tri.p, c->d_pos.p, c->d_faceGroup.p, c->d_groups.p, c->fdir, c->d_pFacetPatch.p, c->d_pFacetSlot.p,
         c->d_pFacetOff.p, c->d_pCorners.p, c->d_pVertOff.p, c->d_pVerts.p, c->d_pEdgeOff.p, c->d_pBlobOff.p,
-        c->d_mc.p, c->d_mt2.p, c->d_blobs.p);
+        c->d_mc.p, c->d_mt2.p, c->d_blobs.p, c->dropCollapsed);
     if (pt.P > 0)
         k_patch_prep<<<pt.P, 32, 0, c->stream>>>(pt.P, c->d_pos.p, c->d_pFacetOff.p, c->d_pFacets.p, c->d_pVertOff.p,
                                                   c->d_pVerts.p, c->d_pEdgeOff.p, c->d_pEdgeInfo.p, c->d_pEdgeSlot.p,
@@ -1547,7 +1549,8 @@ static lf_status forward_all(lf_ctx* c) {
         return forward_set_mixed<false, true>(c, c->mag, nullptr, c->mag.d_pred.p);
     }
     k_face_prep_fwd<<<cdiv(c->T, 128), 128, 0, c->stream>>>(c->T, c->d_tri.p, c->d_pos.p, c->d_faceGroup.p,
-                                                            c->d_groups.p, c->fdir, c->d_fc.p);
+                                                            c->d_groups.p, c->fdir, c->d_fc.p,
+                                                            c->dropCollapsed);
     c->counters.launches++;
     LF_CHECK_LAUNCH(c);
     if (c->sameStations) return forward_set<true, true>(c, c->grav, c->grav.d_pred.p, c->mag.d_pred.p);
@@ -2084,6 +2087,15 @@ extern "C" lf_status lf_autotune(lf_ctx* c, const double* params, int repeats, l
     return LF_OK;
 }
 
+extern "C" lf_status lf_set_collapsed_facets(lf_ctx* c, int mode) {
+    if (!c) return LF_EINVAL;
+    if (mode != LF_COLLAPSED_KEEP && mode != LF_COLLAPSED_DROP)
+        return fail(c, LF_EINVAL, "collapsed-facet mode must be LF_COLLAPSED_KEEP or LF_COLLAPSED_DROP");
+    c->dropCollapsed = mode == LF_COLLAPSED_DROP;
+    c->epoch++;
+    return LF_OK;
+}
+
 extern "C" lf_status lf_set_xy_derivative(lf_ctx* c, int mode, double step) {
     if (!c) return LF_EINVAL;
     if (mode != LF_XY_ANALYTIC && mode != LF_XY_FORWARD_DIFFERENCE)
@@ -2183,7 +2195,8 @@ __global__ void k_pos_shift(int n, const double* __restrict__ base, const double
 // FP64 forward of one set at the current positions into s.d_pred.
 static lf_status forward_one_fp64(lf_ctx* c, StationSet& s, bool grav) {
     k_face_prep_fwd<<<cdiv(c->T, 128), 128, 0, c->stream>>>(c->T, c->d_tri.p, c->d_pos.p, c->d_faceGroup.p,
-                                                            c->d_groups.p, c->fdir, c->d_fc.p);
+                                                            c->d_groups.p, c->fdir, c->d_fc.p,
+                                                            c->dropCollapsed);
     c->counters.launches++;
     return grav ? forward_set<true, false>(c, s, s.d_pred.p, nullptr) : forward_set<false, true>(c, s, nullptr, s.d_pred.p);
 }
@@ -2415,7 +2428,8 @@ extern "C" lf_status lf_unit_response(lf_ctx* c, const double* params, int kind,
                                          : forward_set_mixed<false, true>(c, s, d_g, d_t);
         } else {
             k_face_prep_fwd<<<cdiv(c->T, 128), 128, 0, c->stream>>>(c->T, c->d_tri.p, c->d_pos.p, c->d_faceGroup.p,
-                                                                    c->d_groups.p, c->fdir, c->d_fc.p);
+                                                                    c->d_groups.p, c->fdir, c->d_fc.p,
+                                                            c->dropCollapsed);
             c->counters.launches++;
             st = kind == LF_UNIT_GRAVITY ? forward_set<true, false>(c, s, d_g, d_t)
                                          : forward_set<false, true>(c, s, d_g, d_t);

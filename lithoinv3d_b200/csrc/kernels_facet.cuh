@@ -61,7 +61,7 @@ __device__ __forceinline__ void make_face_f32(const double* m, FaceF32& F) {
 
 __global__ void k_face_prep_mixed(int T, const int32_t* __restrict__ tri, const double* __restrict__ pos,
                                   const int16_t* __restrict__ face_group, const GroupConst* __restrict__ groups, d3 fdir,
-                                  double* __restrict__ mc, FaceF32* __restrict__ mf32) {
+                                  double* __restrict__ mc, FaceF32* __restrict__ mf32, int drop_collapsed) {
     int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= T) return;
     d3 v[3];
@@ -75,7 +75,7 @@ __global__ void k_face_prep_mixed(int T, const int32_t* __restrict__ tri, const 
     double area2 = norm_rn(n);
     double out[NMC];
     for (int k = 0; k < NMC; ++k) out[k] = 0.0;
-    if (!(area2 < kEps)) {
+    if (!(area2 < kEps) && !(drop_collapsed && facet_collapsed(v, area2))) {
         d3 un = div_rn(n, area2);
         const GroupConst& g = groups[face_group[f]];
         d3 m = mk3(g.mdir[0], g.mdir[1], g.mdir[2]);

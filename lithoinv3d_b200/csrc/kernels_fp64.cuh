@@ -88,6 +88,26 @@ __device__ __forceinline__ double lambda_from(double s1, double s2, double d1, d
     return log(num / den);
 }
 
+// Lambda in the symmetric form log((d1 + d2 + L) / (d1 + d2 - L)) =
+// log1p(2 L / (d1 + d2 - L)), equal to lineIntegralTerm's oriented
+// log((s2 + d2) / (s1 + d1)) (d2^2 - d1^2 = s2^2 - s1^2 along the edge's
+// line) wherever that is live.  The local-frame FP64 kernels (mixed near
+// pairs, the analytic derivatives) use it: it depends only on distances,
+// so the rounding of the frame change cannot flip a branch.  Where the
+// reference's branch returns 0 although the station lies off the segment
+// -- exactly on the edge's line, beyond its end point, which synthetic
+// station grids can hit when they share the voxel lattice (s1 + d1 is then
+// an exact 0 in the reference's global coordinates) -- this is the
+// continuous value log(d1 / d2) instead: the reference's forward is
+// discontinuous there and its own finite-difference Jacobian undefined.
+// The FP64 forward keeps lambda_from, bit for bit.  live = the station is
+// not on the segment itself (d1 + d2 > L).
+__device__ __forceinline__ double lambda_sym(double d1, double d2, double L, bool* live) {
+    const double dsum = d1 + d2, den = dsum - L;
+    *live = den > 1e-13 * dsum;
+    return *live ? log1p(2.0 * L / den) : 0.0;
+}
+
 // ------------------------------------------------------------- scatter ----
 // LithologyModel::applyParameterVector (lithology_model.cpp:210-248) step 1:
 // every global DOF writes the (vertex, axis) slots it controls.
@@ -161,13 +181,28 @@ __device__ __forceinline__ d3 cross_rn(d3 a, d3 b) {
 __device__ __forceinline__ double norm_rn(d3 a) { return __dsqrt_rn(dot_rn(a, a)); }
 __device__ __forceinline__ d3 div_rn(d3 a, double s) { return {__ddiv_rn(a.x, s), __ddiv_rn(a.y, s), __ddiv_rn(a.z, s)}; }
 
+// A facet collapsed onto a line: twice-area below 1e-10 x its longest edge
+// squared (control-point interpolation produces them).  Its unit normal is
+// rounding noise, and the reference's TMI facet term, which does not vanish
+// with the area (magnetic_forward.cpp:312-347), is then a discontinuous
+// function of the positions.  The derivative kernels always take such facets
+// as contributing zero; the forward does too when the context drops them
+// (lf_set_collapsed_facets), so that the objective is the function its
+// gradient differentiates.  No reference counterpart.
+__device__ __forceinline__ bool facet_collapsed(const d3 (&v)[3], double area2) {
+    const double l0 = norm_rn(sub_rn(v[1], v[0])), l1 = norm_rn(sub_rn(v[2], v[1])), l2 = norm_rn(sub_rn(v[0], v[2]));
+    const double lm = fmax(l0, fmax(l1, l2));
+    return area2 < 1e-10 * lm * lm;
+}
+
 // Forward constants of one facet (vertices v) in the reference's operation
-// order; out[NFC].
-__device__ __forceinline__ void face_consts_fwd(const d3 (&v)[3], const GroupConst& g, d3 fdir, double (&out)[NFC]) {
+// order; out[NFC].  drop: collapsed facets contribute nothing.
+__device__ __forceinline__ void face_consts_fwd(const d3 (&v)[3], const GroupConst& g, d3 fdir, double (&out)[NFC],
+                                                bool drop = false) {
     // faceNagyContribution / magneticFacet: n = (b-a) x (c-a), unit_n = n / |n|
     d3 n = cross_rn(sub_rn(v[1], v[0]), sub_rn(v[2], v[0]));
     double area2 = norm_rn(n);
-    bool valid = !(area2 < kEps);
+    bool valid = !(area2 < kEps) && !(drop && facet_collapsed(v, area2));
     d3 un = valid ? div_rn(n, area2) : mk3(0, 0, 0);
     d3 m = mk3(g.mdir[0], g.mdir[1], g.mdir[2]);
     out[FC_AX] = v[0].x; out[FC_AY] = v[0].y; out[FC_AZ] = v[0].z;
@@ -190,7 +225,7 @@ __device__ __forceinline__ void face_consts_fwd(const d3 (&v)[3], const GroupCon
 
 __global__ void k_face_prep_fwd(int T, const int32_t* __restrict__ tri, const double* __restrict__ pos,
                                 const int16_t* __restrict__ face_group, const GroupConst* __restrict__ groups,
-                                d3 fdir, double* __restrict__ fc) {
+                                d3 fdir, double* __restrict__ fc, int drop_collapsed) {
     int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= T) return;
     const double* pa = pos + 3 * tri[3 * f];
@@ -198,7 +233,7 @@ __global__ void k_face_prep_fwd(int T, const int32_t* __restrict__ tri, const do
     const double* pc = pos + 3 * tri[3 * f + 2];
     d3 v[3] = {mk3(pa[0], pa[1], pa[2]), mk3(pb[0], pb[1], pb[2]), mk3(pc[0], pc[1], pc[2])};
     double out[NFC];
-    face_consts_fwd(v, groups[face_group[f]], fdir, out);
+    face_consts_fwd(v, groups[face_group[f]], fdir, out, drop_collapsed != 0);
     for (int k = 0; k < NFC; ++k) fc[(size_t)k * T + f] = out[k];
 }
 
@@ -706,11 +741,9 @@ __device__ __forceinline__ void pair_gradient_fp64(const double* C, double gsn, 
     // edges: 0 a->b (e=(1,0)), 1 b->c, 2 c->a
     double e1x = C[GC_E1X], e1y = C[GC_E1Y], e2x = C[GC_E2X], e2y = C[GC_E2Y];
     bool lv0, lv1, lv2;
-    double lam0 = lambda_from(-x, L0 - x, la, lb, &lv0);
-    double s11 = rb.x * e1x + rb.y * e1y, s12 = rc.x * e1x + rc.y * e1y;
-    double lam1 = lambda_from(s11, s12, lb, lc, &lv1);
-    double s21 = rc.x * e2x + rc.y * e2y, s22 = ra.x * e2x + ra.y * e2y;
-    double lam2 = lambda_from(s21, s22, lc, la, &lv2);
+    double lam0 = lambda_sym(la, lb, L0, &lv0);
+    double lam1 = lambda_sym(lb, lc, C[GC_L1], &lv1);
+    double lam2 = lambda_sym(lc, la, C[GC_L2], &lv2);
     // d_perp_i = -r1 . perp_i, perp_i = (-ey, ex, 0)
     double dp0 = y;  // -(r_a.y * 1)
     double dp1 = rb.x * e1y - rb.y * e1x;

@@ -143,8 +143,10 @@ __device__ __forceinline__ bool far_series_ok(float ny, float den, float v0, flo
     return den > 0.f && fabsf(ny) <= 0.125f * den && fmaxf(v0, fmaxf(v1, v2)) <= 0.2f;
 }
 
-// Near pair in FP64, local frame, with the reference's lineIntegralTerm and
-// solidAngle branch semantics.  Adds gz and TMI contributions.
+// Near pair in FP64, local frame: solidAngle's branch semantics, Lambda in
+// the symmetric form (lambda_sym: the reference's value except exactly on an
+// edge's line beyond its end, where the reference's branch gives 0).  Adds
+// gz and TMI contributions.
 __device__ __forceinline__ void pair_near_f64(const double* __restrict__ s, int j, int stride, d3 o, double* gz,
                                               double* tmi) {
 #define M(k) s[(k) * stride + j]
@@ -163,10 +165,10 @@ __device__ __forceinline__ void pair_near_f64(const double* __restrict__ s, int 
         om = 2.0 * atan2(h * (L0 * cy), den);
     }
     bool live;
-    double lam0 = (L0 < kEps) ? 0.0 : lambda_from(-x, rbx, la, lb, &live);
+    double lam0 = (L0 < kEps) ? 0.0 : lambda_sym(la, lb, L0, &live);
     double e1x = M(MC_E1X), e1y = M(MC_E1Y), e2x = M(MC_E2X), e2y = M(MC_E2Y);
-    double lam1 = (M(MC_L1) < kEps) ? 0.0 : lambda_from(rbx * e1x - y * e1y, rcx * e1x + rcy * e1y, lb, lc, &live);
-    double lam2 = (M(MC_L2) < kEps) ? 0.0 : lambda_from(rcx * e2x + rcy * e2y, -x * e2x - y * e2y, lc, la, &live);
+    double lam1 = (M(MC_L1) < kEps) ? 0.0 : lambda_sym(lb, lc, M(MC_L1), &live);
+    double lam2 = (M(MC_L2) < kEps) ? 0.0 : lambda_sym(lc, la, M(MC_L2), &live);
     // d_perp_i = -(r1 . perp_i), perp_i = z x e_i = (-e_y, e_x, 0)
     double dp0 = y;
     double dp1 = rbx * e1y + y * e1x;

@@ -85,7 +85,7 @@ __global__ void __launch_bounds__(128) k_face_prep_patch(int T, const int32_t* _
                                                          const int32_t* __restrict__ edgeOff,
                                                          const int32_t* __restrict__ blobOff,
                                                          double* __restrict__ mc, float* __restrict__ mt2,
-                                                         unsigned char* __restrict__ blobs) {
+                                                         unsigned char* __restrict__ blobs, int drop_collapsed) {
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= T) return;
     d3 v[3];
@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(128) k_face_prep_patch(int T, const int32_t* _
     // reference, which matters for facets collapsed to a line)
     const d3 n = cross_rn(sub_rn(v[1], v[0]), sub_rn(v[2], v[0]));
     const double area2 = norm_rn(n);
-    const bool valid = !(area2 < kEps);
+    const bool valid = !(area2 < kEps) && !(drop_collapsed && facet_collapsed(v, area2));
     double out[NMC];
     for (int k = 0; k < NMC; ++k) out[k] = 0.0;
     double mt[3] = {0.0, 0.0, 0.0}, L[3], mfv = 0.0, sgz = 0.0;

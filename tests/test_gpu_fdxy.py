@@ -26,7 +26,7 @@ def rel(a, b):
 
 @pytest.fixture(scope="module")
 def problem():
-    p = synth.voxel_contact_model(shape=(8, 8, 6), n_side=12, cp_stride=2, freedom_interior=synth.XYZ_FREE)
+    p = synth.voxel_contact_model(shape=(8, 8, 6), n_side=16, cp_stride=2, freedom_interior=synth.XYZ_FREE)
     model = p.build_model()
     t = model.tables()
     x0 = model.assemble_parameters()
