@@ -294,13 +294,19 @@ lf_status lf_mlp_param_count(lf_mlp* m, size_t* n);
 lf_status lf_mlp_get_params(lf_mlp* m, float* host);
 lf_status lf_mlp_set_params(lf_mlp* m, const float* host);
 lf_status lf_mlp_gradients(lf_mlp* m, const float* d_x, const float* d_y, float* loss, float* host_grads);
-/* GEMM engine of the network: LF_GEMM_MMA_SYNC (default: warp-level
- * mma.sync m16n8k16 with ldmatrix, cp.async double buffering) or
- * LF_GEMM_TCGEN05 (5th-generation tensor cores: tcgen05.mma from shared-memory
- * descriptors, accumulator in tensor memory, 128 x 256 or 128 x 128 tiles).
- * Both give the same results to FP32 summation order; at the network's
- * shapes the mma.sync kernel is the faster of the two. */
-enum { LF_GEMM_TCGEN05 = 0, LF_GEMM_MMA_SYNC = 1, LF_GEMM_TCGEN05_TMA = 2 };
+/* GEMM engine of the network:
+ *  LF_GEMM_MMA_SYNC: warp-level mma.sync m16n8k16 with ldmatrix, cp.async
+ *    double buffering;
+ *  LF_GEMM_TCGEN05: 5th-generation tensor cores, tcgen05.mma from
+ *    shared-memory descriptors, accumulator in tensor memory, 128 x 256 or
+ *    128 x 128 tiles, operands staged by cp.async;
+ *  LF_GEMM_TCGEN05_TMA: the same MMA fed by TMA (2-D tensor maps, 128-byte
+ *    swizzle, no multicast) in a warp-specialised pipeline (one producer
+ *    warp, one MMA warp, every warp in the epilogue);
+ *  LF_GEMM_AUTO (default): per GEMM, LF_GEMM_TCGEN05_TMA for K >= 2048 and
+ *    LF_GEMM_MMA_SYNC below (measured faster on each side of that line).
+ * All give the same results to FP32 summation order. */
+enum { LF_GEMM_TCGEN05 = 0, LF_GEMM_MMA_SYNC = 1, LF_GEMM_TCGEN05_TMA = 2, LF_GEMM_AUTO = 3 };
 lf_status lf_mlp_set_engine(lf_mlp* m, int engine);
 /* The network's BF16 GEMM on device buffers: C[M x N] = A[M x K] . B[K x N]
  * with A stored [M][K] (a_trans = 0) or [K][M] (a_trans = 1), B stored

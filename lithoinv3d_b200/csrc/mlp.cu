@@ -72,7 +72,7 @@ struct lf_mlp {
     Buf<__nv_bfloat16> xb, dz, dh;  // input, gradient buffers (bf16)
     Buf<float> pred, loss_blocks;
     int step = 0;
-    int engine = LF_GEMM_MMA_SYNC;  // lf_mlp_set_engine (mma.sync measured faster at the network's shapes)
+    int engine = LF_GEMM_AUTO;  // lf_mlp_set_engine: per GEMM, TMA-fed tcgen05 for deep K, mma.sync otherwise
     std::string err;
 };
 
@@ -162,9 +162,18 @@ static cudaError_t gemm_tma(cudaStream_t stream, int M, int N, int K, const __nv
     return cudaPeekAtLastError();
 }
 
+// LF_GEMM_AUTO: the TMA-fed tcgen05 kernel for deep reductions, where its
+// pipeline pays (measured on B200: 24.7 against 12.2 TFLOP/s at K = 8192 on
+// the network's 256 x 512 first layer, 757 against 290 at 4096^3), the
+// mma.sync kernel for the shallow ones (81 against 52 TFLOP/s at K = 256,
+// 14.0 against 8.9 at K = 512).
+constexpr int kAutoTmaMinK = 2048;
+static int auto_engine(int K) { return K >= kAutoTmaMinK && K % kTcBK == 0 ? LF_GEMM_TCGEN05_TMA : LF_GEMM_MMA_SYNC; }
+
 template <bool A_T, bool B_T, int EPI>
 static cudaError_t gemm_on(int engine, cudaStream_t stream, int M, int N, int K, const __nv_bfloat16* A, int lda,
                            const __nv_bfloat16* B, int ldb, const float* bias, float* Cf, __nv_bfloat16* Cb, int ldc) {
+    if (engine == LF_GEMM_AUTO) engine = auto_engine(K);
     if (engine == LF_GEMM_TCGEN05_TMA) {
         if (N % 256 == 0)
             return gemm_tma<A_T, B_T, EPI, 256>(stream, M, N, K, A, lda, B, ldb, bias, Cf, Cb, ldc);
@@ -382,7 +391,7 @@ extern "C" lf_status lf_mlp_predict(lf_mlp* m, const float* d_x, int rows, float
                                      cudaMemcpyDeviceToDevice, m->stream));
     }
     MLP_TRY(m, cudaStreamSynchronize(m->stream));
-    return m->engine == LF_GEMM_TCGEN05 ? tc_check(m) : LF_OK;
+    return m->engine != LF_GEMM_MMA_SYNC ? tc_check(m) : LF_OK;
 }
 
 // Parameters in the unpadded order: for each layer W [out][in] then b [out].
@@ -470,7 +479,8 @@ extern "C" lf_status lf_set_device_wait_limit(long long polls) {
 }
 
 extern "C" lf_status lf_mlp_set_engine(lf_mlp* m, int engine) {
-    if (!m || (engine != LF_GEMM_TCGEN05 && engine != LF_GEMM_MMA_SYNC && engine != LF_GEMM_TCGEN05_TMA))
+    if (!m || (engine != LF_GEMM_TCGEN05 && engine != LF_GEMM_MMA_SYNC && engine != LF_GEMM_TCGEN05_TMA &&
+               engine != LF_GEMM_AUTO))
         return LF_EINVAL;
     m->engine = engine;
     return LF_OK;
@@ -479,6 +489,7 @@ extern "C" lf_status lf_mlp_set_engine(lf_mlp* m, int engine) {
 extern "C" lf_status lf_gemm_bf16(int engine, int a_trans, int b_trans, int epilogue, int M, int N, int K,
                                   const void* A, int lda, const void* B, int ldb, const float* bias, void* C, int ldc,
                                   void* stream) {
+    if (engine == LF_GEMM_AUTO && K > 0) engine = auto_engine(K);
     const bool tc = engine == LF_GEMM_TCGEN05 || engine == LF_GEMM_TCGEN05_TMA;
     if ((!tc && engine != LF_GEMM_MMA_SYNC) || M <= 0 || N <= 0 || K <= 0 || M % kBM ||
         N % kBN || K % (tc ? kTcBK : kBK) || !A || !B || !C ||

@@ -89,8 +89,10 @@ def rel(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
 
 
-@pytest.mark.parametrize("engine", [0, 1])  # LF_GEMM_TCGEN05, LF_GEMM_MMA_SYNC
-@pytest.mark.parametrize("n_in,width,depth,n_out", [(256, 128, 2, 70), (384, 256, 3, 200)])
+# LF_GEMM_TCGEN05, LF_GEMM_MMA_SYNC, LF_GEMM_TCGEN05_TMA, LF_GEMM_AUTO (the 2048-input case puts the
+# first layer's reduction on the TMA kernel under AUTO)
+@pytest.mark.parametrize("engine", [0, 1, 2, 3])
+@pytest.mark.parametrize("n_in,width,depth,n_out", [(256, 128, 2, 70), (384, 256, 3, 200), (2048, 128, 2, 70)])
 def test_mlp_gradients_match_cpu(n_in, width, depth, n_out, engine):
     batch = 128
     net = Net(n_in, width, depth, n_out, batch, seed=3)
