@@ -134,6 +134,8 @@ def parse():
                     help="x/y vertex derivatives of the gradient: closed form, or per-facet forward differences "
                          "with --xy-step (the large-inversion configuration's h = 0.5 m)")
     ap.add_argument("--xy-step", type=float, default=0.5)
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the context's default launch shapes (short profiling runs)")
     ap.add_argument("--drop-collapsed", action="store_true",
                     help="facets collapsed onto a line contribute nothing to the forward either (their reference "
                          "TMI term is rounding noise and discontinuous)")
@@ -512,7 +514,7 @@ def main():
 
         ctx.set_xy_derivative(XY_FORWARD_DIFFERENCE, args.xy_step)
     ctx.set_graph_mode(True)
-    tuned, _ = ctx.autotune(x0, repeats=3)
+    tuned = ctx.tuning() if args.no_autotune else ctx.autotune(x0, repeats=3)[0]
     np_ = model.n_dofs
     dev = torch.device("cuda", local)
     stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
