@@ -32,7 +32,7 @@ from typing import Optional
 import numpy as np
 
 from . import _native
-from .api import GATHER_CHAIN, PREC_MIXED
+from .api import COLLAPSED_DROP, GATHER_CHAIN, PREC_MIXED
 
 
 class Network:
@@ -151,6 +151,7 @@ class Family:
         self.ctx = problem.make_context(self.model, device=device)
         self.ctx.set_precision(PREC_MIXED)
         self.ctx.set_scatter_stateless(True)  # data that depend on the true model alone
+        self.ctx.set_collapsed_facets(COLLAPSED_DROP)  # the forward the inversions fit
         self.g0, self.m0 = self.ctx.forward(self.x0)
         self.sg = float(np.sqrt(np.mean(self.g0 ** 2)))
         self.sm = float(np.sqrt(np.mean(self.m0 ** 2)))
@@ -204,9 +205,10 @@ def invert(fam: Family, gobs, mobs, gstd, mstd, net: Optional[Network] = None, m
     secant pair (x_k - x0, g(x_k) - g(x0)) at the cost of two gradient
     evaluations; on the c5 family that cost more than it saved (mean wall
     time 1.51x vs 1.62x over plain), so it is off by default.  With `chain`
-    (default) both runs use the chain gather and the stateless scatter: on
-    control-point models the reference's DOF-vertex gather is not the
-    objective's gradient and L-BFGS-B stalls before chi^2 = N.  Returns wall seconds
+    (default) both runs use the chain gather, the stateless scatter and drop
+    collapsed facets: on control-point models the reference's DOF-vertex
+    gather is not the objective's gradient and L-BFGS-B stalls before
+    chi^2 = N.  Returns wall seconds
     (proposals included), objective(+gradient) and forward evaluations, final
     objective, whether the target was reached and whether a proposal was
     taken."""
@@ -218,6 +220,7 @@ def invert(fam: Family, gobs, mobs, gstd, mstd, net: Optional[Network] = None, m
     if chain:  # the objective's own gradient through the control-point interpolation (lf_set_gradient_gather)
         ctx.set_scatter_stateless(True)
         ctx.set_gradient_gather(GATHER_CHAIN)
+        ctx.set_collapsed_facets(COLLAPSED_DROP)  # the objective then has no rounding-noise jumps
     ctx.set_graph_mode(True)
     target = 0.5 * (len(gobs) + len(mobs))  # chi^2 = N  <=>  0.5 sum (r / sigma)^2 = N / 2
     ctx.objective_and_gradient(fam.x0)  # capture the graphs and size the buffers outside the timed region
