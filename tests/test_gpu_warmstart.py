@@ -31,7 +31,10 @@ def test_warm_start_on_config2_family_beats_plain_wall_time():
     training size: the learned start must reach chi^2 = N in less mean wall
     time than plain L-BFGS-B over the held-out models."""
     p = synth.voxel_contact_model()
-    out = experiment(p, n_pairs=6144, n_heldout=8, epochs=30, seed=0, width=512, depth=4, batch=256)
+    out = experiment(p, n_pairs=6144, n_heldout=16, epochs=30, seed=0, width=512, depth=4, batch=256)
     assert out["loss_last"] < 0.5 * out["loss_first"]
-    assert out["learned"]["reached"] >= out["plain"]["reached"]
+    # chi^2 = N lies inside the noise of a few held-out models (both starts end
+    # within a few per cent of it): one such model may fall either way
+    assert out["learned"]["reached"] >= out["plain"]["reached"] - 1
+    assert out["speedup_per_model_geomean"] > 1.5, out["speedup_per_model_geomean"]
     assert out["learned"]["mean_wall_s"] < out["plain"]["mean_wall_s"], (out["learned"], out["plain"])
