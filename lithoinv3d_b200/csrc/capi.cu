@@ -223,9 +223,9 @@ struct lf_ctx {
     uint64_t epoch = 0;
     GraphSet gObjGrad, gObj, gCons;
 
-    // launch shapes chosen by lf_autotune (defaults: measured on the
-    // 19k-facet, 4096-station contact model)
-    lf_tuning tune{148 * 4, 148 * 64, 0, 128, 3.0, LF_FWD_FACET};
+    // launch shapes chosen by lf_autotune (defaults: the autotuner's choice
+    // on the 19k-facet, 4096-station contact model)
+    lf_tuning tune{148 * 128, 148 * 32, 0, 128, 3.0, LF_FWD_FACET};
 
     // Batched bodies (lf_set_station_groups): each group is one body and
     // sees only its own station range [grpStaOff[g], grpStaOff[g+1]) of both
