@@ -1048,6 +1048,7 @@ extern "C" lf_status lf_set_precision(lf_ctx* c, int mode) {
 // --------------------------------------------------------------- internals --
 static constexpr int kFwdThreads = 128;
 static constexpr int kFwdFacetTile = 32;
+static constexpr int kFacetStage = 32;  // facet records per shared-memory stage of k_forward_mixed
 static constexpr int kGradThreads = 32;             // Jacobian rows: one warp of facets per CTA
 static constexpr int kGradWarpsPerBlock = 4;        // objective gradient: one warp per facet
 
@@ -1215,7 +1216,7 @@ static lf_status forward_set_items(lf_ctx* c, const StationSet& s, double* d_gz,
         const int grid = std::min(c->nItems, fwd_blocks(c));
         int slot = prof_begin(c, c->evFwd, c->nFwd);
         if (MIXED)
-            k_forward_mixed_items<GZ, TMI, kFwdFacetTile><<<grid, kFwdThreads, 0, c->stream>>>(
+            k_forward_mixed_items<GZ, TMI, kFacetStage><<<grid, kFwdThreads, 0, c->stream>>>(
                 c->d_items.p, c->nItems, s.d_xyz.p, c->T, c->d_mc.p, c->d_mf32.p, c->tau, GZ ? c->d_partG.p : nullptr,
                 TMI ? c->d_partM.p : nullptr, c->d_nearPairs.p);
         else
@@ -1488,7 +1489,7 @@ static lf_status forward_set_facet(lf_ctx* c, const StationSet& s, double* d_gz,
     if (nch > 0) {
         dim3 grid(cdiv(S, kFwdThreads), nch);
         int slot = prof_begin(c, c->evFwd, c->nFwd);
-        k_forward_mixed<GZ, TMI, kFwdFacetTile><<<grid, kFwdThreads, 0, c->stream>>>(
+        k_forward_mixed<GZ, TMI, kFacetStage><<<grid, kFwdThreads, 0, c->stream>>>(
             S, s.d_xyz.p, c->T, c->d_mc.p, c->d_mf32.p, c->d_chunkBegin.p, c->d_chunkEnd.p, c->tau,
             GZ ? c->d_partG.p : nullptr, TMI ? c->d_partM.p : nullptr, c->d_nearPairs.p);
         prof_end(c, c->evFwd, slot);

@@ -236,7 +236,7 @@ __device__ __forceinline__ void forward_mixed_block(FaceF32* __restrict__ smf, d
                                                     int fb, int fe, float tau,
                                                     double* __restrict__ out_gz, double* __restrict__ out_tmi,
                                                     unsigned long long* __restrict__ near_pairs) {
-    static_assert(FT == 32, "one facet per lane in the near/far test");
+    static_assert(FT % 32 == 0, "one facet per lane in each 32-facet half of the near/far test");
     const int lane = threadIdx.x & 31;
     double ox = 0.0, oy = 0.0, oz = 0.0;
     if (act) { ox = sta[3 * s]; oy = sta[3 * s + 1]; oz = sta[3 * s + 2]; }
@@ -258,56 +258,59 @@ __device__ __forceinline__ void forward_mixed_block(FaceF32* __restrict__ smf, d
             for (int idx = threadIdx.x; idx < nf * kFaceF32Vec; idx += blockDim.x) dst[idx] = __ldg(src + idx);
         }
         __syncthreads();
-        // lane j: facet j of the stage against this warp's box
-        bool valid = false, vfar = false, far = false, mid = false;
-        if (lane < nf && !(smf[lane].size < 0.f)) {
-            valid = true;
-            const float cxw = smf[lane].cenx, cyw = smf[lane].ceny, czw = smf[lane].cenz;
-            const float ddx = fmaxf(0.f, fmaxf(bb[0] - cxw, cxw + bb[3]));
-            const float ddy = fmaxf(0.f, fmaxf(bb[1] - cyw, cyw + bb[4]));
-            const float ddz = fmaxf(0.f, fmaxf(bb[2] - czw, czw + bb[5]));
-            const float d2 = ddx * ddx + ddy * ddy + ddz * ddz;
-            const float lim = tau * smf[lane].size, limMid = 0.5f * lim;
-            vfar = d2 >= 16.f * (lim * lim);
-            far = !vfar && d2 >= lim * lim;
-            mid = !vfar && !far && d2 >= limMid * limMid;
-        }
-        const unsigned vfarMask = __ballot_sync(0xffffffffu, valid && vfar);
-        const unsigned farMask = __ballot_sync(0xffffffffu, valid && far);
-        const unsigned midMask = __ballot_sync(0xffffffffu, valid && mid);
-        const unsigned nearMask = __ballot_sync(0xffffffffu, valid && !vfar && !far && !mid);
-        if (act) {
-            float gacc = 0.f, tacc = 0.f;
-            for (unsigned m = vfarMask; m; m &= m - 1) {
-                const int j = __ffs(m) - 1;
-                pair_far_f32<RULE_TRI3>(&smf[j], ox, oy, oz, &gacc, &tacc);
+        for (int h0 = 0; h0 < nf; h0 += 32) {
+            const FaceF32* __restrict__ sh = smf + h0;
+            // lane j: facet h0 + j of the stage against this warp's box
+            bool valid = false, vfar = false, far = false, mid = false;
+            if (h0 + lane < nf && !(sh[lane].size < 0.f)) {
+                valid = true;
+                const float cxw = sh[lane].cenx, cyw = sh[lane].ceny, czw = sh[lane].cenz;
+                const float ddx = fmaxf(0.f, fmaxf(bb[0] - cxw, cxw + bb[3]));
+                const float ddy = fmaxf(0.f, fmaxf(bb[1] - cyw, cyw + bb[4]));
+                const float ddz = fmaxf(0.f, fmaxf(bb[2] - czw, czw + bb[5]));
+                const float d2 = ddx * ddx + ddy * ddy + ddz * ddz;
+                const float lim = tau * sh[lane].size, limMid = 0.5f * lim;
+                vfar = d2 >= 16.f * (lim * lim);
+                far = !vfar && d2 >= lim * lim;
+                mid = !vfar && !far && d2 >= limMid * limMid;
             }
-            for (unsigned m = farMask; m; m &= m - 1) {
-                const int j = __ffs(m) - 1;
-                pair_far_f32<RULE_DUN6>(&smf[j], ox, oy, oz, &gacc, &tacc);
-            }
-            for (unsigned m = midMask; m; m &= m - 1) {
-                const int j = __ffs(m) - 1;
-                pair_far_f32<RULE_MID28>(&smf[j], ox, oy, oz, &gacc, &tacc);
-            }
-            if (GZ) gz += gacc;
-            if (TMI) tmi += tacc;
-            nearCount += __popc(nearMask);
-        }
-        // Near facets (a few per cent of pairs): the warp copies the facet's
-        // FP64 constants from HBM into its own slot of shared memory (lane k
-        // loads constant k), then every lane reads them from there.
-        double* slot = smn + (threadIdx.x >> 5) * NMC;
-        for (unsigned m = nearMask; m; m &= m - 1) {
-            const int j = __ffs(m) - 1;
-            __syncwarp();
-            if (lane < NMC) slot[lane] = __ldg(mc + (size_t)lane * T + f0 + j);
-            __syncwarp();
+            const unsigned vfarMask = __ballot_sync(0xffffffffu, valid && vfar);
+            const unsigned farMask = __ballot_sync(0xffffffffu, valid && far);
+            const unsigned midMask = __ballot_sync(0xffffffffu, valid && mid);
+            const unsigned nearMask = __ballot_sync(0xffffffffu, valid && !vfar && !far && !mid);
             if (act) {
-                double g1 = 0.0, t1 = 0.0;
-                pair_near_f64(slot, 0, 1, mk3(ox, oy, oz), &g1, &t1);
-                if (GZ) gz += g1;
-                if (TMI) tmi += t1;
+                float gacc = 0.f, tacc = 0.f;
+                for (unsigned m = vfarMask; m; m &= m - 1) {
+                    const int j = __ffs(m) - 1;
+                    pair_far_f32<RULE_TRI3>(&sh[j], ox, oy, oz, &gacc, &tacc);
+                }
+                for (unsigned m = farMask; m; m &= m - 1) {
+                    const int j = __ffs(m) - 1;
+                    pair_far_f32<RULE_DUN6>(&sh[j], ox, oy, oz, &gacc, &tacc);
+                }
+                for (unsigned m = midMask; m; m &= m - 1) {
+                    const int j = __ffs(m) - 1;
+                    pair_far_f32<RULE_MID28>(&sh[j], ox, oy, oz, &gacc, &tacc);
+                }
+                if (GZ) gz += gacc;
+                if (TMI) tmi += tacc;
+                nearCount += __popc(nearMask);
+            }
+            // Near facets (a few per cent of pairs): the warp copies the
+            // facet's FP64 constants from HBM into its own slot of shared
+            // memory (lane k loads constant k), then every lane reads them.
+            double* slot = smn + (threadIdx.x >> 5) * NMC;
+            for (unsigned m = nearMask; m; m &= m - 1) {
+                const int j = __ffs(m) - 1;
+                __syncwarp();
+                if (lane < NMC) slot[lane] = __ldg(mc + (size_t)lane * T + f0 + h0 + j);
+                __syncwarp();
+                if (act) {
+                    double g1 = 0.0, t1 = 0.0;
+                    pair_near_f64(slot, 0, 1, mk3(ox, oy, oz), &g1, &t1);
+                    if (GZ) gz += g1;
+                    if (TMI) tmi += t1;
+                }
             }
         }
     }
