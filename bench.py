@@ -75,7 +75,7 @@ SFU_GRAD_PAIR = 13
 # dram__bytes_write.sum): the facet records (208 bytes each, ~4 MB) or the
 # patch blobs (~5 MB) and the stations come from DRAM once and from L2 for
 # every further station block; the partial sums stay in L2.
-FORWARD_DRAM_BYTES_PER_LAUNCH = {"k_forward_mixed": 7.024e6, "k_forward_patch": 9.605e6}
+FORWARD_DRAM_BYTES_PER_LAUNCH = {"k_forward_mixed": 7.108e6, "k_forward_patch": 9.605e6}
 # Nominal B200 CUDA-core rates at the 1.965 GHz boost clock (no measured
 # figure for these pipes exists in MEASURED_PEAKS.json): FP32 148 SMs x 128
 # lanes x 2 flop; special-function unit 148 x 16 ops; FP64 148 x 64 x 2 flop.
