@@ -72,10 +72,10 @@ SFU_FWD_PAIR = 10   # 3 sqrt + 3 div + 3 log + 1 atan2, one special-function op 
 SFU_GRAD_PAIR = 13
 # DRAM bytes (read + write) of one mixed-precision forward launch on this
 # workload, per engine, from ncu captures (dram__bytes_read.sum +
-# dram__bytes_write.sum): the facet records (208 bytes each, ~4 MB) or the
+# dram__bytes_write.sum): the facet records (224 bytes each, ~4.3 MB) or the
 # patch blobs (~5 MB) and the stations come from DRAM once and from L2 for
 # every further station block; the partial sums stay in L2.
-FORWARD_DRAM_BYTES_PER_LAUNCH = {"k_forward_mixed": 7.108e6, "k_forward_patch": 9.605e6}
+FORWARD_DRAM_BYTES_PER_LAUNCH = {"k_forward_mixed": 7.412e6, "k_forward_patch": 9.605e6}
 # Nominal B200 CUDA-core rates at the 1.965 GHz boost clock (no measured
 # figure for these pipes exists in MEASURED_PEAKS.json): FP32 148 SMs x 128
 # lanes x 2 flop; special-function unit 148 x 16 ops; FP64 148 x 64 x 2 flop.

@@ -231,8 +231,8 @@ lf_status lf_forward(lf_ctx* ctx, const double* params, double* gz, double* tmi)
  *                        edge integrals once per station and patch, shared by
  *                        the patch's facets); lf_autotune times both
  *  far_ratio             mixed precision: facet-distance / facet-size ratio tau
- *                        beyond which a pair is FP32 far field (FP32 28-point
- *                        mid field from tau/2, FP64 nearer); the same value as
+ *                        beyond which a pair is FP32 far field (FP32 mid field
+ *                        from tau/2, FP64 nearer); the same value as
  *                        lf_set_far_field_ratio.  lf_autotune tries
  *                        {2, 2.5, 3, 4} and accepts a ratio only if the mixed
  *                        gz and TMI stay within 0.3e-6 (norm-wise relative) of

@@ -12,10 +12,11 @@ namespace litho_b200 {
 
 // FP32 facet record of the far-field forward, written once per evaluation by
 // k_face_prep_mixed (array [T] in HBM), copied 32 facets at a time into
-// shared memory and read there with 128-bit loads (10 per far pair, 9 beyond
-// 4 tau).  The origin and the unit normal stay FP64: the height above the
-// facet plane can be tiny next to |o - a| (a far top facet seen from 1 m
-// above it).  The last row feeds the per-warp near/far test.
+// shared memory and read there with 128-bit loads (10 per far pair, 9 per
+// very far or mid pair).  The origin and the unit normal stay FP64: the
+// height above the facet plane can be tiny next to |o - a| (a far top facet
+// seen from 1 m above it).  Row 12 feeds the per-warp near/far test, row 13
+// the mid field's analytic gz.
 struct __align__(16) FaceF32 {
     float rx0, rx1, rx2, L0;   // local x axis, |ab|
     float ry0, ry1, ry2, cx;   // local y axis, c.x
@@ -26,8 +27,10 @@ struct __align__(16) FaceF32 {
     double ax, ay, az, zx, zy, zz;
     float cenx, ceny, cenz;    // centroid
     float size;                // longest edge; -1 for a facet that contributes nothing
+    float l2sq, l2l0sq, cxl0;  // |ca|^2, |ca|^2 - |ab|^2, c.x - |ab|
+    float g2;                  // 2 n_z * gz scale (0: no gz term)
 };
-static_assert(sizeof(FaceF32) == 208, "FaceF32 layout");
+static_assert(sizeof(FaceF32) == 224, "FaceF32 layout");
 constexpr int kFaceF32Vec = sizeof(FaceF32) / 16;  // float4 per record
 
 // The far-field record of one facet from its mixed constants m[NMC].
@@ -56,6 +59,10 @@ __device__ __forceinline__ void make_face_f32(const double* m, FaceF32& F) {
     F.zx = M(MC_ZX); F.zy = M(MC_ZY); F.zz = M(MC_ZZ);
     F.cenx = (float)M(MC_CENX); F.ceny = (float)M(MC_CENY); F.cenz = (float)M(MC_CENZ);
     F.size = M(MC_VALID) != 0.0 ? (float)M(MC_SIZE) : -1.f;
+    F.l2sq = (float)(M(MC_L2) * M(MC_L2));
+    F.l2l0sq = (float)(M(MC_L2) * M(MC_L2) - M(MC_L0) * M(MC_L0));
+    F.cxl0 = (float)(M(MC_CX) - M(MC_L0));
+    F.g2 = (float)(2.0 * M(MC_SGZ));
 #undef M
 }
 
@@ -133,12 +140,55 @@ __global__ void k_face_prep_mixed(int T, const int32_t* __restrict__ tri, const 
 }
 
 
-enum { RULE_TRI3 = 0, RULE_DUN6 = 1, RULE_MID28 = 2 };
+enum { RULE_TRI3 = 0, RULE_DUN6 = 1, RULE_MID = 2 };
 
-// Far pair: gz by quadrature (RULE_TRI3 beyond 4 tau, RULE_DUN6 beyond tau,
-// RULE_MID28: Radon's rule on the midpoint subdivision beyond tau/2), TMI
-// analytic, both FP32; o = station (FP64).
-template <int RULE>
+// atanh(v) / v - 1 = v^2/3 + v^4/5 + ... for 0 <= v <= 0.2 (Abramowitz &
+// Stegun 4.1.28 through v^10; the first omitted term is below 2e-9 of the sum).
+__device__ __forceinline__ float atanh_q(float v) {
+    const float v2 = v * v;
+    return v2 * fmaf(v2, fmaf(v2, fmaf(v2, 1.f / 9.f, 1.f / 7.f), 1.f / 5.f), 1.f / 3.f);
+}
+
+// Q(e) = atanh(e) / e - 1 for 0 < e < 1, without the cancellation of
+// "atanh(e) / e - 1" in FP32.  With c = sqrt(1 - e^2) and w = e / (1 + c) =
+// tanh(atanh(e) / 2) (the half-argument formula),
+//   atanh(e) / e = 2 atanh(w) / e = (2 / (1 + c)) (1 + Q(w)),
+// and, as 1 - c = e^2 / (1 + c),  Q(e) = w^2 + (2 / (1 + c)) Q(w): every term
+// is positive.  Each step halves atanh(e); atanh_q takes over at 0.2, which
+// four steps reach for e below 0.997 -- closer to 1 the log form has no
+// cancellation left to fear.
+__device__ __forceinline__ float atanh_q_any(float e) {
+    if (!(e > 0.2f)) return atanh_q(e);
+    float q = 0.f, m = 1.f, v = e;
+#pragma unroll 1
+    for (int it = 0; it < 4 && v > 0.2f && v < 1.f; ++it) {
+        const float r = __fdividef(1.f, 1.f + sqrt_pos((1.f - v) * (1.f + v)));
+        v *= r;
+        q = fmaf(m, v * v, q);
+        m *= 2.f * r;
+    }
+    if (v <= 0.2f) return fmaf(m, atanh_q(v), q);
+    return __fdividef(0.5f * log1pf(__fdividef(2.f * e, 1.f - e)), e) - 1.f;
+}
+
+// Far pair, both FP32, o = station (FP64): TMI analytic; gz by quadrature
+// (RULE_TRI3 beyond 4 tau, RULE_DUN6 beyond tau) or analytically (RULE_MID,
+// the mid field tau/2 <= distance / size < tau).  SHORT (RULE_TRI3 with
+// tau >= 3, so beyond 12 x size): shorter series, no range test.
+//
+// The mid field's gz: the integral of 1/r over the facet is
+//   I = sum_i u_i Lambda_i + z Omega
+// (u_i: distance from the station's projection to edge i's line, positive
+// inside; Gauss-Green in the facet plane, the same identity as the FP64
+// pair's gz).  In FP32 the sum cancels by about distance / size, so it is
+// regrouped around sbar = (s0 + s1 + s2) / 3, s_i = the sum of edge i's two
+// vertex distances, using sum_i u_i L_i = 2A:
+//   I / 2 = 2A / sbar + sum_i (u_i L_i / s_i) (Q_i + (sbar - s_i) / sbar),
+// Q_i = atanh(e_i) / e_i - 1, e_i = L_i / s_i; sbar - s_i comes from the
+// distance differences l_c - l_a = (l_c^2 - l_a^2) / (l_c + l_a), whose
+// numerators are linear in the station.  Every term is then of the size of
+// I itself.
+template <int RULE, bool SHORT = false>
 __device__ __forceinline__ void pair_far_f32(const FaceF32* Fp, double ox, double oy, double oz, float* gz,
                                              float* tmi) {
     const float4* v = reinterpret_cast<const float4*>(Fp);
@@ -158,36 +208,31 @@ __device__ __forceinline__ void pair_far_f32(const FaceF32* Fp, double ox, doubl
     // zero, as in the reference's n_z * (...) product; its quadrature is
     // skipped.  The facet is the same for every lane, so the branch is
     // warp-uniform.
-    float acc = 0.f;
-    if (gq == 0.f) {
-    } else if (RULE == RULE_MID28) {
+    if (RULE != RULE_MID) {
+        float acc = 0.f;
+        if (gq == 0.f) {
+        } else if (RULE == RULE_DUN6) {
+            const float4 qa = v[4], qb = v[5], qc = v[6];
+            const float q[12] = {qa.x, qa.y, qa.z, qa.w, qb.x, qb.y, qb.z, qb.w, qc.x, qc.y, qc.z, qc.w};
 #pragma unroll
-        for (int q = 0; q < 28; ++q) {
-            float px = fmaf(kRadon4Bb[q], L0, fmaf(kRadon4Bc[q], cx, -x)), py = fmaf(kRadon4Bc[q], cy, -y);
-            acc = fmaf(kRadonW[q % 7], rsqrtf(fmaf(px, px, fmaf(py, py, z2))), acc);
-        }
-        acc *= 0.25f;
-    } else if (RULE == RULE_DUN6) {
-        const float4 qa = v[4], qb = v[5], qc = v[6];
-        const float q[12] = {qa.x, qa.y, qa.z, qa.w, qb.x, qb.y, qb.z, qb.w, qc.x, qc.y, qc.z, qc.w};
+            for (int k = 0; k < 6; ++k) {
+                float px = q[2 * k] - x, py = q[2 * k + 1] - y;
+                acc = fmaf(kDun6W[k], rsqrtf(fmaf(px, px, fmaf(py, py, z2))), acc);
+            }
+        } else {
+            const float4 qa = v[7], qb = v[8];
+            const float q[6] = {qa.x, qa.y, qa.z, qa.w, qb.x, qb.y};
 #pragma unroll
-        for (int k = 0; k < 6; ++k) {
-            float px = q[2 * k] - x, py = q[2 * k + 1] - y;
-            acc = fmaf(kDun6W[k], rsqrtf(fmaf(px, px, fmaf(py, py, z2))), acc);
+            for (int k = 0; k < 3; ++k) {
+                float px = q[2 * k] - x, py = q[2 * k + 1] - y;
+                acc += rsqrtf(fmaf(px, px, fmaf(py, py, z2)));
+            }
+            acc *= (1.f / 3.f);
         }
-    } else {
-        const float4 qa = v[7], qb = v[8];
-        const float q[6] = {qa.x, qa.y, qa.z, qa.w, qb.x, qb.y};
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            float px = q[2 * k] - x, py = q[2 * k + 1] - y;
-            acc += rsqrtf(fmaf(px, px, fmaf(py, py, z2)));
-        }
-        acc *= (1.f / 3.f);
+        if (gq != 0.f) *gz += gq * acc;
     }
-    if (gq != 0.f) *gz += gq * acc;
     // TMI: MF * Omega + sum_i MT_i Lambda_i with Omega = 2 atan2(ny, den) and
-    // Lambda_i = 2 atanh(v_i); the record holds 2 MF and 2 MT_i, so the terms
+    // Lambda_i = 2 atanh(e_i); the record holds 2 MF and 2 MT_i, so the terms
     // below are atan2 and atanh.  Scaling by 2 is exact: the bits equal
     // MF * (2 atan2) + MT_i * (2 atanh).
     float rbx = L0 - x, rcx = cx - x, rcy = cy - y;
@@ -198,19 +243,67 @@ __device__ __forceinline__ void pair_far_f32(const FaceF32* Fp, double ox, doubl
     float dac = fmaf(-x, rcx, fmaf(-y, rcy, z2));
     float dbc = fmaf(rbx, rcx, fmaf(-y, rcy, z2));
     float den = la * lb * lc + dab * lc + dac * lb + dbc * la;
-    const float ny = -z * (L0 * cy);
-    const float e0 = __fdividef(L0, la + lb), e1 = __fdividef(L1, lb + lc), e2 = __fdividef(L2, lc + la);
+    const float l0cy = L0 * cy;
+    const float ny = -z * l0cy;
     float om, l0, l1, l2;
-    if (far_series_ok(ny, den, e0, e1, e2)) {
-        om = atan_series(__fdividef(ny, den));
-        l0 = atanh_series(e0);
-        l1 = atanh_series(e1);
-        l2 = atanh_series(e2);
+    if (RULE == RULE_MID) {
+        const float s0 = la + lb;
+        const float r0 = __fdividef(1.f, s0), r1 = __fdividef(1.f, lb + lc), r2 = __fdividef(1.f, lc + la);
+        const float e0 = L0 * r0, e1 = L1 * r1, e2 = L2 * r2;
+        float q0, q1, q2;
+        if (far_series_ok(ny, den, e0, e1, e2)) {
+            om = atan_series(__fdividef(ny, den));
+            q0 = atanh_q(e0);
+            q1 = atanh_q(e1);
+            q2 = atanh_q(e2);
+        } else {
+            om = atan2_far(ny, den);
+            q0 = atanh_q_any(e0);
+            q1 = atanh_q_any(e1);
+            q2 = atanh_q_any(e2);
+        }
+        l0 = fmaf(e0, q0, e0);
+        l1 = fmaf(e1, q1, e1);
+        l2 = fmaf(e2, q2, e2);
+        const float4 v13 = v[13];  // |ca|^2, |ca|^2 - |ab|^2, c.x - |ab|, 2 n_z gscale
+        if (v13.w != 0.f) {
+            const float k = __fdividef(0.5f, s0 + lc);  // 1 / (3 sbar)
+            const float tx = x + x, ty = y + y;
+            const float dba = L0 * (L0 - tx) * r0;                          // l_b - l_a
+            const float dca = fmaf(-cx, tx, fmaf(-cy, ty, v13.x)) * r2;     // l_c - l_a
+            const float dcb = fmaf(-v13.z, tx, fmaf(-cy, ty, v13.y)) * r1;  // l_c - l_b
+            // u_i L_i / s_i for the edges ab (u = y), bc and ca
+            const float w0 = y * L0 * r0, w1 = fmaf(rbx, cy, y * v13.z) * r1, w2 = fmaf(x, cy, -y * cx) * r2;
+            float h = w0 * (q0 + (dca + dcb) * k);
+            h = fmaf(w1, q1 - (dba + dca) * k, h);
+            h = fmaf(w2, q2 + (dba - dcb) * k, h);
+            h = fmaf(3.f * l0cy, k, h);  // 2A / sbar
+            h = fmaf(z, om, h);          // I / 2
+            *gz += v13.w * h;
+        }
     } else {
-        om = atan2_far(ny, den);
-        l0 = 0.5f * lam_f32(la, lb, L0);
-        l1 = 0.5f * lam_f32(lb, lc, L1);
-        l2 = 0.5f * lam_f32(lc, la, L2);
+        const float e0 = __fdividef(L0, la + lb), e1 = __fdividef(L1, lb + lc), e2 = __fdividef(L2, lc + la);
+        if (SHORT) {
+            // Beyond 12 x size every vertex lies beyond 11.3 x size, so
+            // e_i < 0.045 (the series through e^5 leaves 1e-9 of the sum) and
+            // the solid angle is below 0.0035 (|t| < 0.002: through t^3 leaves
+            // 1e-12); den > 0 and the range test holds there.
+            const float t = __fdividef(ny, den);
+            om = t * fmaf(t * t, -1.f / 3.f, 1.f);
+            l0 = e0 * fmaf(e0 * e0, fmaf(e0 * e0, 0.2f, 1.f / 3.f), 1.f);
+            l1 = e1 * fmaf(e1 * e1, fmaf(e1 * e1, 0.2f, 1.f / 3.f), 1.f);
+            l2 = e2 * fmaf(e2 * e2, fmaf(e2 * e2, 0.2f, 1.f / 3.f), 1.f);
+        } else if (far_series_ok(ny, den, e0, e1, e2)) {
+            om = atan_series(__fdividef(ny, den));
+            l0 = atanh_series(e0);
+            l1 = atanh_series(e1);
+            l2 = atanh_series(e2);
+        } else {
+            om = atan2_far(ny, den);
+            l0 = 0.5f * lam_f32(la, lb, L0);
+            l1 = 0.5f * lam_f32(lb, lc, L1);
+            l2 = 0.5f * lam_f32(lc, la, L2);
+        }
     }
     *tmi += v3.x * om + v3.y * l0 + v3.z * l1 + v3.w * l2;
 }
@@ -225,7 +318,7 @@ __device__ __forceinline__ void pair_far_f32(const FaceF32* Fp, double ox, doubl
 // is decided per (warp, facet): lane j tests facet j of the stage against the
 // warp's station bounding box -- centroid at least 4 tau x size away: very
 // far (FP32, 3-point gz); at least tau x size: far (FP32, 6-point gz); at
-// least tau/2 x size: mid (FP32, 28-point gz); else near (FP64 analytic) --
+// least tau/2 x size: mid (FP32, analytic gz); else near (FP64 analytic) --
 // and the warp walks each class warp-uniformly.
 // One CTA's work: station s (this thread; act = s is a station of the
 // block) against facets [fb, fe); out_gz[s] / out_tmi[s] receive the sums.
@@ -280,9 +373,16 @@ __device__ __forceinline__ void forward_mixed_block(FaceF32* __restrict__ smf, d
             const unsigned nearMask = __ballot_sync(0xffffffffu, valid && !vfar && !far && !mid);
             if (act) {
                 float gacc = 0.f, tacc = 0.f;
-                for (unsigned m = vfarMask; m; m &= m - 1) {
-                    const int j = __ffs(m) - 1;
-                    pair_far_f32<RULE_TRI3>(&sh[j], ox, oy, oz, &gacc, &tacc);
+                if (tau >= 3.f) {
+                    for (unsigned m = vfarMask; m; m &= m - 1) {
+                        const int j = __ffs(m) - 1;
+                        pair_far_f32<RULE_TRI3, true>(&sh[j], ox, oy, oz, &gacc, &tacc);
+                    }
+                } else {
+                    for (unsigned m = vfarMask; m; m &= m - 1) {
+                        const int j = __ffs(m) - 1;
+                        pair_far_f32<RULE_TRI3>(&sh[j], ox, oy, oz, &gacc, &tacc);
+                    }
                 }
                 for (unsigned m = farMask; m; m &= m - 1) {
                     const int j = __ffs(m) - 1;
@@ -290,7 +390,7 @@ __device__ __forceinline__ void forward_mixed_block(FaceF32* __restrict__ smf, d
                 }
                 for (unsigned m = midMask; m; m &= m - 1) {
                     const int j = __ffs(m) - 1;
-                    pair_far_f32<RULE_MID28>(&sh[j], ox, oy, oz, &gacc, &tacc);
+                    pair_far_f32<RULE_MID>(&sh[j], ox, oy, oz, &gacc, &tacc);
                 }
                 if (GZ) gz += gacc;
                 if (TMI) tmi += tacc;
