@@ -149,6 +149,11 @@ __device__ __forceinline__ float atanh_q(float v) {
     return v2 * fmaf(v2, fmaf(v2, fmaf(v2, 1.f / 9.f, 1.f / 7.f), 1.f / 5.f), 1.f / 3.f);
 }
 
+// (atanh(v) / v - 1) / v^2 = 1/3 + v^2/5 + ... + v^8/11, in v2 = v^2.
+__device__ __forceinline__ float atanh_q11(float v2) {
+    return fmaf(v2, fmaf(v2, fmaf(v2, fmaf(v2, 1.f / 11.f, 1.f / 9.f), 1.f / 7.f), 1.f / 5.f), 1.f / 3.f);
+}
+
 // Q(e) = atanh(e) / e - 1 for 0 < e < 1, without the cancellation of
 // "atanh(e) / e - 1" in FP32.  With c = sqrt(1 - e^2) and w = e / (1 + c) =
 // tanh(atanh(e) / 2) (the half-argument formula),
@@ -173,8 +178,9 @@ __device__ __forceinline__ float atanh_q_any(float e) {
 
 // Far pair, both FP32, o = station (FP64): TMI analytic; gz by quadrature
 // (RULE_TRI3 beyond 4 tau, RULE_DUN6 beyond tau) or analytically (RULE_MID,
-// the mid field tau/2 <= distance / size < tau).  SHORT (RULE_TRI3 with
-// tau >= 3, so beyond 12 x size): shorter series, no range test.
+// the mid field tau/2 <= distance / size < tau).  SHORT (tau >= 3, so very
+// far pairs lie beyond 12 x size and far ones beyond 3 x size): series of the
+// length those distances need, and no range test.
 //
 // The mid field's gz: the integral of 1/r over the facet is
 //   I = sum_i u_i Lambda_i + z Omega
@@ -283,16 +289,28 @@ __device__ __forceinline__ void pair_far_f32(const FaceF32* Fp, double ox, doubl
         }
     } else {
         const float e0 = __fdividef(L0, la + lb), e1 = __fdividef(L1, lb + lc), e2 = __fdividef(L2, lc + la);
-        if (SHORT) {
-            // Beyond 12 x size every vertex lies beyond 11.3 x size, so
+        if (SHORT && RULE == RULE_TRI3) {
+            // Beyond 12 x size every vertex lies beyond 11.3 x size (a vertex
+            // is within 2/3 of a median, so within size, of the centroid):
             // e_i < 0.045 (the series through e^5 leaves 1e-9 of the sum) and
-            // the solid angle is below 0.0035 (|t| < 0.002: through t^3 leaves
-            // 1e-12); den > 0 and the range test holds there.
+            // the solid angle, below area / distance^2, under 0.0035 (|t| <
+            // 0.002: through t^3 leaves 1e-12); den > 0 and the range test
+            // holds there.
             const float t = __fdividef(ny, den);
             om = t * fmaf(t * t, -1.f / 3.f, 1.f);
             l0 = e0 * fmaf(e0 * e0, fmaf(e0 * e0, 0.2f, 1.f / 3.f), 1.f);
             l1 = e1 * fmaf(e1 * e1, fmaf(e1 * e1, 0.2f, 1.f / 3.f), 1.f);
             l2 = e2 * fmaf(e2 * e2, fmaf(e2 * e2, 0.2f, 1.f / 3.f), 1.f);
+        } else if (SHORT) {
+            // Beyond 3 x size every vertex lies beyond 2.33 x size: e_i < 0.215
+            // (one term more than atanh_series, through e^11, leaves 8e-10)
+            // and |t| < 0.04 (through t^5 leaves 6e-10); the vertices' view
+            // angles stay below 25 degrees, so den > 0.
+            const float t = __fdividef(ny, den), t2 = t * t;
+            om = t * fmaf(t2, fmaf(t2, 0.2f, -1.f / 3.f), 1.f);
+            l0 = e0 * fmaf(e0 * e0, atanh_q11(e0 * e0), 1.f);
+            l1 = e1 * fmaf(e1 * e1, atanh_q11(e1 * e1), 1.f);
+            l2 = e2 * fmaf(e2 * e2, atanh_q11(e2 * e2), 1.f);
         } else if (far_series_ok(ny, den, e0, e1, e2)) {
             om = atan_series(__fdividef(ny, den));
             l0 = atanh_series(e0);
@@ -378,15 +396,19 @@ __device__ __forceinline__ void forward_mixed_block(FaceF32* __restrict__ smf, d
                         const int j = __ffs(m) - 1;
                         pair_far_f32<RULE_TRI3, true>(&sh[j], ox, oy, oz, &gacc, &tacc);
                     }
+                    for (unsigned m = farMask; m; m &= m - 1) {
+                        const int j = __ffs(m) - 1;
+                        pair_far_f32<RULE_DUN6, true>(&sh[j], ox, oy, oz, &gacc, &tacc);
+                    }
                 } else {
                     for (unsigned m = vfarMask; m; m &= m - 1) {
                         const int j = __ffs(m) - 1;
                         pair_far_f32<RULE_TRI3>(&sh[j], ox, oy, oz, &gacc, &tacc);
                     }
-                }
-                for (unsigned m = farMask; m; m &= m - 1) {
-                    const int j = __ffs(m) - 1;
-                    pair_far_f32<RULE_DUN6>(&sh[j], ox, oy, oz, &gacc, &tacc);
+                    for (unsigned m = farMask; m; m &= m - 1) {
+                        const int j = __ffs(m) - 1;
+                        pair_far_f32<RULE_DUN6>(&sh[j], ox, oy, oz, &gacc, &tacc);
+                    }
                 }
                 for (unsigned m = midMask; m; m &= m - 1) {
                     const int j = __ffs(m) - 1;
