@@ -50,6 +50,21 @@ def test_mixed_forward_voxel_full_size():
     assert rel(tmi[sub], om.forward_tmi(p.mag_xyz[sub])) < MIXED_TOL
 
 
+@pytest.mark.parametrize("tau", [2.0, 2.5, 4.0])
+def test_mixed_forward_far_ratios(tau):
+    """Far-field ratios other than the default 3: below 3 the far pairs keep
+    the range-tested series and the mid field (analytic gz) moves to within
+    one or two facet sizes, where atanh(e)/e - 1 takes its half-argument
+    steps (e > 0.2); above 3 the far pairs take the shortened series."""
+    p = synth.voxel_contact_model(shape=(16, 16, 8), n_side=24, cp_stride=4, freedom_interior=synth.XYZ_FREE)
+    ctx, om, x, idx = _case(p)
+    ctx.set_far_field_ratio(tau)
+    gz, tmi = ctx.forward(x)
+    assert rel(gz, om.forward_gz(p.grav_xyz)) < MIXED_TOL
+    assert rel(tmi, om.forward_tmi(p.mag_xyz)) < MIXED_TOL
+    assert ctx.near_pairs() < 0.5 * len(p.grav_xyz) * p.n_triangles()
+
+
 def test_mixed_all_near_is_fp64():
     p = synth.voxel_contact_model(shape=(10, 10, 6), n_side=12, cp_stride=2)
     ctx, om, x, idx = _case(p)
