@@ -13,7 +13,7 @@ namespace litho_b200 {
 // FP32 facet record of the far-field forward, written once per evaluation by
 // k_face_prep_mixed (array [T] in HBM), copied 32 facets at a time into
 // shared memory and read there with 128-bit loads (10 per far pair, 9 per
-// very far or mid pair).  The origin and the unit normal stay FP64: the
+// very far pair, 8 per mid pair).  The origin and the unit normal stay FP64: the
 // height above the facet plane can be tiny next to |o - a| (a far top facet
 // seen from 1 m above it).  Row 12 feeds the per-warp near/far test, row 13
 // the mid field's analytic gz.
