@@ -305,3 +305,43 @@ def test_apply_to_model_on_a_built_model():
     m.build_shared_vertex_sync()
     assert m.n_dofs == want.n_dofs < full
     assert np.array_equal(m.assemble_parameters(), want.assemble_parameters())
+
+
+@pytest.mark.skipif(not os.path.exists(REF_INI), reason="oracle/_ref/ini_ref is built only where the reference tree is")
+def test_real_configs_read_as_the_reference_reads_them(tmp_path):
+    """The reference's own run configurations (apps/forrestania/*.ini): every
+    key of every section through both parsers, save's bytes, and fromIni's
+    typed fields from the reference parser's answers."""
+    root = os.environ.get("LITHO_REFERENCE")
+    if not root:
+        pytest.skip("LITHO_REFERENCE (the reference tree) is not set")
+    import glob
+    from lithoinv3d_b200.config import _SPEC
+
+    files = sorted(glob.glob(os.path.join(root, "apps/forrestania/*.ini")))
+    if not files:
+        pytest.skip("reference configurations not present")
+    for f in files:
+        ours = IniConfig()
+        assert ours.load(f)
+        keys = [(s, k) for s in ours.sections() for k in ours.data[s]]
+        assert keys, f
+        queries = ["S\t%s\t%s\t" % sk for sk in keys]
+        queries += ["%s\t%s\t%s\t%s" % ({"int": "I", "double": "D", "bool": "B"}[kind], sec, key,
+                                        ("1" if default else "0") if kind == "bool" else repr(default))
+                    for _, sec, key, kind, default in _SPEC if kind in ("int", "double", "bool")]
+        saved = tmp_path / "saved.ini"
+        queries.append("W\t%s" % saved)
+        out = subprocess.run([REF_INI, f], input="\n".join(queries) + "\n", capture_output=True, text=True,
+                             check=True).stdout.split("\n")
+        assert out[0] == "1"
+        assert out[1:1 + len(keys)] == [ours.get_string(s, k) for s, k in keys], f
+        cfg = InversionConfig.from_ini(ours)
+        typed = [sp for sp in _SPEC if sp[3] in ("int", "double", "bool")]
+        for (name, _, _, kind, _), got in zip(typed, out[1 + len(keys):]):
+            v = getattr(cfg, name)
+            if kind == "double":
+                assert _same_double(float(got), v), (f, name, got, v)
+            else:
+                assert int(got) == int(v), (f, name, got, v)
+        assert saved.read_bytes() == ours.dumps().encode("latin-1"), f
